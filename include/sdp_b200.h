@@ -1,0 +1,339 @@
+/*
+ * sdp_b200 — B200 (sm_100a) imaging major/minor cycle behind the reference's
+ * PREESM actor C ABI.
+ *
+ * Two layers are exported by libsdp_b200.so:
+ *
+ *  1. Actor drop-ins.  Same symbol names and argument lists as the reference
+ *     actors in param_code/code_*_1core/include/*.h compiled with
+ *     SINGLE_PRECISION = 1 (PRECISION = float, common.h:62-71), so the
+ *     generated PREESM schedule (generated/Core0.c) links against this
+ *     library unchanged.  Every pointer is a HOST pointer, as in the
+ *     reference; each call stages its inputs to the GPU, runs the CUDA path
+ *     and copies its outputs back before returning.  They return void like
+ *     the reference; failures are reported through sdp_last_status() /
+ *     sdp_last_error() and, when sdp_set_abort_on_error(1) is set (or
+ *     SDP_ABORT_ON_ERROR=1 in the environment), by printing the error and
+ *     calling exit(EXIT_FAILURE) as the reference's setup actors do
+ *     (src/top.c:85-89).
+ *
+ *  2. Device-resident layer (sdp_*).  Device pointers, an explicit CUDA
+ *     stream passed as void*, and an int status (SDP_OK = 0).  The actor
+ *     drop-ins are thin staging wrappers over these calls.
+ *
+ * There is no CPU fallback: without a usable CUDA device every call fails
+ * with SDP_ERR_CUDA.
+ */
+#ifndef SDP_B200_H
+#define SDP_B200_H
+
+#include <stddef.h>
+
+#ifdef __cplusplus
+#include <cstdbool>
+extern "C" {
+#else
+#include <stdbool.h>
+#endif
+
+/* ---------------------------------------------------------------------------
+ * ABI types — layout-identical to the reference's C structs
+ * (common.h:137-168 int2 / float2 / float3, and Config common.h:187-265,
+ * sizeof 360 on x86-64).
+ * ------------------------------------------------------------------------- */
+typedef struct { int x, y; } sdp_int2;
+typedef struct { float x, y; } sdp_float2;
+typedef struct { float x, y, z; } sdp_float3;
+
+typedef struct sdp_config {
+    bool retain_device_mem;
+    int num_major_cycles;
+    int num_recievers;
+    int num_baselines;
+    int grid_size;
+    double cell_size;
+    const char *output_path;
+    const char *dirty_image_output;
+    int gpu_max_threads_per_block;
+    int gpu_max_threads_per_block_dimension;
+    bool right_ascension;
+    bool save_dirty_image;
+    bool save_residual_image;
+    bool save_extracted_sources;
+    bool save_predicted_visibilities;
+    bool save_estimated_gains;
+    bool perform_system_test;
+    const char *system_test_image;
+    const char *system_test_sources;
+    const char *system_test_visibilities;
+    const char *system_test_gains;
+    const char *default_gains_file;
+    const char *output_gains_file;
+    bool perform_gain_calibration;
+    bool use_default_gains;
+    int max_calibration_cycles;
+    int number_cal_major_cycles;
+    bool force_weight_to_one;
+    double frequency_hz;
+    int oversampling;
+    double uv_scale;
+    int num_visibilities;
+    int num_kernels;
+    int total_kernel_samples;
+    double max_w;
+    double w_scale;
+    const char *kernel_real_file;
+    const char *kernel_imag_file;
+    const char *kernel_support_file;
+    const char *degridding_kernel_real_file;
+    const char *degridding_kernel_imag_file;
+    const char *degridding_kernel_support_file;
+    const char *visibility_source_file;
+    unsigned int number_minor_cycles_cal;
+    unsigned int number_minor_cycles_img;
+    double loop_gain;
+    double weak_source_percent_gc;
+    double weak_source_percent_img;
+    double noise_factor;
+    double psf_max_value;
+    const char *model_sources_output;
+    const char *residual_image_output;
+    const char *psf_input_file;
+    const char *psf_image_output;
+    const char *clean_psf_image_output;
+    const char *model_image_output;
+    const char *final_image_output;
+    int num_sources;
+    const char *predicted_vis_output;
+} sdp_config;
+
+/* ---------------------------------------------------------------------------
+ * Status and error reporting
+ * ------------------------------------------------------------------------- */
+enum {
+    SDP_OK = 0,
+    SDP_ERR_INVALID = 1,  /* NULL pointer, negative or inconsistent size  */
+    SDP_ERR_RANGE = 2,    /* size beyond a documented limit                */
+    SDP_ERR_CUDA = 3,     /* CUDA runtime error or no usable device         */
+    SDP_ERR_NOMEM = 4,    /* device allocation failed                        */
+    SDP_ERR_TIMEOUT = 5,  /* a bounded device-side wait gave up             */
+    SDP_ERR_DATA = 6      /* input data outside the grid / kernel tables     */
+};
+
+int sdp_last_status(void);           /* status of the calling thread's last failing call */
+const char *sdp_last_error(void);    /* message for it ("" when none)                     */
+void sdp_clear_error(void);
+void sdp_set_abort_on_error(int on); /* 1: print and exit(EXIT_FAILURE) on error         */
+int sdp_version(void);               /* 100 * major + minor                               */
+
+/* Degridding mode of the std_degridding drop-in (process wide).
+ * SDP_DEGRID_NEAREST (default) reproduces the reference exactly: the value
+ * is the nearest grid cell (degridgrid.c:193-200).  SDP_DEGRID_CONV returns
+ * the normalised kernel convolution the reference computes and then
+ * discards (degridgrid.c:147-191). */
+enum { SDP_DEGRID_NEAREST = 0, SDP_DEGRID_CONV = 1 };
+int sdp_set_degrid_mode(int mode);
+int sdp_get_degrid_mode(void);
+
+/* ---------------------------------------------------------------------------
+ * Layer 1: actor drop-ins (host pointers, reference signatures)
+ * ------------------------------------------------------------------------- */
+
+/* degridgrid.h:10-11 — snap uvw to the 1/OS fine grid (simplification must be 0). */
+void correct_to_finegrid(int NUM_VISIBILITIES, int GRID_SIZE, int OVERSAMPLING_FACTOR, int PERFORM_SIMPLIFICATION,
+                         sdp_float3 *vis_uvw_coords, sdp_float2 *input_visibilities, sdp_config *config,
+                         sdp_float2 *output_visibilities, sdp_float3 *output_finegrid_vis_coords,
+                         int *num_output_visibilities);
+
+/* degridgrid.h:13-14 — w-projection gridding. */
+void std_gridding(int GRID_SIZE, int NUM_VISIBILITIES, int NUM_KERNELS, int TOTAL_KERNEL_SAMPLES,
+                  int OVERSAMPLING_FACTOR, int BYPASS, int *maj_iter, int *num_corrected_visibilities,
+                  sdp_float2 *kernels, sdp_int2 *kernel_supports, sdp_float3 *corrected_vis_uvw_coords,
+                  sdp_float2 *visibilities, sdp_config *config, sdp_float2 *prev_grid, sdp_float2 *output_grid);
+
+/* degridgrid.h:16-18 — degridding (mode per sdp_set_degrid_mode). */
+void std_degridding(int GRID_SIZE, int NUM_VISIBILITIES, int NUM_KERNELS, int TOTAL_KERNEL_SAMPLES,
+                    int OVERSAMPLING_FACTOR, sdp_float2 *kernels, sdp_int2 *kernel_supports, sdp_float2 *input_grid,
+                    sdp_float3 *corrected_vis_uvw_coords, int *num_corrected_visibilities, sdp_config *config,
+                    sdp_float2 *output_visibilities);
+
+/* degridgrid.h:20-23 — grid-to-grid: nearest-cell sample, regrid with the w = 0 kernel. */
+void g2g_degridgrid(int GRID_SIZE, int NUM_VISIBILITIES, int NUM_GRIDDING_KERNELS, int NUM_DEGRIDDING_KERNELS,
+                    int TOTAL_GRIDDING_KERNEL_SAMPLES, int TOTAL_DEGRIDDING_KERNEL_SAMPLES, int OVERSAMPLING_FACTOR,
+                    sdp_float2 *gridding_kernels, sdp_int2 *gridding_kernel_supports, sdp_float2 *degridding_kernels,
+                    sdp_int2 *degridding_kernel_supports, sdp_float2 *input_grid,
+                    sdp_float3 *corrected_vis_uvw_coords, int *num_corrected_visibilities, sdp_config *config,
+                    sdp_float2 *output_grid);
+
+/* degridgrid.h:25 */
+void subtract_image_space(int GRID_SIZE, float *measurements, float *estimate, float *result);
+/* degridgrid.h:27 (a sink: does nothing, as in the reference) */
+void degridding_kernel_sink(int NUM_DEGRIDDING_KERNELS, int TOTAL_DEGRIDDING_KERNEL_SAMPLES, sdp_int2 *supports,
+                            sdp_float2 *kernels);
+
+/* gridding_run.h:12-13 — DFT-pipeline gridder (snapped coordinates, inclusive taps, OS = 16). */
+void gridding_actor(int GRID_SIZE, int NUM_VISIBILITIES, int NUM_KERNELS, int TOTAL_KERNEL_SAMPLES,
+                    sdp_float2 *kernels, sdp_int2 *kernel_supports, sdp_float3 *vis_uvw_coords,
+                    sdp_float2 *visibilities, sdp_config *config, sdp_float2 *uv_grid);
+/* gridding_run.h:15-17 — the gridder behind gridding_actor; accumulates into grid. */
+void gridding_CPU(sdp_float2 *grid, const sdp_float2 *kernel, const sdp_int2 *supports, const sdp_float3 *vis_uvw,
+                  const sdp_float2 *vis, const int num_vis, const int oversampling, const int grid_size,
+                  const double uv_scale, const double w_scale);
+/* gridding_run.h:21 */
+void add_visibilities(int NUM_VISIBILITIES, sdp_float2 *v1, sdp_float2 *v2, sdp_float2 *output);
+
+/* fft_run.h:13-21 */
+void fft_shift_complex_to_complex_actor(int GRID_SIZE, sdp_float2 *uv_grid_in, sdp_config *config,
+                                        sdp_float2 *uv_grid_out);
+void CUFFT_EXECUTE_FORWARD_C2C_actor(int GRID_SIZE, sdp_float2 *uv_grid_in, sdp_float2 *uv_grid_out);
+void CUFFT_EXECUTE_INVERSE_C2C_actor(int GRID_SIZE, sdp_float2 *uv_grid_in, sdp_float2 *uv_grid_out);
+void fft_shift_complex_to_real_actor(int GRID_SIZE, sdp_float2 *uv_grid, sdp_config *config, float *dirty_image);
+void fft_shift_real_to_complex_actor(int GRID_SIZE, float *image, sdp_config *config, sdp_float2 *fourier);
+
+/* convolution_correction_run.h:11-12.  prolate holds GRID_SIZE/2 entries;
+ * the reference also reads prolate[GRID_SIZE/2] (one past the end); here that
+ * entry is taken as the spheroidal at nu = 1, which is 0. */
+void execute_convolution_correction_actor(int GRID_SIZE, float *dirty_image_in, float *prolate, sdp_config *config,
+                                          float *dirty_image_out);
+void execute_inv_convolution_correction_actor(int GRID_SIZE, float *dirty_image_in, float *prolate,
+                                              sdp_config *config, float *dirty_image_out);
+
+/* dft_run.h:15-16 */
+void dft_actor(int NUM_VISIBILITIES, int NUM_MAX_SOURCES, sdp_float3 *sources, sdp_float3 *vis_uvw_coords,
+               int *num_sources, sdp_config *config, sdp_float2 *visibilities);
+
+/* deconvolution_run.h:14-15 — the live Hogbom CLEAN of
+ * preesm_pipelines/simsdp_fft_imaging_pipeline/Code/src/CPU/deconvolution_run.c:197-311
+ * (the param_code copy has its body commented out). */
+void hogbom_clean(int GRID_SIZE, int NUM_MINOR_CYCLES, int MAX_SOURCES, float *residual, float *psf,
+                  sdp_int2 *partial_psf_halfdims, sdp_config *config, float *current_model, int *num_sources_out,
+                  sdp_float3 *sources_out, float *output_model);
+
+/* splitmerge.h:15-21 */
+void split_visibilities(sdp_config *config, int NUM_VISIBILITIES, int SLICES, sdp_float2 *measured_visibilities,
+                        sdp_float3 *vis_coords, sdp_float2 *visibilities, sdp_float3 *out_vis_coords,
+                        sdp_config *output_configs, sdp_config *output_config);
+void merge_gridded_visibilities(int GRID_SIZE, int SLICES, sdp_float2 *grids, sdp_float2 *output_grid);
+void merge_configs(sdp_config *in_configs, sdp_config *out_config);
+void split_fftdegrid_visibilities(int NUM_VISIBILITIES, int SLICES, int GRID_SIZE, sdp_config *config,
+                                  sdp_float3 *vis_coords, sdp_float2 *measured_visibilities, int *num_corrected_vis,
+                                  int *maj_iter, sdp_float2 *output_visibilities, sdp_float3 *out_vis_coords,
+                                  sdp_config *output_configs, int *num_vis, int *maj_iter_out);
+void split_uvgrid(int GRID_SIZE, int SLICES, sdp_float2 *input_grid, sdp_float2 *output_grid);
+
+/* gains_apply_run.h:31 */
+void subtract_from_measurements_finegrid(int NUM_VISIBILITIES, sdp_float2 *gridded_measured_vis,
+                                         sdp_float2 *input_vis, int *num_finegrid_vis, sdp_float2 *delta_vis);
+
+/* top.h:17, 31-41, 43-45 — setup math (file-reading setup actors are not exported). */
+void config_struct_set_up(int GRID_SIZE, int NUM_KERNELS, sdp_config *config);
+void correction_set_up(int GRID_SIZE, float *prolate);
+void create_1D_half_prolate(float *prolate, int grid_size);
+double prolate_spheroidal(double nu);
+void config_struct_set_up_sequel(sdp_config *config_in, double *psf_max_value, sdp_config *config_out);
+void clean_psf_host_set_up(int GRID_SIZE, int GAUSSIAN_CLEAN_PSF, sdp_config *config, float *dirty_psf,
+                           float *clean_psf, sdp_int2 *partial_psf_halfdims);
+void model_set_up(int GRID_SIZE, sdp_config *config, float *initial_image);
+void sources_set_up(int MAX_SOURCES, int *num_sources, sdp_float3 *sources);
+
+/* ---------------------------------------------------------------------------
+ * Layer 2: device-resident API (device pointers, stream as void*, int status)
+ * ------------------------------------------------------------------------- */
+
+/* Geometry shared by gridding and degridding (Config fields uv_scale,
+ * w_scale, oversampling and GRID_SIZE). */
+typedef struct sdp_geometry {
+    int grid_size;     /* even, 8 <= grid_size <= 32768            */
+    int oversampling;  /* 1 <= oversampling <= 64                   */
+    double uv_scale;
+    double w_scale;
+} sdp_geometry;
+
+/* One W-projection kernel set: planes concatenated, supports[p] = (half
+ * support, sample offset) as kernel_host_set_up builds them (top.c:256-261). */
+typedef struct sdp_wkernels {
+    const sdp_float2 *kernels;   /* device */
+    const sdp_int2 *supports;    /* device */
+    int num_kernels;             /* planes */
+    int total_samples;           /* entries of kernels                          */
+    int max_half_support;        /* max over planes of supports[p].x (host value) */
+} sdp_wkernels;
+
+/* Gridding semantics. */
+enum {
+    SDP_GRID_STD = 0,         /* std_gridding: taps [ceil(p-hs), ceil(p+hs))                 */
+    SDP_GRID_SNAPPED = 1      /* gridding_CPU: snapped p, taps [ceil(p-hs), floor(p+hs)]      */
+};
+
+/* Visibility set binned by uv tile (and w-plane) once, reused by every
+ * gridding / degridding pass of a major cycle. */
+typedef struct sdp_visplan sdp_visplan;
+
+int sdp_visplan_create(sdp_visplan **plan, const sdp_geometry *geom, const sdp_wkernels *grid_kernels,
+                       const sdp_wkernels *degrid_kernels, int num_vis, const sdp_float3 *uvw, int grid_mode,
+                       void *stream);
+int sdp_visplan_destroy(sdp_visplan *plan);
+int sdp_visplan_num_work_items(const sdp_visplan *plan, int *count); /* blocking read */
+/* Measured visibilities (original order) copied into plan order. */
+int sdp_visplan_set_measured(sdp_visplan *plan, const sdp_float2 *measured, void *stream);
+/* grid: output_grid (G^2, zeroed first unless accumulate) += vis (original order) convolved. */
+int sdp_visplan_grid(sdp_visplan *plan, const sdp_float2 *vis, sdp_float2 *grid, int accumulate, void *stream);
+/* degrid with mode SDP_DEGRID_*; predicted written in original order. */
+int sdp_visplan_degrid(sdp_visplan *plan, const sdp_float2 *model_grid, sdp_float2 *predicted, int mode,
+                       void *stream);
+/* Fused visibility pass of one FFT-pipeline major cycle:
+ * predicted = degrid(model_grid); delta = measured - predicted;
+ * residual_grid = grid(delta).  predicted/delta may be NULL (not stored). */
+int sdp_visplan_cycle(sdp_visplan *plan, const sdp_float2 *model_grid, int degrid_mode, sdp_float2 *predicted,
+                      sdp_float2 *delta, sdp_float2 *residual_grid, void *stream);
+
+/* Element-wise and setup kernels (device pointers). */
+int sdp_degrid_nearest(int grid_size, double uv_scale, int num_vis, const sdp_float3 *uvw, const sdp_float2 *grid,
+                       sdp_float2 *out, void *stream);
+int sdp_correct_to_finegrid(int grid_size, int oversampling, double uv_scale, int num_vis, const sdp_float3 *uvw,
+                            sdp_float3 *out_uvw, void *stream);
+int sdp_subtract_vis(int num_vis, const sdp_float2 *measured, const sdp_float2 *predicted, sdp_float2 *delta,
+                     void *stream);
+int sdp_subtract_image(int grid_size, const float *a, const float *b, float *out, void *stream);
+int sdp_merge_grids(int grid_size, int slices, const sdp_float2 *grids, sdp_float2 *out, void *stream);
+int sdp_fft_shift_c2c(int grid_size, const sdp_float2 *in, sdp_float2 *out, void *stream);
+int sdp_fft_shift_c2r(int grid_size, const sdp_float2 *in, float *out, void *stream);
+int sdp_fft_shift_r2c(int grid_size, const float *in, sdp_float2 *out, void *stream);
+int sdp_conv_correction(int grid_size, const float *in, const float *prolate_ext, float *out, void *stream);
+int sdp_prolate_table(int grid_size, float *prolate_ext, void *stream); /* G/2 + 1 entries, last = 0 */
+
+/* 2-D complex FFT, FFTW sign convention (-1 forward, +1 inverse), unnormalised.
+ * Power-of-two grid_size from 16 to 16384; in may equal out. */
+int sdp_fft2d(int grid_size, const sdp_float2 *in, sdp_float2 *out, int sign, void *stream);
+/* Fused imaging transforms of the FFT pipeline:
+ * image = taper_correct(shift_c2r(iFFT(shift_c2c(grid))))  and
+ * grid  = shift_c2c(FFT(shift_r2c(image))).  work: G^2 complex scratch. */
+int sdp_grid_to_image(int grid_size, const sdp_float2 *grid, const float *prolate_ext, sdp_float2 *work,
+                      float *image, void *stream);
+int sdp_image_to_grid(int grid_size, const float *image, sdp_float2 *work, sdp_float2 *grid, void *stream);
+
+/* DFT predict: sources (l, m, I); phase argument in FP64 (north-star
+ * precision), sin/cos in FP32 after exact range reduction. */
+int sdp_dft(int num_vis, int num_sources, const sdp_float3 *sources, const sdp_float3 *uvw, sdp_float2 *vis,
+            void *stream);
+
+/* Hogbom CLEAN on the device, reference semantics.  psf holds G^2 entries.
+ * On return (after the stream completes) *num_sources_dev holds the count. */
+typedef struct sdp_clean_params {
+    int grid_size;
+    int num_minor_cycles;
+    int max_sources;
+    double loop_gain;
+    double noise_factor;
+    double weak_source_percent;
+    double psf_max_value;
+    double cell_size;
+} sdp_clean_params;
+int sdp_hogbom_workspace_bytes(int grid_size, size_t *bytes);
+int sdp_hogbom(const sdp_clean_params *p, float *residual_inout, const float *psf, float *model_inout,
+               sdp_float3 *sources, int *num_sources_dev, void *workspace, size_t workspace_bytes, void *stream);
+
+#ifdef __cplusplus
+}
+#endif
+#endif
