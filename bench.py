@@ -1,0 +1,445 @@
+"""Benchmark: visibilities gridded + degridded per second on B200.
+
+One step = one major-cycle visibility pass of the FFT imaging pipeline over
+every visibility of the workload: W-projection degridding of the model grid
+(convolutional, the value degridgrid.c:147-191 computes), subtraction from
+the measured visibilities (gains_apply_run.c:273-297) and W-projection
+gridding of the residual visibilities (degridgrid.c:69-125).  Workload: the
+256-antenna, 10 km log-spiral array, 120 time steps -> 3,916,800
+visibilities, 2048^2 grid, 17 w-planes of half support 4, oversampling 16
+(seeded synthetic data; no public dataset is used).
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl b200|reference]
+
+value: device-resident throughput (inputs in HBM, L2 flushed between timed
+steps, CUDA events, max over ranks).  e2e: the same pass through the
+reference-facing C ABI (std_degridding, subtract_from_measurements_finegrid,
+std_gridding) with pinned host buffers and the host<->device copies inside
+the timed region.  --impl reference times the reference's own actor code
+compiled from its sources (oracle/_ref) on the host cores.
+"""
+from __future__ import annotations
+
+import argparse
+import ctypes as C
+import json
+import math
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+from concurrent.futures import ThreadPoolExecutor
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent
+PKG = ROOT / "simsdp-generic-imaging-pipeline_b200"
+sys.path.insert(0, str(PKG))
+
+import synth  # noqa: E402
+
+METRIC = "vis/s gridded+degridded"
+UNIT = "vis/s"
+PROFILES = ROOT / "profiles"
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
+    ap.add_argument("--e2e-steps", type=int, default=3)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--cpu-sample", type=int, default=200_000, help="visibilities per CPU-baseline step")
+    return ap.parse_args()
+
+
+def workload(rank: int):
+    """C2-shaped workload; each rank images its own frequency channel (weak
+    scaling by channel, the reference's spectral parallelism)."""
+    freq = 140e6 * (1.0 + 0.05 * rank)
+    return synth.make_workload("c2_2048", 256, 5000.0, "spiral", 120, 2048, 200, 1e-3, 1.0, 1e-4, 17, 4,
+                               freq_hz=freq, seed=2 + rank, compute_vis=False)
+
+
+def algorithmic_bytes(n_vis: int, G: int) -> int:
+    """Compulsory HBM bytes of one fused pass: uvw (12 B) and measured vis (8 B)
+    read once per visibility, model grid read and residual grid written once."""
+    return n_vis * (12 + 8) + 2 * 8 * G * G
+
+
+def algorithmic_flops(n_vis: int, taps: int) -> int:
+    """Complex multiply-add per tap in both directions: 8 flops x 2."""
+    return n_vis * taps * 16
+
+
+def read_traffic(kernel: str):
+    """dram bytes per launch from the committed ncu summary, if present."""
+    f = PROFILES / f"{kernel}.txt"
+    if not f.exists():
+        return None
+    for line in f.read_text().splitlines():
+        if line.startswith("traffic_bytes_per_launch:"):
+            try:
+                return int(float(line.split(":", 1)[1].split()[0]))
+            except ValueError:
+                return None
+    return None
+
+
+class ClockSampler:
+    """nvidia-smi clock / throttle sampling during the timed region."""
+
+    def __init__(self, index: int):
+        self.index = index
+        self.proc = None
+        self.lines = []
+
+    def __enter__(self):
+        q = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.hw_slowdown,"
+             "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+             "clocks_event_reasons.sw_power_cap")
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.index), f"--query-gpu={q}",
+                                          "--format=csv,noheader,nounits", "-lms", "100"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.thread.start()
+        except FileNotFoundError:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def __exit__(self, *exc):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self):
+        sm, mx, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in self.lines:
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) < 7:
+                continue
+            try:
+                sm.append(float(parts[0]))
+                mx.append(float(parts[1]))
+            except ValueError:
+                continue
+            for name, v in zip(names, parts[3:7]):
+                if v.lower().startswith("active"):
+                    reasons.add(name)
+        if not sm:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": [], "samples": 0}
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": max(mx), "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+# ---------------------------------------------------------------------------
+# Reference arm / CPU baseline: the reference's actors on the host cores
+# ---------------------------------------------------------------------------
+def cpu_reference_pass(w, uvw_c, model_grid, sample: int, threads: int):
+    """Runs std_degridding + subtract_from_measurements_finegrid + std_gridding
+    of the reference (compiled from its sources, oracle/_ref; the oracle port
+    when that is absent) on `sample` visibilities split over `threads` slices,
+    as the reference's SLICES schedule does, and returns (seconds, kind)."""
+    sys.path.insert(0, str(ROOT / "oracle"))
+    import oracle as O
+    G, OS = w.cfg.grid_size, w.cfg.oversampling
+    cfg = O.make_config(G, w.cfg.uv_scale, w.cfg.w_scale, OS)
+    if O.RefLib.available("f32", "fast"):
+        lib, kind = O.RefLib("f32", "fast"), "reference"
+    elif O.RefLib.available("f32"):
+        lib, kind = O.RefLib("f32"), "reference"
+    else:
+        lib, kind = None, "port"
+    o = O.Oracle("f32") if lib is None else None
+    idx = np.linspace(0, uvw_c.shape[0] - 1, sample).astype(np.int64)
+    uvw = np.ascontiguousarray(uvw_c[idx])
+    vis = np.ascontiguousarray(w.vis[idx])
+    slices = np.array_split(np.arange(sample), threads)
+
+    def run(sl):
+        u = np.ascontiguousarray(uvw[sl])
+        v = np.ascontiguousarray(vis[sl])
+        if lib is not None:
+            pred = lib.std_degridding(cfg, G, OS, w.dkernels, w.supports, model_grid, u)
+            delta = lib.subtract_finegrid(v, pred)
+            return lib.std_gridding(cfg, G, OS, w.gkernels, w.supports, u, delta)
+        pred = o.std_degridding(G, OS, w.dkernels, w.supports, model_grid, u, w.cfg.uv_scale, w.cfg.w_scale, False)
+        delta = o.subtract_vis(v, pred)
+        return o.std_gridding(G, OS, w.gkernels, w.supports, u, delta, w.cfg.uv_scale, w.cfg.w_scale)
+
+    # silence the reference's progress printf
+    devnull = os.open(os.devnull, os.O_WRONLY)
+    saved = os.dup(1)
+    sys.stdout.flush()
+    os.dup2(devnull, 1)
+    try:
+        t0 = time.perf_counter()
+        with ThreadPoolExecutor(max_workers=threads) as ex:
+            grids = list(ex.map(run, slices))
+        if lib is not None and len(grids) > 1:
+            lib.merge_grids(G, np.concatenate(grids, axis=0))
+        t1 = time.perf_counter()
+    finally:
+        sys.stdout.flush()
+        os.dup2(saved, 1)
+        os.close(saved)
+        os.close(devnull)
+    return t1 - t0, kind
+
+
+def cpu_threads() -> int:
+    """Host threads for the CPU arm: every core, up to 64 (each slice owns a
+    full G^2 grid, as in the reference's SLICES schedule)."""
+    try:
+        n = len(os.sched_getaffinity(0))
+    except AttributeError:
+        n = os.cpu_count() or 1
+    return max(1, min(64, n))
+
+
+def reference_arm(args):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return 0
+    w = workload(0)
+    G = w.cfg.grid_size
+    threads = cpu_threads()
+    rng = np.random.default_rng(5)
+    model_grid = (rng.standard_normal((G * G, 2)) * 1e-3).astype(np.float32)
+    uvw_c = snap_host(w)
+    sample = max(threads * 2000, args.cpu_sample)
+    for _ in range(max(0, args.warmup)):
+        cpu_reference_pass(w, uvw_c, model_grid, min(sample, 20_000), threads)
+    times = []
+    kind = "port"
+    for _ in range(args.steps):
+        t, kind = cpu_reference_pass(w, uvw_c, model_grid, sample, threads)
+        times.append(t)
+    t = statistics.mean(times)
+    value = sample / t
+    line = {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": t * 1e3, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "config": {"workload": f"{w.name}: {w.num_vis} vis, G=2048, 17 w-planes hs=4 OS=16; "
+                               f"bounded sample of {sample} vis per step", "degrid": "convolutional"},
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": kind,
+                         "sample": f"{sample} visibilities of the workload per step, {threads} slices"},
+        "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def snap_host(w):
+    """Fine-grid snap of the uvw (degridgrid.c:24-25, 52-54), on the host in
+    numpy with the reference's rounding; used only to feed the CPU arm the
+    same coordinates the GPU arm grids."""
+    G, OS, us = w.cfg.grid_size, w.cfg.oversampling, w.cfg.uv_scale
+    u = w.uvw.astype(np.float64)
+    fx = np.trunc((u[:, 0] * us + G // 2) * OS + 0.5)
+    fy = np.trunc((u[:, 1] * us + G // 2) * OS + 0.5)
+    out = np.empty_like(w.uvw)
+    out[:, 0] = ((fx / OS - G // 2) / us).astype(np.float32)
+    out[:, 1] = ((fy / OS - G // 2) / us).astype(np.float32)
+    out[:, 2] = w.uvw[:, 2]
+    return out
+
+
+# ---------------------------------------------------------------------------
+# B200 arm
+# ---------------------------------------------------------------------------
+def b200_arm(args):
+    import torch
+    import torch.distributed as dist
+    import sdp_b200 as S
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        torch.cuda.set_device(local)
+        import datetime
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    dev = torch.device("cuda", local)
+    torch.cuda.set_device(dev)
+    lib = S.load()
+    D = S.Device(lib)
+    A = S.Actors(lib)
+    stream = torch.cuda.current_stream()
+
+    w = workload(rank)
+    G, OS, NK = w.cfg.grid_size, w.cfg.oversampling, w.cfg.num_kernels
+    N = w.num_vis
+    taps = (2 * w.half_support) ** 2
+
+    # ---- device-resident inputs -------------------------------------------------------
+    uvw_raw = torch.from_numpy(w.uvw).to(dev)
+    uvw = torch.empty_like(uvw_raw)
+    D.correct_to_finegrid(G, OS, w.cfg.uv_scale, uvw_raw, uvw)
+    gk = torch.from_numpy(w.gkernels).to(dev)
+    dk = torch.from_numpy(w.dkernels).to(dev)
+    sup = torch.from_numpy(w.supports).to(dev)
+    wk_g = S.Device.wkernels(gk, sup, w.supports)
+    wk_d = S.Device.wkernels(dk, sup, w.supports)
+    # measured visibilities: DFT of the 200-point sky on the GPU plus noise
+    sky = torch.from_numpy(w.sky.astype(np.float32)).to(dev)
+    measured = torch.empty((N, 2), dtype=torch.float32, device=dev)
+    D.dft(sky, uvw, measured)
+    gen = torch.Generator(device=dev).manual_seed(17 + rank)
+    measured += 1e-4 * torch.randn(measured.shape, device=dev, generator=gen)
+    # model: 200 CLEAN-like components on the image, to a model grid
+    model_img = torch.zeros(G * G, dtype=torch.float32, device=dev)
+    pix = torch.randint(G // 4, 3 * G // 4, (200, 2), device=dev, generator=gen)
+    model_img[pix[:, 1] * G + pix[:, 0]] = torch.rand(200, device=dev, generator=gen)
+    work = torch.empty((G * G, 2), dtype=torch.float32, device=dev)
+    model_grid = torch.empty((G * G, 2), dtype=torch.float32, device=dev)
+    D.image_to_grid(G, model_img, work, model_grid)
+    residual = torch.empty((G * G, 2), dtype=torch.float32, device=dev)
+    plan = D.plan(G, OS, w.cfg.uv_scale, w.cfg.w_scale, uvw, wk_g, wk_d, keep=(uvw, gk, dk, sup))
+    plan.set_measured(measured)
+    plan.check_flags()
+    n_items = plan.num_work_items()
+    flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device=dev)  # 256 MB > L2
+
+    def step():
+        plan.cycle(model_grid, residual, S.SDP_DEGRID_CONV)
+
+    for _ in range(max(3, args.warmup)):
+        step()
+    torch.cuda.synchronize()
+    plan.check_flags()
+
+    # ---- timed region (device) ---------------------------------------------------------
+    starts = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+    ends = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+    if world > 1:
+        dist.barrier()
+    torch.cuda.synchronize()
+    with ClockSampler(local) as clocks:
+        for i in range(args.steps):
+            flush.zero_()
+            starts[i].record(stream)
+            step()
+            ends[i].record(stream)
+        torch.cuda.synchronize()
+    if world > 1:
+        dist.barrier()
+    step_ms = [s.elapsed_time(e) for s, e in zip(starts, ends)]
+    t_step = sum(step_ms) / len(step_ms)
+    t_max = torch.tensor([t_step], dtype=torch.float64, device=dev)
+    if world > 1:
+        dist.all_reduce(t_max, op=dist.ReduceOp.MAX)
+    t_step = float(t_max.item())
+    value = world * N / (t_step * 1e-3)
+
+    # ---- roofline of the dominant kernel (the fused tile kernel) -----------------------
+    alg_bytes = algorithmic_bytes(N, G)
+    achieved = alg_bytes / (t_step * 1e-3) / 1e9
+    peaks = {}
+    pf = ROOT / "MEASURED_PEAKS.json"
+    if pf.exists():
+        peaks = json.loads(pf.read_text())
+    peak = float(peaks.get("hbm_gbs", 6650.0))
+    peak_src = "measured" if "hbm_gbs" in peaks else "fallback"
+    traffic = read_traffic("k_tiles_cycle_conv_c2_2048")
+
+    # ---- e2e through the reference-facing C ABI with pinned host buffers ---------------
+    uvw_h = torch.empty((N, 3), dtype=torch.float32).pin_memory()
+    uvw_h.copy_(uvw.cpu())
+    meas_h = torch.empty((N, 2), dtype=torch.float32).pin_memory()
+    meas_h.copy_(measured.cpu())
+    mgrid_h = torch.empty((G * G, 2), dtype=torch.float32).pin_memory()
+    mgrid_h.copy_(model_grid.cpu())
+    pred_h = torch.empty((N, 2), dtype=torch.float32).pin_memory()
+    delta_h = torch.empty((N, 2), dtype=torch.float32).pin_memory()
+    grid_h = torch.empty((G * G, 2), dtype=torch.float32).pin_memory()
+    gk_h, dk_h, sup_h = w.gkernels, w.dkernels, w.supports
+    cfg = S.make_config(G, w.cfg.uv_scale, w.cfg.w_scale, OS)
+    uvw_n, meas_n, mgrid_n = uvw_h.numpy(), meas_h.numpy(), mgrid_h.numpy()
+    pred_n, delta_n, grid_n = pred_h.numpy(), delta_h.numpy(), grid_h.numpy()
+    A.set_degrid_mode(S.SDP_DEGRID_CONV)
+
+    def e2e_step():
+        A.std_degridding(cfg, G, OS, dk_h, sup_h, mgrid_n, uvw_n, out=pred_n)
+        A.subtract_finegrid(meas_n, pred_n, out=delta_n)
+        A.std_gridding(cfg, G, OS, gk_h, sup_h, uvw_n, delta_n, out=grid_n)
+
+    e2e_step()
+    torch.cuda.synchronize()
+    if world > 1:
+        dist.barrier()
+    t0 = time.perf_counter()
+    for _ in range(args.e2e_steps):
+        e2e_step()
+    t_e2e = (time.perf_counter() - t0) / args.e2e_steps
+    t_e2e_t = torch.tensor([t_e2e], dtype=torch.float64, device=dev)
+    if world > 1:
+        dist.all_reduce(t_e2e_t, op=dist.ReduceOp.MAX)
+    t_e2e = float(t_e2e_t.item())
+    A.set_degrid_mode(S.SDP_DEGRID_NEAREST)
+    ksz = gk_h.nbytes + sup_h.nbytes
+    h2d = (N * 12 + G * G * 8 + ksz) + (2 * N * 8) + (ksz + N * 12 + N * 8)
+    d2h = N * 8 + N * 8 + G * G * 8
+
+    # ---- CPU baseline (rank 0, N = 1) --------------------------------------------------
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        threads = cpu_threads()
+        sample = max(threads * 2000, args.cpu_sample)
+        t_cpu, kind = cpu_reference_pass(w, uvw_h.numpy(), mgrid_n, sample, threads)
+        cpu = {"value": sample / t_cpu, "unit": UNIT, "cores": threads, "kind": kind,
+               "sample": f"{sample} visibilities of the workload, {threads} slices on {threads} threads"}
+
+    line = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+        "warmup": max(3, args.warmup), "ms_per_step": t_step, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "config": {"workload": f"{w.name}: 256 antennas, 10 km log spiral, 120 time steps, {N} vis per channel, "
+                               f"G=2048, 17 w-planes hs=4 OS=16, one channel per GPU",
+                   "degrid": "convolutional (normalised, degridgrid.c:147-191)",
+                   "l2": "flushed between timed steps (256 MB write)", "work_items": n_items},
+        "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                     "frac": achieved / peak, "traffic": traffic, "peak_source": peak_src,
+                     "kernel": "k_tiles<STD, OP_CYCLE_CONV>",
+                     "algorithmic_bytes_per_launch": alg_bytes,
+                     "fp32_flops_per_launch": algorithmic_flops(N, taps)},
+        "e2e": {"value": world * N / t_e2e, "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
+                "path": "std_degridding + subtract_from_measurements_finegrid + std_gridding (host buffers)"},
+        "gpu_launches": args.steps,
+        "clocks": clocks.summary(),
+    }
+    if cpu is not None:
+        line["cpu_baseline"] = cpu
+    plan.close()
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    return 0
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        return reference_arm(args)
+    return b200_arm(args)
+
+
+if __name__ == "__main__":
+    sys.exit(main())

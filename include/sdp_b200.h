@@ -286,6 +286,14 @@ int sdp_visplan_degrid(sdp_visplan *plan, const sdp_float2 *model_grid, sdp_floa
  * residual_grid = grid(delta).  predicted/delta may be NULL (not stored). */
 int sdp_visplan_cycle(sdp_visplan *plan, const sdp_float2 *model_grid, int degrid_mode, sdp_float2 *predicted,
                       sdp_float2 *delta, sdp_float2 *residual_grid, void *stream);
+/* g2g_degridgrid on a plan built with grid_mode SDP_GRID_G2G:
+ * out_grid = regrid(nearest_cell(in_grid)) with the plane-0 gridding kernel. */
+enum { SDP_GRID_G2G = 2 };
+int sdp_visplan_g2g(sdp_visplan *plan, const sdp_float2 *in_grid, sdp_float2 *out_grid, void *stream);
+/* Reads and clears the plan's device-side data flags (blocking): returns
+ * SDP_ERR_DATA when a visibility addressed a w-plane beyond the kernel
+ * tables or a support wider than declared. */
+int sdp_visplan_check(sdp_visplan *plan, void *stream);
 
 /* Element-wise and setup kernels (device pointers). */
 int sdp_degrid_nearest(int grid_size, double uv_scale, int num_vis, const sdp_float3 *uvw, const sdp_float2 *grid,
@@ -294,6 +302,7 @@ int sdp_correct_to_finegrid(int grid_size, int oversampling, double uv_scale, in
                             sdp_float3 *out_uvw, void *stream);
 int sdp_subtract_vis(int num_vis, const sdp_float2 *measured, const sdp_float2 *predicted, sdp_float2 *delta,
                      void *stream);
+int sdp_add_vis(int num_vis, const sdp_float2 *a, const sdp_float2 *b, sdp_float2 *out, void *stream);
 int sdp_subtract_image(int grid_size, const float *a, const float *b, float *out, void *stream);
 int sdp_merge_grids(int grid_size, int slices, const sdp_float2 *grids, sdp_float2 *out, void *stream);
 int sdp_fft_shift_c2c(int grid_size, const sdp_float2 *in, sdp_float2 *out, void *stream);
@@ -301,6 +310,9 @@ int sdp_fft_shift_c2r(int grid_size, const sdp_float2 *in, float *out, void *str
 int sdp_fft_shift_r2c(int grid_size, const float *in, sdp_float2 *out, void *stream);
 int sdp_conv_correction(int grid_size, const float *in, const float *prolate_ext, float *out, void *stream);
 int sdp_prolate_table(int grid_size, float *prolate_ext, void *stream); /* G/2 + 1 entries, last = 0 */
+/* top.c:530-595: Gaussian clean beam from the dirty PSF; halfdims_dev: 2 ints. */
+int sdp_clean_psf(int grid_size, double psf_max_value, const float *dirty_psf, float *clean_psf, int *halfdims_dev,
+                  void *stream);
 
 /* 2-D complex FFT, FFTW sign convention (-1 forward, +1 inverse), unnormalised.
  * Power-of-two grid_size from 16 to 16384; in may equal out. */

@@ -315,7 +315,11 @@ class RefLib:
     def std_degridding(self, cfg: Config, grid_size, os_, kernels, supports, grid, uvw, num=None):
         k = self._a(kernels, 2)
         s = np.ascontiguousarray(supports, dtype=np.int32)
-        g = self._a(grid, 2)
+        # The nearest-cell read (degridgrid.c:194-199) has no bounds check; a
+        # point at the top edge reads past the grid.  Zero rows appended after
+        # the grid make that read defined (0), the value the oracle assigns.
+        g = np.zeros((grid_size * grid_size + 2 * grid_size, 2), dtype=self.dtype)
+        g[: grid_size * grid_size] = self._a(grid, 2)
         uvw = self._a(uvw, 3)
         n = uvw.shape[0] if num is None else num
         out = np.zeros((uvw.shape[0], 2), dtype=self.dtype)
@@ -338,7 +342,10 @@ class RefLib:
         dk = self._a(dk, 2)
         gs = np.ascontiguousarray(gs, dtype=np.int32)
         ds = np.ascontiguousarray(ds, dtype=np.int32)
-        g = self._a(in_grid, 2)
+        # as in std_degridding: the nearest-cell read (degridgrid.c:273-279) is
+        # only checked below; zero rows past the grid make it defined
+        g = np.zeros((grid_size * grid_size + 2 * grid_size, 2), dtype=self.dtype)
+        g[: grid_size * grid_size] = self._a(in_grid, 2)
         uvw = self._a(uvw, 3)
         out = np.zeros((grid_size * grid_size, 2), dtype=self.dtype)
         nc = _i(uvw.shape[0])

@@ -144,7 +144,16 @@ void or_std_degridding(int grid_size, int os, int n, const REAL *kernels_, const
                     else if (u >= grid_center) cu = (grid_center - u) + grid_center;
                     int kx = abs((int)R_ROUND((cu - pos.x) * os));
                     int k_idx = w_offset + ky * (hs + 1) * os + kx;
-                    R2 ks = kernels[k_idx];
+                    R2 ks;
+                    if (kx < (hs + 1) * os && ky < (hs + 1) * os) {
+                        ks = kernels[k_idx];
+                    } else {
+                        /* a mirrored tap can land just past the quarter-plane row
+                         * (|du| = hs + 1); the reference then reads a neighbouring
+                         * sample.  Defined here as a zero sample. */
+                        ks.x = 0;
+                        ks.y = 0;
+                    }
                     ks.y *= conjugate;
                     /* The mirror of :153-154/:167-168 sends v = G/2 to row G, one past
                      * the grid (an out-of-bounds read in the reference).  Such a tap

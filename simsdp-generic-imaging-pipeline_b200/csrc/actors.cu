@@ -1,0 +1,758 @@
+// Actor drop-ins: the reference's PREESM actor symbols with their C
+// signatures (param_code/code_*_1core/include/*.h, PRECISION = float), over
+// host buffers.  Each call stages its inputs into the calling thread's
+// device buffers, runs the device layer on the thread's stream, copies the
+// outputs back and synchronises, so the generated schedule's call order and
+// buffer ownership are unchanged.  Pure bookkeeping actors that only copy
+// buffers (split/merge of configs, identity corrections, bypass) copy on the
+// host exactly as the reference does; every computing actor runs on the GPU
+// and fails (sdp_last_status) rather than falling back to the CPU.
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+
+#include <algorithm>
+
+#include "internal.cuh"
+
+using namespace sdp;
+
+namespace {
+
+int g_degrid_mode = SDP_DEGRID_NEAREST;
+
+// Buffer slots of the thread context.
+enum Slot {
+    S_UVW = 0,
+    S_VIS,
+    S_VIS2,
+    S_OUTVIS,
+    S_GKERN,
+    S_GSUP,
+    S_DKERN,
+    S_DSUP,
+    S_GRID,
+    S_GRID2,
+    S_IMG,
+    S_IMG2,
+    S_PROLATE,
+    S_PLAN,
+    S_PSF,
+    S_MODEL,
+    S_SRC,
+    S_WS,
+    S_COUNT
+};
+
+struct Stage {
+    ThreadCtx *ctx = nullptr;
+    cudaStream_t st = nullptr;
+    int init()
+    {
+        SDP_TRY(thread_ctx(&ctx));
+        st = ctx->stream;
+        return SDP_OK;
+    }
+    template <class T>
+    int up(int slot, const void *host, size_t count, T **dev, size_t alloc_count = 0)
+    {
+        void *p = nullptr;
+        size_t bytes = sizeof(T) * std::max(count, alloc_count);
+        SDP_TRY(ctx_buffer(ctx, slot, bytes, &p));
+        if (count) SDP_CUDA_TRY(cudaMemcpyAsync(p, host, sizeof(T) * count, cudaMemcpyHostToDevice, st));
+        *dev = static_cast<T *>(p);
+        return SDP_OK;
+    }
+    template <class T>
+    int buf(int slot, size_t count, T **dev)
+    {
+        void *p = nullptr;
+        SDP_TRY(ctx_buffer(ctx, slot, sizeof(T) * std::max<size_t>(count, 1), &p));
+        *dev = static_cast<T *>(p);
+        return SDP_OK;
+    }
+    template <class T>
+    int down(void *host, const T *dev, size_t count)
+    {
+        if (count) SDP_CUDA_TRY(cudaMemcpyAsync(host, dev, sizeof(T) * count, cudaMemcpyDeviceToHost, st));
+        return SDP_OK;
+    }
+    int sync()
+    {
+        SDP_CUDA_TRY(cudaStreamSynchronize(st));
+        return SDP_OK;
+    }
+};
+
+int max_half_support(const sdp_int2 *sup, int nk)
+{
+    int m = 0;
+    for (int i = 0; i < nk; ++i) m = std::max(m, sup[i].x);
+    return m;
+}
+
+#define ACTOR(name, call)                 \
+    do {                                  \
+        if ((call) != SDP_OK) actor_fail(name); \
+    } while (0)
+
+// Builds a transient plan in the thread's buffers for (uvw already on device).
+int transient_plan(Stage &s, sdp_visplan *p, const sdp_geometry *geom, const sdp_wkernels *gk,
+                   const sdp_wkernels *dk, int n, int mode, const sdp_float3 *d_uvw)
+{
+    SDP_TRY(visplan_setup(p, geom, gk, dk, n, mode));
+    void *arena = nullptr;
+    SDP_TRY(ctx_buffer(s.ctx, S_PLAN, visplan_arena_bytes(p), &arena));
+    p->owns_arena = false;
+    return visplan_build(p, arena, reinterpret_cast<const float3 *>(d_uvw), s.st);
+}
+
+// ---------------------------------------------------------------------------
+int do_correct_to_finegrid(int N, int G, int OS, int simplify, sdp_float3 *uvw, sdp_float2 *in_vis, sdp_config *cfg,
+                           sdp_float2 *out_vis, sdp_float3 *out_uvw, int *num_out)
+{
+    SDP_CHECK_ARG(N >= 0 && uvw && in_vis && cfg && out_vis && out_uvw && num_out, "bad argument");
+    if (simplify != 0)
+        return set_error(SDP_ERR_INVALID,
+                         "PERFORM_SIMPLIFICATION = 1 (hash-map merge) is not provided; the schedules pass 0");
+    Stage s;
+    SDP_TRY(s.init());
+    sdp_float3 *d_uvw, *d_out;
+    SDP_TRY(s.up(S_UVW, uvw, N, &d_uvw));
+    SDP_TRY(s.buf(S_GRID, N, &d_out));
+    SDP_TRY(sdp_correct_to_finegrid(G, OS, cfg->uv_scale, N, d_uvw, d_out, s.st));
+    SDP_TRY(s.down(out_uvw, d_out, N));
+    SDP_TRY(s.sync());
+    // degridgrid.c:16, 51: the visibilities pass through unchanged
+    memmove(out_vis, in_vis, sizeof(sdp_float2) * (size_t)N);
+    *num_out = N;
+    return SDP_OK;
+}
+
+int do_std_gridding(int G, int NV, int NK, int TKS, int OS, int BYPASS, int *maj_iter, int *num_corr,
+                    sdp_float2 *kernels, sdp_int2 *sup, sdp_float3 *uvw, sdp_float2 *vis, sdp_config *cfg,
+                    sdp_float2 *prev_grid, sdp_float2 *out_grid)
+{
+    SDP_CHECK_ARG(G > 0 && out_grid && cfg, "bad argument");
+    const size_t G2 = (size_t)G * G;
+    if (BYPASS && maj_iter && *maj_iter > 0) {  // degridgrid.c:75-79
+        SDP_CHECK_ARG(prev_grid, "prev_grid is NULL");
+        memmove(out_grid, prev_grid, sizeof(sdp_float2) * G2);
+        return SDP_OK;
+    }
+    SDP_CHECK_ARG(num_corr && kernels && sup && (uvw && vis || *num_corr == 0), "bad argument");
+    const int n = *num_corr;
+    SDP_CHECK_ARG(n >= 0 && NK >= 1 && TKS >= 1, "bad sizes (n %d, NK %d, TKS %d)", n, NK, TKS);
+    (void)NV;
+    Stage s;
+    SDP_TRY(s.init());
+    sdp_float2 *d_k, *d_vis, *d_grid;
+    sdp_int2 *d_sup;
+    sdp_float3 *d_uvw;
+    SDP_TRY(s.up(S_GKERN, kernels, TKS, &d_k));
+    SDP_TRY(s.up(S_GSUP, sup, NK, &d_sup));
+    SDP_TRY(s.up(S_UVW, uvw, n, &d_uvw));
+    SDP_TRY(s.up(S_VIS, vis, n, &d_vis));
+    SDP_TRY(s.buf(S_GRID, G2, &d_grid));
+    sdp_geometry geom{G, OS, cfg->uv_scale, cfg->w_scale};
+    sdp_wkernels wk{d_k, d_sup, NK, TKS, max_half_support(sup, NK)};
+    sdp_visplan p;
+    SDP_TRY(transient_plan(s, &p, &geom, &wk, &wk, n, SDP_GRID_STD, d_uvw));
+    SDP_TRY(sdp_visplan_grid(&p, d_vis, d_grid, 0, s.st));
+    SDP_TRY(s.down(out_grid, d_grid, G2));
+    SDP_TRY(visplan_check_flags(&p, s.st));
+    return SDP_OK;
+}
+
+int do_std_degridding(int G, int NV, int NK, int TKS, int OS, sdp_float2 *kernels, sdp_int2 *sup, sdp_float2 *grid,
+                      sdp_float3 *uvw, int *num_corr, sdp_config *cfg, sdp_float2 *out)
+{
+    SDP_CHECK_ARG(G > 0 && NV >= 0 && out && cfg && num_corr && grid, "bad argument");
+    const int n = *num_corr;
+    SDP_CHECK_ARG(n >= 0 && n <= NV, "num_corrected_visibilities %d outside [0, %d]", n, NV);
+    const size_t G2 = (size_t)G * G;
+    Stage s;
+    SDP_TRY(s.init());
+    sdp_float3 *d_uvw;
+    sdp_float2 *d_grid, *d_out;
+    SDP_TRY(s.up(S_UVW, uvw, n, &d_uvw));
+    SDP_TRY(s.up(S_GRID, grid, G2, &d_grid));
+    SDP_TRY(s.buf(S_OUTVIS, std::max(NV, 1), &d_out));
+    // degridgrid.c:132: every output entry starts at zero
+    SDP_CUDA_TRY(cudaMemsetAsync(d_out, 0, sizeof(sdp_float2) * (size_t)NV, s.st));
+    if (g_degrid_mode == SDP_DEGRID_NEAREST) {
+        SDP_TRY(sdp_degrid_nearest(G, cfg->uv_scale, n, d_uvw, d_grid, d_out, s.st));
+        SDP_TRY(s.down(out, d_out, NV));
+        SDP_TRY(s.sync());
+        return SDP_OK;
+    }
+    SDP_CHECK_ARG(kernels && sup && NK >= 1 && TKS >= 1, "bad kernel arguments");
+    sdp_float2 *d_k;
+    sdp_int2 *d_sup;
+    SDP_TRY(s.up(S_DKERN, kernels, TKS, &d_k));
+    SDP_TRY(s.up(S_DSUP, sup, NK, &d_sup));
+    sdp_geometry geom{G, OS, cfg->uv_scale, cfg->w_scale};
+    sdp_wkernels wk{d_k, d_sup, NK, TKS, max_half_support(sup, NK)};
+    sdp_visplan p;
+    SDP_TRY(transient_plan(s, &p, &geom, &wk, &wk, n, SDP_GRID_STD, d_uvw));
+    SDP_TRY(sdp_visplan_degrid(&p, d_grid, d_out, SDP_DEGRID_CONV, s.st));
+    SDP_TRY(s.down(out, d_out, NV));
+    SDP_TRY(visplan_check_flags(&p, s.st));
+    return SDP_OK;
+}
+
+int do_g2g(int G, int NV, int NGK, int NDK, int TGK, int TDK, int OS, sdp_float2 *gk, sdp_int2 *gs, sdp_float2 *dk,
+           sdp_int2 *ds, sdp_float2 *in_grid, sdp_float3 *uvw, int *num_corr, sdp_config *cfg, sdp_float2 *out_grid)
+{
+    SDP_CHECK_ARG(G > 0 && gk && gs && in_grid && num_corr && cfg && out_grid, "bad argument");
+    (void)NV;
+    (void)dk;
+    (void)ds;
+    (void)NDK;
+    (void)TDK;
+    const int n = *num_corr;
+    SDP_CHECK_ARG(n >= 0 && (n == 0 || uvw), "bad visibility arguments");
+    const size_t G2 = (size_t)G * G;
+    Stage s;
+    SDP_TRY(s.init());
+    sdp_float2 *d_k, *d_in, *d_out;
+    sdp_int2 *d_sup;
+    sdp_float3 *d_uvw;
+    SDP_TRY(s.up(S_GKERN, gk, TGK, &d_k));
+    SDP_TRY(s.up(S_GSUP, gs, NGK, &d_sup));
+    SDP_TRY(s.up(S_UVW, uvw, n, &d_uvw));
+    SDP_TRY(s.up(S_GRID, in_grid, G2, &d_in));
+    SDP_TRY(s.buf(S_GRID2, G2, &d_out));
+    sdp_geometry geom{G, OS, cfg->uv_scale, cfg->w_scale};
+    // plane 0 only (degridgrid.c:215); the degridding set's convolution is
+    // discarded by the reference (:272-285), so it is not evaluated
+    sdp_wkernels wk{d_k, d_sup, NGK, TGK, std::max(0, gs[0].x)};
+    sdp_visplan p;
+    SDP_TRY(transient_plan(s, &p, &geom, &wk, &wk, n, kPlanG2G, d_uvw));
+    SDP_TRY(sdp_visplan_g2g(&p, d_in, d_out, s.st));
+    SDP_TRY(s.down(out_grid, d_out, G2));
+    SDP_TRY(visplan_check_flags(&p, s.st));
+    return SDP_OK;
+}
+
+int do_gridding_snapped(sdp_float2 *grid, const sdp_float2 *kernels, const sdp_int2 *sup, int NK, int TKS,
+                        const sdp_float3 *uvw, const sdp_float2 *vis, int n, int OS, int G, double uv_scale,
+                        double w_scale, bool accumulate)
+{
+    SDP_CHECK_ARG(G > 0 && grid && kernels && sup && (n == 0 || (uvw && vis)) && n >= 0, "bad argument");
+    const size_t G2 = (size_t)G * G;
+    Stage s;
+    SDP_TRY(s.init());
+    sdp_float2 *d_k, *d_vis, *d_grid;
+    sdp_int2 *d_sup;
+    sdp_float3 *d_uvw;
+    SDP_TRY(s.up(S_GKERN, kernels, TKS, &d_k));
+    SDP_TRY(s.up(S_GSUP, sup, NK, &d_sup));
+    SDP_TRY(s.up(S_UVW, uvw, n, &d_uvw));
+    SDP_TRY(s.up(S_VIS, vis, n, &d_vis));
+    if (accumulate) {
+        SDP_TRY(s.up(S_GRID, grid, G2, &d_grid));
+    } else {
+        SDP_TRY(s.buf(S_GRID, G2, &d_grid));
+    }
+    sdp_geometry geom{G, OS, uv_scale, w_scale};
+    sdp_wkernels wk{d_k, d_sup, NK, TKS, max_half_support(sup, NK)};
+    sdp_visplan p;
+    SDP_TRY(transient_plan(s, &p, &geom, &wk, &wk, n, SDP_GRID_SNAPPED, d_uvw));
+    SDP_TRY(sdp_visplan_grid(&p, d_vis, d_grid, accumulate ? 1 : 0, s.st));
+    SDP_TRY(s.down(grid, d_grid, G2));
+    SDP_TRY(visplan_check_flags(&p, s.st));
+    return SDP_OK;
+}
+
+// Highest plane index gridding_CPU will address, and the kernel samples the
+// used planes span (gridding_CPU receives no NUM_KERNELS argument).
+void snapped_extent(const sdp_int2 *sup, const sdp_float3 *uvw, int n, double w_scale, int OS, int *nk, int *tks)
+{
+    int maxp = 0;
+    for (int i = 0; i < n; ++i) {
+        float a = fabsf((float)((double)uvw[i].z * w_scale));
+        int pl = (int)roundf(sqrtf(a));
+        maxp = std::max(maxp, pl);
+    }
+    *nk = maxp + 1;
+    int t = 0;
+    for (int p = 0; p <= maxp; ++p) {
+        int e = sup[p].y + (sup[p].x + 1) * OS * (sup[p].x + 1) * OS;
+        t = std::max(t, e);
+    }
+    *tks = std::max(t, 1);
+}
+
+int do_vis_binary(int n, const sdp_float2 *a, const sdp_float2 *b, sdp_float2 *o, bool subtract)
+{
+    SDP_CHECK_ARG(n >= 0 && a && b && o, "bad argument");
+    Stage s;
+    SDP_TRY(s.init());
+    sdp_float2 *da, *db, *dout;
+    SDP_TRY(s.up(S_VIS, a, n, &da));
+    SDP_TRY(s.up(S_VIS2, b, n, &db));
+    SDP_TRY(s.buf(S_OUTVIS, n, &dout));
+    if (subtract) {
+        SDP_TRY(sdp_subtract_vis(n, da, db, dout, s.st));
+    } else {
+        SDP_TRY(sdp_add_vis(n, da, db, dout, s.st));
+    }
+    SDP_TRY(s.down(o, dout, n));
+    return s.sync();
+}
+
+int do_shift(int G, const void *in, void *out, int kind)
+{
+    SDP_CHECK_ARG(G > 0 && in && out, "bad argument");
+    const size_t G2 = (size_t)G * G;
+    Stage s;
+    SDP_TRY(s.init());
+    if (kind == 0) {  // c2c
+        sdp_float2 *di, *dout;
+        SDP_TRY(s.up(S_GRID, in, G2, &di));
+        SDP_TRY(s.buf(S_GRID2, G2, &dout));
+        SDP_TRY(sdp_fft_shift_c2c(G, di, dout, s.st));
+        SDP_TRY(s.down(out, dout, G2));
+    } else if (kind == 1) {  // c2r
+        sdp_float2 *di;
+        float *dout;
+        SDP_TRY(s.up(S_GRID, in, G2, &di));
+        SDP_TRY(s.buf(S_IMG, G2, &dout));
+        SDP_TRY(sdp_fft_shift_c2r(G, di, dout, s.st));
+        SDP_TRY(s.down(out, dout, G2));
+    } else {  // r2c
+        float *di;
+        sdp_float2 *dout;
+        SDP_TRY(s.up(S_IMG, in, G2, &di));
+        SDP_TRY(s.buf(S_GRID2, G2, &dout));
+        SDP_TRY(sdp_fft_shift_r2c(G, di, dout, s.st));
+        SDP_TRY(s.down(out, dout, G2));
+    }
+    return s.sync();
+}
+
+int do_fft(int G, const sdp_float2 *in, sdp_float2 *out, int sign)
+{
+    SDP_CHECK_ARG(G > 0 && in && out, "bad argument");
+    const size_t G2 = (size_t)G * G;
+    Stage s;
+    SDP_TRY(s.init());
+    sdp_float2 *di, *dout;
+    SDP_TRY(s.up(S_GRID, in, G2, &di));
+    SDP_TRY(s.buf(S_GRID2, G2, &dout));
+    SDP_TRY(sdp_fft2d(G, di, dout, sign, s.st));
+    SDP_TRY(s.down(out, dout, G2));
+    return s.sync();
+}
+
+int do_conv_correction(int G, const float *in, const float *prolate, float *out)
+{
+    SDP_CHECK_ARG(G > 0 && G % 2 == 0 && in && prolate && out, "bad argument");
+    const size_t G2 = (size_t)G * G;
+    Stage s;
+    SDP_TRY(s.init());
+    float *di, *dp, *dout;
+    SDP_TRY(s.up(S_IMG, in, G2, &di));
+    // G/2 entries from the caller plus the defined entry G/2 = 0
+    SDP_TRY(s.up(S_PROLATE, prolate, (size_t)G / 2, &dp, (size_t)G / 2 + 1));
+    SDP_CUDA_TRY(cudaMemsetAsync(dp + G / 2, 0, sizeof(float), s.st));
+    SDP_TRY(s.buf(S_IMG2, G2, &dout));
+    SDP_TRY(sdp_conv_correction(G, di, dp, dout, s.st));
+    SDP_TRY(s.down(out, dout, G2));
+    return s.sync();
+}
+
+int do_dft(int NV, int NMAX, const sdp_float3 *sources, const sdp_float3 *uvw, const int *num_sources,
+           sdp_float2 *vis)
+{
+    SDP_CHECK_ARG(NV >= 0 && num_sources && vis && (NV == 0 || uvw), "bad argument");
+    const int ns = *num_sources;
+    SDP_CHECK_ARG(ns >= 0 && (ns == 0 || sources), "bad source arguments (num_sources %d)", ns);
+    (void)NMAX;
+    Stage s;
+    SDP_TRY(s.init());
+    sdp_float3 *dsrc, *duvw;
+    sdp_float2 *dvis;
+    SDP_TRY(s.up(S_SRC, sources, ns, &dsrc));
+    SDP_TRY(s.up(S_UVW, uvw, NV, &duvw));
+    SDP_TRY(s.buf(S_OUTVIS, NV, &dvis));
+    SDP_TRY(sdp_dft(NV, ns, dsrc, duvw, dvis, s.st));
+    SDP_TRY(s.down(vis, dvis, NV));
+    return s.sync();
+}
+
+int do_hogbom(int G, int NMINOR, int MAXSRC, const float *residual, const float *psf, const sdp_config *cfg,
+              const float *model, int *num_out, sdp_float3 *sources, float *out_model)
+{
+    SDP_CHECK_ARG(G > 0 && residual && psf && cfg && model && num_out && out_model, "bad argument");
+    SDP_CHECK_ARG(NMINOR >= 0 && MAXSRC >= 0 && (sources || MAXSRC == 0 || NMINOR == 0), "bad sizes");
+    const size_t G2 = (size_t)G * G;
+    Stage s;
+    SDP_TRY(s.init());
+    float *dr, *dpsf, *dm;
+    sdp_float3 *dsrc;
+    int *dcount;
+    SDP_TRY(s.up(S_IMG, residual, G2, &dr));
+    SDP_TRY(s.up(S_PSF, psf, G2, &dpsf));
+    SDP_TRY(s.up(S_MODEL, model, G2, &dm));
+    const int cap = std::max(1, std::min(NMINOR, MAXSRC));
+    SDP_TRY(s.buf(S_SRC, (size_t)cap, &dsrc));
+    SDP_TRY(s.buf(S_COUNT, 1, &dcount));
+    size_t wsb = 0;
+    SDP_TRY(sdp_hogbom_workspace_bytes(G, &wsb));
+    void *ws = nullptr;
+    SDP_TRY(ctx_buffer(s.ctx, S_WS, wsb, &ws));
+    sdp_clean_params p{G, NMINOR, MAXSRC, cfg->loop_gain, cfg->noise_factor, cfg->weak_source_percent_img,
+                       cfg->psf_max_value, cfg->cell_size};
+    SDP_TRY(sdp_hogbom(&p, dr, dpsf, dm, dsrc, dcount, ws, wsb, s.st));
+    int count = 0;
+    SDP_TRY(s.down(&count, dcount, 1));
+    SDP_TRY(s.down(out_model, dm, G2));
+    SDP_TRY(s.sync());
+    *num_out = count;
+    if (count > 0) {
+        SDP_TRY(s.down(sources, dsrc, (size_t)count));
+        SDP_TRY(s.sync());
+    }
+    return SDP_OK;
+}
+
+int do_merge(int G, int slices, const sdp_float2 *grids, sdp_float2 *out)
+{
+    SDP_CHECK_ARG(G > 0 && slices >= 0 && grids && out, "bad argument");
+    const size_t G2 = (size_t)G * G;
+    Stage s;
+    SDP_TRY(s.init());
+    sdp_float2 *dg, *dout;
+    SDP_TRY(s.up(S_GRID, grids, G2 * slices, &dg));
+    SDP_TRY(s.buf(S_GRID2, G2, &dout));
+    SDP_TRY(sdp_merge_grids(G, slices, dg, dout, s.st));
+    SDP_TRY(s.down(out, dout, G2));
+    return s.sync();
+}
+
+int do_subtract_image(int G, const float *a, const float *b, float *o)
+{
+    SDP_CHECK_ARG(G > 0 && a && b && o, "bad argument");
+    const size_t G2 = (size_t)G * G;
+    Stage s;
+    SDP_TRY(s.init());
+    float *da, *db, *dout;
+    SDP_TRY(s.up(S_IMG, a, G2, &da));
+    SDP_TRY(s.up(S_IMG2, b, G2, &db));
+    SDP_TRY(s.buf(S_GRID, G2, &dout));
+    SDP_TRY(sdp_subtract_image(G, da, db, dout, s.st));
+    SDP_TRY(s.down(o, dout, G2));
+    return s.sync();
+}
+
+int do_prolate(int G, float *prolate)
+{
+    SDP_CHECK_ARG(G >= 2 && G % 2 == 0 && prolate, "bad argument");
+    Stage s;
+    SDP_TRY(s.init());
+    float *dp;
+    SDP_TRY(s.buf(S_PROLATE, (size_t)G / 2 + 1, &dp));
+    SDP_TRY(sdp_prolate_table(G, dp, s.st));
+    SDP_TRY(s.down(prolate, dp, (size_t)G / 2));
+    return s.sync();
+}
+
+}  // namespace
+
+// ===========================================================================
+// Exported actors
+// ===========================================================================
+SDP_EXPORT int sdp_set_degrid_mode(int mode)
+{
+    SDP_CHECK_ARG(mode == SDP_DEGRID_NEAREST || mode == SDP_DEGRID_CONV, "degrid mode %d unknown", mode);
+    g_degrid_mode = mode;
+    return SDP_OK;
+}
+
+SDP_EXPORT int sdp_get_degrid_mode(void) { return g_degrid_mode; }
+
+SDP_EXPORT void correct_to_finegrid(int NUM_VISIBILITIES, int GRID_SIZE, int OVERSAMPLING_FACTOR,
+                                    int PERFORM_SIMPLIFICATION, sdp_float3 *vis_uvw_coords,
+                                    sdp_float2 *input_visibilities, sdp_config *config,
+                                    sdp_float2 *output_visibilities, sdp_float3 *output_finegrid_vis_coords,
+                                    int *num_output_visibilities)
+{
+    ACTOR("correct_to_finegrid",
+          do_correct_to_finegrid(NUM_VISIBILITIES, GRID_SIZE, OVERSAMPLING_FACTOR, PERFORM_SIMPLIFICATION,
+                                 vis_uvw_coords, input_visibilities, config, output_visibilities,
+                                 output_finegrid_vis_coords, num_output_visibilities));
+}
+
+SDP_EXPORT void std_gridding(int GRID_SIZE, int NUM_VISIBILITIES, int NUM_KERNELS, int TOTAL_KERNEL_SAMPLES,
+                             int OVERSAMPLING_FACTOR, int BYPASS, int *maj_iter, int *num_corrected_visibilities,
+                             sdp_float2 *kernels, sdp_int2 *kernel_supports, sdp_float3 *corrected_vis_uvw_coords,
+                             sdp_float2 *visibilities, sdp_config *config, sdp_float2 *prev_grid,
+                             sdp_float2 *output_grid)
+{
+    ACTOR("std_gridding", do_std_gridding(GRID_SIZE, NUM_VISIBILITIES, NUM_KERNELS, TOTAL_KERNEL_SAMPLES,
+                                          OVERSAMPLING_FACTOR, BYPASS, maj_iter, num_corrected_visibilities, kernels,
+                                          kernel_supports, corrected_vis_uvw_coords, visibilities, config, prev_grid,
+                                          output_grid));
+}
+
+SDP_EXPORT void std_degridding(int GRID_SIZE, int NUM_VISIBILITIES, int NUM_KERNELS, int TOTAL_KERNEL_SAMPLES,
+                               int OVERSAMPLING_FACTOR, sdp_float2 *kernels, sdp_int2 *kernel_supports,
+                               sdp_float2 *input_grid, sdp_float3 *corrected_vis_uvw_coords,
+                               int *num_corrected_visibilities, sdp_config *config, sdp_float2 *output_visibilities)
+{
+    ACTOR("std_degridding", do_std_degridding(GRID_SIZE, NUM_VISIBILITIES, NUM_KERNELS, TOTAL_KERNEL_SAMPLES,
+                                              OVERSAMPLING_FACTOR, kernels, kernel_supports, input_grid,
+                                              corrected_vis_uvw_coords, num_corrected_visibilities, config,
+                                              output_visibilities));
+}
+
+SDP_EXPORT void g2g_degridgrid(int GRID_SIZE, int NUM_VISIBILITIES, int NUM_GRIDDING_KERNELS,
+                               int NUM_DEGRIDDING_KERNELS, int TOTAL_GRIDDING_KERNEL_SAMPLES,
+                               int TOTAL_DEGRIDDING_KERNEL_SAMPLES, int OVERSAMPLING_FACTOR,
+                               sdp_float2 *gridding_kernels, sdp_int2 *gridding_kernel_supports,
+                               sdp_float2 *degridding_kernels, sdp_int2 *degridding_kernel_supports,
+                               sdp_float2 *input_grid, sdp_float3 *corrected_vis_uvw_coords,
+                               int *num_corrected_visibilities, sdp_config *config, sdp_float2 *output_grid)
+{
+    ACTOR("g2g_degridgrid",
+          do_g2g(GRID_SIZE, NUM_VISIBILITIES, NUM_GRIDDING_KERNELS, NUM_DEGRIDDING_KERNELS,
+                 TOTAL_GRIDDING_KERNEL_SAMPLES, TOTAL_DEGRIDDING_KERNEL_SAMPLES, OVERSAMPLING_FACTOR,
+                 gridding_kernels, gridding_kernel_supports, degridding_kernels, degridding_kernel_supports,
+                 input_grid, corrected_vis_uvw_coords, num_corrected_visibilities, config, output_grid));
+}
+
+SDP_EXPORT void subtract_image_space(int GRID_SIZE, float *measurements, float *estimate, float *result)
+{
+    ACTOR("subtract_image_space", do_subtract_image(GRID_SIZE, measurements, estimate, result));
+}
+
+SDP_EXPORT void degridding_kernel_sink(int, int, sdp_int2 *, sdp_float2 *) {}
+
+SDP_EXPORT void gridding_actor(int GRID_SIZE, int NUM_VISIBILITIES, int NUM_KERNELS, int TOTAL_KERNEL_SAMPLES,
+                               sdp_float2 *kernels, sdp_int2 *kernel_supports, sdp_float3 *vis_uvw_coords,
+                               sdp_float2 *visibilities, sdp_config *config, sdp_float2 *uv_grid)
+{
+    // gridding_run.c:8, 42-44: zeroed grid, oversampling fixed at 16
+    int status = SDP_OK;
+    if (!config) status = set_error(SDP_ERR_INVALID, "config is NULL");
+    if (status == SDP_OK)
+        status = do_gridding_snapped(uv_grid, kernels, kernel_supports, NUM_KERNELS, TOTAL_KERNEL_SAMPLES,
+                                     vis_uvw_coords, visibilities, NUM_VISIBILITIES, 16, GRID_SIZE, config->uv_scale,
+                                     config->w_scale, false);
+    if (status != SDP_OK) actor_fail("gridding_actor");
+}
+
+SDP_EXPORT void gridding_CPU(sdp_float2 *grid, const sdp_float2 *kernel, const sdp_int2 *supports,
+                             const sdp_float3 *vis_uvw, const sdp_float2 *vis, const int num_vis,
+                             const int oversampling, const int grid_size, const double uv_scale,
+                             const double w_scale)
+{
+    int status = SDP_OK;
+    if (!supports || (num_vis > 0 && !vis_uvw)) status = set_error(SDP_ERR_INVALID, "bad argument");
+    int nk = 1, tks = 1;
+    if (status == SDP_OK) snapped_extent(supports, vis_uvw, num_vis, w_scale, oversampling, &nk, &tks);
+    if (status == SDP_OK)
+        status = do_gridding_snapped(grid, kernel, supports, nk, tks, vis_uvw, vis, num_vis, oversampling, grid_size,
+                                     uv_scale, w_scale, true);
+    if (status != SDP_OK) actor_fail("gridding_CPU");
+}
+
+SDP_EXPORT void add_visibilities(int NUM_VISIBILITIES, sdp_float2 *v1, sdp_float2 *v2, sdp_float2 *output)
+{
+    ACTOR("add_visibilities", do_vis_binary(NUM_VISIBILITIES, v1, v2, output, false));
+}
+
+SDP_EXPORT void fft_shift_complex_to_complex_actor(int GRID_SIZE, sdp_float2 *uv_grid_in, sdp_config *,
+                                                   sdp_float2 *uv_grid_out)
+{
+    ACTOR("fft_shift_complex_to_complex_actor", do_shift(GRID_SIZE, uv_grid_in, uv_grid_out, 0));
+}
+
+SDP_EXPORT void CUFFT_EXECUTE_FORWARD_C2C_actor(int GRID_SIZE, sdp_float2 *uv_grid_in, sdp_float2 *uv_grid_out)
+{
+    ACTOR("CUFFT_EXECUTE_FORWARD_C2C_actor", do_fft(GRID_SIZE, uv_grid_in, uv_grid_out, -1));
+}
+
+SDP_EXPORT void CUFFT_EXECUTE_INVERSE_C2C_actor(int GRID_SIZE, sdp_float2 *uv_grid_in, sdp_float2 *uv_grid_out)
+{
+    ACTOR("CUFFT_EXECUTE_INVERSE_C2C_actor", do_fft(GRID_SIZE, uv_grid_in, uv_grid_out, +1));
+}
+
+SDP_EXPORT void fft_shift_complex_to_real_actor(int GRID_SIZE, sdp_float2 *uv_grid, sdp_config *, float *dirty_image)
+{
+    ACTOR("fft_shift_complex_to_real_actor", do_shift(GRID_SIZE, uv_grid, dirty_image, 1));
+}
+
+SDP_EXPORT void fft_shift_real_to_complex_actor(int GRID_SIZE, float *image, sdp_config *, sdp_float2 *fourier)
+{
+    ACTOR("fft_shift_real_to_complex_actor", do_shift(GRID_SIZE, image, fourier, 2));
+}
+
+SDP_EXPORT void execute_convolution_correction_actor(int GRID_SIZE, float *dirty_image_in, float *prolate,
+                                                     sdp_config *, float *dirty_image_out)
+{
+    ACTOR("execute_convolution_correction_actor", do_conv_correction(GRID_SIZE, dirty_image_in, prolate,
+                                                                      dirty_image_out));
+}
+
+SDP_EXPORT void execute_inv_convolution_correction_actor(int GRID_SIZE, float *dirty_image_in, float *,
+                                                         sdp_config *, float *dirty_image_out)
+{
+    // convolution_correction_run.c:61: identity copy
+    if (GRID_SIZE > 0 && dirty_image_in && dirty_image_out)
+        memmove(dirty_image_out, dirty_image_in, sizeof(float) * (size_t)GRID_SIZE * GRID_SIZE);
+}
+
+SDP_EXPORT void dft_actor(int NUM_VISIBILITIES, int NUM_MAX_SOURCES, sdp_float3 *sources, sdp_float3 *vis_uvw_coords,
+                          int *num_sources, sdp_config *, sdp_float2 *visibilities)
+{
+    ACTOR("dft_actor", do_dft(NUM_VISIBILITIES, NUM_MAX_SOURCES, sources, vis_uvw_coords, num_sources, visibilities));
+}
+
+SDP_EXPORT void hogbom_clean(int GRID_SIZE, int NUM_MINOR_CYCLES, int MAX_SOURCES, float *residual, float *psf,
+                             sdp_int2 *, sdp_config *config, float *current_model, int *num_sources_out,
+                             sdp_float3 *sources_out, float *output_model)
+{
+    ACTOR("hogbom_clean", do_hogbom(GRID_SIZE, NUM_MINOR_CYCLES, MAX_SOURCES, residual, psf, config, current_model,
+                                    num_sources_out, sources_out, output_model));
+}
+
+SDP_EXPORT void split_visibilities(sdp_config *config, int NUM_VISIBILITIES, int SLICES,
+                                   sdp_float2 *measured_visibilities, sdp_float3 *vis_coords,
+                                   sdp_float2 *visibilities, sdp_float3 *out_vis_coords, sdp_config *output_configs,
+                                   sdp_config *output_config)
+{
+    // splitmerge.c:3-12: copies only
+    memmove(visibilities, measured_visibilities, sizeof(sdp_float2) * (size_t)NUM_VISIBILITIES);
+    memmove(out_vis_coords, vis_coords, sizeof(sdp_float3) * (size_t)NUM_VISIBILITIES);
+    for (int i = 0; i < SLICES; ++i) output_configs[i] = *config;
+    *output_config = *config;
+}
+
+SDP_EXPORT void merge_gridded_visibilities(int GRID_SIZE, int SLICES, sdp_float2 *grids, sdp_float2 *output_grid)
+{
+    ACTOR("merge_gridded_visibilities", do_merge(GRID_SIZE, SLICES, grids, output_grid));
+}
+
+SDP_EXPORT void merge_configs(sdp_config *in_configs, sdp_config *out_config) { *out_config = in_configs[0]; }
+
+SDP_EXPORT void split_fftdegrid_visibilities(int NUM_VISIBILITIES, int SLICES, int, sdp_config *config,
+                                             sdp_float3 *vis_coords, sdp_float2 *measured_visibilities,
+                                             int *num_corrected_vis, int *maj_iter,
+                                             sdp_float2 *output_visibilities, sdp_float3 *out_vis_coords,
+                                             sdp_config *output_configs, int *num_vis, int *maj_iter_out)
+{
+    // splitmerge.c:30-48: copies and per-slice counts (remainder dropped)
+    memmove(out_vis_coords, vis_coords, sizeof(sdp_float3) * (size_t)NUM_VISIBILITIES);
+    memmove(output_visibilities, measured_visibilities, sizeof(sdp_float2) * (size_t)NUM_VISIBILITIES);
+    for (int i = 0; i < SLICES; ++i) {
+        output_configs[i] = *config;
+        maj_iter_out[i] = *maj_iter;
+    }
+    int left = *num_corrected_vis;
+    const int ideal = SLICES > 0 ? NUM_VISIBILITIES / SLICES : 0;
+    for (int i = 0; i < SLICES; ++i) {
+        const int cur = left > ideal ? ideal : left;
+        left -= cur;
+        num_vis[i] = cur;
+    }
+}
+
+SDP_EXPORT void split_uvgrid(int GRID_SIZE, int SLICES, sdp_float2 *input_grid, sdp_float2 *output_grid)
+{
+    const size_t G2 = (size_t)GRID_SIZE * GRID_SIZE;
+    for (int i = 0; i < SLICES; ++i) memmove(output_grid + (size_t)i * G2, input_grid, sizeof(sdp_float2) * G2);
+}
+
+SDP_EXPORT void subtract_from_measurements_finegrid(int NUM_VISIBILITIES, sdp_float2 *gridded_measured_vis,
+                                                    sdp_float2 *input_vis, int *num_finegrid_vis,
+                                                    sdp_float2 *delta_vis)
+{
+    int status = SDP_OK;
+    if (!num_finegrid_vis) status = set_error(SDP_ERR_INVALID, "num_finegrid_vis is NULL");
+    else if (*num_finegrid_vis > NUM_VISIBILITIES || *num_finegrid_vis < 0)
+        status = set_error(SDP_ERR_INVALID, "num_finegrid_vis %d outside [0, %d]", *num_finegrid_vis, NUM_VISIBILITIES);
+    if (status == SDP_OK) status = do_vis_binary(*num_finegrid_vis, gridded_measured_vis, input_vis, delta_vis, true);
+    if (status != SDP_OK) actor_fail("subtract_from_measurements_finegrid");
+}
+
+// --------------------------- setup (top.c) ---------------------------------
+SDP_EXPORT void config_struct_set_up(int GRID_SIZE, int NUM_KERNELS, sdp_config *c)
+{
+    // top.c:9-68: the numeric fields and file names the reference assigns
+    c->gpu_max_threads_per_block = 1024;
+    c->gpu_max_threads_per_block_dimension = 32;
+    c->cell_size = 8.52211548825356E-06;
+    c->frequency_hz = 299792458.0;
+    c->dirty_image_output = "gleam_small_dirty_image.csv";
+    c->right_ascension = true;
+    c->visibility_source_file = "data/input/GLEAM_small_visibilities_corrupted.csv";
+    c->output_path = "data/output/small/";
+    c->perform_system_test = false;
+    c->system_test_image = "";
+    c->system_test_sources = "";
+    c->system_test_visibilities = "";
+    c->default_gains_file = "data/input/TrueGainsNotRotated.csv";
+    c->output_gains_file = "estimated_gains.csv";
+    c->use_default_gains = true;
+    c->max_w = 1895.410847844;
+    c->w_scale = pow((double)(NUM_KERNELS - 1), 2.0) / c->max_w;
+    c->oversampling = 16;
+    c->uv_scale = c->cell_size * GRID_SIZE;
+    c->kernel_real_file = "data/input/kernels/new/wproj_manualconj_gridding_kernels_real_x16.csv";
+    c->kernel_imag_file = "data/input/kernels/new/wproj_manualconj_gridding_kernels_imag_x16.csv";
+    c->kernel_support_file = "data/input/kernels/new/wproj_manualconj_gridding_kernel_supports_x16.csv";
+    c->degridding_kernel_real_file = "data/input/kernels/new/wproj_manualconj_degridding_kernels_real_x16.csv";
+    c->degridding_kernel_imag_file = "data/input/kernels/new/wproj_manualconj_degridding_kernels_imag_x16.csv";
+    c->degridding_kernel_support_file = "data/input/kernels/new/wproj_manualconj_degridding_kernel_supports_x16.csv";
+    c->force_weight_to_one = true;
+    c->loop_gain = 0.1;
+    c->weak_source_percent_gc = 0.005;
+    c->weak_source_percent_img = 0.0002;
+    c->psf_max_value = 0.0;
+    c->noise_factor = 1.5;
+    c->model_sources_output = "sample_model_sources.csv";
+    c->residual_image_output = "residual_image.csv";
+    c->psf_input_file = "data/input/gleam_small_psf.csv";
+    c->psf_image_output = "dirty_psf.csv";
+    c->clean_psf_image_output = "clean_psf.csv";
+    c->model_image_output = "model.csv";
+    c->final_image_output = "deconvolved.csv";
+    c->predicted_vis_output = "predicted_visibilities.csv";
+}
+
+SDP_EXPORT void correction_set_up(int GRID_SIZE, float *prolate)
+{
+    if (!prolate) {
+        set_error(SDP_ERR_INVALID, "prolate is NULL");
+        actor_fail("correction_set_up");
+        return;
+    }
+    ACTOR("correction_set_up", do_prolate(GRID_SIZE, prolate));
+}
+
+SDP_EXPORT void create_1D_half_prolate(float *prolate, int grid_size)
+{
+    ACTOR("create_1D_half_prolate", do_prolate(grid_size, prolate));
+}
+
+SDP_EXPORT double prolate_spheroidal(double nu) { return prolate_host(nu); }
+
+SDP_EXPORT void config_struct_set_up_sequel(sdp_config *config_in, double *psf_max_value, sdp_config *config_out)
+{
+    memmove(config_out, config_in, sizeof(sdp_config));
+    config_out->psf_max_value = *psf_max_value;
+}
+
+SDP_EXPORT void model_set_up(int GRID_SIZE, sdp_config *, float *initial_image)
+{
+    if (initial_image) memset(initial_image, 0, sizeof(float) * (size_t)GRID_SIZE * GRID_SIZE);
+}
+
+SDP_EXPORT void sources_set_up(int MAX_SOURCES, int *num_sources, sdp_float3 *sources)
+{
+    if (num_sources) *num_sources = 0;
+    if (sources) memset(sources, 0, sizeof(sdp_float3) * (size_t)MAX_SOURCES);
+}

@@ -1,0 +1,510 @@
+"""ctypes front end of libsdp_b200.so.
+
+Two layers, matching include/sdp_b200.h:
+
+* ``Actors``: the reference's PREESM actors (host numpy arrays in, host
+  numpy arrays out), called through the exported C symbols exactly as the
+  generated schedule calls them.  Method names and argument order follow the
+  reference actors (param_code/code_*_1core/include/*.h).
+* ``Device``: the device-resident sdp_* layer on torch CUDA tensors (torch is
+  used only to own device memory and streams; every computation is a kernel
+  of libsdp_b200.so).
+
+Loading fails loudly when the library is missing; there is no fallback.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import re
+from pathlib import Path
+
+import numpy as np
+
+HERE = Path(__file__).resolve().parent
+LIB_PATH = HERE / "libsdp_b200.so"
+HEADER = HERE.parent / "include" / "sdp_b200.h"
+
+SDP_OK = 0
+SDP_DEGRID_NEAREST = 0
+SDP_DEGRID_CONV = 1
+SDP_GRID_STD = 0
+SDP_GRID_SNAPPED = 1
+SDP_GRID_G2G = 2
+
+_i = C.c_int
+_d = C.c_double
+_p = C.c_void_p
+_sz = C.c_size_t
+
+
+class SdpError(RuntimeError):
+    def __init__(self, status: int, message: str):
+        super().__init__(f"sdp status {status}: {message}")
+        self.status = status
+
+
+class Config(C.Structure):
+    """Layout of the reference's Config (common.h:187-265) == sdp_config."""
+    _fields_ = [
+        ("retain_device_mem", C.c_bool), ("num_major_cycles", _i), ("num_recievers", _i),
+        ("num_baselines", _i), ("grid_size", _i), ("cell_size", _d), ("output_path", _p),
+        ("dirty_image_output", _p), ("gpu_max_threads_per_block", _i),
+        ("gpu_max_threads_per_block_dimension", _i), ("right_ascension", C.c_bool),
+        ("save_dirty_image", C.c_bool), ("save_residual_image", C.c_bool),
+        ("save_extracted_sources", C.c_bool), ("save_predicted_visibilities", C.c_bool),
+        ("save_estimated_gains", C.c_bool), ("perform_system_test", C.c_bool),
+        ("system_test_image", _p), ("system_test_sources", _p), ("system_test_visibilities", _p),
+        ("system_test_gains", _p), ("default_gains_file", _p), ("output_gains_file", _p),
+        ("perform_gain_calibration", C.c_bool), ("use_default_gains", C.c_bool),
+        ("max_calibration_cycles", _i), ("number_cal_major_cycles", _i), ("force_weight_to_one", C.c_bool),
+        ("frequency_hz", _d), ("oversampling", _i), ("uv_scale", _d), ("num_visibilities", _i),
+        ("num_kernels", _i), ("total_kernel_samples", _i), ("max_w", _d), ("w_scale", _d),
+        ("kernel_real_file", _p), ("kernel_imag_file", _p), ("kernel_support_file", _p),
+        ("degridding_kernel_real_file", _p), ("degridding_kernel_imag_file", _p),
+        ("degridding_kernel_support_file", _p), ("visibility_source_file", _p),
+        ("number_minor_cycles_cal", C.c_uint), ("number_minor_cycles_img", C.c_uint), ("loop_gain", _d),
+        ("weak_source_percent_gc", _d), ("weak_source_percent_img", _d), ("noise_factor", _d),
+        ("psf_max_value", _d), ("model_sources_output", _p), ("residual_image_output", _p),
+        ("psf_input_file", _p), ("psf_image_output", _p), ("clean_psf_image_output", _p),
+        ("model_image_output", _p), ("final_image_output", _p), ("num_sources", _i),
+        ("predicted_vis_output", _p),
+    ]
+
+
+assert C.sizeof(Config) == 360
+
+
+def make_config(grid_size: int, uv_scale: float, w_scale: float, oversampling: int = 16,
+                cell_size: float = 8.52211548825356e-06, psf_max_value: float = 0.0, loop_gain: float = 0.1,
+                noise_factor: float = 1.5, weak_source_percent_img: float = 0.0002) -> Config:
+    c = Config()
+    c.grid_size = grid_size
+    c.uv_scale = uv_scale
+    c.w_scale = w_scale
+    c.oversampling = oversampling
+    c.cell_size = cell_size
+    c.psf_max_value = psf_max_value
+    c.loop_gain = loop_gain
+    c.noise_factor = noise_factor
+    c.weak_source_percent_img = weak_source_percent_img
+    c.frequency_hz = 299792458.0
+    c.right_ascension = True
+    c.force_weight_to_one = True
+    return c
+
+
+class Geometry(C.Structure):
+    _fields_ = [("grid_size", _i), ("oversampling", _i), ("uv_scale", _d), ("w_scale", _d)]
+
+
+class WKernels(C.Structure):
+    _fields_ = [("kernels", _p), ("supports", _p), ("num_kernels", _i), ("total_samples", _i),
+                ("max_half_support", _i)]
+
+
+class CleanParams(C.Structure):
+    _fields_ = [("grid_size", _i), ("num_minor_cycles", _i), ("max_sources", _i), ("loop_gain", _d),
+                ("noise_factor", _d), ("weak_source_percent", _d), ("psf_max_value", _d), ("cell_size", _d)]
+
+
+def header_functions(header: Path = HEADER) -> list[str]:
+    """Names of every function declared in include/sdp_b200.h."""
+    text = header.read_text()
+    text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
+    names = re.findall(r"^\s*(?:const\s+)?[A-Za-z_][A-Za-z0-9_]*\s*\**\s*([A-Za-z_][A-Za-z0-9_]*)\s*\(",
+                       text, flags=re.M)
+    return [n for n in names if n not in ("if", "for", "while", "return", "sizeof")]
+
+
+_lib = None
+
+
+def load(path: Path | str | None = None) -> C.CDLL:
+    """Loads libsdp_b200.so (raises when it is missing: there is no fallback)."""
+    global _lib
+    if _lib is not None and path is None:
+        return _lib
+    p = Path(path) if path else LIB_PATH
+    if not p.exists():
+        raise FileNotFoundError(f"{p} is not built; run python {HERE / 'build.py'}")
+    lib = C.CDLL(str(p))
+    lib.sdp_last_error.restype = C.c_char_p
+    lib.prolate_spheroidal.restype = _d
+    lib.prolate_spheroidal.argtypes = [_d]
+    for name in ("sdp_visplan_create",):
+        getattr(lib, name).restype = _i
+    lib.gridding_CPU.argtypes = [_p, _p, _p, _p, _p, _i, _i, _i, _d, _d]
+    if path is None:
+        _lib = lib
+    return lib
+
+
+def check(status: int, lib: C.CDLL | None = None) -> None:
+    if status != SDP_OK:
+        lib = lib or load()
+        raise SdpError(status, lib.sdp_last_error().decode())
+
+
+def _ptr(a):
+    if a is None:
+        return None
+    assert a.flags["C_CONTIGUOUS"]
+    return a.ctypes.data_as(_p)
+
+
+def _f32(x, cols=None):
+    a = np.ascontiguousarray(x, dtype=np.float32)
+    if cols is not None:
+        a = a.reshape(-1, cols)
+    return a
+
+
+# ---------------------------------------------------------------------------
+# Actor layer (host arrays)
+# ---------------------------------------------------------------------------
+class Actors:
+    """Calls the exported actor symbols the way the PREESM schedule does."""
+
+    def __init__(self, lib: C.CDLL | None = None):
+        self.lib = lib or load()
+
+    def _status(self):
+        st = self.lib.sdp_last_status()
+        if st != SDP_OK:
+            msg = self.lib.sdp_last_error().decode()
+            self.lib.sdp_clear_error()
+            raise SdpError(st, msg)
+
+    def set_degrid_mode(self, mode: int):
+        check(self.lib.sdp_set_degrid_mode(_i(mode)), self.lib)
+
+    def std_gridding(self, cfg: Config, grid_size, os_, kernels, supports, uvw, vis, num=None, out=None):
+        k = _f32(kernels, 2)
+        s = np.ascontiguousarray(supports, dtype=np.int32)
+        uvw = _f32(uvw, 3)
+        vis = _f32(vis, 2)
+        n = uvw.shape[0] if num is None else num
+        grid = np.empty((grid_size * grid_size, 2), dtype=np.float32) if out is None else out
+        maj = _i(0)
+        nc = _i(n)
+        self.lib.sdp_clear_error()
+        self.lib.std_gridding(_i(grid_size), _i(uvw.shape[0]), _i(s.shape[0]), _i(k.shape[0]), _i(os_), _i(0),
+                              C.byref(maj), C.byref(nc), _ptr(k), _ptr(s), _ptr(uvw), _ptr(vis), C.byref(cfg), None,
+                              _ptr(grid))
+        self._status()
+        return grid
+
+    def std_degridding(self, cfg: Config, grid_size, os_, kernels, supports, grid, uvw, num=None, out=None):
+        k = _f32(kernels, 2)
+        s = np.ascontiguousarray(supports, dtype=np.int32)
+        g = _f32(grid, 2)
+        uvw = _f32(uvw, 3)
+        n = uvw.shape[0] if num is None else num
+        o = np.empty((uvw.shape[0], 2), dtype=np.float32) if out is None else out
+        nc = _i(n)
+        self.lib.sdp_clear_error()
+        self.lib.std_degridding(_i(grid_size), _i(uvw.shape[0]), _i(s.shape[0]), _i(k.shape[0]), _i(os_), _ptr(k),
+                                _ptr(s), _ptr(g), _ptr(uvw), C.byref(nc), C.byref(cfg), _ptr(o))
+        self._status()
+        return o
+
+    def subtract_finegrid(self, measured, predicted, num=None, out=None):
+        m = _f32(measured, 2)
+        p = _f32(predicted, 2)
+        n = m.shape[0] if num is None else num
+        o = np.zeros_like(m) if out is None else out
+        nc = _i(n)
+        self.lib.sdp_clear_error()
+        self.lib.subtract_from_measurements_finegrid(_i(m.shape[0]), _ptr(m), _ptr(p), C.byref(nc), _ptr(o))
+        self._status()
+        return o
+
+    def g2g_degridgrid(self, cfg: Config, grid_size, os_, gk, gs, dk, ds, in_grid, uvw):
+        gk = _f32(gk, 2)
+        dk = _f32(dk, 2)
+        gs = np.ascontiguousarray(gs, dtype=np.int32)
+        ds = np.ascontiguousarray(ds, dtype=np.int32)
+        g = _f32(in_grid, 2)
+        uvw = _f32(uvw, 3)
+        out = np.empty((grid_size * grid_size, 2), dtype=np.float32)
+        nc = _i(uvw.shape[0])
+        self.lib.sdp_clear_error()
+        self.lib.g2g_degridgrid(_i(grid_size), _i(uvw.shape[0]), _i(gs.shape[0]), _i(ds.shape[0]), _i(gk.shape[0]),
+                                _i(dk.shape[0]), _i(os_), _ptr(gk), _ptr(gs), _ptr(dk), _ptr(ds), _ptr(g), _ptr(uvw),
+                                C.byref(nc), C.byref(cfg), _ptr(out))
+        self._status()
+        return out
+
+    def gridding_actor(self, cfg: Config, grid_size, kernels, supports, uvw, vis):
+        k = _f32(kernels, 2)
+        s = np.ascontiguousarray(supports, dtype=np.int32)
+        uvw = _f32(uvw, 3)
+        vis = _f32(vis, 2)
+        grid = np.empty((grid_size * grid_size, 2), dtype=np.float32)
+        self.lib.sdp_clear_error()
+        self.lib.gridding_actor(_i(grid_size), _i(uvw.shape[0]), _i(s.shape[0]), _i(k.shape[0]), _ptr(k), _ptr(s),
+                                _ptr(uvw), _ptr(vis), C.byref(cfg), _ptr(grid))
+        self._status()
+        return grid
+
+    def gridding_cpu(self, grid, kernels, supports, uvw, vis, os_, grid_size, uv_scale, w_scale):
+        g = _f32(grid, 2).copy()
+        k = _f32(kernels, 2)
+        s = np.ascontiguousarray(supports, dtype=np.int32)
+        uvw = _f32(uvw, 3)
+        vis = _f32(vis, 2)
+        self.lib.sdp_clear_error()
+        self.lib.gridding_CPU(_ptr(g), _ptr(k), _ptr(s), _ptr(uvw), _ptr(vis), uvw.shape[0], os_, grid_size,
+                              uv_scale, w_scale)
+        self._status()
+        return g
+
+    def correct_to_finegrid(self, cfg: Config, grid_size, os_, uvw, vis, simplify=0):
+        uvw = _f32(uvw, 3)
+        vis = _f32(vis, 2)
+        n = uvw.shape[0]
+        ov = np.zeros_like(vis)
+        ou = np.zeros_like(uvw)
+        cnt = _i(0)
+        self.lib.sdp_clear_error()
+        self.lib.correct_to_finegrid(_i(n), _i(grid_size), _i(os_), _i(simplify), _ptr(uvw), _ptr(vis),
+                                     C.byref(cfg), _ptr(ov), _ptr(ou), C.byref(cnt))
+        self._status()
+        return ov, ou, cnt.value
+
+    def fft_shift_c2c(self, cfg, grid_size, x):
+        x = _f32(x, 2)
+        out = np.empty_like(x)
+        self.lib.sdp_clear_error()
+        self.lib.fft_shift_complex_to_complex_actor(_i(grid_size), _ptr(x), C.byref(cfg), _ptr(out))
+        self._status()
+        return out
+
+    def fft_shift_c2r(self, cfg, grid_size, x):
+        x = _f32(x, 2)
+        out = np.empty(x.shape[0], dtype=np.float32)
+        self.lib.sdp_clear_error()
+        self.lib.fft_shift_complex_to_real_actor(_i(grid_size), _ptr(x), C.byref(cfg), _ptr(out))
+        self._status()
+        return out
+
+    def fft_shift_r2c(self, cfg, grid_size, x):
+        x = _f32(x)
+        out = np.empty((x.shape[0], 2), dtype=np.float32)
+        self.lib.sdp_clear_error()
+        self.lib.fft_shift_real_to_complex_actor(_i(grid_size), _ptr(x), C.byref(cfg), _ptr(out))
+        self._status()
+        return out
+
+    def fft(self, grid_size, x, inverse):
+        x = _f32(x, 2)
+        out = np.empty_like(x)
+        fn = self.lib.CUFFT_EXECUTE_INVERSE_C2C_actor if inverse else self.lib.CUFFT_EXECUTE_FORWARD_C2C_actor
+        self.lib.sdp_clear_error()
+        fn(_i(grid_size), _ptr(x), _ptr(out))
+        self._status()
+        return out
+
+    def half_prolate(self, grid_size):
+        out = np.zeros(grid_size // 2, dtype=np.float32)
+        self.lib.sdp_clear_error()
+        self.lib.create_1D_half_prolate(_ptr(out), _i(grid_size))
+        self._status()
+        return out
+
+    def conv_correction(self, cfg, grid_size, image, prolate):
+        x = _f32(image)
+        p = _f32(prolate)[: grid_size // 2].copy()
+        out = np.empty_like(x)
+        self.lib.sdp_clear_error()
+        self.lib.execute_convolution_correction_actor(_i(grid_size), _ptr(x), _ptr(p), C.byref(cfg), _ptr(out))
+        self._status()
+        return out
+
+    def dft(self, cfg, sources, uvw):
+        s = _f32(sources, 3)
+        uvw = _f32(uvw, 3)
+        out = np.empty((uvw.shape[0], 2), dtype=np.float32)
+        ns = _i(s.shape[0])
+        self.lib.sdp_clear_error()
+        self.lib.dft_actor(_i(uvw.shape[0]), _i(s.shape[0]), _ptr(s), _ptr(uvw), C.byref(ns), C.byref(cfg), _ptr(out))
+        self._status()
+        return out
+
+    def hogbom(self, cfg, grid_size, num_minor, max_sources, residual, psf, model=None):
+        r = _f32(residual).reshape(-1)
+        p = _f32(psf).reshape(-1)
+        m = np.zeros_like(r) if model is None else _f32(model).reshape(-1)
+        out_model = np.empty_like(r)
+        src = np.zeros((max(max_sources, 1), 3), dtype=np.float32)
+        n = _i(0)
+        hd = np.zeros(2, dtype=np.int32)
+        self.lib.sdp_clear_error()
+        self.lib.hogbom_clean(_i(grid_size), _i(num_minor), _i(max_sources), _ptr(r), _ptr(p), _ptr(hd), C.byref(cfg),
+                              _ptr(m), C.byref(n), _ptr(src), _ptr(out_model))
+        self._status()
+        return n.value, src[:n.value].copy(), out_model
+
+    def merge_grids(self, grid_size, grids):
+        g = _f32(grids, 2)
+        slices = g.shape[0] // (grid_size * grid_size)
+        out = np.empty((grid_size * grid_size, 2), dtype=np.float32)
+        self.lib.sdp_clear_error()
+        self.lib.merge_gridded_visibilities(_i(grid_size), _i(slices), _ptr(g), _ptr(out))
+        self._status()
+        return out
+
+    def subtract_image(self, grid_size, a, b):
+        a = _f32(a)
+        b = _f32(b)
+        out = np.empty_like(a)
+        self.lib.sdp_clear_error()
+        self.lib.subtract_image_space(_i(grid_size), _ptr(a), _ptr(b), _ptr(out))
+        self._status()
+        return out
+
+    def add_visibilities(self, a, b):
+        a = _f32(a, 2)
+        b = _f32(b, 2)
+        out = np.empty_like(a)
+        self.lib.sdp_clear_error()
+        self.lib.add_visibilities(_i(a.shape[0]), _ptr(a), _ptr(b), _ptr(out))
+        self._status()
+        return out
+
+    def clean_psf(self, cfg, grid_size, dirty_psf):
+        d = _f32(dirty_psf).reshape(-1)
+        out = np.empty_like(d)
+        hd = np.zeros(2, dtype=np.int32)
+        self.lib.sdp_clear_error()
+        self.lib.clean_psf_host_set_up(_i(grid_size), _i(1), C.byref(cfg), _ptr(d), _ptr(out), _ptr(hd))
+        self._status()
+        return out, hd
+
+
+# ---------------------------------------------------------------------------
+# Device layer (torch CUDA tensors)
+# ---------------------------------------------------------------------------
+def _dp(t):
+    """Device pointer of a contiguous torch tensor (or None)."""
+    if t is None:
+        return None
+    assert t.is_cuda and t.is_contiguous()
+    return _p(t.data_ptr())
+
+
+def _stream(s=None):
+    import torch
+    s = s if s is not None else torch.cuda.current_stream()
+    return _p(s.cuda_stream)
+
+
+class VisPlan:
+    """Owns an sdp_visplan (visibilities binned by uv tile and w-plane)."""
+
+    def __init__(self, lib, geom: Geometry, gk: WKernels, dk: WKernels | None, uvw, mode: int, stream=None,
+                 keep=()):
+        self.lib = lib
+        self.geom = geom
+        self._keep = keep  # tensors the plan points at
+        self.gk = gk
+        self.dk = dk or gk
+        self.n = int(uvw.shape[0])
+        self.handle = _p()
+        check(lib.sdp_visplan_create(C.byref(self.handle), C.byref(geom), C.byref(self.gk), C.byref(self.dk),
+                                     _i(self.n), _dp(uvw), _i(mode), _stream(stream)), lib)
+
+    def close(self):
+        if self.handle:
+            check(self.lib.sdp_visplan_destroy(self.handle), self.lib)
+            self.handle = _p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def num_work_items(self) -> int:
+        c = _i(0)
+        check(self.lib.sdp_visplan_num_work_items(self.handle, C.byref(c)), self.lib)
+        return c.value
+
+    def set_measured(self, vis, stream=None):
+        check(self.lib.sdp_visplan_set_measured(self.handle, _dp(vis), _stream(stream)), self.lib)
+
+    def grid(self, vis, grid, accumulate=False, stream=None):
+        check(self.lib.sdp_visplan_grid(self.handle, _dp(vis), _dp(grid), _i(1 if accumulate else 0),
+                                        _stream(stream)), self.lib)
+
+    def degrid(self, model_grid, predicted, mode=SDP_DEGRID_CONV, stream=None):
+        check(self.lib.sdp_visplan_degrid(self.handle, _dp(model_grid), _dp(predicted), _i(mode), _stream(stream)),
+              self.lib)
+
+    def cycle(self, model_grid, residual_grid, mode=SDP_DEGRID_CONV, predicted=None, delta=None, stream=None):
+        check(self.lib.sdp_visplan_cycle(self.handle, _dp(model_grid), _i(mode), _dp(predicted), _dp(delta),
+                                         _dp(residual_grid), _stream(stream)), self.lib)
+
+    def g2g(self, in_grid, out_grid, stream=None):
+        check(self.lib.sdp_visplan_g2g(self.handle, _dp(in_grid), _dp(out_grid), _stream(stream)), self.lib)
+
+    def check_flags(self, stream=None):
+        check(self.lib.sdp_visplan_check(self.handle, _stream(stream)), self.lib)
+
+
+class Device:
+    """Device-resident layer over torch CUDA tensors."""
+
+    def __init__(self, lib: C.CDLL | None = None):
+        self.lib = lib or load()
+
+    @staticmethod
+    def wkernels(kernels, supports_dev, supports_host) -> WKernels:
+        sh = np.asarray(supports_host).reshape(-1, 2)
+        return WKernels(_dp(kernels), _dp(supports_dev), int(sh.shape[0]), int(kernels.shape[0]),
+                        int(sh[:, 0].max()))
+
+    def plan(self, grid_size, oversampling, uv_scale, w_scale, uvw, gk: WKernels, dk: WKernels | None = None,
+             mode=SDP_GRID_STD, stream=None, keep=()) -> VisPlan:
+        geom = Geometry(grid_size, oversampling, uv_scale, w_scale)
+        return VisPlan(self.lib, geom, gk, dk, uvw, mode, stream, keep)
+
+    def degrid_nearest(self, grid_size, uv_scale, uvw, grid, out, stream=None):
+        check(self.lib.sdp_degrid_nearest(_i(grid_size), _d(uv_scale), _i(uvw.shape[0]), _dp(uvw), _dp(grid),
+                                          _dp(out), _stream(stream)), self.lib)
+
+    def correct_to_finegrid(self, grid_size, oversampling, uv_scale, uvw, out, stream=None):
+        check(self.lib.sdp_correct_to_finegrid(_i(grid_size), _i(oversampling), _d(uv_scale), _i(uvw.shape[0]),
+                                               _dp(uvw), _dp(out), _stream(stream)), self.lib)
+
+    def subtract_vis(self, a, b, out, stream=None):
+        check(self.lib.sdp_subtract_vis(_i(a.shape[0]), _dp(a), _dp(b), _dp(out), _stream(stream)), self.lib)
+
+    def fft2d(self, grid_size, x, out, sign, stream=None):
+        check(self.lib.sdp_fft2d(_i(grid_size), _dp(x), _dp(out), _i(sign), _stream(stream)), self.lib)
+
+    def grid_to_image(self, grid_size, grid, prolate_ext, work, image, stream=None):
+        check(self.lib.sdp_grid_to_image(_i(grid_size), _dp(grid), _dp(prolate_ext), _dp(work), _dp(image),
+                                         _stream(stream)), self.lib)
+
+    def image_to_grid(self, grid_size, image, work, grid, stream=None):
+        check(self.lib.sdp_image_to_grid(_i(grid_size), _dp(image), _dp(work), _dp(grid), _stream(stream)),
+              self.lib)
+
+    def prolate_table(self, grid_size, out, stream=None):
+        check(self.lib.sdp_prolate_table(_i(grid_size), _dp(out), _stream(stream)), self.lib)
+
+    def dft(self, sources, uvw, vis, stream=None):
+        check(self.lib.sdp_dft(_i(uvw.shape[0]), _i(sources.shape[0]), _dp(sources), _dp(uvw), _dp(vis),
+                               _stream(stream)), self.lib)
+
+    def hogbom_workspace_bytes(self, grid_size) -> int:
+        b = _sz(0)
+        check(self.lib.sdp_hogbom_workspace_bytes(_i(grid_size), C.byref(b)), self.lib)
+        return b.value
+
+    def hogbom(self, params: CleanParams, residual, psf, model, sources, count, workspace, stream=None):
+        check(self.lib.sdp_hogbom(C.byref(params), _dp(residual), _dp(psf), _dp(model), _dp(sources), _dp(count),
+                                  _dp(workspace), _sz(workspace.numel() * workspace.element_size()),
+                                  _stream(stream)), self.lib)
