@@ -344,6 +344,21 @@ typedef struct sdp_clean_params {
 int sdp_hogbom_workspace_bytes(int grid_size, size_t *bytes);
 int sdp_hogbom(const sdp_clean_params *p, float *residual_inout, const float *psf, float *model_inout,
                sdp_float3 *sources, int *num_sources_dev, void *workspace, size_t workspace_bytes, void *stream);
+/* No counterpart in the reference.  sdp_hogbom for callers that cannot
+ * allocate device memory (a runtime that fixes all its memory before it
+ * starts, as the PREESM schedule does with its static arena, and must not
+ * call an allocator, which can block, while it runs; or a program whose
+ * device memory belongs to another allocator).  Same arguments and results
+ * as sdp_hogbom, without the workspace: the minor-cycle state and per-block
+ * partials live in one fixed 65,792-byte device array per GPU (held until
+ * the process exits), so grid_size is limited to 4096 (larger sizes return
+ * SDP_ERR_RANGE).  It calls no cudaMalloc/cudaFree.  The first call on a
+ * device looks up the array's device address (cudaGetSymbolAddress); make
+ * that first call before any stream capture.  Every call clears the state
+ * it needs; calls that overlap on the GPU share the array and race, so
+ * serialise them (one stream, or events). */
+int sdp_hogbom_noalloc(const sdp_clean_params *p, float *residual_inout, const float *psf, float *model_inout,
+                       sdp_float3 *sources, int *num_sources_dev, void *stream);
 
 #ifdef __cplusplus
 }

@@ -271,3 +271,90 @@ SDP_EXPORT int sdp_hogbom(const sdp_clean_params *p, float *residual, const floa
     SDP_LAUNCH_CHECK();
     return SDP_OK;
 }
+
+// ---------------------------------------------------------------------------
+// Hogbom CLEAN without any device allocation.
+//
+// For callers that cannot call cudaMalloc: a dataflow runtime that, like the
+// reference's PREESM schedule (one static arena, generated/Core0.c:19), fixes
+// all of its memory before the schedule starts and must not take an
+// allocator call (which can block and synchronise the device) in the middle
+// of it, or a host program whose device memory is owned by another allocator.
+// The caller still passes the residual, PSF, model and source buffers; the
+// minor-cycle state and the per-block partial results live in the fixed
+// array below, one per GPU, kept until the process exits.
+// ---------------------------------------------------------------------------
+#include <mutex>
+
+namespace sdp {
+
+constexpr int kNoAllocMaxGrid = 4096;  // grid_size limit of sdp_hogbom_noalloc
+constexpr size_t kNoAllocStateBytes = 256;
+// state + one (double sum, float max, int index) partial per image row
+constexpr size_t kNoAllocScratchBytes = kNoAllocStateBytes + 16 * (size_t)kNoAllocMaxGrid;  // 65,792 B
+
+static_assert(sizeof(CleanState) <= kNoAllocStateBytes, "CLEAN state must fit its slot");
+
+static __device__ __align__(256) unsigned char g_clean_scratch[kNoAllocScratchBytes];
+
+static std::mutex g_clean_scratch_mutex;
+static void *g_clean_scratch_addr[128];
+
+// Device address of g_clean_scratch on the current device, looked up once per
+// device (the host-side name of the array is not a device address).
+static int clean_scratch_address(void **out)
+{
+    int dev = 0;
+    SDP_CUDA_TRY(cudaGetDevice(&dev));
+    if (dev < 0 || dev >= 128) return set_error(SDP_ERR_RANGE, "device ordinal %d beyond 127", dev);
+    std::lock_guard<std::mutex> lock(g_clean_scratch_mutex);
+    if (g_clean_scratch_addr[dev] == nullptr) {
+        void *p = nullptr;
+        cudaError_t e = cudaGetSymbolAddress(&p, g_clean_scratch);
+        if (e != cudaSuccess) return cuda_error(e, "cudaGetSymbolAddress(g_clean_scratch)");
+        g_clean_scratch_addr[dev] = p;
+    }
+    *out = g_clean_scratch_addr[dev];
+    return SDP_OK;
+}
+
+}  // namespace sdp
+
+SDP_EXPORT int sdp_hogbom_noalloc(const sdp_clean_params *p, float *residual, const float *psf, float *model,
+                                  sdp_float3 *sources, int *num_sources_dev, void *stream)
+{
+    SDP_CHECK_ARG(p && residual && psf && model, "NULL argument");
+    SDP_CHECK_ARG(p->grid_size >= 2, "grid_size %d", p->grid_size);
+    if (p->grid_size > kNoAllocMaxGrid)
+        return set_error(SDP_ERR_RANGE,
+                         "sdp_hogbom_noalloc: grid_size %d exceeds its fixed scratch limit of %d; use sdp_hogbom",
+                         p->grid_size, kNoAllocMaxGrid);
+    SDP_CHECK_ARG(p->num_minor_cycles >= 0, "num_minor_cycles %d", p->num_minor_cycles);
+    SDP_CHECK_ARG(p->num_minor_cycles == 0 || sources, "sources is NULL");
+    SDP_CHECK_ARG(p->psf_max_value != 0.0, "psf_max_value is 0");
+    const int G = p->grid_size;
+    void *base = nullptr;
+    SDP_TRY(clean_scratch_address(&base));  // first call on a device: symbol lookup
+    char *w = static_cast<char *>(base);
+    const int nb = G;  // one partial per block, G blocks
+    CleanWs ws;
+    ws.st = reinterpret_cast<CleanState *>(w);
+    ws.psum = reinterpret_cast<double *>(w + kNoAllocStateBytes);
+    ws.pmax = reinterpret_cast<float *>(w + kNoAllocStateBytes + 8 * (size_t)nb);
+    ws.pidx = reinterpret_cast<int *>(w + kNoAllocStateBytes + 12 * (size_t)nb);
+    ws.nblocks = nb;
+    cudaStream_t st = as_stream(stream);
+    // every call starts from a cleared state (the array keeps the last call's contents)
+    SDP_CUDA_TRY(cudaMemsetAsync(ws.st, 0, sizeof(CleanState), st));
+    const int cap = std::max(0, std::min(p->num_minor_cycles, p->max_sources));
+    float3 *src = reinterpret_cast<float3 *>(sources);
+    for (int it = 0; it < p->num_minor_cycles; ++it) {
+        k_clean_step<<<nb, kCleanThreads, 0, st>>>(G, residual, psf, p->loop_gain, p->psf_max_value, ws, 1);
+        k_clean_select<<<1, 1024, 0, st>>>(G, cap, residual, model, src, p->loop_gain, p->noise_factor,
+                                          p->weak_source_percent, p->psf_max_value, ws);
+    }
+    k_clean_step<<<nb, kCleanThreads, 0, st>>>(G, residual, psf, p->loop_gain, p->psf_max_value, ws, 0);
+    k_clean_finish<<<1, 256, 0, st>>>(G, p->cell_size, cap, src, ws, num_sources_dev);
+    SDP_LAUNCH_CHECK();
+    return SDP_OK;
+}

@@ -504,6 +504,12 @@ class Device:
         check(self.lib.sdp_hogbom_workspace_bytes(_i(grid_size), C.byref(b)), self.lib)
         return b.value
 
+    def hogbom_noalloc(self, params: CleanParams, residual, psf, model, sources, count, stream=None):
+        """sdp_hogbom_noalloc: Hogbom with its scratch in a fixed device array
+        (no device allocation; grid_size <= 4096)."""
+        check(self.lib.sdp_hogbom_noalloc(C.byref(params), _dp(residual), _dp(psf), _dp(model), _dp(sources),
+                                          _dp(count), _stream(stream)), self.lib)
+
     def hogbom(self, params: CleanParams, residual, psf, model, sources, count, workspace, stream=None):
         check(self.lib.sdp_hogbom(C.byref(params), _dp(residual), _dp(psf), _dp(model), _dp(sources), _dp(count),
                                   _dp(workspace), _sz(workspace.numel() * workspace.element_size()),
