@@ -30,6 +30,11 @@ struct sdp_visplan {
     int *item_counter = nullptr;  // device scalar
     int *flags = nullptr;         // device scalar
     float2 *measured = nullptr;   // plan order
+    int phase_major = 0;          // kernel tables copied phase-major (OS a power of two)
+    int *gpoff = nullptr;         // plane offsets into the gridding table in use
+    int *dpoff = nullptr;         // plane offsets into the degridding table in use
+    float2 *gk2 = nullptr;        // phase-major gridding kernels
+    float2 *dk2 = nullptr;        // phase-major degridding kernels
     void *arena = nullptr;
     bool owns_arena = true;
 };

@@ -33,7 +33,6 @@ namespace sdp {
 
 constexpr int kTile = 32;
 constexpr int kChunk = 1024;
-constexpr int kWarps = 4;          // warps per CTA of the tile kernels
 constexpr int kMaxHalfSupport = 15;
 
 enum : int {
@@ -49,13 +48,16 @@ enum : int { FLAG_PLANE = 1, FLAG_SUPPORT = 2, FLAG_BOX = 4 };
 
 struct PlanDev {
     int G, gc, OS, nk_g, nk_d, ntx, nty, W, S;
+    int phase_major, os_mask, os_shift;
     double uv_scale, w_scale;
-    const float2 *gk;  // gridding kernels
-    const int2 *gs;    // gridding supports
-    const float2 *dk;  // degridding kernels
-    const int2 *ds;    // degridding supports
-    const VisRec *rec; // plan order
-    const int4 *items; // (tile, begin, end, -)
+    const float2 *gk;   // gridding kernels (phase-major copy when phase_major)
+    const int2 *gs;     // gridding supports (hs used; offsets superseded by gpoff)
+    const int *gpoff;   // gridding plane offsets into gk
+    const float2 *dk;   // degridding kernels
+    const int2 *ds;     // degridding supports
+    const int *dpoff;   // degridding plane offsets into dk
+    const VisRec *rec;  // plan order
+    const int4 *items;  // (tile, begin, end, -)
     const int *n_items;
     int *item_counter;
     int *flags;
@@ -266,24 +268,60 @@ __device__ __forceinline__ int mirror(int v, int gc)
     return v;
 }
 
-template <int GMODE, int OP>
-__global__ void __launch_bounds__(kWarps * 32) k_tiles(PlanDev P, const float2 *__restrict__ vis_in,
-                                                      const float2 *__restrict__ in_grid,
-                                                      float2 *__restrict__ out_grid, float2 *__restrict__ pred_out,
-                                                      float2 *__restrict__ delta_out,
-                                                      const float2 *__restrict__ measured)
+// Kernel-table address of sample (ky, kx) of a plane.  The plan re-lays the
+// tables out phase-major (k_relayout): with A = hs + 1 and OS a power of
+// two, sample (ky, kx) is stored at
+//   poff + ((ky % OS) * OS + kx % OS) * A^2 + (ky / OS) * A + kx / OS,
+// so the taps of one visibility (a fixed sub-sample phase per axis, or its
+// mirror) read a few short contiguous runs instead of one 32-byte sector per
+// tap.  For other OS the plan keeps the reference layout ky * A * OS + kx.
+__device__ __forceinline__ int kcol(const PlanDev &P, int A, int kx)
 {
-    extern __shared__ float2 smem[];
+    return P.phase_major ? ((kx & P.os_mask) * A * A + (kx >> P.os_shift)) : kx;
+}
+
+__device__ __forceinline__ int krow(const PlanDev &P, int A, int ky)
+{
+    return P.phase_major ? ((ky & P.os_mask) * P.OS * A * A + (ky >> P.os_shift) * A) : ky * A * P.OS;
+}
+
+constexpr int kThreads = 256;  // 8 warps per CTA of the tile kernels
+
+// One CTA per work item (persistent, items pulled from an atomic queue).
+// LG lanes serve one visibility, so a warp works on 32 / LG visibilities at
+// once.  Shared memory holds the input-grid tile (degridding, nearest cell)
+// and the output subgrid as separate real / imaginary planes, both
+// (32 + 2 hs_max)^2.
+//
+// Fast path (a visibility whose tap box lies inside the grid and the tile,
+// with at most LG taps per axis and one support for both directions): lane
+// c of the group owns tap column c and also computes the kernel-row offset
+// and subgrid row of tap row c; a tap-row loop then broadcasts the row
+// information with one shuffle per row, so each tap costs a kernel load, a
+// shared load or two shared atomics and the multiply-adds.  Every other
+// visibility (grid edges, where the reference mirrors or skips taps, 2 hs + 1
+// taps, differing supports) takes the general path, which evaluates the
+// reference's index arithmetic tap by tap.
+template <int GMODE, int OP, int LG>
+__global__ void __launch_bounds__(kThreads) k_tiles(PlanDev P, const float2 *__restrict__ vis_in,
+                                                   const float2 *__restrict__ in_grid,
+                                                   float2 *__restrict__ out_grid, float2 *__restrict__ pred_out,
+                                                   float2 *__restrict__ delta_out,
+                                                   const float2 *__restrict__ measured)
+{
+    extern __shared__ float smem_f[];
     constexpr bool kGrids = (OP != OP_DEGRID);
+    constexpr bool kConv = (OP == OP_DEGRID || OP == OP_CYCLE_CONV);
+    constexpr bool kStageIn = (OP != OP_GRID);
+    constexpr int VPW = 32 / LG;
+    const int S = P.S, SS = S * S;
+    float2 *mtile = reinterpret_cast<float2 *>(smem_f);
+    float *sub_re = smem_f + (kStageIn ? 2 * SS : 0);
+    float *sub_im = sub_re + SS;
     const int lane = threadIdx.x & 31;
     const int warp = threadIdx.x >> 5;
-    const int W = P.W, S = P.S, SS = S * S;
-    float2 *sub = smem + (size_t)warp * SS;
-    // lane -> (column, row phase) of the W x W tap box
-    const int R = 32 / W;  // rows handled in parallel
-    const int col = lane % W;
-    const int row0 = lane / W;
-    const bool lane_active = row0 < R;
+    const int grp = lane / LG;
+    const int cl = lane % LG;
     const float fos = (float)P.OS;
     __shared__ int s_item;
 
@@ -293,148 +331,275 @@ __global__ void __launch_bounds__(kWarps * 32) k_tiles(PlanDev P, const float2 *
         const int item = s_item;
         if (item >= *P.n_items) break;
         const int4 it = P.items[item];
-        const int tile = it.x;
-        const int ox = (tile % P.ntx) * kTile;  // subgrid origin in grid cells
-        const int oy = (tile / P.ntx) * kTile;
-        if (kGrids) {
-            for (int k = lane; k < SS; k += 32) sub[k] = make_float2(0.f, 0.f);
-            __syncwarp();
-        }
-        // contiguous slice of the item per warp (keeps w-plane runs together)
-        const int len = it.z - it.y;
-        const int per = (len + kWarps - 1) / kWarps;
-        const int b = it.y + warp * per;
-        const int e = min(it.z, b + per);
-        for (int r = b; r < e; ++r) {
-            const VisRec rec = P.rec[r];
+        const int ox = (it.x % P.ntx) * kTile;  // tile origin in grid cells
+        const int oy = (it.x / P.ntx) * kTile;
+        if (kGrids)
+            for (int k = threadIdx.x; k < 2 * SS; k += kThreads) sub_re[k] = 0.f;
+        if (kStageIn)
+            for (int k = threadIdx.x; k < SS; k += kThreads) {
+                const int gy = oy + k / S, gx = ox + k % S;
+                mtile[k] = (gx < P.G && gy < P.G) ? __ldg(&in_grid[(size_t)gy * P.G + gx]) : make_float2(0.f, 0.f);
+            }
+        __syncthreads();
+
+        for (int base = it.y + warp * VPW; base < it.z; base += (kThreads / 32) * VPW) {
+            const int r = base + grp;
+            const bool valid = r < it.z;
+            VisRec rec;
+            if (valid) {
+                rec = P.rec[r];
+            } else {
+                rec.px = 0.f;
+                rec.py = 0.f;
+                rec.meta = 0;
+                rec.idx = 0;
+            }
             const int plane = rec.meta & 0xffff;
             const float conj = (rec.meta < 0) ? -1.f : 1.f;
 
+            // ---------------- tap geometry and the fast-path test ----------------
+            const int hs_d = kConv ? P.ds[plane].x : 0;
+            const int hs_g = kGrids ? P.gs[plane].x : 0;
+            const int hs = kGrids ? hs_g : hs_d;
+            const float lox = ceilf(__fsub_rn(rec.px, (float)hs));
+            const float loy = ceilf(__fsub_rn(rec.py, (float)hs));
+            int ncols, nrows;
+            if (GMODE == SDP_GRID_SNAPPED) {  // gridding_run.c:84-112: inclusive floor bound
+                ncols = (int)(floorf(__fadd_rn(rec.px, (float)hs)) - lox) + 1;
+                nrows = (int)(floorf(__fadd_rn(rec.py, (float)hs)) - loy) + 1;
+            } else {  // degridgrid.c:93, 103
+                ncols = (int)(ceilf(__fadd_rn(rec.px, (float)hs)) - lox);
+                nrows = (int)(ceilf(__fadd_rn(rec.py, (float)hs)) - loy);
+            }
+            const int ix0 = (int)lox + P.gc, iy0 = (int)loy + P.gc;  // grid index of the first tap
+            const int tx0 = ix0 - ox, ty0 = iy0 - oy;                // ... and in the tile
+            const bool fast = valid && (!(kConv && kGrids) || hs_d == hs_g) && ncols <= LG && nrows <= LG &&
+                              ix0 >= 0 && iy0 >= 0 && ix0 + ncols <= P.G && iy0 + nrows <= P.G && tx0 >= 0 &&
+                              ty0 >= 0 && tx0 + ncols <= S && ty0 + nrows <= S;
+            const unsigned fmask = __ballot_sync(0xffffffffu, fast);
+            int colp_d = 0, colp_g = 0, lx = 0, rowpack = 0;
+            bool colok = false;
+            if (fast) {
+                const int A = hs + 1;
+                colok = cl < ncols;
+                const int kc = kcol(P, A, ref_kidx((int)lox + cl, rec.px, fos));
+                if (kConv) colp_d = P.dpoff[plane] + kc;
+                if (kGrids) colp_g = P.gpoff[plane] + kc;
+                lx = tx0 + cl;
+                // row cl of the box: kernel-row offset and tile row, packed
+                rowpack = (krow(P, A, ref_kidx((int)loy + cl, rec.py, fos)) << 6) | (ty0 + cl);
+            }
+
             // ---------------- degrid (prediction) ----------------
             float2 value = make_float2(0.f, 0.f);
-            if (OP == OP_DEGRID || OP == OP_CYCLE_CONV) {
-                const int2 sp = P.ds[plane];
-                const int hs = sp.x;
-                const int stride = (hs + 1) * P.OS;
-                const float lox = ceilf(__fsub_rn(rec.px, (float)hs));
-                const float hix = ceilf(__fadd_rn(rec.px, (float)hs));
-                const float loy = ceilf(__fsub_rn(rec.py, (float)hs));
-                const float hiy = ceilf(__fadd_rn(rec.py, (float)hs));
-                float2 acc = make_float2(0.f, 0.f);
+            if (kConv) {
+                // sum gv * Re(k) and gv * Im(k) separately; the conjugation of
+                // k for w < 0 (degridgrid.c:143, 175) is applied after the sum
+                float2 a1 = make_float2(0.f, 0.f), a2 = make_float2(0.f, 0.f);
                 float nrm = 0.f;
-                const int u = (int)lox + col;
-                if (lane_active && (float)u < hix) {
-                    const int cu = mirror(u, P.gc);
-                    const int kx = ref_kidx(cu, rec.px, fos);
-                    for (int rr = row0; rr < W; rr += R) {
-                        const int v = (int)loy + rr;
-                        if (!((float)v < hiy)) break;
-                        const int cv = mirror(v, P.gc);
-                        const int ky = ref_kidx(cv, rec.py, fos);
-                        float2 ks = make_float2(0.f, 0.f);
-                        if (kx < stride && ky < stride) ks = __ldg(&P.dk[sp.y + ky * stride + kx]);
-                        ks.y *= conj;
-                        float2 gv = make_float2(0.f, 0.f);
-                        const int gx = cu + P.gc, gy = cv + P.gc;
-                        if (gx >= 0 && gy >= 0 && gx < P.G && gy < P.G) gv = __ldg(&in_grid[(size_t)gy * P.G + gx]);
-                        cmac(acc, gv, ks);
-                        nrm = fmaf(ks.x, ks.x, fmaf(ks.y, ks.y, nrm));
+                if (fast) {
+#pragma unroll
+                    for (int rr = 0; rr < LG; ++rr) {
+                        const int pk = __shfl_sync(fmask, rowpack, grp * LG + rr);
+                        if (rr < nrows && colok) {
+                            const float2 ks = __ldg(&P.dk[colp_d + (pk >> 6)]);
+                            const float2 gv = mtile[(pk & 63) * S + lx];
+                            a1.x = fmaf(gv.x, ks.x, a1.x);
+                            a1.y = fmaf(gv.y, ks.x, a1.y);
+                            a2.x = fmaf(gv.x, ks.y, a2.x);
+                            a2.y = fmaf(gv.y, ks.y, a2.y);
+                            nrm = fmaf(ks.x, ks.x, fmaf(ks.y, ks.y, nrm));
+                        }
+                    }
+                } else if (valid) {
+                    // general path: degridgrid.c:147-186 tap by tap, edges mirrored
+                    const int A = hs_d + 1, stride = A * P.OS;
+                    const float dlox = ceilf(__fsub_rn(rec.px, (float)hs_d));
+                    const float dloy = ceilf(__fsub_rn(rec.py, (float)hs_d));
+                    const int dnc = (int)(ceilf(__fadd_rn(rec.px, (float)hs_d)) - dlox);
+                    const int dnr = (int)(ceilf(__fadd_rn(rec.py, (float)hs_d)) - dloy);
+                    const int off = P.dpoff[plane];
+                    for (int c = cl; c < dnc; c += LG) {
+                        const int cu = mirror((int)dlox + c, P.gc);
+                        const int kx = ref_kidx(cu, rec.px, fos);
+                        const bool kx_ok = kx < stride;
+                        const int colp = off + kcol(P, A, kx);
+                        const int gx = cu + P.gc;
+                        const int tx = gx - ox;
+                        for (int rr = 0; rr < dnr; ++rr) {
+                            const int cv = mirror((int)dloy + rr, P.gc);
+                            const int ky = ref_kidx(cv, rec.py, fos);
+                            float2 ks = make_float2(0.f, 0.f);
+                            if (kx_ok && ky < stride) ks = __ldg(&P.dk[colp + krow(P, A, ky)]);
+                            const int gy = cv + P.gc;
+                            const int ty = gy - oy;
+                            float2 gv;
+                            if ((unsigned)tx < (unsigned)S && (unsigned)ty < (unsigned)S) {
+                                gv = mtile[ty * S + tx];
+                            } else if (gx >= 0 && gy >= 0 && gx < P.G && gy < P.G) {
+                                gv = __ldg(&in_grid[(size_t)gy * P.G + gx]);
+                            } else {
+                                gv = make_float2(0.f, 0.f);
+                            }
+                            a1.x = fmaf(gv.x, ks.x, a1.x);
+                            a1.y = fmaf(gv.y, ks.x, a1.y);
+                            a2.x = fmaf(gv.x, ks.y, a2.x);
+                            a2.y = fmaf(gv.y, ks.y, a2.y);
+                            nrm = fmaf(ks.x, ks.x, fmaf(ks.y, ks.y, nrm));
+                        }
                     }
                 }
 #pragma unroll
-                for (int o = 16; o > 0; o >>= 1) {
-                    acc.x += __shfl_xor_sync(0xffffffffu, acc.x, o);
-                    acc.y += __shfl_xor_sync(0xffffffffu, acc.y, o);
+                for (int o = LG / 2; o > 0; o >>= 1) {
+                    a1.x += __shfl_xor_sync(0xffffffffu, a1.x, o);
+                    a1.y += __shfl_xor_sync(0xffffffffu, a1.y, o);
+                    a2.x += __shfl_xor_sync(0xffffffffu, a2.x, o);
+                    a2.y += __shfl_xor_sync(0xffffffffu, a2.y, o);
                     nrm += __shfl_xor_sync(0xffffffffu, nrm, o);
                 }
-                // degridgrid.c:188-191 (the .y fallback uses the new .x)
+                // gv * (kr + i conj ki) summed; then degridgrid.c:188-191
+                // (the .y fallback uses the new .x)
+                const float sx = fmaf(-conj, a2.y, a1.x);
+                const float sy = fmaf(conj, a2.x, a1.y);
                 const float cn = __fsqrt_rn(nrm);
-                const float nx = (cn < 1e-5f) ? __fdiv_rn(acc.x, 1e-5f) : __fdiv_rn(acc.x, cn);
-                const float ny = (cn < 1e-5f) ? __fdiv_rn(nx, 1e-5f) : __fdiv_rn(acc.y, cn);
+                const float nx = (cn < 1e-5f) ? __fdiv_rn(sx, 1e-5f) : __fdiv_rn(sx, cn);
+                const float ny = (cn < 1e-5f) ? __fdiv_rn(nx, 1e-5f) : __fdiv_rn(sy, cn);
                 value = make_float2(nx, ny);
             } else if (OP == OP_CYCLE_NEAR || OP == OP_G2G) {
                 // degridgrid.c:194-200 / :273-285
                 const int x = ref_nearest(rec.px, P.gc), y = ref_nearest(rec.py, P.gc);
-                const long long gi = (long long)x + (long long)y * P.G;
-                if (gi >= 0 && gi < (long long)P.G * P.G) value = __ldg(&in_grid[gi]);
+                const int tx = x - ox, ty = y - oy;
+                if ((unsigned)tx < (unsigned)S && (unsigned)ty < (unsigned)S && x < P.G && y < P.G) {
+                    value = mtile[ty * S + tx];
+                } else {
+                    const long long gi = (long long)x + (long long)y * P.G;
+                    if (gi >= 0 && gi < (long long)P.G * P.G) value = __ldg(&in_grid[gi]);
+                }
             }
 
-            float2 gval;
+            float2 gval = make_float2(0.f, 0.f);
             if (OP == OP_GRID) {
-                gval = __ldg(&vis_in[rec.idx]);
+                if (valid) gval = __ldg(&vis_in[rec.idx]);
             } else if (OP == OP_G2G) {
                 gval = value;
             } else if (OP == OP_CYCLE_CONV || OP == OP_CYCLE_NEAR) {
-                const float2 m = measured[r];
-                gval = make_float2(__fsub_rn(m.x, value.x), __fsub_rn(m.y, value.y));
-                if (lane == 0) {
-                    if (pred_out) pred_out[rec.idx] = value;
-                    if (delta_out) delta_out[rec.idx] = gval;
+                if (valid) {
+                    const float2 m = measured[r];
+                    gval = make_float2(__fsub_rn(m.x, value.x), __fsub_rn(m.y, value.y));
+                    if (cl == 0) {
+                        if (pred_out) pred_out[rec.idx] = value;
+                        if (delta_out) delta_out[rec.idx] = gval;
+                    }
                 }
             } else {  // OP_DEGRID
-                if (lane == 0) pred_out[rec.idx] = value;
+                if (valid && cl == 0) pred_out[rec.idx] = value;
             }
 
             // ---------------- grid ----------------
             if (kGrids) {
-                const int2 sp = P.gs[plane];
-                const int hs = sp.x;
-                const int stride = (hs + 1) * P.OS;
-                const float lox = ceilf(__fsub_rn(rec.px, (float)hs));
-                const float loy = ceilf(__fsub_rn(rec.py, (float)hs));
-                float hix, hiy;
-                if (GMODE == SDP_GRID_SNAPPED) {  // inclusive floor bound
-                    hix = floorf(__fadd_rn(rec.px, (float)hs)) + 0.5f;
-                    hiy = floorf(__fadd_rn(rec.py, (float)hs)) + 0.5f;
-                } else {
-                    hix = ceilf(__fadd_rn(rec.px, (float)hs));
-                    hiy = ceilf(__fadd_rn(rec.py, (float)hs));
-                }
-                const int u = (int)lox + col;
-                const int gx = u + P.gc;
-                if (lane_active && (float)u < hix && gx >= 0 && gx < P.G) {
-                    const int kx = ref_kidx(u, rec.px, fos);
-                    const int lx = gx - ox;
-                    for (int rr = row0; rr < W; rr += R) {
-                        const int v = (int)loy + rr;
-                        if (!((float)v < hiy)) break;
-                        const int gy = v + P.gc;
-                        if (gy < 0 || gy >= P.G) continue;
-                        const int ky = ref_kidx(v, rec.py, fos);
-                        float2 ks = __ldg(&P.gk[sp.y + ky * stride + kx]);
-                        ks.y *= conj;
-                        float2 &cell = sub[(gy - oy) * S + lx];
-                        float2 acc = cell;
-                        cmac(acc, gval, ks);
-                        cell = acc;
+                // vis * (kr + i conj ki): re = vr kr - (conj vi) ki, im = vi kr + (conj vr) ki
+                const float ca = conj * gval.y, cb = conj * gval.x;
+                if (fast) {
+#pragma unroll
+                    for (int rr = 0; rr < LG; ++rr) {
+                        const int pk = __shfl_sync(fmask, rowpack, grp * LG + rr);
+                        if (rr < nrows && colok) {
+                            const float2 ks = __ldg(&P.gk[colp_g + (pk >> 6)]);
+                            const int cell = (pk & 63) * S + lx;
+                            atomicAdd(sub_re + cell, fmaf(-ca, ks.y, gval.x * ks.x));
+                            atomicAdd(sub_im + cell, fmaf(cb, ks.y, gval.y * ks.x));
+                        }
+                    }
+                } else if (valid) {
+                    // general path: degridgrid.c:93-122 / gridding_run.c:104-132 tap by tap
+                    const int A = hs_g + 1, stride = A * P.OS;
+                    const int off = P.gpoff[plane];
+                    for (int c = cl; c < ncols; c += LG) {
+                        const int u = (int)lox + c;
+                        const int gx = u + P.gc;
+                        if (gx < 0 || gx >= P.G) continue;
+                        const int tx = gx - ox;
+                        const int kx = ref_kidx(u, rec.px, fos);
+                        if (kx >= stride || (unsigned)tx >= (unsigned)S) {  // cannot happen for a valid plan
+                            atomicOr(P.flags, FLAG_BOX);
+                            continue;
+                        }
+                        const int colp = off + kcol(P, A, kx);
+                        for (int rr = 0; rr < nrows; ++rr) {
+                            const int v = (int)loy + rr;
+                            const int gy = v + P.gc;
+                            if (gy < 0 || gy >= P.G) continue;
+                            const int ty = gy - oy;
+                            const int ky = ref_kidx(v, rec.py, fos);
+                            if (ky >= stride || (unsigned)ty >= (unsigned)S) {
+                                atomicOr(P.flags, FLAG_BOX);
+                                continue;
+                            }
+                            const float2 ks = __ldg(&P.gk[colp + krow(P, A, ky)]);
+                            const int cell = ty * S + tx;
+                            atomicAdd(sub_re + cell, fmaf(-ca, ks.y, gval.x * ks.x));
+                            atomicAdd(sub_im + cell, fmaf(cb, ks.y, gval.y * ks.x));
+                        }
                     }
                 }
-                if (lane == 0) {
-                    // a box wider than W would lose taps: flag it
-                    if ((float)((int)lox + W) < hix || (float)((int)loy + W) < hiy) atomicOr(P.flags, FLAG_BOX);
-                }
-                __syncwarp();
             }
         }
         if (kGrids) {
             __syncthreads();
-            // flush: sum the warps' subgrids, one vector atomic per touched cell
-            for (int k = threadIdx.x; k < SS; k += blockDim.x) {
-                float2 s = smem[k];
-#pragma unroll
-                for (int w = 1; w < kWarps; ++w) {
-                    float2 t = smem[(size_t)w * SS + k];
-                    s.x += t.x;
-                    s.y += t.y;
-                }
-                if (s.x != 0.f || s.y != 0.f) {
+            // flush: one vector atomic per touched cell of the subgrid
+            for (int k = threadIdx.x; k < SS; k += kThreads) {
+                const float2 v = make_float2(sub_re[k], sub_im[k]);
+                if (v.x != 0.f || v.y != 0.f) {
                     const int gy = oy + k / S, gx = ox + k % S;
-                    if (gx < P.G && gy < P.G) atomicAdd(&out_grid[(size_t)gy * P.G + gx], s);
+                    if (gx < P.G && gy < P.G) atomicAdd(&out_grid[(size_t)gy * P.G + gx], v);
                 }
             }
         }
         __syncthreads();
     }
+}
+
+// Phase-major copy of a kernel set (see kcol / krow).  One thread per output
+// sample; plane p of the source starts at supports[p].y, of the copy at
+// poff[p] (planes packed back to back).
+__global__ void k_relayout(const float2 *__restrict__ src, long long src_total, const int2 *__restrict__ sup,
+                           const int *__restrict__ poff, int nk, int OS, int os_shift, int max_per_plane,
+                           float2 *__restrict__ dst)
+{
+    const int p = blockIdx.y;
+    if (p >= nk) return;
+    const int hs = sup[p].x;
+    if (hs < 0) return;
+    const int A = hs + 1, stride = A * OS;
+    // planes wider than the plan's maximum are never addressed (binning flags them)
+    const int n = stride * stride;
+    if (n > max_per_plane) return;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        const int ky = i / stride, kx = i % stride;
+        const long long si = (long long)sup[p].y + i;
+        const float2 v = (sup[p].y >= 0 && si < src_total) ? src[si] : make_float2(0.f, 0.f);
+        const int di = ((ky & (OS - 1)) * OS + (kx & (OS - 1))) * A * A + (ky >> os_shift) * A + (kx >> os_shift);
+        dst[poff[p] + di] = v;
+    }
+}
+
+// Packed plane offsets of the copy (one thread; nk is small).  A plane wider
+// than hs_max takes no room: binning never lets a visibility use it.
+__global__ void k_plane_offsets(const int2 *__restrict__ sup, int nk, int OS, int hs_max, int *__restrict__ poff)
+{
+    if (threadIdx.x != 0 || blockIdx.x != 0) return;
+    int o = 0;
+    for (int p = 0; p < nk; ++p) {
+        poff[p] = o;
+        const int hs = sup[p].x;
+        if (hs >= 0 && hs <= hs_max) o += (hs + 1) * OS * (hs + 1) * OS;
+    }
+}
+
+// Identity offsets (reference layout kept): poff[p] = supports[p].y.
+__global__ void k_plane_offsets_identity(const int2 *__restrict__ sup, int nk, int *__restrict__ poff)
+{
+    for (int p = blockIdx.x * blockDim.x + threadIdx.x; p < nk; p += gridDim.x * blockDim.x) poff[p] = sup[p].y;
 }
 
 __global__ void k_gather_sorted(const float2 *__restrict__ src, const int *__restrict__ perm, int n,
@@ -471,10 +636,16 @@ static PlanDev plan_dev(const sdp_visplan *p)
     d.S = p->S;
     d.uv_scale = p->geom.uv_scale;
     d.w_scale = p->geom.w_scale;
-    d.gk = reinterpret_cast<const float2 *>(p->gk.kernels);
+    d.phase_major = p->phase_major;
+    d.os_mask = p->geom.oversampling - 1;
+    d.os_shift = 0;
+    while ((1 << d.os_shift) < p->geom.oversampling) ++d.os_shift;
+    d.gk = p->phase_major ? p->gk2 : reinterpret_cast<const float2 *>(p->gk.kernels);
     d.gs = reinterpret_cast<const int2 *>(p->gk.supports);
-    d.dk = reinterpret_cast<const float2 *>(p->dk.kernels);
+    d.gpoff = p->gpoff;
+    d.dk = p->phase_major ? p->dk2 : reinterpret_cast<const float2 *>(p->dk.kernels);
     d.ds = reinterpret_cast<const int2 *>(p->dk.supports);
+    d.dpoff = p->dpoff;
     d.rec = p->rec;
     d.items = p->items;
     d.n_items = p->n_items;
@@ -520,6 +691,11 @@ static void plan_layout(const sdp_visplan *p, size_t *off, size_t *total)
     off[9] = o; o = align_up(o + sizeof(int) * nb_scan, 256);                             // scan scratch
     off[10] = o; o = align_up(o + sizeof(int) * 4, 256);                                  // scalars
     off[11] = o; o = align_up(o + sizeof(float2) * (size_t)std::max(n, 1), 256);          // measured
+    off[12] = o; o = align_up(o + sizeof(int) * (size_t)p->gk.num_kernels, 256);          // gpoff
+    off[13] = o; o = align_up(o + sizeof(int) * (size_t)p->dk.num_kernels, 256);          // dpoff
+    const size_t per = (size_t)(p->hs_max + 1) * p->geom.oversampling * (p->hs_max + 1) * p->geom.oversampling;
+    off[14] = o; o = align_up(o + (p->phase_major ? sizeof(float2) * per * p->gk.num_kernels : 0), 256);  // gk2
+    off[15] = o; o = align_up(o + (p->phase_major ? sizeof(float2) * per * p->dk.num_kernels : 0), 256);  // dk2
     *total = o;
 }
 
@@ -546,19 +722,21 @@ int visplan_setup(sdp_visplan *p, const sdp_geometry *geom, const sdp_wkernels *
     p->hs_max = std::max(gk->max_half_support, dk->max_half_support);
     p->W = 2 * p->hs_max + 1;
     p->S = kTile + 2 * p->hs_max;
+    const int os = geom->oversampling;
+    p->phase_major = (os & (os - 1)) == 0 ? 1 : 0;
     return SDP_OK;
 }
 
 size_t visplan_arena_bytes(const sdp_visplan *p)
 {
-    size_t off[12], total;
+    size_t off[16], total;
     plan_layout(p, off, &total);
     return total;
 }
 
 int visplan_build(sdp_visplan *p, void *arena, const float3 *uvw, cudaStream_t st)
 {
-    size_t off[12], total;
+    size_t off[16], total;
     plan_layout(p, off, &total);
     char *a = static_cast<char *>(arena);
     p->arena = arena;
@@ -577,7 +755,36 @@ int visplan_build(sdp_visplan *p, void *arena, const float3 *uvw, cudaStream_t s
     p->item_counter = scalars + 1;
     p->flags = scalars + 2;
     p->measured = reinterpret_cast<float2 *>(a + off[11]);
+    p->gpoff = reinterpret_cast<int *>(a + off[12]);
+    p->dpoff = reinterpret_cast<int *>(a + off[13]);
+    p->gk2 = reinterpret_cast<float2 *>(a + off[14]);
+    p->dk2 = reinterpret_cast<float2 *>(a + off[15]);
     const int n = p->n;
+
+    // kernel tables: phase-major copies (or the caller's tables as they are)
+    {
+        const int os = p->geom.oversampling;
+        int os_shift = 0;
+        while ((1 << os_shift) < os) ++os_shift;
+        const int per = (p->hs_max + 1) * os * (p->hs_max + 1) * os;
+        const sdp_wkernels *sets[2] = {&p->gk, &p->dk};
+        int *poffs[2] = {p->gpoff, p->dpoff};
+        float2 *dsts[2] = {p->gk2, p->dk2};
+        for (int t = 0; t < 2; ++t) {
+            const int2 *sup = reinterpret_cast<const int2 *>(sets[t]->supports);
+            const int nk = sets[t]->num_kernels;
+            if (p->phase_major) {
+                k_plane_offsets<<<1, 32, 0, st>>>(sup, nk, os, p->hs_max, poffs[t]);
+                dim3 grid((per + 255) / 256, nk);
+                k_relayout<<<grid, 256, 0, st>>>(reinterpret_cast<const float2 *>(sets[t]->kernels),
+                                                 (long long)sets[t]->total_samples, sup, poffs[t], nk, os, os_shift,
+                                                 per, dsts[t]);
+            } else {
+                k_plane_offsets_identity<<<(nk + 255) / 256, 256, 0, st>>>(sup, nk, poffs[t]);
+            }
+            SDP_LAUNCH_CHECK();
+        }
+    }
 
     SDP_CUDA_TRY(cudaMemsetAsync(counts, 0, sizeof(int) * ((size_t)p->nbins + 1), st));
     SDP_CUDA_TRY(cudaMemsetAsync(scalars, 0, sizeof(int) * 4, st));
@@ -689,30 +896,40 @@ SDP_EXPORT int sdp_visplan_set_measured(sdp_visplan *p, const sdp_float2 *measur
 
 namespace sdp {
 
-static int launch_tiles(sdp_visplan *p, int op, const float2 *vis_in, const float2 *in_grid, float2 *out_grid,
-                        float2 *pred, float2 *delta, cudaStream_t st)
+template <int LG>
+static int launch_tiles_lg(sdp_visplan *p, int op, const float2 *vis_in, const float2 *in_grid, float2 *out_grid,
+                           float2 *pred, float2 *delta, cudaStream_t st)
 {
     PlanDev d = plan_dev(p);
-    const size_t smem = (op == OP_DEGRID) ? 0 : sizeof(float2) * (size_t)kWarps * p->S * p->S;
-    SDP_CUDA_TRY(cudaMemsetAsync(p->item_counter, 0, sizeof(int), st));
+    const size_t SS = (size_t)p->S * p->S;
+    const size_t smem = sizeof(float2) * SS * ((op != OP_GRID ? 1 : 0) + (op != OP_DEGRID ? 1 : 0));
     void (*fn)(PlanDev, const float2 *, const float2 *, float2 *, float2 *, float2 *, const float2 *) = nullptr;
     const bool snapped = (p->mode == SDP_GRID_SNAPPED);
     switch (op) {
-    case OP_GRID: fn = snapped ? k_tiles<SDP_GRID_SNAPPED, OP_GRID> : k_tiles<SDP_GRID_STD, OP_GRID>; break;
-    case OP_DEGRID: fn = k_tiles<SDP_GRID_STD, OP_DEGRID>; break;
-    case OP_CYCLE_CONV: fn = k_tiles<SDP_GRID_STD, OP_CYCLE_CONV>; break;
-    case OP_CYCLE_NEAR: fn = k_tiles<SDP_GRID_STD, OP_CYCLE_NEAR>; break;
-    case OP_G2G: fn = k_tiles<SDP_GRID_STD, OP_G2G>; break;
+    case OP_GRID: fn = snapped ? k_tiles<SDP_GRID_SNAPPED, OP_GRID, LG> : k_tiles<SDP_GRID_STD, OP_GRID, LG>; break;
+    case OP_DEGRID: fn = k_tiles<SDP_GRID_STD, OP_DEGRID, LG>; break;
+    case OP_CYCLE_CONV: fn = k_tiles<SDP_GRID_STD, OP_CYCLE_CONV, LG>; break;
+    case OP_CYCLE_NEAR: fn = k_tiles<SDP_GRID_STD, OP_CYCLE_NEAR, LG>; break;
+    case OP_G2G: fn = k_tiles<SDP_GRID_STD, OP_G2G, LG>; break;
     default: return set_error(SDP_ERR_INVALID, "internal: op %d", op);
     }
     if (smem > 48 * 1024) SDP_CUDA_TRY(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     int per_sm = 0;
-    SDP_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, kWarps * 32, smem));
+    SDP_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, kThreads, smem));
     if (per_sm < 1) return set_error(SDP_ERR_RANGE, "tile kernel does not fit (%zu B shared memory)", smem);
-    const int grid = per_sm * num_sms();
-    fn<<<grid, kWarps * 32, smem, st>>>(d, vis_in, in_grid, out_grid, pred, delta, p->measured);
+    SDP_CUDA_TRY(cudaMemsetAsync(p->item_counter, 0, sizeof(int), st));
+    fn<<<per_sm * num_sms(), kThreads, smem, st>>>(d, vis_in, in_grid, out_grid, pred, delta, p->measured);
     SDP_LAUNCH_CHECK();
     return SDP_OK;
+}
+
+static int launch_tiles(sdp_visplan *p, int op, const float2 *vis_in, const float2 *in_grid, float2 *out_grid,
+                        float2 *pred, float2 *delta, cudaStream_t st)
+{
+    // lanes per visibility: the tap columns (2 hs + 1 at most) in at most two passes
+    if (2 * p->hs_max <= 8) return launch_tiles_lg<8>(p, op, vis_in, in_grid, out_grid, pred, delta, st);
+    if (2 * p->hs_max <= 16) return launch_tiles_lg<16>(p, op, vis_in, in_grid, out_grid, pred, delta, st);
+    return launch_tiles_lg<32>(p, op, vis_in, in_grid, out_grid, pred, delta, st);
 }
 
 }  // namespace sdp
