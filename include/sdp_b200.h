@@ -341,6 +341,12 @@ typedef struct sdp_clean_params {
     double psf_max_value;
     double cell_size;
 } sdp_clean_params;
+/* Workspace for sdp_hogbom.  For grid_size up to about 2750 (G^2 floats
+ * spread over the SMs' shared memory) the CLEAN runs as one persistent
+ * cooperative kernel with the residual held on chip and one bounded grid
+ * barrier per minor cycle; if a barrier wait gives up (about one second),
+ * *num_sources_dev is set to -1.  Larger images use one launch per minor
+ * cycle. */
 int sdp_hogbom_workspace_bytes(int grid_size, size_t *bytes);
 int sdp_hogbom(const sdp_clean_params *p, float *residual_inout, const float *psf, float *model_inout,
                sdp_float3 *sources, int *num_sources_dev, void *workspace, size_t workspace_bytes, void *stream);
@@ -359,6 +365,13 @@ int sdp_hogbom(const sdp_clean_params *p, float *residual_inout, const float *ps
  * serialise them (one stream, or events). */
 int sdp_hogbom_noalloc(const sdp_clean_params *p, float *residual_inout, const float *psf, float *model_inout,
                        sdp_float3 *sources, int *num_sources_dev, void *stream);
+
+/* Failure-detection self test (no counterpart in the reference): launches
+ * nblocks (1..64) blocks that wait at a grid barrier one arrival short of
+ * complete.  Each wait gives up after spin_limit sleeps of about 64 ns, so
+ * the kernel ends; *status receives SDP_ERR_TIMEOUT when the bounded wait
+ * reported the timeout (the expected result), SDP_OK otherwise. */
+int sdp_selftest_bounded_wait(int nblocks, long long spin_limit, int *status);
 
 #ifdef __cplusplus
 }

@@ -17,12 +17,12 @@
 // of the reference's float recurrence, which only matters when |max| sits
 // within rounding of the noise threshold.
 //
-// One minor cycle is two launches: k_clean_step applies the previous
-// component's PSF subtraction and reduces (max, index, sum) per block in the
-// same pass over the image; k_clean_select (one block) finishes the
-// reduction, applies the stopping rule and records the component.  After a
-// stop every later launch returns at once, so a fixed number of launches can
-// be captured in a CUDA graph.
+// One minor cycle is one launch (k_clean_cycle): every block applies the
+// previous component's PSF subtraction to its rows and reduces (max, index,
+// sum) in the same pass over the image; the last block to finish (a
+// completion counter) applies the stopping rule and records the component.
+// After a stop every later launch returns at once, so a fixed number of
+// launches can be captured in a CUDA graph.
 #include <algorithm>
 
 #include "common.cuh"
@@ -36,7 +36,7 @@ struct CleanState {
     int mx, my;
     float val;     // max_val of the pending component
     float first_z; // flux of the first component (the weak-source test, :239)
-    int pad;
+    unsigned done; // blocks finished in the current minor cycle
 };
 
 struct CleanWs {
@@ -47,9 +47,8 @@ struct CleanWs {
     int nblocks;
 };
 
-constexpr int kCleanThreads = 256;
 
-static int clean_blocks() { return num_sms() * 4; }
+static int clean_blocks() { return num_sms() * 8; }
 
 static void clean_layout(int nb, size_t *off, size_t *total)
 {
@@ -69,44 +68,15 @@ __device__ __forceinline__ void better(float &v, int &i, float v2, int i2)
     }
 }
 
-// Subtract the pending component from r[i] (reference :266-272).
-__device__ __forceinline__ void subtract_component(float *__restrict__ r, const float *__restrict__ psf, int G,
-                                                   size_t i, const CleanState &s, double gain, double psf_max)
-{
-    const int y = (int)(i / G), x = (int)(i % G);
-    const int half = G / 2;
-    const int sx = min(s.mx, half), sy = min(s.my, half);
-    const int ex = min(G - s.mx, half), ey = min(G - s.my, half);
-    if (x < s.mx - sx || x >= s.mx + ex || y < s.my - sy || y >= s.my + ey) return;
-    const long long pi = (long long)(y - s.my + half) * G + (G - (x - s.mx + half));
-    const float pv = (pi < (long long)G * G) ? psf[pi] : 0.f;
-    const double t = __dmul_rn(__dmul_rn(__dmul_rn(gain, (double)s.val), (double)pv), psf_max);
-    r[i] = __double2float_rn(__dsub_rn((double)r[i], t));
-}
 
-__global__ void __launch_bounds__(kCleanThreads) k_clean_step(int G, float *__restrict__ r,
-                                                             const float *__restrict__ psf, double gain,
-                                                             double psf_max, CleanWs ws, int reduce)
+// Block-wide (max |r|, first index) and sum reduction; result in thread 0.
+__device__ __forceinline__ void block_reduce(float &bv, int &bi, double &sum)
 {
-    const CleanState s = *ws.st;
-    if (s.stop && !s.pending) return;
-    const size_t n = (size_t)G * G;
-    float bv = -1.f;
-    int bi = 0x7fffffff;
-    double sum = 0.0;
-    for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
-        if (s.pending) subtract_component(r, psf, G, i, s, gain, psf_max);
-        if (reduce) {
-            const float a = fabsf(r[i]);
-            better(bv, bi, a, (int)i);
-            if (i >= 1) sum += (double)a;
-        }
-    }
-    if (!reduce) return;
     __shared__ float sv[32];
     __shared__ int si[32];
     __shared__ double ss[32];
-    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    const int tid = threadIdx.x;
+    const int lane = tid & 31, wid = tid >> 5;
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) {
         float v2 = __shfl_xor_sync(0xffffffffu, bv, o);
@@ -132,61 +102,20 @@ __global__ void __launch_bounds__(kCleanThreads) k_clean_step(int G, float *__re
             better(bv, bi, v2, i2);
             sum += __shfl_xor_sync(0xffffffffu, sum, o);
         }
-        if (lane == 0) {
-            ws.pmax[blockIdx.x] = bv;
-            ws.pidx[blockIdx.x] = bi;
-            ws.psum[blockIdx.x] = sum;
-        }
     }
 }
 
-__global__ void k_clean_select(int G, int max_records, const float *__restrict__ r,
-                               float *__restrict__ model, float3 *__restrict__ src, double gain, double noise,
-                               double weak, double psf_max, CleanWs ws)
+// Stopping rule and component bookkeeping of one minor cycle (:235-256).
+__device__ void select_component(int G, int max_records, float curr_max, int idx, double sum,
+                                 const float *__restrict__ r, float *__restrict__ model, float3 *__restrict__ src,
+                                 double gain, double noise, double weak, double psf_max, CleanState *st)
 {
-    CleanState *st = ws.st;
-    if (st->stop) {
-        if (threadIdx.x == 0) st->pending = 0;
-        return;
-    }
-    float bv = -1.f;
-    int bi = 0x7fffffff;
-    double sum = 0.0;
-    for (int b = threadIdx.x; b < ws.nblocks; b += blockDim.x) {
-        better(bv, bi, ws.pmax[b], ws.pidx[b]);
-        sum += ws.psum[b];
-    }
-    __shared__ float sv[32];
-    __shared__ int si[32];
-    __shared__ double ss[32];
-    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) {
-        float v2 = __shfl_xor_sync(0xffffffffu, bv, o);
-        int i2 = __shfl_xor_sync(0xffffffffu, bi, o);
-        better(bv, bi, v2, i2);
-        sum += __shfl_xor_sync(0xffffffffu, sum, o);
-    }
-    if (lane == 0) {
-        sv[wid] = bv;
-        si[wid] = bi;
-        ss[wid] = sum;
-    }
-    __syncthreads();
-    if (threadIdx.x != 0) return;
-    const int nw = blockDim.x / 32;
-    for (int w = 1; w < nw; ++w) {
-        better(sv[0], si[0], sv[w], si[w]);
-        ss[0] += ss[w];
-    }
-    float curr_max = sv[0];
-    int idx = si[0];
     if (curr_max <= 0.f) {  // all zero (or empty): the reference keeps index 0
         curr_max = 0.f;
         idx = 0;
     }
     const long long n = (long long)G * G;
-    const float avg = (n > 1) ? (float)(ss[0] / (double)(n - 1)) : 0.f;
+    const float avg = (n > 1) ? (float)(sum / (double)(n - 1)) : 0.f;
     const bool extracting_noise = (double)fabsf(curr_max) < noise * (double)avg * gain;       // :238
     const bool weak_source = st->count > 0 && (double)fabsf(curr_max) < (double)fabsf(st->first_z) * weak;  // :239
     if (extracting_noise || weak_source) {
@@ -194,7 +123,7 @@ __global__ void k_clean_select(int G, int max_records, const float *__restrict__
         st->pending = 0;
         return;
     }
-    const float max_val = __double2float_rn(__ddiv_rn((double)r[idx], psf_max));          // :247
+    const float max_val = __double2float_rn(__ddiv_rn((double)__ldcg(&r[idx]), psf_max));  // :247
     const int mx = idx % G, my = idx / G;
     const float z = __double2float_rn(__dmul_rn((double)max_val, gain));
     if (st->count == 0) st->first_z = z;
@@ -207,6 +136,129 @@ __global__ void k_clean_select(int G, int max_records, const float *__restrict__
     st->mx = mx;
     st->my = my;
     st->val = max_val;
+}
+
+// Subtraction of the pending component at pixel (y, x) (:266-272).
+__device__ __forceinline__ float clean_pixel(float v, int x, bool row_in, int x0, int x1, long long pbase,
+                                             long long g2, const float *__restrict__ psf, double scale,
+                                             double psf_max)
+{
+    if (row_in && x >= x0 && x < x1) {
+        const long long pi = pbase - x;  // mirrored in x; index G*G reads 0
+        const float pv = (pi < g2) ? __ldg(&psf[pi]) : 0.f;
+        v = __double2float_rn(__dsub_rn((double)v, __dmul_rn(__dmul_rn(scale, (double)pv), psf_max)));
+    }
+    return v;
+}
+
+constexpr int kCleanThreads = 256;
+constexpr int kCleanUnroll = 4;  // independent 4-pixel chunks in flight per thread
+
+// One minor cycle in one launch: every block subtracts the pending
+// component's PSF (:263-272, PSF mirrored in x, column G wrapping to the
+// next row, psf[G*G] read as 0) from its share of the image, 4 pixels per
+// vector load and several loads in flight per thread, and reduces max |r|,
+// its first index and the sum of |r| over indices >= 1; the last block to
+// finish reduces the block results and applies the stopping rule
+// (select = 1).  select = 0 only applies the pending subtraction.
+__global__ void __launch_bounds__(kCleanThreads) k_clean_cycle(int G, float *__restrict__ r,
+                                                              const float *__restrict__ psf,
+                                                              float *__restrict__ model, float3 *__restrict__ src,
+                                                              int max_records, double gain, double noise,
+                                                              double weak, double psf_max, CleanWs ws, int select)
+{
+    const CleanState s = *ws.st;
+    if (s.stop && !s.pending) return;
+    const int half = G / 2;
+    const int x0 = s.mx - min(s.mx, half), x1 = s.mx + min(G - s.mx, half);
+    const int y0 = s.my - min(s.my, half), y1 = s.my + min(G - s.my, half);
+    const long long g2 = (long long)G * G;
+    const double scale = __dmul_rn(gain, (double)s.val);
+    const bool pending = s.pending != 0;
+    float bv = -1.f;
+    int bi = 0x7fffffff;
+    double sum = 0.0;
+    const unsigned ug = (unsigned)G;
+    if ((G & 3) == 0) {
+        // 4-pixel chunks (a chunk never crosses a row when G % 4 == 0)
+        const unsigned nchunks = (unsigned)(g2 >> 2);
+        const unsigned stride = gridDim.x * kCleanThreads;
+        for (unsigned c0 = blockIdx.x * kCleanThreads + threadIdx.x; c0 < nchunks; c0 += stride * kCleanUnroll) {
+            float4 v[kCleanUnroll];
+#pragma unroll
+            for (int u = 0; u < kCleanUnroll; ++u) {
+                const unsigned c = c0 + u * stride;
+                v[u] = (c < nchunks) ? reinterpret_cast<const float4 *>(r)[c] : make_float4(0.f, 0.f, 0.f, 0.f);
+            }
+#pragma unroll
+            for (int u = 0; u < kCleanUnroll; ++u) {
+                const unsigned c = c0 + u * stride;
+                if (c >= nchunks) continue;
+                const unsigned i0 = c << 2;
+                const int y = (int)(i0 / ug), x = (int)(i0 - (unsigned)y * ug);
+                if (pending && y >= y0 && y < y1 && x + 3 >= x0 && x < x1) {
+                    const long long pbase = (long long)(y - s.my + half) * G + (G + s.mx - half);
+                    v[u].x = clean_pixel(v[u].x, x, true, x0, x1, pbase, g2, psf, scale, psf_max);
+                    v[u].y = clean_pixel(v[u].y, x + 1, true, x0, x1, pbase, g2, psf, scale, psf_max);
+                    v[u].z = clean_pixel(v[u].z, x + 2, true, x0, x1, pbase, g2, psf, scale, psf_max);
+                    v[u].w = clean_pixel(v[u].w, x + 3, true, x0, x1, pbase, g2, psf, scale, psf_max);
+                    reinterpret_cast<float4 *>(r)[c] = v[u];
+                }
+                if (select) {
+                    const int i = (int)i0;
+                    better(bv, bi, fabsf(v[u].x), i);
+                    better(bv, bi, fabsf(v[u].y), i + 1);
+                    better(bv, bi, fabsf(v[u].z), i + 2);
+                    better(bv, bi, fabsf(v[u].w), i + 3);
+                    sum += (double)(i >= 1 ? fabsf(v[u].x) : 0.f) + (double)fabsf(v[u].y) + (double)fabsf(v[u].z) +
+                           (double)fabsf(v[u].w);
+                }
+            }
+        }
+    } else {
+        for (unsigned i = blockIdx.x * kCleanThreads + threadIdx.x; i < (unsigned)g2; i += gridDim.x * kCleanThreads) {
+            const int y = (int)(i / ug), x = (int)(i - (unsigned)y * ug);
+            float v = r[i];
+            if (pending && y >= y0 && y < y1 && x >= x0 && x < x1) {
+                const long long pbase = (long long)(y - s.my + half) * G + (G + s.mx - half);
+                v = clean_pixel(v, x, true, x0, x1, pbase, g2, psf, scale, psf_max);
+                r[i] = v;
+            }
+            if (select) {
+                better(bv, bi, fabsf(v), (int)i);
+                if (i >= 1) sum += (double)fabsf(v);
+            }
+        }
+    }
+    if (!select) return;
+    block_reduce(bv, bi, sum);
+    __shared__ bool is_last;
+    const int tid = threadIdx.x;
+    if (tid == 0) {
+        ws.pmax[blockIdx.x] = bv;
+        ws.pidx[blockIdx.x] = bi;
+        ws.psum[blockIdx.x] = sum;
+        __threadfence();
+        const unsigned ticket = atomicAdd(&ws.st->done, 1u);
+        is_last = (ticket == gridDim.x - 1);
+    }
+    __syncthreads();
+    if (!is_last) return;
+    // last block: reduce the per-block results (read past L1) and select
+    __threadfence();
+    bv = -1.f;
+    bi = 0x7fffffff;
+    sum = 0.0;
+    for (int b = tid; b < (int)gridDim.x; b += kCleanThreads) {
+        better(bv, bi, __ldcg(&ws.pmax[b]), __ldcg(&ws.pidx[b]));
+        sum += __ldcg(&ws.psum[b]);
+    }
+    block_reduce(bv, bi, sum);
+    if (tid == 0) {
+        CleanState *st = ws.st;
+        st->done = 0;
+        select_component(G, max_records, bv, bi, sum, r, model, src, gain, noise, weak, psf_max, st);
+    }
 }
 
 // :297-306: pixel coordinates to (x - G/2) * cell_size.
@@ -223,6 +275,297 @@ __global__ void k_clean_finish(int G, double cell, int max_records, float3 *__re
     if (threadIdx.x == 0 && count_out) *count_out = n;
 }
 
+// ---------------------------------------------------------------------------
+// Persistent variant: the residual stays in shared memory for all minor
+// cycles.  Used when the image fits on chip (G^2 floats over all SMs, at
+// most kPersistSlice floats per SM, i.e. G <= 2752 on 148 SMs).
+//
+// One CTA per SM (cooperative launch, so all CTAs are resident), each owning
+// a contiguous slice of pixels.  A minor cycle: apply the pending component
+// to the slice, reduce (max |r|, first index, signed value, sum |r|) per
+// block, publish it (double-buffered by cycle parity), one grid barrier,
+// then every block reduces all block results in the same order and takes
+// the same decision, so no second barrier is needed.  Block 0 records the
+// component and updates the model.  The barrier waits are bounded: after
+// kBarrierSpins sleeps a block sets an error flag, every block leaves at its
+// next barrier, and the host reads SDP_ERR_TIMEOUT.
+// ---------------------------------------------------------------------------
+struct PPart {
+    float amax;
+    int idx;
+    float val;
+    int pad;
+    double sum;
+};
+
+struct CleanBar {
+    unsigned count;
+    unsigned gen;
+    int err;
+    int pad;
+};
+
+constexpr int kPersistThreads = 1024;
+constexpr int kPersistSlice = 51200;            // floats of residual per block (200 KB)
+constexpr long long kBarrierSpins = 16000000;   // x ~64 ns sleeps: about one second
+
+__device__ __forceinline__ void better3(float &v, int &i, float &sv, float v2, int i2, float sv2)
+{
+    if (v2 > v || (v2 == v && i2 < i)) {
+        v = v2;
+        i = i2;
+        sv = sv2;
+    }
+}
+
+// Bounded grid barrier (sense by generation).  Returns false after a timeout
+// or when another block has timed out.
+__device__ bool grid_sync(CleanBar *bar, unsigned nblocks, unsigned &gen, long long spin_limit)
+{
+    __shared__ int s_ok;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        __threadfence();
+        const unsigned g = gen;
+        int ok = 1;
+        if (atomicAdd(&bar->count, 1u) == nblocks - 1) {
+            atomicExch(&bar->count, 0u);
+            __threadfence();
+            atomicAdd(&bar->gen, 1u);
+        } else {
+            long long spins = 0;
+            while (atomicAdd(&bar->gen, 0u) == g) {
+                if (atomicAdd(&bar->err, 0) != 0) {
+                    ok = 0;
+                    break;
+                }
+                if (++spins > spin_limit) {
+                    atomicExch(&bar->err, 1);
+                    ok = 0;
+                    break;
+                }
+                __nanosleep(64);
+            }
+        }
+        __threadfence();
+        if (atomicAdd(&bar->err, 0) != 0) ok = 0;
+        s_ok = ok;
+    }
+    __syncthreads();
+    gen += 1;
+    return s_ok != 0;
+}
+
+__device__ __forceinline__ void block_reduce3(float &bv, int &bi, float &bs, double &sum)
+{
+    __shared__ float sv[32], sval[32];
+    __shared__ int si[32];
+    __shared__ double ss[32];
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        const float v2 = __shfl_xor_sync(0xffffffffu, bv, o);
+        const int i2 = __shfl_xor_sync(0xffffffffu, bi, o);
+        const float s2 = __shfl_xor_sync(0xffffffffu, bs, o);
+        better3(bv, bi, bs, v2, i2, s2);
+        sum += __shfl_xor_sync(0xffffffffu, sum, o);
+    }
+    if (lane == 0) {
+        sv[wid] = bv;
+        si[wid] = bi;
+        sval[wid] = bs;
+        ss[wid] = sum;
+    }
+    __syncthreads();
+    if (wid == 0) {
+        const int nw = blockDim.x / 32;
+        bv = (lane < nw) ? sv[lane] : -1.f;
+        bi = (lane < nw) ? si[lane] : 0x7fffffff;
+        bs = (lane < nw) ? sval[lane] : 0.f;
+        sum = (lane < nw) ? ss[lane] : 0.0;
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) {
+            const float v2 = __shfl_xor_sync(0xffffffffu, bv, o);
+            const int i2 = __shfl_xor_sync(0xffffffffu, bi, o);
+            const float s2 = __shfl_xor_sync(0xffffffffu, bs, o);
+            better3(bv, bi, bs, v2, i2, s2);
+            sum += __shfl_xor_sync(0xffffffffu, sum, o);
+        }
+    }
+    __syncthreads();
+}
+
+__global__ void __launch_bounds__(kPersistThreads, 1) k_clean_persistent(
+    int G, float *__restrict__ r, const float *__restrict__ psf, float *__restrict__ model,
+    float3 *__restrict__ src, int *__restrict__ count_out, int max_records, int num_minor, double gain,
+    double noise, double weak, double psf_max, double cell, PPart *__restrict__ parts, CleanBar *bar, int P,
+    long long spin_limit)
+{
+    extern __shared__ float sr[];
+    __shared__ int s_pending, s_mx, s_my, s_stop;
+    __shared__ float s_val;
+    const int tid = threadIdx.x;
+    const unsigned nb = gridDim.x;
+    const long long g2 = (long long)G * G;
+    const long long p0 = (long long)blockIdx.x * P;
+    const int n = (int)max(0LL, min(p0 + P, g2) - p0);
+    for (int k = tid; k < n; k += kPersistThreads) sr[k] = r[p0 + k];
+    if (tid == 0) {
+        s_pending = 0;
+        s_stop = 0;
+        s_mx = 0;
+        s_my = 0;
+        s_val = 0.f;
+    }
+    __syncthreads();
+    unsigned gen = 0;
+    int count = 0;
+    float first_z = 0.f;
+    const int half = G / 2;
+    const int step_y = kPersistThreads / G, step_x = kPersistThreads - (kPersistThreads / G) * G;
+    bool ok = true;
+    for (int it = 0; it <= num_minor; ++it) {
+        const bool apply_only = (it == num_minor);
+        const int pending = s_pending, mx = s_mx, my = s_my;
+        const double scale = __dmul_rn(gain, (double)s_val);
+        const int x0 = mx - min(mx, half), x1 = mx + min(G - mx, half);
+        const int y0 = my - min(my, half), y1 = my + min(G - my, half);
+        float bv = -1.f, bs = 0.f;
+        int bi = 0x7fffffff;
+        double sum = 0.0;
+        // pixel k = tid + m * kPersistThreads of the slice; (y, x) advanced
+        // incrementally, four pixels' PSF loads in flight per thread
+        int i = (int)p0 + tid;
+        int y = i / G, x = i - y * G;
+        for (int k = tid; k < n; k += 4 * kPersistThreads) {
+            float v[4], pv[4];
+            int ii[4];
+            bool in[4];
+#pragma unroll
+            for (int u = 0; u < 4; ++u) {
+                const bool live = k + u * kPersistThreads < n;
+                ii[u] = i;
+                v[u] = live ? sr[k + u * kPersistThreads] : 0.f;
+                in[u] = live && pending && y >= y0 && y < y1 && x >= x0 && x < x1;
+                pv[u] = 0.f;
+                if (in[u]) {
+                    const long long pi = (long long)(y - my + half) * G + (G + mx - half) - x;
+                    if (pi < g2) pv[u] = __ldg(&psf[pi]);
+                }
+                i += kPersistThreads;
+                x += step_x;
+                y += step_y;
+                if (x >= G) {
+                    x -= G;
+                    y += 1;
+                }
+            }
+#pragma unroll
+            for (int u = 0; u < 4; ++u) {
+                if (k + u * kPersistThreads >= n) break;
+                float w = v[u];
+                if (in[u]) {
+                    w = __double2float_rn(__dsub_rn((double)w, __dmul_rn(__dmul_rn(scale, (double)pv[u]), psf_max)));
+                    sr[k + u * kPersistThreads] = w;
+                }
+                if (!apply_only) {
+                    const float a = fabsf(w);
+                    better3(bv, bi, bs, a, ii[u], w);
+                    if (ii[u] >= 1) sum += (double)a;
+                }
+            }
+        }
+        if (apply_only) break;
+        block_reduce3(bv, bi, bs, sum);
+        PPart *buf = parts + (size_t)(it & 1) * nb;
+        if (tid == 0) buf[blockIdx.x] = PPart{bv, bi, bs, 0, sum};
+        if (!grid_sync(bar, nb, gen, spin_limit)) {
+            ok = false;
+            break;
+        }
+        // every block reduces all block results identically
+        bv = -1.f;
+        bi = 0x7fffffff;
+        bs = 0.f;
+        sum = 0.0;
+        for (unsigned b = tid; b < nb; b += kPersistThreads) {
+            const PPart *pq = buf + b;
+            better3(bv, bi, bs, __ldcg(&pq->amax), __ldcg(&pq->idx), __ldcg(&pq->val));
+            sum += __ldcg(&pq->sum);
+        }
+        block_reduce3(bv, bi, bs, sum);
+        if (tid == 0) {
+            float curr_max = bv;
+            int idx = bi;
+            float sval = bs;
+            if (curr_max <= 0.f) {  // all zero (or empty): the reference keeps index 0
+                curr_max = 0.f;
+                idx = 0;
+                sval = 0.f;
+            }
+            const float avg = (g2 > 1) ? (float)(sum / (double)(g2 - 1)) : 0.f;
+            const bool extracting_noise = (double)fabsf(curr_max) < noise * (double)avg * gain;            // :238
+            const bool weak_source = count > 0 && (double)fabsf(curr_max) < (double)fabsf(first_z) * weak;  // :239
+            if (extracting_noise || weak_source) {
+                s_stop = 1;
+                s_pending = 0;
+            } else {
+                const float max_val = __double2float_rn(__ddiv_rn((double)sval, psf_max));  // :247
+                const float z = __double2float_rn(__dmul_rn((double)max_val, gain));
+                if (count == 0) first_z = z;
+                if (blockIdx.x == 0) {
+                    if (count < max_records) src[count] = make_float3((float)(idx % G), (float)(idx / G), z);
+                    model[idx] = __double2float_rn(__dadd_rn((double)model[idx], __dmul_rn((double)max_val, gain)));
+                }
+                count += 1;
+                s_pending = 1;
+                s_mx = idx % G;
+                s_my = idx / G;
+                s_val = max_val;
+            }
+        }
+        __syncthreads();
+        if (s_stop) break;
+    }
+    __syncthreads();
+    for (int k = tid; k < n; k += kPersistThreads) r[p0 + k] = sr[k];
+    if (blockIdx.x == 0 && tid == 0) {
+        const int nrec = min(count, max_records);
+        for (int k = 0; k < nrec; ++k) {  // :297-306
+            float3 q = src[k];
+            q.x = __double2float_rn(__dmul_rn((double)__fsub_rn(q.x, (float)(G / 2)), cell));
+            q.y = __double2float_rn(__dmul_rn((double)__fsub_rn(q.y, (float)(G / 2)), cell));
+            src[k] = q;
+        }
+        if (count_out) *count_out = ok ? nrec : -1;
+    }
+}
+
+// Bounded-wait self test: a barrier that one block never reaches.  Every
+// waiting block gives up after spin_limit sleeps and the kernel ends with
+// the error flag set (the host reads SDP_ERR_TIMEOUT).
+__global__ void k_barrier_timeout_probe(CleanBar *bar, long long spin_limit)
+{
+    unsigned gen = 0;
+    // gridDim.x blocks wait for gridDim.x + 1 arrivals: the last one never comes
+    grid_sync(bar, gridDim.x + 1, gen, spin_limit);
+}
+
+static void persist_layout(int nb, size_t base, size_t *bar_off, size_t *parts_off, size_t *total)
+{
+    *bar_off = base;
+    *parts_off = base + 64;
+    *total = *parts_off + sizeof(PPart) * 2 * (size_t)nb;
+}
+
+static int persistent_fits(int G, int *nb_out)
+{
+    const int nb = num_sms();
+    const long long P = (((long long)G * G + nb - 1) / nb + 3) / 4 * 4;
+    *nb_out = nb;
+    return P <= kPersistSlice;
+}
+
 }  // namespace sdp
 
 using namespace sdp;
@@ -230,8 +573,10 @@ using namespace sdp;
 SDP_EXPORT int sdp_hogbom_workspace_bytes(int G, size_t *bytes)
 {
     SDP_CHECK_ARG(bytes != nullptr && G >= 2, "bad argument");
-    size_t off[4];
-    clean_layout(clean_blocks(), off, bytes);
+    size_t off[4], base, bar, parts, total;
+    clean_layout(clean_blocks(), off, &base);
+    persist_layout(num_sms(), base, &bar, &parts, &total);
+    *bytes = total;
     return SDP_OK;
 }
 
@@ -244,31 +589,85 @@ SDP_EXPORT int sdp_hogbom(const sdp_clean_params *p, float *residual, const floa
     SDP_CHECK_ARG(p->num_minor_cycles == 0 || sources, "sources is NULL");
     SDP_CHECK_ARG(p->psf_max_value != 0.0, "psf_max_value is 0");
     const int G = p->grid_size;
-    const int nb = clean_blocks();
-    size_t off[4], need;
-    clean_layout(nb, off, &need);
+    size_t need = 0;
+    SDP_TRY(sdp_hogbom_workspace_bytes(G, &need));
     if (ws_bytes < need) return set_error(SDP_ERR_RANGE, "hogbom workspace %zu B < %zu B", ws_bytes, need);
+    cudaStream_t st = as_stream(stream);
     char *w = static_cast<char *>(workspace);
+    // the stored component list is bounded by the caller's buffer (MAX_SOURCES)
+    const int cap = std::max(0, std::min(p->num_minor_cycles, p->max_sources));
+    float3 *src = reinterpret_cast<float3 *>(sources);
+
+    int pnb = 0;
+    if (persistent_fits(G, &pnb)) {
+        size_t off[4], base, bar_off, parts_off, total;
+        clean_layout(clean_blocks(), off, &base);
+        persist_layout(pnb, base, &bar_off, &parts_off, &total);
+        CleanBar *bar = reinterpret_cast<CleanBar *>(w + bar_off);
+        PPart *parts = reinterpret_cast<PPart *>(w + parts_off);
+        const int P = (int)((((long long)G * G + pnb - 1) / pnb + 3) / 4 * 4);
+        const size_t smem = sizeof(float) * (size_t)P;
+        auto fn = k_clean_persistent;
+        SDP_CUDA_TRY(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+        int per_sm = 0;
+        SDP_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, kPersistThreads, smem));
+        if (per_sm >= 1) {
+            SDP_CUDA_TRY(cudaMemsetAsync(bar, 0, sizeof(CleanBar), st));
+            int Gv = G, nminor = p->num_minor_cycles, maxr = cap;
+            double gain = p->loop_gain, noise = p->noise_factor, weak = p->weak_source_percent,
+                   pmax = p->psf_max_value, cell = p->cell_size;
+            int *cnt = num_sources_dev;
+            int Pv = P;
+            long long spins = kBarrierSpins;
+            void *args[] = {&Gv, &residual, (void *)&psf, &model, &src, &cnt, &maxr, &nminor, &gain, &noise,
+                            &weak, &pmax, &cell, &parts, &bar, &Pv, &spins};
+            SDP_CUDA_TRY(cudaLaunchCooperativeKernel((const void *)fn, dim3(pnb), dim3(kPersistThreads), args, smem,
+                                                     st));
+            return SDP_OK;
+        }
+    }
+
+    // general path: one launch per minor cycle
+    const int nb = std::max(1, std::min((int)(((long long)G * G / 4 + kCleanThreads - 1) / kCleanThreads),
+                                        clean_blocks()));
+    size_t off[4], base;
+    clean_layout(nb, off, &base);
     CleanWs ws;
     ws.st = reinterpret_cast<CleanState *>(w + off[0]);
     ws.psum = reinterpret_cast<double *>(w + off[1]);
     ws.pmax = reinterpret_cast<float *>(w + off[2]);
     ws.pidx = reinterpret_cast<int *>(w + off[3]);
     ws.nblocks = nb;
-    cudaStream_t st = as_stream(stream);
     SDP_CUDA_TRY(cudaMemsetAsync(ws.st, 0, sizeof(CleanState), st));
-    // the stored component list is bounded by the caller's buffer (MAX_SOURCES)
-    const int cap = std::max(0, std::min(p->num_minor_cycles, p->max_sources));
-    float3 *src = reinterpret_cast<float3 *>(sources);
-    for (int it = 0; it < p->num_minor_cycles; ++it) {
-        k_clean_step<<<nb, kCleanThreads, 0, st>>>(G, residual, psf, p->loop_gain, p->psf_max_value, ws, 1);
-        k_clean_select<<<1, 1024, 0, st>>>(G, cap, residual, model, src, p->loop_gain, p->noise_factor,
-                                          p->weak_source_percent, p->psf_max_value, ws);
-    }
+    const dim3 block(kCleanThreads);
+    for (int it = 0; it < p->num_minor_cycles; ++it)
+        k_clean_cycle<<<nb, block, 0, st>>>(G, residual, psf, model, src, cap, p->loop_gain, p->noise_factor,
+                                            p->weak_source_percent, p->psf_max_value, ws, 1);
     // subtract the last component so residual_inout is the final residual
-    k_clean_step<<<nb, kCleanThreads, 0, st>>>(G, residual, psf, p->loop_gain, p->psf_max_value, ws, 0);
+    k_clean_cycle<<<nb, block, 0, st>>>(G, residual, psf, model, src, cap, p->loop_gain, p->noise_factor,
+                                        p->weak_source_percent, p->psf_max_value, ws, 0);
     k_clean_finish<<<1, 256, 0, st>>>(G, p->cell_size, cap, src, ws, num_sources_dev);
     SDP_LAUNCH_CHECK();
+    return SDP_OK;
+}
+
+SDP_EXPORT int sdp_selftest_bounded_wait(int nblocks, long long spin_limit, int *status)
+{
+    SDP_CHECK_ARG(status != nullptr && nblocks >= 1 && nblocks <= 64 && spin_limit >= 1, "bad argument");
+    *status = SDP_OK;
+    CleanBar *bar = nullptr;
+    SDP_CUDA_TRY(cudaMalloc(&bar, sizeof(CleanBar)));
+    int err = 0;
+    cudaError_t e = cudaMemset(bar, 0, sizeof(CleanBar));
+    if (e == cudaSuccess) {
+        k_barrier_timeout_probe<<<nblocks, 32>>>(bar, spin_limit);
+        e = cudaGetLastError();
+    }
+    if (e == cudaSuccess) e = cudaDeviceSynchronize();
+    if (e == cudaSuccess) e = cudaMemcpy(&err, &bar->err, sizeof(int), cudaMemcpyDeviceToHost);
+    cudaFree(bar);
+    if (e != cudaSuccess) return cuda_error(e, "bounded-wait self test");
+    *status = err ? SDP_ERR_TIMEOUT : SDP_OK;
     return SDP_OK;
 }
 
@@ -336,7 +735,9 @@ SDP_EXPORT int sdp_hogbom_noalloc(const sdp_clean_params *p, float *residual, co
     void *base = nullptr;
     SDP_TRY(clean_scratch_address(&base));  // first call on a device: symbol lookup
     char *w = static_cast<char *>(base);
-    const int nb = G;  // one partial per block, G blocks
+    // blocks: at most one per 1024 pixels, hence <= G / 4 <= kNoAllocMaxGrid partials
+    const int nb = std::max(1, std::min((int)(((long long)G * G / 4 + kCleanThreads - 1) / kCleanThreads),
+                                        std::min(clean_blocks(), G)));
     CleanWs ws;
     ws.st = reinterpret_cast<CleanState *>(w);
     ws.psum = reinterpret_cast<double *>(w + kNoAllocStateBytes);
@@ -348,12 +749,12 @@ SDP_EXPORT int sdp_hogbom_noalloc(const sdp_clean_params *p, float *residual, co
     SDP_CUDA_TRY(cudaMemsetAsync(ws.st, 0, sizeof(CleanState), st));
     const int cap = std::max(0, std::min(p->num_minor_cycles, p->max_sources));
     float3 *src = reinterpret_cast<float3 *>(sources);
-    for (int it = 0; it < p->num_minor_cycles; ++it) {
-        k_clean_step<<<nb, kCleanThreads, 0, st>>>(G, residual, psf, p->loop_gain, p->psf_max_value, ws, 1);
-        k_clean_select<<<1, 1024, 0, st>>>(G, cap, residual, model, src, p->loop_gain, p->noise_factor,
-                                          p->weak_source_percent, p->psf_max_value, ws);
-    }
-    k_clean_step<<<nb, kCleanThreads, 0, st>>>(G, residual, psf, p->loop_gain, p->psf_max_value, ws, 0);
+    const dim3 block(kCleanThreads);
+    for (int it = 0; it < p->num_minor_cycles; ++it)
+        k_clean_cycle<<<nb, block, 0, st>>>(G, residual, psf, model, src, cap, p->loop_gain, p->noise_factor,
+                                            p->weak_source_percent, p->psf_max_value, ws, 1);
+    k_clean_cycle<<<nb, block, 0, st>>>(G, residual, psf, model, src, cap, p->loop_gain, p->noise_factor,
+                                        p->weak_source_percent, p->psf_max_value, ws, 0);
     k_clean_finish<<<1, 256, 0, st>>>(G, p->cell_size, cap, src, ws, num_sources_dev);
     SDP_LAUNCH_CHECK();
     return SDP_OK;

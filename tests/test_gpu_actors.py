@@ -269,3 +269,37 @@ def test_empty_and_error_paths(sdp, actors, golden):
     assert e.value.status == 6
     with pytest.raises(sdp.SdpError):
         actors.fft(24, np.zeros((24 * 24, 2), np.float32), False)
+
+
+@pytest.mark.parametrize("G", [1024, 2048])
+def test_hogbom_large_bit_exact_vs_oracle(sdp, actors, oracle32, G):
+    """The persistent on-chip CLEAN (G <= ~2750) against the oracle at full size."""
+    rng = np.random.default_rng(G)
+    yy, xx = np.mgrid[0:G, 0:G]
+    psf = np.exp(-((xx - G // 2) ** 2 + (yy - G // 2) ** 2) / 18.0).astype(np.float32)
+    psf /= psf.max()
+    res = (0.001 * rng.standard_normal((G, G))).astype(np.float32)
+    for _ in range(40):
+        x0, y0 = rng.integers(8, G - 8, 2)
+        res += (rng.uniform(0.05, 1.0) * np.roll(np.roll(psf, y0 - G // 2, 0), x0 - G // 2, 1)).astype(np.float32)
+    res, psf = res.reshape(-1), psf.reshape(-1)
+    cfg = sdp.make_config(G, 1.0, 1.0, psf_max_value=4.0, cell_size=1e-5)
+    n1, s1, m1, _ = oracle32.hogbom(G, 200, 200, res, psf, 4.0, 1e-5)
+    n2, s2, m2 = actors.hogbom(cfg, G, 200, 200, res, psf)
+    assert n1 == n2 == 200
+    np.testing.assert_array_equal(s2, s1)
+    np.testing.assert_array_equal(m2, m1)
+
+
+def test_bounded_wait_reports_timeout(sdp):
+    """Failure detection without a GPU fault: a grid barrier that one arrival
+    short of complete gives up after its bounded wait and reports
+    SDP_ERR_TIMEOUT; the context stays usable afterwards."""
+    import ctypes as C
+    import torch
+    lib = sdp.load()
+    st = C.c_int(-1)
+    sdp.check(lib.sdp_selftest_bounded_wait(C.c_int(4), C.c_longlong(200_000), C.byref(st)), lib)
+    assert st.value == 5  # SDP_ERR_TIMEOUT
+    x = torch.ones(1024, device="cuda")
+    assert float(x.sum().item()) == 1024.0
