@@ -49,11 +49,12 @@ PROFILES = ROOT / "profiles"
 def parse():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--steps", type=int, default=50)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--e2e-steps", type=int, default=3)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-major-cycle", action="store_true")
     ap.add_argument("--cpu-sample", type=int, default=200_000, help="visibilities per CPU-baseline step")
     return ap.parse_args()
 
@@ -92,58 +93,71 @@ def read_traffic(kernel: str):
 
 
 class ClockSampler:
-    """nvidia-smi clock / throttle sampling during the timed region."""
+    """SM clock and clock-event (throttle) reasons, read through NVML every
+    ~2 ms in a background thread; mark() opens and closes the window whose
+    samples are summarised (the timed region).  Reading only."""
+
+    REASONS = {"hw_slowdown": 0x8, "sw_thermal_slowdown": 0x20, "hw_thermal_slowdown": 0x40,
+               "sw_power_cap": 0x4}
 
     def __init__(self, index: int):
         self.index = index
-        self.proc = None
-        self.lines = []
+        self.samples = []
+        self.window = [None, None]
+        self._stop = threading.Event()
+        self.thread = None
+        self.ok = False
 
     def __enter__(self):
-        q = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.hw_slowdown,"
-             "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
-             "clocks_event_reasons.sw_power_cap")
         try:
-            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.index), f"--query-gpu={q}",
-                                          "--format=csv,noheader,nounits", "-lms", "100"],
-                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
-            self.thread = threading.Thread(target=self._read, daemon=True)
+            import pynvml
+            pynvml.nvmlInit()
+            self.nv = pynvml
+            self.h = pynvml.nvmlDeviceGetHandleByIndex(self.index)
+            self.max_mhz = pynvml.nvmlDeviceGetMaxClockInfo(self.h, pynvml.NVML_CLOCK_SM)
+            self.ok = True
+            self.thread = threading.Thread(target=self._run, daemon=True)
             self.thread.start()
-        except FileNotFoundError:
-            self.proc = None
+        except Exception:
+            self.ok = False
         return self
 
-    def _read(self):
-        for line in self.proc.stdout:
-            self.lines.append(line.strip())
+    def _run(self):
+        nv = self.nv
+        while not self._stop.is_set():
+            try:
+                mhz = nv.nvmlDeviceGetClockInfo(self.h, nv.NVML_CLOCK_SM)
+                try:
+                    reasons = nv.nvmlDeviceGetCurrentClocksEventReasons(self.h)
+                except AttributeError:
+                    reasons = nv.nvmlDeviceGetCurrentClocksThrottleReasons(self.h)
+                self.samples.append((time.perf_counter(), mhz, reasons))
+            except Exception:
+                pass
+            time.sleep(0.002)
+
+    def mark(self, which: int):
+        self.window[which] = time.perf_counter()
 
     def __exit__(self, *exc):
-        if self.proc:
-            self.proc.terminate()
-            try:
-                self.proc.wait(timeout=5)
-            except subprocess.TimeoutExpired:
-                self.proc.kill()
+        self._stop.set()
+        if self.thread:
+            self.thread.join(timeout=2)
 
     def summary(self):
-        sm, mx, reasons = [], [], set()
-        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        for line in self.lines:
-            parts = [p.strip() for p in line.split(",")]
-            if len(parts) < 7:
-                continue
-            try:
-                sm.append(float(parts[0]))
-                mx.append(float(parts[1]))
-            except ValueError:
-                continue
-            for name, v in zip(names, parts[3:7]):
-                if v.lower().startswith("active"):
+        if not self.ok:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": [], "samples": 0, "source": "nvml unavailable"}
+        t0, t1 = self.window
+        sel = [s for s in self.samples if (t0 is None or s[0] >= t0) and (t1 is None or s[0] <= t1)]
+        if not sel:
+            sel = self.samples[-5:]
+        reasons = set()
+        for _, _, r in sel:
+            for name, bit in self.REASONS.items():
+                if r & bit:
                     reasons.add(name)
-        if not sm:
-            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": [], "samples": 0}
-        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": max(mx), "reasons": sorted(reasons),
-                "samples": len(sm)}
+        return {"sm_mhz": statistics.median([s[1] for s in sel]) if sel else None, "sm_max_mhz": self.max_mhz,
+                "reasons": sorted(reasons), "samples": len(sel), "source": "nvml, 2 ms"}
 
 
 # ---------------------------------------------------------------------------
@@ -319,6 +333,7 @@ def b200_arm(args):
     def step():
         plan.cycle(model_grid, residual, S.SDP_DEGRID_CONV)
 
+    clocks = ClockSampler(local).__enter__()
     for _ in range(max(3, args.warmup)):
         step()
     torch.cuda.synchronize()
@@ -330,13 +345,15 @@ def b200_arm(args):
     if world > 1:
         dist.barrier()
     torch.cuda.synchronize()
-    with ClockSampler(local) as clocks:
-        for i in range(args.steps):
-            flush.zero_()
-            starts[i].record(stream)
-            step()
-            ends[i].record(stream)
-        torch.cuda.synchronize()
+    clocks.mark(0)
+    for i in range(args.steps):
+        flush.zero_()
+        starts[i].record(stream)
+        step()
+        ends[i].record(stream)
+    torch.cuda.synchronize()
+    clocks.mark(1)
+    clocks.__exit__(None, None, None)
     if world > 1:
         dist.barrier()
     step_ms = [s.elapsed_time(e) for s, e in zip(starts, ends)]
@@ -357,6 +374,40 @@ def b200_arm(args):
     peak = float(peaks.get("hbm_gbs", 6650.0))
     peak_src = "measured" if "hbm_gbs" in peaks else "fallback"
     traffic = read_traffic("k_tiles_cycle_conv_c2_2048")
+
+    # ---- whole major cycle (device pipeline, CUDA graph): image->grid, fused
+    #      vis pass, grid->image, 200 Hogbom minor cycles ---------------------------------
+    major = None
+    if not args.no_major_cycle:
+        ones = torch.zeros((N, 2), dtype=torch.float32, device=dev)
+        ones[:, 0] = 1.0
+        pgrid = torch.empty((G * G, 2), dtype=torch.float32, device=dev)
+        plan.grid(ones, pgrid)
+        prol = torch.empty(G // 2 + 1, dtype=torch.float32, device=dev)
+        D.prolate_table(G, prol)
+        psf = torch.empty(G * G, dtype=torch.float32, device=dev)
+        D.grid_to_image(G, pgrid, prol, work, psf)
+        psf_max = float(psf.max().item())
+        psf /= psf_max
+        del ones, pgrid
+        pcfg = S.PipelineConfig(G, OS, w.cfg.uv_scale, w.cfg.w_scale, w.cfg.cell_size, 200, 200, 0.1, 1.5, 0.0002,
+                                psf_max, S.SDP_DEGRID_CONV, S.SDP_COORD_F32, 0, 1)
+        pl = D.pipeline(pcfg, uvw, measured, psf, wk_g, wk_d, keep=(uvw, gk, dk, sup))
+        for _ in range(2):
+            pl.major_cycle()
+        torch.cuda.synchronize()
+        n_cyc = max(2, min(5, args.steps))
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(n_cyc):
+            pl.major_cycle()
+        e1.record(stream)
+        torch.cuda.synchronize()
+        t_cyc = e0.elapsed_time(e1) / n_cyc
+        major = {"ms_per_major_cycle": t_cyc, "vis_per_s": N / (t_cyc * 1e-3), "minor_cycles": 200,
+                 "cuda_graph": pl.graph_active(), "graph_error": pl.graph_error(),
+                 "stages": "image->grid FFT, fused degrid/subtract/grid, grid->image FFT + taper, Hogbom x200"}
+        pl.close()
 
     # ---- e2e through the reference-facing C ABI with pinned host buffers ---------------
     uvw_h = torch.empty((N, 3), dtype=torch.float32).pin_memory()
@@ -423,6 +474,8 @@ def b200_arm(args):
         "gpu_launches": args.steps,
         "clocks": clocks.summary(),
     }
+    if major is not None:
+        line["major_cycle"] = major
     if cpu is not None:
         line["cpu_baseline"] = cpu
     plan.close()

@@ -259,11 +259,21 @@ typedef struct sdp_wkernels {
     int max_half_support;        /* max over planes of supports[p].x (host value) */
 } sdp_wkernels;
 
-/* Gridding semantics. */
+/* Gridding semantics (low byte of grid_mode). */
 enum {
     SDP_GRID_STD = 0,         /* std_gridding: taps [ceil(p-hs), ceil(p+hs))                 */
     SDP_GRID_SNAPPED = 1      /* gridding_CPU: snapped p, taps [ceil(p-hs), floor(p+hs)]      */
 };
+/* Plan flags, OR-ed into grid_mode.
+ * SDP_PLAN_COORD_F64: grid coordinates, tap boxes, kernel indices and nearest
+ *   cells follow the reference's double build (PRECISION = double) instead
+ *   of its float build; the kernel products stay FP32.  Use it to match the
+ *   FP64 oracle: the float build's ceil/round decisions differ from the
+ *   double build's for coordinates within an ulp of an integer.
+ * SDP_PLAN_SNAP: apply correct_to_finegrid (degridgrid.c:24-25, 52-54) to
+ *   the raw uvw at plan build, in the plan's coordinate precision, so the
+ *   snapped coordinates are never rounded to float in between. */
+enum { SDP_PLAN_COORD_F64 = 0x100, SDP_PLAN_SNAP = 0x200 };
 
 /* Visibility set binned by uv tile (and w-plane) once, reused by every
  * gridding / degridding pass of a major cycle. */
@@ -365,6 +375,53 @@ int sdp_hogbom(const sdp_clean_params *p, float *residual_inout, const float *ps
  * serialise them (one stream, or events). */
 int sdp_hogbom_noalloc(const sdp_clean_params *p, float *residual_inout, const float *psf, float *model_inout,
                        sdp_float3 *sources, int *num_sources_dev, void *stream);
+
+/* ---------------------------------------------------------------------------
+ * Device-resident major cycle of the FFT imaging pipeline
+ * (code_fft_1core/generated/Core0.c, delta_k / psi_k):
+ *   model image -> [shift, FFT, shift] -> model grid -> [degrid, subtract
+ *   from measured, grid] -> residual grid -> [shift, iFFT, shift, taper]
+ *   -> residual image -> [Hogbom] -> components, model image += components.
+ * The model image starts at zero; each call of sdp_pipeline_major_cycle runs
+ * one cycle on the stream (captured once as a CUDA graph when use_graph).
+ * ------------------------------------------------------------------------- */
+enum { SDP_COORD_F32 = 0, SDP_COORD_F64 = 1 };
+
+typedef struct sdp_pipeline_config {
+    int grid_size;            /* power of two, 16..16384                                  */
+    int oversampling;
+    double uv_scale, w_scale, cell_size;
+    int num_minor_cycles, max_sources;
+    double loop_gain, noise_factor, weak_source_percent, psf_max_value;
+    int degrid_mode;          /* SDP_DEGRID_NEAREST (reference) or SDP_DEGRID_CONV        */
+    int coord_mode;           /* SDP_COORD_F32 (float build) or SDP_COORD_F64 (double build) */
+    int snap;                 /* 1: the uvw given are raw and are snapped to the fine grid */
+    int use_graph;            /* 1: capture the cycle as a CUDA graph                      */
+} sdp_pipeline_config;
+
+typedef struct sdp_pipeline sdp_pipeline;
+/* uvw and measured (N each) are device pointers; psf (G^2, normalised to
+ * peak 1) may be host or device memory.  All three are copied.  The kernel
+ * tables are copied when the oversampling is a power of two; otherwise the
+ * pipeline reads the caller's tables, which must outlive it. */
+int sdp_pipeline_create(sdp_pipeline **p, const sdp_pipeline_config *cfg, const sdp_wkernels *grid_kernels,
+                        const sdp_wkernels *degrid_kernels, int num_vis, const sdp_float3 *uvw,
+                        const sdp_float2 *measured, const float *psf, void *stream);
+int sdp_pipeline_major_cycle(sdp_pipeline *p, void *stream);
+/* Device pointers owned by the pipeline: the last cycle's residual image,
+ * the model image, the last cycle's components (x, y in radians, flux) and
+ * their count. */
+int sdp_pipeline_outputs(sdp_pipeline *p, float **residual_image, float **model_image, sdp_float3 **sources,
+                         int **num_sources);
+/* Copies the outputs (host or device destinations, any may be NULL;
+ * sources: max_sources entries) and synchronises the stream. */
+int sdp_pipeline_copy_outputs(sdp_pipeline *p, float *residual_image, float *model_image, sdp_float3 *sources,
+                              int *num_sources, void *stream);
+int sdp_pipeline_graph_active(const sdp_pipeline *p);
+/* Why the graph capture was refused ("" when it was not). */
+const char *sdp_pipeline_graph_error(const sdp_pipeline *p);
+int sdp_pipeline_visplan(sdp_pipeline *p, sdp_visplan **plan);
+int sdp_pipeline_destroy(sdp_pipeline *p);
 
 /* Failure-detection self test (no counterpart in the reference): launches
  * nblocks (1..64) blocks that wait at a grid barrier one arrival short of

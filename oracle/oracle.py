@@ -454,3 +454,42 @@ class RefLib:
         hd = np.zeros(2, dtype=np.int32)
         self.lib.clean_psf_host_set_up(_i(grid_size), _i(1), C.byref(cfg), _ptr(d), _ptr(out), _ptr(hd))
         return out, hd
+
+
+def fft_pipeline(o: Oracle, G, OS, uvw_raw, vis, gk, dk, supports, uv_scale, w_scale, psf, psf_max, cell,
+                 cycles, minor, max_sources, nearest=True, loop_gain=0.1, noise_factor=1.5, weak=0.0002):
+    """The FFT pipeline's major cycles in the order of the generated schedule
+    (code_fft_1core/generated/Core0.c: correct_to_finegrid :3101 once, then
+    per cycle the model -> inverse taper (identity) -> fft_shift r2c -> FFTW
+    forward -> fft_shift c2c -> std_degridding -> subtract -> std_gridding ->
+    fft_shift c2c -> FFTW backward -> fft_shift c2r -> taper -> hogbom_clean),
+    with the live Hogbom and one visibility slice (the schedule's four slices
+    only split the same sums).  Returns per cycle (residual image, model
+    image, number of components, components)."""
+    _, uvw_c, _ = o.correct_to_finegrid(G, OS, uvw_raw, vis, uv_scale)
+    prolate = o.half_prolate(G)
+    model = np.zeros(G * G, dtype=o.dtype)
+    out = []
+    for _ in range(cycles):
+        mg = o.fft_shift_c2c(G, o.fft2d(G, o.fft_shift_r2c(G, model), -1))
+        pred = o.std_degridding(G, OS, dk, supports, mg, uvw_c, uv_scale, w_scale, nearest=nearest)
+        delta = o.subtract_vis(vis, pred)
+        rg = o.std_gridding(G, OS, gk, supports, uvw_c, delta, uv_scale, w_scale)
+        img = o.conv_correction(G, o.fft_shift_c2r(G, o.fft2d(G, o.fft_shift_c2c(G, rg), +1)), prolate)
+        n, src, model, _ = o.hogbom(G, minor, max_sources, img, psf, psf_max, cell, model=model,
+                                    loop_gain=loop_gain, noise_factor=noise_factor, weak=weak)
+        out.append((img.copy(), model.copy(), n, src))
+    return out
+
+
+def dirty_psf(o: Oracle, G, OS, uvw_raw, gk, supports, uv_scale, w_scale):
+    """PSF of the array as the pipeline images it: unit visibilities gridded,
+    transformed and taper-corrected, then cropped and normalised as
+    psf_host_set_up does (top.c:453-515).  Returns (psf, psf_max)."""
+    ones = np.zeros((uvw_raw.shape[0], 2), dtype=o.dtype)
+    ones[:, 0] = 1.0
+    _, uvw_c, _ = o.correct_to_finegrid(G, OS, uvw_raw, ones, uv_scale)
+    g = o.std_gridding(G, OS, gk, supports, uvw_c, ones, uv_scale, w_scale)
+    img = o.conv_correction(G, o.fft_shift_c2r(G, o.fft2d(G, o.fft_shift_c2c(G, g), +1)), o.half_prolate(G))
+    mx, psf = o.psf_crop_normalise(G, img)
+    return psf, mx

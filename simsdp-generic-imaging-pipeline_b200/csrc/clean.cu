@@ -25,7 +25,7 @@
 // launches can be captured in a CUDA graph.
 #include <algorithm>
 
-#include "common.cuh"
+#include "internal.cuh"
 
 namespace sdp {
 
@@ -583,6 +583,14 @@ SDP_EXPORT int sdp_hogbom_workspace_bytes(int G, size_t *bytes)
 SDP_EXPORT int sdp_hogbom(const sdp_clean_params *p, float *residual, const float *psf, float *model,
                           sdp_float3 *sources, int *num_sources_dev, void *workspace, size_t ws_bytes, void *stream)
 {
+    return hogbom_launch(p, residual, psf, model, sources, num_sources_dev, workspace, ws_bytes, true,
+                         as_stream(stream));
+}
+
+int sdp::hogbom_launch(const sdp_clean_params *p, float *residual, const float *psf, float *model,
+                       sdp_float3 *sources, int *num_sources_dev, void *workspace, size_t ws_bytes,
+                       bool allow_persistent, cudaStream_t st)
+{
     SDP_CHECK_ARG(p && residual && psf && model && workspace, "NULL argument");
     SDP_CHECK_ARG(p->grid_size >= 2, "grid_size %d", p->grid_size);
     SDP_CHECK_ARG(p->num_minor_cycles >= 0, "num_minor_cycles %d", p->num_minor_cycles);
@@ -592,14 +600,13 @@ SDP_EXPORT int sdp_hogbom(const sdp_clean_params *p, float *residual, const floa
     size_t need = 0;
     SDP_TRY(sdp_hogbom_workspace_bytes(G, &need));
     if (ws_bytes < need) return set_error(SDP_ERR_RANGE, "hogbom workspace %zu B < %zu B", ws_bytes, need);
-    cudaStream_t st = as_stream(stream);
     char *w = static_cast<char *>(workspace);
     // the stored component list is bounded by the caller's buffer (MAX_SOURCES)
     const int cap = std::max(0, std::min(p->num_minor_cycles, p->max_sources));
     float3 *src = reinterpret_cast<float3 *>(sources);
 
     int pnb = 0;
-    if (persistent_fits(G, &pnb)) {
+    if (allow_persistent && persistent_fits(G, &pnb)) {
         size_t off[4], base, bar_off, parts_off, total;
         clean_layout(clean_blocks(), off, &base);
         persist_layout(pnb, base, &bar_off, &parts_off, &total);

@@ -114,6 +114,46 @@ __device__ __forceinline__ float ref_snap(float p, int os)
 {
     return __fdiv_rn(roundf(__fmul_rn(p, (float)os)), (float)os);
 }
+
+// The same expressions in the reference's double build (PRECISION = double,
+// common.h:78-83, 114-134): every intermediate stays in double.
+__device__ __forceinline__ double ref_grid_pos(double u, double uv_scale) { return __dmul_rn(u, uv_scale); }
+
+__device__ __forceinline__ int ref_widx_std(double z, double w_scale)
+{
+    return __double2int_rz(__dadd_rn(__dsqrt_rn(fabs(__dmul_rn(z, w_scale))), 0.5));
+}
+
+__device__ __forceinline__ int ref_widx_round(double z, double w_scale)
+{
+    return (int)round(__dsqrt_rn(fabs(__dmul_rn(z, w_scale))));
+}
+
+__device__ __forceinline__ int ref_kidx(int g, double p, double os)
+{
+    return abs((int)round(__dmul_rn(__dsub_rn((double)g, p), os)));
+}
+
+__device__ __forceinline__ int ref_nearest(double p, int gc)
+{
+    return __double2int_rz(__dadd_rn(__dadd_rn(p, (double)gc), 0.5));
+}
+
+__device__ __forceinline__ double ref_snap(double p, int os)
+{
+    return __ddiv_rn(round(__dmul_rn(p, (double)os)), (double)os);
+}
+
+// correct_to_finegrid in PRECISION T (degridgrid.c:24-25, 52-54): the
+// snapped coordinate as the build stores it.
+template <typename T>
+__device__ __forceinline__ T ref_finegrid(float u, int G, int os, double uv_scale)
+{
+    const double half = (double)(G / 2);
+    const double t = __dadd_rn(__dmul_rn(__dadd_rn(__dmul_rn((double)u, uv_scale), half), (double)os), 0.5);
+    const long long f = __double2ll_rz(t);
+    return (T)__ddiv_rn(__dsub_rn(__ddiv_rn((double)f, (double)os), half), uv_scale);
+}
 #endif
 
 }  // namespace sdp

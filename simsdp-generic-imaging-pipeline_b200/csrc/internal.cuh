@@ -5,14 +5,20 @@
 
 namespace sdp {
 
-struct VisRec {
-    float px, py;  // grid coordinates (reference rounding; snapped in SNAPPED mode)
-    int meta;      // bits 0-15 plane, bit 31 conjugate (w < 0)
-    int idx;       // original visibility index
+// Visibility record in plan order.  T is the PRECISION of the reference
+// build whose index arithmetic the plan reproduces: float (the default
+// build) or double (the FP64 build).
+template <typename T>
+struct Rec {
+    T px, py;  // grid coordinates (reference rounding; snapped in SNAPPED mode)
+    int meta;  // bits 0-15 plane, bit 31 conjugate (w < 0)
+    int idx;   // original visibility index
 };
-static_assert(sizeof(VisRec) == 16, "record is one 16-byte load");
+static_assert(sizeof(Rec<float>) == 16, "float record is one 16-byte load");
+static_assert(sizeof(Rec<double>) == 24, "double record is 24 bytes");
 
-// Plan modes beyond the public SDP_GRID_STD / SDP_GRID_SNAPPED.
+// Plan modes: the low byte is SDP_GRID_STD / SDP_GRID_SNAPPED / SDP_GRID_G2G,
+// flags SDP_PLAN_COORD_F64 and SDP_PLAN_SNAP above it.
 constexpr int kPlanG2G = 2;
 
 }  // namespace sdp
@@ -23,12 +29,15 @@ struct sdp_visplan {
     int mode;
     int n;
     int ntx, nty, nk, nbins, ntiles, hs_max, W, S;
-    sdp::VisRec *rec = nullptr;
+    void *rec = nullptr;          // Rec<float> or Rec<double>
+    int coord_f64 = 0;            // index arithmetic of the double build
+    int snap = 0;                 // correct_to_finegrid applied to the uvw at plan build
     int *perm = nullptr;
     int4 *items = nullptr;
     int *n_items = nullptr;       // device scalar
     int *item_counter = nullptr;  // device scalar
     int *flags = nullptr;         // device scalar
+    int *kshare = nullptr;        // device scalar: bit 0 set = degridding set differs from gridding set, bit 1 = differs from its conjugate
     float2 *measured = nullptr;   // plan order
     int phase_major = 0;          // kernel tables copied phase-major (OS a power of two)
     int *gpoff = nullptr;         // plane offsets into the gridding table in use
@@ -48,6 +57,7 @@ int visplan_setup(sdp_visplan *p, const sdp_geometry *geom, const sdp_wkernels *
 size_t visplan_arena_bytes(const sdp_visplan *p);
 // Bins the visibilities into the arena (which must hold visplan_arena_bytes).
 int visplan_build(sdp_visplan *p, void *arena, const float3 *uvw, cudaStream_t st);
+size_t visplan_record_bytes(const sdp_visplan *p);
 // Reads and clears the device error flags (blocking on st).
 int visplan_check_flags(sdp_visplan *p, cudaStream_t st);
 
@@ -56,5 +66,10 @@ int check_fft_size(int G);
 
 // Host-side Schwab prolate spheroidal (same evaluation as the device table).
 double prolate_host(double nu);
+
+// sdp_hogbom with a choice of the persistent on-chip kernel (when it fits)
+// or one launch per minor cycle.
+int hogbom_launch(const sdp_clean_params *p, float *residual, const float *psf, float *model, sdp_float3 *sources,
+                  int *num_sources_dev, void *workspace, size_t ws_bytes, bool allow_persistent, cudaStream_t st);
 
 }  // namespace sdp

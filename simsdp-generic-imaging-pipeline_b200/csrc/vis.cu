@@ -56,11 +56,12 @@ struct PlanDev {
     const float2 *dk;   // degridding kernels
     const int2 *ds;     // degridding supports
     const int *dpoff;   // degridding plane offsets into dk
-    const VisRec *rec;  // plan order
+    const void *rec;    // plan order, Rec<float> or Rec<double>
     const int4 *items;  // (tile, begin, end, -)
     const int *n_items;
     int *item_counter;
     int *flags;
+    const int *kdiff;  // bit 0: degridding set != gridding set; bit 1: != its conjugate
 };
 
 // ----------------------------------------------------------------------------
@@ -167,31 +168,52 @@ static int exclusive_scan(const int *in, int *out, int n, int *scratch, cudaStre
 }
 
 // ----------------------------------------------------------------------------
+// Arithmetic of the two reference builds (correctly rounded, no contraction)
+// ----------------------------------------------------------------------------
+__device__ __forceinline__ float tadd(float a, float b) { return __fadd_rn(a, b); }
+__device__ __forceinline__ double tadd(double a, double b) { return __dadd_rn(a, b); }
+__device__ __forceinline__ float tsub(float a, float b) { return __fsub_rn(a, b); }
+__device__ __forceinline__ double tsub(double a, double b) { return __dsub_rn(a, b); }
+__device__ __forceinline__ float tceil(float a) { return ceilf(a); }
+__device__ __forceinline__ double tceil(double a) { return ceil(a); }
+__device__ __forceinline__ float tfloor(float a) { return floorf(a); }
+__device__ __forceinline__ double tfloor(double a) { return floor(a); }
+
+// ----------------------------------------------------------------------------
 // Binning
 // ----------------------------------------------------------------------------
 __device__ __forceinline__ int floor_div(int a, int b) { return (a >= 0) ? a / b : -((-a + b - 1) / b); }
 
-// Computes the record of each visibility and its bin key.
-__global__ void k_bin(const float3 *__restrict__ uvw, int n, int mode, int G, int OS, double uv_scale,
+// Computes the record of each visibility and its bin key.  snap applies
+// correct_to_finegrid (degridgrid.c:24-25, 52-54) in precision T first.
+template <typename T>
+__global__ void k_bin(const float3 *__restrict__ uvw, int n, int mode, int snap, int G, int OS, double uv_scale,
                       double w_scale, const int2 *__restrict__ sup, const int2 *__restrict__ dsup, int nk, int nkd,
-                      long long ntot_g, long long ntot_d, int hs_max, int ntx, int nty, VisRec *__restrict__ rec_tmp,
+                      long long ntot_g, long long ntot_d, int hs_max, int ntx, int nty, Rec<T> *__restrict__ rec_tmp,
                       int *__restrict__ keys, int *__restrict__ counts, int *__restrict__ flags)
 {
     int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
     float3 c = uvw[i];
-    VisRec r;
-    r.px = ref_grid_pos(c.x, uv_scale);
-    r.py = ref_grid_pos(c.y, uv_scale);
+    Rec<T> r;
+    if (snap) {
+        const T fu = ref_finegrid<T>(c.x, G, OS, uv_scale), fv = ref_finegrid<T>(c.y, G, OS, uv_scale);
+        r.px = ref_grid_pos(fu, uv_scale);
+        r.py = ref_grid_pos(fv, uv_scale);
+    } else {
+        r.px = ref_grid_pos((T)c.x, uv_scale);
+        r.py = ref_grid_pos((T)c.y, uv_scale);
+    }
+    const T cz = (T)c.z;
     int plane;
     if (mode == SDP_GRID_SNAPPED) {
-        plane = ref_widx_round(c.z, w_scale);
+        plane = ref_widx_round(cz, w_scale);
         r.px = ref_snap(r.px, OS);
         r.py = ref_snap(r.py, OS);
     } else if (mode == kPlanG2G) {  // g2g: plane forced to 0 (degridgrid.c:215)
         plane = 0;
     } else {
-        plane = ref_widx_std(c.z, w_scale);
+        plane = ref_widx_std(cz, w_scale);
     }
     r.meta = plane | ((c.z < 0.0f) ? (int)0x80000000u : 0);
     r.idx = i;
@@ -208,8 +230,8 @@ __global__ void k_bin(const float3 *__restrict__ uvw, int n, int mode, int G, in
             ed > ntot_d) {
             atomicOr(flags, FLAG_SUPPORT);
         } else {
-            int lox = (int)ceilf(__fsub_rn(r.px, (float)hs)) + G / 2;
-            int loy = (int)ceilf(__fsub_rn(r.py, (float)hs)) + G / 2;
+            int lox = (int)tceil(tsub(r.px, (T)hs)) + G / 2;
+            int loy = (int)tceil(tsub(r.py, (T)hs)) + G / 2;
             int tx = min(max(floor_div(lox, kTile), 0), ntx - 1);
             int ty = min(max(floor_div(loy, kTile), 0), nty - 1);
             key = (ty * ntx + tx) * nk + plane;
@@ -220,8 +242,9 @@ __global__ void k_bin(const float3 *__restrict__ uvw, int n, int mode, int G, in
     keys[i] = key;
 }
 
-__global__ void k_scatter(const VisRec *__restrict__ rec_tmp, const int *__restrict__ keys, int n,
-                          const int *__restrict__ offsets, int *__restrict__ fill, VisRec *__restrict__ rec,
+template <typename T>
+__global__ void k_scatter(const Rec<T> *__restrict__ rec_tmp, const int *__restrict__ keys, int n,
+                          const int *__restrict__ offsets, int *__restrict__ fill, Rec<T> *__restrict__ rec,
                           int *__restrict__ perm)
 {
     int i = blockIdx.x * blockDim.x + threadIdx.x;
@@ -302,8 +325,8 @@ constexpr int kThreads = 256;  // 8 warps per CTA of the tile kernels
 // visibility (grid edges, where the reference mirrors or skips taps, 2 hs + 1
 // taps, differing supports) takes the general path, which evaluates the
 // reference's index arithmetic tap by tap.
-template <int GMODE, int OP, int LG>
-__global__ void __launch_bounds__(kThreads) k_tiles(PlanDev P, const float2 *__restrict__ vis_in,
+template <typename T, int GMODE, int OP, int LG>
+__global__ void __launch_bounds__(kThreads, 4) k_tiles(PlanDev P, const float2 *__restrict__ vis_in,
                                                    const float2 *__restrict__ in_grid,
                                                    float2 *__restrict__ out_grid, float2 *__restrict__ pred_out,
                                                    float2 *__restrict__ delta_out,
@@ -318,12 +341,26 @@ __global__ void __launch_bounds__(kThreads) k_tiles(PlanDev P, const float2 *__r
     float2 *mtile = reinterpret_cast<float2 *>(smem_f);
     float *sub_re = smem_f + (kStageIn ? 2 * SS : 0);
     float *sub_im = sub_re + SS;
+    // per-plane constants {hs_d, degrid offset, hs_g, grid offset}, loaded once
+    int4 *planes = reinterpret_cast<int4 *>(smem_f + (kStageIn ? 2 * SS : 0) + (kGrids ? 2 * SS : 0));
+    for (int k = threadIdx.x; k < P.nk_g; k += kThreads)
+        planes[k] = make_int4(kConv && k < P.nk_d ? P.ds[k].x : 0, kConv && k < P.nk_d ? P.dpoff[k] : 0,
+                              kGrids ? P.gs[k].x : 0, kGrids ? P.gpoff[k] : 0);
     const int lane = threadIdx.x & 31;
     const int warp = threadIdx.x >> 5;
     const int grp = lane / LG;
     const int cl = lane % LG;
-    const float fos = (float)P.OS;
+    const T fos = (T)P.OS;
+    const Rec<T> *__restrict__ recs = static_cast<const Rec<T> *>(P.rec);
     __shared__ int s_item;
+    // When the degridding set equals the gridding set or its conjugate (bit
+    // for bit, checked at plan build), the fast path of a cycle reads each
+    // kernel sample once and keeps it in registers for the gridding pass.
+    constexpr bool kShareable = (OP == OP_CYCLE_CONV) && LG == 8;
+    const int kdiff = kShareable ? *P.kdiff : 3;
+    const bool share = (kdiff & 1) == 0 || (kdiff & 2) == 0;
+    const float share_sign = (kdiff & 1) == 0 ? 1.f : -1.f;
+    float2 ksr[kShareable ? LG : 1];
 
     for (;;) {
         if (threadIdx.x == 0) s_item = atomicAdd(P.item_counter, 1);
@@ -345,12 +382,12 @@ __global__ void __launch_bounds__(kThreads) k_tiles(PlanDev P, const float2 *__r
         for (int base = it.y + warp * VPW; base < it.z; base += (kThreads / 32) * VPW) {
             const int r = base + grp;
             const bool valid = r < it.z;
-            VisRec rec;
+            Rec<T> rec;
             if (valid) {
-                rec = P.rec[r];
+                rec = recs[r];
             } else {
-                rec.px = 0.f;
-                rec.py = 0.f;
+                rec.px = (T)0;
+                rec.py = (T)0;
                 rec.meta = 0;
                 rec.idx = 0;
             }
@@ -358,18 +395,19 @@ __global__ void __launch_bounds__(kThreads) k_tiles(PlanDev P, const float2 *__r
             const float conj = (rec.meta < 0) ? -1.f : 1.f;
 
             // ---------------- tap geometry and the fast-path test ----------------
-            const int hs_d = kConv ? P.ds[plane].x : 0;
-            const int hs_g = kGrids ? P.gs[plane].x : 0;
+            const int4 pl = planes[plane];
+            const int hs_d = kConv ? pl.x : 0;
+            const int hs_g = kGrids ? pl.z : 0;
             const int hs = kGrids ? hs_g : hs_d;
-            const float lox = ceilf(__fsub_rn(rec.px, (float)hs));
-            const float loy = ceilf(__fsub_rn(rec.py, (float)hs));
+            const T lox = tceil(tsub(rec.px, (T)hs));
+            const T loy = tceil(tsub(rec.py, (T)hs));
             int ncols, nrows;
             if (GMODE == SDP_GRID_SNAPPED) {  // gridding_run.c:84-112: inclusive floor bound
-                ncols = (int)(floorf(__fadd_rn(rec.px, (float)hs)) - lox) + 1;
-                nrows = (int)(floorf(__fadd_rn(rec.py, (float)hs)) - loy) + 1;
+                ncols = (int)(tfloor(tadd(rec.px, (T)hs)) - lox) + 1;
+                nrows = (int)(tfloor(tadd(rec.py, (T)hs)) - loy) + 1;
             } else {  // degridgrid.c:93, 103
-                ncols = (int)(ceilf(__fadd_rn(rec.px, (float)hs)) - lox);
-                nrows = (int)(ceilf(__fadd_rn(rec.py, (float)hs)) - loy);
+                ncols = (int)(tceil(tadd(rec.px, (T)hs)) - lox);
+                nrows = (int)(tceil(tadd(rec.py, (T)hs)) - loy);
             }
             const int ix0 = (int)lox + P.gc, iy0 = (int)loy + P.gc;  // grid index of the first tap
             const int tx0 = ix0 - ox, ty0 = iy0 - oy;                // ... and in the tile
@@ -383,8 +421,8 @@ __global__ void __launch_bounds__(kThreads) k_tiles(PlanDev P, const float2 *__r
                 const int A = hs + 1;
                 colok = cl < ncols;
                 const int kc = kcol(P, A, ref_kidx((int)lox + cl, rec.px, fos));
-                if (kConv) colp_d = P.dpoff[plane] + kc;
-                if (kGrids) colp_g = P.gpoff[plane] + kc;
+                if (kConv) colp_d = pl.y + kc;
+                if (kGrids) colp_g = pl.w + kc;
                 lx = tx0 + cl;
                 // row cl of the box: kernel-row offset and tile row, packed
                 rowpack = (krow(P, A, ref_kidx((int)loy + cl, rec.py, fos)) << 6) | (ty0 + cl);
@@ -403,6 +441,7 @@ __global__ void __launch_bounds__(kThreads) k_tiles(PlanDev P, const float2 *__r
                         const int pk = __shfl_sync(fmask, rowpack, grp * LG + rr);
                         if (rr < nrows && colok) {
                             const float2 ks = __ldg(&P.dk[colp_d + (pk >> 6)]);
+                            if constexpr (kShareable) ksr[rr] = ks;
                             const float2 gv = mtile[(pk & 63) * S + lx];
                             a1.x = fmaf(gv.x, ks.x, a1.x);
                             a1.y = fmaf(gv.y, ks.x, a1.y);
@@ -414,11 +453,11 @@ __global__ void __launch_bounds__(kThreads) k_tiles(PlanDev P, const float2 *__r
                 } else if (valid) {
                     // general path: degridgrid.c:147-186 tap by tap, edges mirrored
                     const int A = hs_d + 1, stride = A * P.OS;
-                    const float dlox = ceilf(__fsub_rn(rec.px, (float)hs_d));
-                    const float dloy = ceilf(__fsub_rn(rec.py, (float)hs_d));
-                    const int dnc = (int)(ceilf(__fadd_rn(rec.px, (float)hs_d)) - dlox);
-                    const int dnr = (int)(ceilf(__fadd_rn(rec.py, (float)hs_d)) - dloy);
-                    const int off = P.dpoff[plane];
+                    const T dlox = tceil(tsub(rec.px, (T)hs_d));
+                    const T dloy = tceil(tsub(rec.py, (T)hs_d));
+                    const int dnc = (int)(tceil(tadd(rec.px, (T)hs_d)) - dlox);
+                    const int dnr = (int)(tceil(tadd(rec.py, (T)hs_d)) - dloy);
+                    const int off = pl.y;
                     for (int c = cl; c < dnc; c += LG) {
                         const int cu = mirror((int)dlox + c, P.gc);
                         const int kx = ref_kidx(cu, rec.px, fos);
@@ -461,9 +500,13 @@ __global__ void __launch_bounds__(kThreads) k_tiles(PlanDev P, const float2 *__r
                 // (the .y fallback uses the new .x)
                 const float sx = fmaf(-conj, a2.y, a1.x);
                 const float sy = fmaf(conj, a2.x, a1.y);
+                // (one correctly rounded reciprocal instead of two divides: the
+                // sum's order already differs from the reference's)
                 const float cn = __fsqrt_rn(nrm);
-                const float nx = (cn < 1e-5f) ? __fdiv_rn(sx, 1e-5f) : __fdiv_rn(sx, cn);
-                const float ny = (cn < 1e-5f) ? __fdiv_rn(nx, 1e-5f) : __fdiv_rn(sy, cn);
+                const bool tiny = cn < 1e-5f;
+                const float inv = tiny ? 1e5f : __frcp_rn(cn);
+                const float nx = sx * inv;
+                const float ny = tiny ? nx * inv : sy * inv;
                 value = make_float2(nx, ny);
             } else if (OP == OP_CYCLE_NEAR || OP == OP_G2G) {
                 // degridgrid.c:194-200 / :273-285
@@ -504,7 +547,13 @@ __global__ void __launch_bounds__(kThreads) k_tiles(PlanDev P, const float2 *__r
                     for (int rr = 0; rr < LG; ++rr) {
                         const int pk = __shfl_sync(fmask, rowpack, grp * LG + rr);
                         if (rr < nrows && colok) {
-                            const float2 ks = __ldg(&P.gk[colp_g + (pk >> 6)]);
+                            float2 ks;
+                            if constexpr (kShareable) {
+                                ks = share ? make_float2(ksr[rr].x, share_sign * ksr[rr].y)
+                                           : __ldg(&P.gk[colp_g + (pk >> 6)]);
+                            } else {
+                                ks = __ldg(&P.gk[colp_g + (pk >> 6)]);
+                            }
                             const int cell = (pk & 63) * S + lx;
                             atomicAdd(sub_re + cell, fmaf(-ca, ks.y, gval.x * ks.x));
                             atomicAdd(sub_im + cell, fmaf(cb, ks.y, gval.y * ks.x));
@@ -513,7 +562,7 @@ __global__ void __launch_bounds__(kThreads) k_tiles(PlanDev P, const float2 *__r
                 } else if (valid) {
                     // general path: degridgrid.c:93-122 / gridding_run.c:104-132 tap by tap
                     const int A = hs_g + 1, stride = A * P.OS;
-                    const int off = P.gpoff[plane];
+                    const int off = pl.w;
                     for (int c = cl; c < ncols; c += LG) {
                         const int u = (int)lox + c;
                         const int gx = u + P.gc;
@@ -596,6 +645,39 @@ __global__ void k_plane_offsets(const int2 *__restrict__ sup, int nk, int OS, in
     }
 }
 
+// Sets bit 0 of *diff when some sample of the degridding set differs from
+// the gridding set, bit 1 when some sample differs from the gridding set's
+// conjugate (equal supports required; `related` = 0 sets both).  The tile
+// kernel reads each sample once for both passes when a bit is clear.
+__global__ void k_kernels_differ(const int2 *__restrict__ gs, const int2 *__restrict__ ds,
+                                 const int *__restrict__ gpoff, const int *__restrict__ dpoff,
+                                 const float2 *__restrict__ gk, const float2 *__restrict__ dk, int related, int nk,
+                                 int OS, int max_per_plane, int *diff)
+{
+    const int p = blockIdx.y;
+    if (!related) {
+        if (threadIdx.x == 0 && blockIdx.x == 0) atomicOr(diff, 3);
+        return;
+    }
+    if (p >= nk) return;
+    const int hs = gs[p].x;
+    if (ds[p].x != hs) {
+        if (threadIdx.x == 0 && blockIdx.x == 0) atomicOr(diff, 3);
+        return;
+    }
+    if (hs < 0) return;
+    const int n = (hs + 1) * OS * (hs + 1) * OS;
+    if (n > max_per_plane) return;
+    int d = 0;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        const float2 a = gk[gpoff[p] + i], b = dk[dpoff[p] + i];
+        const bool re = __float_as_uint(a.x) == __float_as_uint(b.x);
+        if (!re || __float_as_uint(a.y) != __float_as_uint(b.y)) d |= 1;
+        if (!re || (__float_as_uint(a.y) ^ 0x80000000u) != __float_as_uint(b.y)) d |= 2;
+    }
+    if (d) atomicOr(diff, d);
+}
+
 // Identity offsets (reference layout kept): poff[p] = supports[p].y.
 __global__ void k_plane_offsets_identity(const int2 *__restrict__ sup, int nk, int *__restrict__ poff)
 {
@@ -646,6 +728,7 @@ static PlanDev plan_dev(const sdp_visplan *p)
     d.dk = p->phase_major ? p->dk2 : reinterpret_cast<const float2 *>(p->dk.kernels);
     d.ds = reinterpret_cast<const int2 *>(p->dk.supports);
     d.dpoff = p->dpoff;
+    d.kdiff = p->kshare;
     d.rec = p->rec;
     d.items = p->items;
     d.n_items = p->n_items;
@@ -679,8 +762,9 @@ static void plan_layout(const sdp_visplan *p, size_t *off, size_t *total)
     const int n = p->n;
     size_t o = 0;
     const size_t nb_scan = (size_t)((std::max(p->nbins, p->ntiles) + kScanBlock - 1) / kScanBlock + 2);
-    off[0] = o; o = align_up(o + sizeof(VisRec) * (size_t)std::max(n, 1), 256);           // rec
-    off[1] = o; o = align_up(o + sizeof(VisRec) * (size_t)std::max(n, 1), 256);           // rec_tmp
+    const size_t rb = visplan_record_bytes(p);
+    off[0] = o; o = align_up(o + rb * (size_t)std::max(n, 1), 256);                       // rec
+    off[1] = o; o = align_up(o + rb * (size_t)std::max(n, 1), 256);                       // rec_tmp
     off[2] = o; o = align_up(o + sizeof(int) * (size_t)std::max(n, 1), 256);              // perm
     off[3] = o; o = align_up(o + sizeof(int) * (size_t)std::max(n, 1), 256);              // keys
     off[4] = o; o = align_up(o + sizeof(int) * ((size_t)p->nbins + 1), 256);              // counts / fill
@@ -699,9 +783,19 @@ static void plan_layout(const sdp_visplan *p, size_t *off, size_t *total)
     *total = o;
 }
 
-int visplan_setup(sdp_visplan *p, const sdp_geometry *geom, const sdp_wkernels *gk, const sdp_wkernels *dk, int n,
-                  int mode)
+size_t visplan_record_bytes(const sdp_visplan *p)
 {
+    return p->coord_f64 ? sizeof(Rec<double>) : sizeof(Rec<float>);
+}
+
+int visplan_setup(sdp_visplan *p, const sdp_geometry *geom, const sdp_wkernels *gk, const sdp_wkernels *dk, int n,
+                  int mode_flags)
+{
+    const int mode = mode_flags & 0xff;
+    SDP_CHECK_ARG((mode_flags & ~(0xff | SDP_PLAN_COORD_F64 | SDP_PLAN_SNAP)) == 0, "unknown plan flags 0x%x",
+                  mode_flags);
+    p->coord_f64 = (mode_flags & SDP_PLAN_COORD_F64) ? 1 : 0;
+    p->snap = (mode_flags & SDP_PLAN_SNAP) ? 1 : 0;
     SDP_TRY(check_geometry(geom));
     SDP_TRY(check_kernels(gk, "gridding"));
     if (dk == nullptr) dk = gk;
@@ -740,8 +834,8 @@ int visplan_build(sdp_visplan *p, void *arena, const float3 *uvw, cudaStream_t s
     plan_layout(p, off, &total);
     char *a = static_cast<char *>(arena);
     p->arena = arena;
-    p->rec = reinterpret_cast<VisRec *>(a + off[0]);
-    VisRec *rec_tmp = reinterpret_cast<VisRec *>(a + off[1]);
+    p->rec = a + off[0];
+    void *rec_tmp = a + off[1];
     p->perm = reinterpret_cast<int *>(a + off[2]);
     int *keys = reinterpret_cast<int *>(a + off[3]);
     int *counts = reinterpret_cast<int *>(a + off[4]);
@@ -754,6 +848,7 @@ int visplan_build(sdp_visplan *p, void *arena, const float3 *uvw, cudaStream_t s
     p->n_items = scalars;
     p->item_counter = scalars + 1;
     p->flags = scalars + 2;
+    p->kshare = scalars + 3;
     p->measured = reinterpret_cast<float2 *>(a + off[11]);
     p->gpoff = reinterpret_cast<int *>(a + off[12]);
     p->dpoff = reinterpret_cast<int *>(a + off[13]);
@@ -761,6 +856,7 @@ int visplan_build(sdp_visplan *p, void *arena, const float3 *uvw, cudaStream_t s
     p->dk2 = reinterpret_cast<float2 *>(a + off[15]);
     const int n = p->n;
 
+    SDP_CUDA_TRY(cudaMemsetAsync(scalars, 0, sizeof(int) * 4, st));
     // kernel tables: phase-major copies (or the caller's tables as they are)
     {
         const int os = p->geom.oversampling;
@@ -784,24 +880,45 @@ int visplan_build(sdp_visplan *p, void *arena, const float3 *uvw, cudaStream_t s
             }
             SDP_LAUNCH_CHECK();
         }
+        // is the degridding set the gridding set, or its conjugate, bit for bit?
+        const int related = p->phase_major && p->gk.num_kernels == p->dk.num_kernels;
+        const int nk = related ? p->gk.num_kernels : 1;
+        k_kernels_differ<<<dim3((per + 255) / 256, nk), 256, 0, st>>>(
+            reinterpret_cast<const int2 *>(p->gk.supports), reinterpret_cast<const int2 *>(p->dk.supports), p->gpoff,
+            p->dpoff, p->gk2, p->dk2, related, nk, os, per, p->kshare);
+        SDP_LAUNCH_CHECK();
     }
 
     SDP_CUDA_TRY(cudaMemsetAsync(counts, 0, sizeof(int) * ((size_t)p->nbins + 1), st));
-    SDP_CUDA_TRY(cudaMemsetAsync(scalars, 0, sizeof(int) * 4, st));
     if (n > 0) {
-        k_bin<<<(n + 255) / 256, 256, 0, st>>>(uvw, n, p->mode, p->geom.grid_size, p->geom.oversampling,
-                                               p->geom.uv_scale, p->geom.w_scale,
-                                               reinterpret_cast<const int2 *>(p->gk.supports),
-                                               reinterpret_cast<const int2 *>(p->dk.supports), p->gk.num_kernels,
-                                               p->dk.num_kernels, (long long)p->gk.total_samples,
-                                               (long long)p->dk.total_samples, p->hs_max, p->ntx, p->nty, rec_tmp,
-                                               keys, counts, p->flags);
+        const int2 *gs = reinterpret_cast<const int2 *>(p->gk.supports);
+        const int2 *ds = reinterpret_cast<const int2 *>(p->dk.supports);
+        if (p->coord_f64) {
+            k_bin<double><<<(n + 255) / 256, 256, 0, st>>>(
+                uvw, n, p->mode, p->snap, p->geom.grid_size, p->geom.oversampling, p->geom.uv_scale, p->geom.w_scale,
+                gs, ds, p->gk.num_kernels, p->dk.num_kernels, (long long)p->gk.total_samples,
+                (long long)p->dk.total_samples, p->hs_max, p->ntx, p->nty, static_cast<Rec<double> *>(rec_tmp), keys,
+                counts, p->flags);
+        } else {
+            k_bin<float><<<(n + 255) / 256, 256, 0, st>>>(
+                uvw, n, p->mode, p->snap, p->geom.grid_size, p->geom.oversampling, p->geom.uv_scale, p->geom.w_scale,
+                gs, ds, p->gk.num_kernels, p->dk.num_kernels, (long long)p->gk.total_samples,
+                (long long)p->dk.total_samples, p->hs_max, p->ntx, p->nty, static_cast<Rec<float> *>(rec_tmp), keys,
+                counts, p->flags);
+        }
         SDP_LAUNCH_CHECK();
     }
     SDP_TRY(exclusive_scan(counts, offsets, p->nbins, scan_scratch, st));
     SDP_CUDA_TRY(cudaMemsetAsync(counts, 0, sizeof(int) * ((size_t)p->nbins + 1), st));
     if (n > 0) {
-        k_scatter<<<(n + 255) / 256, 256, 0, st>>>(rec_tmp, keys, n, offsets, counts, p->rec, p->perm);
+        if (p->coord_f64)
+            k_scatter<double><<<(n + 255) / 256, 256, 0, st>>>(static_cast<const Rec<double> *>(rec_tmp), keys, n,
+                                                               offsets, counts, static_cast<Rec<double> *>(p->rec),
+                                                               p->perm);
+        else
+            k_scatter<float><<<(n + 255) / 256, 256, 0, st>>>(static_cast<const Rec<float> *>(rec_tmp), keys, n,
+                                                              offsets, counts, static_cast<Rec<float> *>(p->rec),
+                                                              p->perm);
         SDP_LAUNCH_CHECK();
     }
     k_item_counts<<<(p->ntiles + 255) / 256, 256, 0, st>>>(offsets, p->ntiles, p->nk, item_counts);
@@ -896,21 +1013,22 @@ SDP_EXPORT int sdp_visplan_set_measured(sdp_visplan *p, const sdp_float2 *measur
 
 namespace sdp {
 
-template <int LG>
+template <typename T, int LG>
 static int launch_tiles_lg(sdp_visplan *p, int op, const float2 *vis_in, const float2 *in_grid, float2 *out_grid,
                            float2 *pred, float2 *delta, cudaStream_t st)
 {
     PlanDev d = plan_dev(p);
     const size_t SS = (size_t)p->S * p->S;
-    const size_t smem = sizeof(float2) * SS * ((op != OP_GRID ? 1 : 0) + (op != OP_DEGRID ? 1 : 0));
+    const size_t smem = sizeof(float2) * SS * ((op != OP_GRID ? 1 : 0) + (op != OP_DEGRID ? 1 : 0)) +
+                        sizeof(int4) * (size_t)p->gk.num_kernels;
     void (*fn)(PlanDev, const float2 *, const float2 *, float2 *, float2 *, float2 *, const float2 *) = nullptr;
     const bool snapped = (p->mode == SDP_GRID_SNAPPED);
     switch (op) {
-    case OP_GRID: fn = snapped ? k_tiles<SDP_GRID_SNAPPED, OP_GRID, LG> : k_tiles<SDP_GRID_STD, OP_GRID, LG>; break;
-    case OP_DEGRID: fn = k_tiles<SDP_GRID_STD, OP_DEGRID, LG>; break;
-    case OP_CYCLE_CONV: fn = k_tiles<SDP_GRID_STD, OP_CYCLE_CONV, LG>; break;
-    case OP_CYCLE_NEAR: fn = k_tiles<SDP_GRID_STD, OP_CYCLE_NEAR, LG>; break;
-    case OP_G2G: fn = k_tiles<SDP_GRID_STD, OP_G2G, LG>; break;
+    case OP_GRID: fn = snapped ? k_tiles<T, SDP_GRID_SNAPPED, OP_GRID, LG> : k_tiles<T, SDP_GRID_STD, OP_GRID, LG>; break;
+    case OP_DEGRID: fn = k_tiles<T, SDP_GRID_STD, OP_DEGRID, LG>; break;
+    case OP_CYCLE_CONV: fn = k_tiles<T, SDP_GRID_STD, OP_CYCLE_CONV, LG>; break;
+    case OP_CYCLE_NEAR: fn = k_tiles<T, SDP_GRID_STD, OP_CYCLE_NEAR, LG>; break;
+    case OP_G2G: fn = k_tiles<T, SDP_GRID_STD, OP_G2G, LG>; break;
     default: return set_error(SDP_ERR_INVALID, "internal: op %d", op);
     }
     if (smem > 48 * 1024) SDP_CUDA_TRY(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
@@ -927,9 +1045,14 @@ static int launch_tiles(sdp_visplan *p, int op, const float2 *vis_in, const floa
                         float2 *pred, float2 *delta, cudaStream_t st)
 {
     // lanes per visibility: the tap columns (2 hs + 1 at most) in at most two passes
-    if (2 * p->hs_max <= 8) return launch_tiles_lg<8>(p, op, vis_in, in_grid, out_grid, pred, delta, st);
-    if (2 * p->hs_max <= 16) return launch_tiles_lg<16>(p, op, vis_in, in_grid, out_grid, pred, delta, st);
-    return launch_tiles_lg<32>(p, op, vis_in, in_grid, out_grid, pred, delta, st);
+    if (p->coord_f64) {
+        if (2 * p->hs_max <= 8) return launch_tiles_lg<double, 8>(p, op, vis_in, in_grid, out_grid, pred, delta, st);
+        if (2 * p->hs_max <= 16) return launch_tiles_lg<double, 16>(p, op, vis_in, in_grid, out_grid, pred, delta, st);
+        return launch_tiles_lg<double, 32>(p, op, vis_in, in_grid, out_grid, pred, delta, st);
+    }
+    if (2 * p->hs_max <= 8) return launch_tiles_lg<float, 8>(p, op, vis_in, in_grid, out_grid, pred, delta, st);
+    if (2 * p->hs_max <= 16) return launch_tiles_lg<float, 16>(p, op, vis_in, in_grid, out_grid, pred, delta, st);
+    return launch_tiles_lg<float, 32>(p, op, vis_in, in_grid, out_grid, pred, delta, st);
 }
 
 }  // namespace sdp
@@ -937,7 +1060,7 @@ static int launch_tiles(sdp_visplan *p, int op, const float2 *vis_in, const floa
 SDP_EXPORT int sdp_visplan_grid(sdp_visplan *p, const sdp_float2 *vis, sdp_float2 *grid, int accumulate, void *stream)
 {
     SDP_CHECK_ARG(p && grid && (vis || p->n == 0), "NULL argument");
-    SDP_CHECK_ARG(p->mode != 2, "plan was built for g2g; use sdp_visplan_g2g");
+    SDP_CHECK_ARG(p->mode != kPlanG2G, "plan was built for g2g; use sdp_visplan_g2g");
     cudaStream_t st = as_stream(stream);
     const size_t G2 = (size_t)p->geom.grid_size * p->geom.grid_size;
     if (!accumulate) SDP_CUDA_TRY(cudaMemsetAsync(grid, 0, sizeof(float2) * G2, st));
@@ -981,7 +1104,7 @@ SDP_EXPORT int sdp_visplan_cycle(sdp_visplan *p, const sdp_float2 *model_grid, i
 SDP_EXPORT int sdp_visplan_g2g(sdp_visplan *p, const sdp_float2 *in_grid, sdp_float2 *out_grid, void *stream)
 {
     SDP_CHECK_ARG(p && in_grid && out_grid, "NULL argument");
-    SDP_CHECK_ARG(p->mode == 2, "plan was not built for g2g");
+    SDP_CHECK_ARG(p->mode == kPlanG2G, "plan was not built for g2g");
     cudaStream_t st = as_stream(stream);
     const size_t G2 = (size_t)p->geom.grid_size * p->geom.grid_size;
     SDP_CUDA_TRY(cudaMemsetAsync(out_grid, 0, sizeof(float2) * G2, st));

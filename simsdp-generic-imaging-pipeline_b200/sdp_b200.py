@@ -453,6 +453,66 @@ class VisPlan:
         check(self.lib.sdp_visplan_check(self.handle, _stream(stream)), self.lib)
 
 
+SDP_COORD_F32 = 0
+SDP_COORD_F64 = 1
+SDP_PLAN_COORD_F64 = 0x100
+SDP_PLAN_SNAP = 0x200
+
+
+class PipelineConfig(C.Structure):
+    _fields_ = [("grid_size", _i), ("oversampling", _i), ("uv_scale", _d), ("w_scale", _d), ("cell_size", _d),
+                ("num_minor_cycles", _i), ("max_sources", _i), ("loop_gain", _d), ("noise_factor", _d),
+                ("weak_source_percent", _d), ("psf_max_value", _d), ("degrid_mode", _i), ("coord_mode", _i),
+                ("snap", _i), ("use_graph", _i)]
+
+
+class Pipeline:
+    """Owns an sdp_pipeline: the device-resident FFT-pipeline major cycle."""
+
+    def __init__(self, lib, cfg: PipelineConfig, gk: WKernels, dk: WKernels | None, uvw, measured, psf,
+                 stream=None, keep=()):
+        self.lib = lib
+        self.cfg = cfg
+        self._keep = keep
+        self.handle = _p()
+        self.G = cfg.grid_size
+        check(lib.sdp_pipeline_create(C.byref(self.handle), C.byref(cfg), C.byref(gk),
+                                      C.byref(dk) if dk is not None else None, _i(int(uvw.shape[0])), _dp(uvw),
+                                      _dp(measured), _dp(psf), _stream(stream)), lib)
+
+    def major_cycle(self, stream=None):
+        check(self.lib.sdp_pipeline_major_cycle(self.handle, _stream(stream)), self.lib)
+
+    def graph_active(self) -> bool:
+        return bool(self.lib.sdp_pipeline_graph_active(self.handle))
+
+    def graph_error(self) -> str:
+        self.lib.sdp_pipeline_graph_error.restype = C.c_char_p
+        return self.lib.sdp_pipeline_graph_error(self.handle).decode()
+
+    def outputs(self, stream=None):
+        """(residual image, model image, components (n, 3), n) as numpy."""
+        G = self.G
+        res = np.empty(G * G, dtype=np.float32)
+        model = np.empty(G * G, dtype=np.float32)
+        src = np.zeros((max(1, self.cfg.max_sources), 3), dtype=np.float32)
+        n = C.c_int(0)
+        check(self.lib.sdp_pipeline_copy_outputs(self.handle, _ptr(res), _ptr(model), _ptr(src), C.byref(n),
+                                                 _stream(stream)), self.lib)
+        return res, model, src[: max(0, n.value)].copy(), n.value
+
+    def close(self):
+        if self.handle:
+            check(self.lib.sdp_pipeline_destroy(self.handle), self.lib)
+            self.handle = _p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
 class Device:
     """Device-resident layer over torch CUDA tensors."""
 
@@ -469,6 +529,10 @@ class Device:
              mode=SDP_GRID_STD, stream=None, keep=()) -> VisPlan:
         geom = Geometry(grid_size, oversampling, uv_scale, w_scale)
         return VisPlan(self.lib, geom, gk, dk, uvw, mode, stream, keep)
+
+    def pipeline(self, cfg: PipelineConfig, uvw, measured, psf, gk: WKernels, dk: WKernels | None = None,
+                 stream=None, keep=()) -> Pipeline:
+        return Pipeline(self.lib, cfg, gk, dk, uvw, measured, psf, stream, keep)
 
     def degrid_nearest(self, grid_size, uv_scale, uvw, grid, out, stream=None):
         check(self.lib.sdp_degrid_nearest(_i(grid_size), _d(uv_scale), _i(uvw.shape[0]), _dp(uvw), _dp(grid),
