@@ -23,6 +23,8 @@
 // completion counter) applies the stopping rule and records the component.
 // After a stop every later launch returns at once, so a fixed number of
 // launches can be captured in a CUDA graph.
+#include <cuda/atomic>
+
 #include <algorithm>
 
 #include "internal.cuh"
@@ -283,31 +285,34 @@ __global__ void k_clean_finish(int G, double cell, int max_records, float3 *__re
 // One CTA per SM (cooperative launch, so all CTAs are resident), each owning
 // a contiguous slice of pixels.  A minor cycle: apply the pending component
 // to the slice, reduce (max |r|, first index, signed value, sum |r|) per
-// block, publish it (double-buffered by cycle parity), one grid barrier,
-// then every block reduces all block results in the same order and takes
-// the same decision, so no second barrier is needed.  Block 0 records the
-// component and updates the model.  The barrier waits are bounded: after
-// kBarrierSpins sleeps a block sets an error flag, every block leaves at its
-// next barrier, and the host reads SDP_ERR_TIMEOUT.
+// block and publish it with a release-stored flag (results double-buffered
+// by cycle parity).  Warp 0 of every block then waits for all blocks' flags
+// (acquire loads, no shared counter), reduces the results in the same order
+// and takes the same decision, so the blocks stay in step without a second
+// barrier.  Block 0 records the component and adds it to the model while
+// the next minor cycle runs.  Waits are bounded: after kBarrierSpins polls a
+// block sets an error flag, every block stops at its next wait, and the host
+// reads SDP_ERR_TIMEOUT.
 // ---------------------------------------------------------------------------
 struct PPart {
-    float amax;
-    int idx;
-    float val;
+    float amax;  // max |r| of the block's slice
+    int idx;     // its first pixel index
+    float val;   // r there (signed)
+    int flag;    // minor cycle + 1 once the fields above are written
+    double sum;  // sum of |r| over the slice
+    float a0;    // |r[0]| (block 0): the running mean skips index 0
     int pad;
-    double sum;
 };
 
 struct CleanBar {
-    unsigned count;
-    unsigned gen;
     int err;
-    int pad;
+    int pad[15];
 };
 
 constexpr int kPersistThreads = 1024;
-constexpr int kPersistSlice = 51200;            // floats of residual per block (200 KB)
-constexpr long long kBarrierSpins = 16000000;   // x ~64 ns sleeps: about one second
+constexpr int kPersistSlice = 51200;           // floats of residual per block (200 KB)
+constexpr int kBatch = 8;                      // pixels per thread whose PSF loads are in flight together
+constexpr long long kBarrierSpins = 4000000;   // polls of ~32 ns sleep + an L2 read: one to two seconds
 
 __device__ __forceinline__ void better3(float &v, int &i, float &sv, float v2, int i2, float sv2)
 {
@@ -318,42 +323,26 @@ __device__ __forceinline__ void better3(float &v, int &i, float &sv, float v2, i
     }
 }
 
-// Bounded grid barrier (sense by generation).  Returns false after a timeout
-// or when another block has timed out.
-__device__ bool grid_sync(CleanBar *bar, unsigned nblocks, unsigned &gen, long long spin_limit)
+// Waits (one warp) until the results of blocks 0..nb-1 in buf carry flag
+// `target`.  Bounded: after spin_limit polls of one flag, or once another
+// block has timed out, it sets bar->err and returns false.
+__device__ bool wait_results(PPart *buf, int nb, int target, CleanBar *bar, long long spin_limit)
 {
-    __shared__ int s_ok;
-    __syncthreads();
-    if (threadIdx.x == 0) {
-        __threadfence();
-        const unsigned g = gen;
-        int ok = 1;
-        if (atomicAdd(&bar->count, 1u) == nblocks - 1) {
-            atomicExch(&bar->count, 0u);
-            __threadfence();
-            atomicAdd(&bar->gen, 1u);
-        } else {
-            long long spins = 0;
-            while (atomicAdd(&bar->gen, 0u) == g) {
-                if (atomicAdd(&bar->err, 0) != 0) {
-                    ok = 0;
-                    break;
-                }
-                if (++spins > spin_limit) {
-                    atomicExch(&bar->err, 1);
-                    ok = 0;
-                    break;
-                }
-                __nanosleep(64);
+    cuda::atomic_ref<int, cuda::thread_scope_device> err(bar->err);
+    int fail = 0;
+    for (int b = (int)(threadIdx.x & 31); b < nb && !fail; b += 32) {
+        cuda::atomic_ref<int, cuda::thread_scope_device> flag(buf[b].flag);
+        long long spins = 0;
+        while (flag.load(cuda::memory_order_acquire) != target) {
+            if (err.load(cuda::memory_order_relaxed) != 0 || ++spins > spin_limit) {
+                err.store(1, cuda::memory_order_relaxed);
+                fail = 1;
+                break;
             }
+            __nanosleep(32);
         }
-        __threadfence();
-        if (atomicAdd(&bar->err, 0) != 0) ok = 0;
-        s_ok = ok;
     }
-    __syncthreads();
-    gen += 1;
-    return s_ok != 0;
+    return !__any_sync(0xffffffffu, fail);
 }
 
 __device__ __forceinline__ void block_reduce3(float &bv, int &bi, float &bs, double &sum)
@@ -402,57 +391,59 @@ __global__ void __launch_bounds__(kPersistThreads, 1) k_clean_persistent(
     long long spin_limit)
 {
     extern __shared__ float sr[];
-    __shared__ int s_pending, s_mx, s_my, s_stop;
+    __shared__ int s_pending, s_mx, s_my, s_stop, s_fail;
     __shared__ float s_val;
     const int tid = threadIdx.x;
-    const unsigned nb = gridDim.x;
-    const long long g2 = (long long)G * G;
-    const long long p0 = (long long)blockIdx.x * P;
-    const int n = (int)max(0LL, min(p0 + P, g2) - p0);
+    const int nb = (int)gridDim.x;
+    const int g2 = G * G;  // the persistent path holds G <= 2752 images
+    const int p0 = blockIdx.x * P;
+    const int n = max(0, min(p0 + P, g2) - p0);
     for (int k = tid; k < n; k += kPersistThreads) sr[k] = r[p0 + k];
     if (tid == 0) {
         s_pending = 0;
         s_stop = 0;
+        s_fail = 0;
         s_mx = 0;
         s_my = 0;
         s_val = 0.f;
     }
     __syncthreads();
-    unsigned gen = 0;
     int count = 0;
     float first_z = 0.f;
+    int model_idx = -1;  // block 0, thread 0: component not yet added to the model
+    double model_add = 0.0;
     const int half = G / 2;
     const int step_y = kPersistThreads / G, step_x = kPersistThreads - (kPersistThreads / G) * G;
-    bool ok = true;
     for (int it = 0; it <= num_minor; ++it) {
         const bool apply_only = (it == num_minor);
         const int pending = s_pending, mx = s_mx, my = s_my;
         const double scale = __dmul_rn(gain, (double)s_val);
-        const int x0 = mx - min(mx, half), x1 = mx + min(G - mx, half);
-        const int y0 = my - min(my, half), y1 = my + min(G - my, half);
+        const int x0 = mx - min(mx, half), wx = min(mx, half) + min(G - mx, half);
+        const int y0 = my - min(my, half), wy = min(my, half) + min(G - my, half);
+        // PSF sample of pixel (y, x): psf[(y - my + G/2) G + (G - (x - mx + G/2))]
+        // (x-mirrored; column G runs into the next PSF row, and past the
+        // last row reads as 0), i.e. psf[y G - x + pofs]
+        const int pofs = (half - my) * G + G + mx - half;
         float bv = -1.f, bs = 0.f;
         int bi = 0x7fffffff;
-        double sum = 0.0;
-        // pixel k = tid + m * kPersistThreads of the slice; (y, x) advanced
-        // incrementally, four pixels' PSF loads in flight per thread
-        int i = (int)p0 + tid;
-        int y = i / G, x = i - y * G;
-        for (int k = tid; k < n; k += 4 * kPersistThreads) {
-            float v[4], pv[4];
-            int ii[4];
-            bool in[4];
+        // pixel k = tid + m * 1024 of the slice, (y, x) advanced
+        // incrementally; kBatch pixels at a time, their PSF loads issued
+        // together so the L2 latency is paid once per batch
+        int y = (p0 + tid) / G, x = (p0 + tid) - y * G;
+        float rsum = 0.f;
+        for (int kb = tid; kb < n; kb += kBatch * kPersistThreads) {
+            float w[kBatch], pv[kBatch];
+            int ii[kBatch];
+            bool in[kBatch];
 #pragma unroll
-            for (int u = 0; u < 4; ++u) {
-                const bool live = k + u * kPersistThreads < n;
-                ii[u] = i;
-                v[u] = live ? sr[k + u * kPersistThreads] : 0.f;
-                in[u] = live && pending && y >= y0 && y < y1 && x >= x0 && x < x1;
-                pv[u] = 0.f;
-                if (in[u]) {
-                    const long long pi = (long long)(y - my + half) * G + (G + mx - half) - x;
-                    if (pi < g2) pv[u] = __ldg(&psf[pi]);
-                }
-                i += kPersistThreads;
+            for (int u = 0; u < kBatch; ++u) {
+                const int k = kb + u * kPersistThreads;
+                const bool live = k < n;
+                ii[u] = y * G + x;
+                w[u] = live ? sr[k] : 0.f;
+                in[u] = live && pending && (unsigned)(y - y0) < (unsigned)wy && (unsigned)(x - x0) < (unsigned)wx;
+                const int pi = ii[u] - 2 * x + pofs;
+                pv[u] = (in[u] && pi < g2) ? __ldg(&psf[pi]) : 0.f;
                 x += step_x;
                 y += step_y;
                 if (x >= G) {
@@ -461,67 +452,103 @@ __global__ void __launch_bounds__(kPersistThreads, 1) k_clean_persistent(
                 }
             }
 #pragma unroll
-            for (int u = 0; u < 4; ++u) {
-                if (k + u * kPersistThreads >= n) break;
-                float w = v[u];
+            for (int u = 0; u < kBatch; ++u) {
+                float wv = w[u];
                 if (in[u]) {
-                    w = __double2float_rn(__dsub_rn((double)w, __dmul_rn(__dmul_rn(scale, (double)pv[u]), psf_max)));
-                    sr[k + u * kPersistThreads] = w;
+                    wv = __double2float_rn(__dsub_rn((double)wv, __dmul_rn(__dmul_rn(scale, (double)pv[u]), psf_max)));
+                    sr[kb + u * kPersistThreads] = wv;
                 }
-                if (!apply_only) {
-                    const float a = fabsf(w);
-                    better3(bv, bi, bs, a, ii[u], w);
-                    if (ii[u] >= 1) sum += (double)a;
+                const float a = fabsf(wv);
+                if (a > bv) {  // pixels visited in increasing index: the first maximum wins
+                    bv = a;
+                    bi = ii[u];
+                    bs = wv;
                 }
+                rsum += a;  // 0 for the padding past the slice
             }
         }
         if (apply_only) break;
+        double sum = (double)rsum;
         block_reduce3(bv, bi, bs, sum);
         PPart *buf = parts + (size_t)(it & 1) * nb;
-        if (tid == 0) buf[blockIdx.x] = PPart{bv, bi, bs, 0, sum};
-        if (!grid_sync(bar, nb, gen, spin_limit)) {
-            ok = false;
-            break;
-        }
-        // every block reduces all block results identically
-        bv = -1.f;
-        bi = 0x7fffffff;
-        bs = 0.f;
-        sum = 0.0;
-        for (unsigned b = tid; b < nb; b += kPersistThreads) {
-            const PPart *pq = buf + b;
-            better3(bv, bi, bs, __ldcg(&pq->amax), __ldcg(&pq->idx), __ldcg(&pq->val));
-            sum += __ldcg(&pq->sum);
-        }
-        block_reduce3(bv, bi, bs, sum);
         if (tid == 0) {
-            float curr_max = bv;
-            int idx = bi;
-            float sval = bs;
-            if (curr_max <= 0.f) {  // all zero (or empty): the reference keeps index 0
-                curr_max = 0.f;
-                idx = 0;
-                sval = 0.f;
+            PPart *mine = buf + blockIdx.x;
+            mine->amax = bv;
+            mine->idx = bi;
+            mine->val = bs;
+            mine->sum = sum;
+            mine->a0 = (blockIdx.x == 0 && n > 0) ? fabsf(sr[0]) : 0.f;
+            cuda::atomic_ref<int, cuda::thread_scope_device>(mine->flag).store(it + 1, cuda::memory_order_release);
+            // block 0 adds the previous component to the model here, off the
+            // critical path (model updates keep the reference's order)
+            if (model_idx >= 0) {
+                model[model_idx] = __double2float_rn(__dadd_rn((double)model[model_idx], model_add));
+                model_idx = -1;
             }
-            const float avg = (g2 > 1) ? (float)(sum / (double)(g2 - 1)) : 0.f;
-            const bool extracting_noise = (double)fabsf(curr_max) < noise * (double)avg * gain;            // :238
-            const bool weak_source = count > 0 && (double)fabsf(curr_max) < (double)fabsf(first_z) * weak;  // :239
-            if (extracting_noise || weak_source) {
-                s_stop = 1;
-                s_pending = 0;
-            } else {
-                const float max_val = __double2float_rn(__ddiv_rn((double)sval, psf_max));  // :247
-                const float z = __double2float_rn(__dmul_rn((double)max_val, gain));
-                if (count == 0) first_z = z;
-                if (blockIdx.x == 0) {
-                    if (count < max_records) src[count] = make_float3((float)(idx % G), (float)(idx / G), z);
-                    model[idx] = __double2float_rn(__dadd_rn((double)model[idx], __dmul_rn((double)max_val, gain)));
+        }
+        // warp 0 of every block waits for every block's result of this
+        // minor cycle, reduces them in the same order and takes the same
+        // decision
+        if (tid < 32) {
+            bv = -1.f;
+            bi = 0x7fffffff;
+            bs = 0.f;
+            sum = 0.0;
+            float a0 = 0.f;
+            const int fail = wait_results(buf, nb, it + 1, bar, spin_limit) ? 0 : 1;
+            if (!fail)
+                for (int b = tid; b < nb; b += 32) {
+                    const PPart *pq = buf + b;
+                    better3(bv, bi, bs, __ldcg(&pq->amax), __ldcg(&pq->idx), __ldcg(&pq->val));
+                    sum += __ldcg(&pq->sum);
+                    if (b == 0) a0 = __ldcg(&pq->a0);
                 }
-                count += 1;
-                s_pending = 1;
-                s_mx = idx % G;
-                s_my = idx / G;
-                s_val = max_val;
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1) {
+                const float v2 = __shfl_xor_sync(0xffffffffu, bv, o);
+                const int i2 = __shfl_xor_sync(0xffffffffu, bi, o);
+                const float s2 = __shfl_xor_sync(0xffffffffu, bs, o);
+                better3(bv, bi, bs, v2, i2, s2);
+                sum += __shfl_xor_sync(0xffffffffu, sum, o);
+            }
+            a0 = __shfl_sync(0xffffffffu, a0, 0);
+            if (tid == 0) {
+                if (fail) {
+                    s_fail = 1;
+                    s_stop = 1;
+                    s_pending = 0;
+                } else {
+                    float curr_max = bv;
+                    int idx = bi;
+                    float sval = bs;
+                    if (curr_max <= 0.f) {  // all zero (or empty): the reference keeps index 0
+                        curr_max = 0.f;
+                        idx = 0;
+                        sval = 0.f;
+                    }
+                    const float avg = (g2 > 1) ? (float)(__dsub_rn(sum, (double)a0) / (double)(g2 - 1)) : 0.f;
+                    const bool extracting_noise = (double)fabsf(curr_max) < noise * (double)avg * gain;  // :238
+                    const bool weak_source =
+                        count > 0 && (double)fabsf(curr_max) < (double)fabsf(first_z) * weak;  // :239
+                    if (extracting_noise || weak_source) {
+                        s_stop = 1;
+                        s_pending = 0;
+                    } else {
+                        const float max_val = __double2float_rn(__ddiv_rn((double)sval, psf_max));  // :247
+                        const float z = __double2float_rn(__dmul_rn((double)max_val, gain));
+                        if (count == 0) first_z = z;
+                        if (blockIdx.x == 0) {
+                            if (count < max_records) src[count] = make_float3((float)(idx % G), (float)(idx / G), z);
+                            model_idx = idx;  // :256, added after the next publish
+                            model_add = __dmul_rn((double)max_val, gain);
+                        }
+                        count += 1;
+                        s_pending = 1;
+                        s_mx = idx % G;
+                        s_my = idx / G;
+                        s_val = max_val;
+                    }
+                }
             }
         }
         __syncthreads();
@@ -529,6 +556,7 @@ __global__ void __launch_bounds__(kPersistThreads, 1) k_clean_persistent(
     }
     __syncthreads();
     for (int k = tid; k < n; k += kPersistThreads) r[p0 + k] = sr[k];
+    if (model_idx >= 0) model[model_idx] = __double2float_rn(__dadd_rn((double)model[model_idx], model_add));
     if (blockIdx.x == 0 && tid == 0) {
         const int nrec = min(count, max_records);
         for (int k = 0; k < nrec; ++k) {  // :297-306
@@ -537,18 +565,18 @@ __global__ void __launch_bounds__(kPersistThreads, 1) k_clean_persistent(
             q.y = __double2float_rn(__dmul_rn((double)__fsub_rn(q.y, (float)(G / 2)), cell));
             src[k] = q;
         }
-        if (count_out) *count_out = ok ? nrec : -1;
+        if (count_out) *count_out = s_fail ? -1 : nrec;
     }
 }
 
-// Bounded-wait self test: a barrier that one block never reaches.  Every
-// waiting block gives up after spin_limit sleeps and the kernel ends with
-// the error flag set (the host reads SDP_ERR_TIMEOUT).
-__global__ void k_barrier_timeout_probe(CleanBar *bar, long long spin_limit)
+// Bounded-wait self test: every block publishes its result and waits for
+// one more block than there are.  Each gives up after spin_limit polls and
+// the kernel ends with the error flag set (the host reads SDP_ERR_TIMEOUT).
+__global__ void k_wait_timeout_probe(PPart *parts, CleanBar *bar, long long spin_limit)
 {
-    unsigned gen = 0;
-    // gridDim.x blocks wait for gridDim.x + 1 arrivals: the last one never comes
-    grid_sync(bar, gridDim.x + 1, gen, spin_limit);
+    if (threadIdx.x == 0)
+        cuda::atomic_ref<int, cuda::thread_scope_device>(parts[blockIdx.x].flag).store(1, cuda::memory_order_release);
+    if (threadIdx.x < 32) wait_results(parts, (int)gridDim.x + 1, 1, bar, spin_limit);
 }
 
 static void persist_layout(int nb, size_t base, size_t *bar_off, size_t *parts_off, size_t *total)
@@ -620,6 +648,7 @@ int sdp::hogbom_launch(const sdp_clean_params *p, float *residual, const float *
         SDP_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, kPersistThreads, smem));
         if (per_sm >= 1) {
             SDP_CUDA_TRY(cudaMemsetAsync(bar, 0, sizeof(CleanBar), st));
+            SDP_CUDA_TRY(cudaMemsetAsync(parts, 0, sizeof(PPart) * 2 * (size_t)pnb, st));
             int Gv = G, nminor = p->num_minor_cycles, maxr = cap;
             double gain = p->loop_gain, noise = p->noise_factor, weak = p->weak_source_percent,
                    pmax = p->psf_max_value, cell = p->cell_size;
@@ -662,17 +691,21 @@ SDP_EXPORT int sdp_selftest_bounded_wait(int nblocks, long long spin_limit, int 
 {
     SDP_CHECK_ARG(status != nullptr && nblocks >= 1 && nblocks <= 64 && spin_limit >= 1, "bad argument");
     *status = SDP_OK;
-    CleanBar *bar = nullptr;
-    SDP_CUDA_TRY(cudaMalloc(&bar, sizeof(CleanBar)));
+    // one allocation: the error flag, then nblocks + 1 result slots
+    const size_t bytes = 64 + sizeof(PPart) * ((size_t)nblocks + 1);
+    char *mem = nullptr;
+    SDP_CUDA_TRY(cudaMalloc(&mem, bytes));
+    CleanBar *bar = reinterpret_cast<CleanBar *>(mem);
+    PPart *parts = reinterpret_cast<PPart *>(mem + 64);
     int err = 0;
-    cudaError_t e = cudaMemset(bar, 0, sizeof(CleanBar));
+    cudaError_t e = cudaMemset(mem, 0, bytes);
     if (e == cudaSuccess) {
-        k_barrier_timeout_probe<<<nblocks, 32>>>(bar, spin_limit);
+        k_wait_timeout_probe<<<nblocks, 32>>>(parts, bar, spin_limit);
         e = cudaGetLastError();
     }
     if (e == cudaSuccess) e = cudaDeviceSynchronize();
     if (e == cudaSuccess) e = cudaMemcpy(&err, &bar->err, sizeof(int), cudaMemcpyDeviceToHost);
-    cudaFree(bar);
+    cudaFree(mem);
     if (e != cudaSuccess) return cuda_error(e, "bounded-wait self test");
     *status = err ? SDP_ERR_TIMEOUT : SDP_OK;
     return SDP_OK;

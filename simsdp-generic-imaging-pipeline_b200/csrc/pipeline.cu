@@ -37,6 +37,7 @@ struct sdp_pipeline {
     cudaEvent_t ev_in = nullptr, ev_out = nullptr;
     int graph_failed = 0;
     int in_capture = 0;
+    int capture_persistent = 1;  // capture CLEAN as the cooperative kernel (first attempt)
     int cycles_run = 0;
     char graph_error[256] = {0};
 };
@@ -58,10 +59,10 @@ static int run_cycle(sdp_pipeline *p, cudaStream_t st)
                                      cudaMemcpyDeviceToDevice, st));
         sdp_clean_params cp{G, c.num_minor_cycles, c.max_sources, c.loop_gain, c.noise_factor,
                             c.weak_source_percent, c.psf_max_value, c.cell_size};
-        // inside a graph capture CLEAN runs as one launch per minor cycle
-        // (the persistent cooperative kernel is launched directly otherwise)
+        // the persistent cooperative kernel, or one launch per minor cycle
+        // when a capture of the cooperative launch was refused
         SDP_TRY(hogbom_launch(&cp, p->clean_scratch, p->psf, p->model_image, p->sources, p->num_sources,
-                              p->clean_ws, p->clean_ws_bytes, !p->in_capture, st));
+                              p->clean_ws, p->clean_ws_bytes, !p->in_capture || p->capture_persistent, st));
     }
     return SDP_OK;
 }
@@ -181,7 +182,10 @@ SDP_EXPORT int sdp_pipeline_major_cycle(sdp_pipeline *p, void *stream)
     cudaStream_t st = p->stream;
     SDP_CUDA_TRY(cudaEventRecord(p->ev_in, caller));
     SDP_CUDA_TRY(cudaStreamWaitEvent(st, p->ev_in, 0));
-    if (p->cfg.use_graph && !p->graph_failed && !p->graph) {
+    // first with CLEAN as the cooperative kernel, then with one launch per
+    // minor cycle, then eagerly
+    for (int attempt = 0; attempt < 2 && p->cfg.use_graph && !p->graph_failed && !p->graph; ++attempt) {
+        p->capture_persistent = attempt == 0;
         cudaGraph_t g = nullptr;
         cudaError_t e = cudaStreamBeginCapture(st, cudaStreamCaptureModeRelaxed);
         int status = SDP_OK;
@@ -200,12 +204,15 @@ SDP_EXPORT int sdp_pipeline_major_cycle(sdp_pipeline *p, void *stream)
         }
         if (g) cudaGraphDestroy(g);
         if (e != cudaSuccess || status != SDP_OK || !p->graph) {
-            // capture refused (or a launch inside it failed): run eagerly from now on
             snprintf(p->graph_error, sizeof(p->graph_error), "%s: %s", where,
                      e != cudaSuccess ? cudaGetErrorString(e) : "launch failed during capture");
             cudaGetLastError();
             sdp_clear_error();
             p->graph = nullptr;
+            // (the message of a refused first attempt stays readable through
+            // sdp_pipeline_graph_error when the second succeeds)
+            if (attempt == 0) continue;
+            // capture refused (or a launch inside it failed): run eagerly from now on
             p->graph_failed = 1;
         }
     }

@@ -688,7 +688,9 @@ __global__ void k_gather_sorted(const float2 *__restrict__ src, const int *__res
                                 float2 *__restrict__ dst)
 {
     int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i < n) dst[i] = src[perm[i]];
+    if (i >= n) return;
+    const int j = perm[i];  // -1 past the binned records (visibilities flagged out of the tables)
+    dst[i] = (j >= 0 && j < n) ? src[j] : make_float2(0.f, 0.f);
 }
 
 __global__ void k_fill_zero2(float2 *p, size_t n)
@@ -910,6 +912,7 @@ int visplan_build(sdp_visplan *p, void *arena, const float3 *uvw, cudaStream_t s
     }
     SDP_TRY(exclusive_scan(counts, offsets, p->nbins, scan_scratch, st));
     SDP_CUDA_TRY(cudaMemsetAsync(counts, 0, sizeof(int) * ((size_t)p->nbins + 1), st));
+    if (n > 0) SDP_CUDA_TRY(cudaMemsetAsync(p->perm, 0xff, sizeof(int) * (size_t)n, st));  // unbinned slots: -1
     if (n > 0) {
         if (p->coord_f64)
             k_scatter<double><<<(n + 255) / 256, 256, 0, st>>>(static_cast<const Rec<double> *>(rec_tmp), keys, n,
