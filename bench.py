@@ -39,6 +39,7 @@ ROOT = Path(__file__).resolve().parent
 PKG = ROOT / "simsdp-generic-imaging-pipeline_b200"
 sys.path.insert(0, str(PKG))
 
+import channels  # noqa: E402
 import synth  # noqa: E402
 
 METRIC = "vis/s gridded+degridded"
@@ -358,10 +359,7 @@ def b200_arm(args):
         dist.barrier()
     step_ms = [s.elapsed_time(e) for s, e in zip(starts, ends)]
     t_step = sum(step_ms) / len(step_ms)
-    t_max = torch.tensor([t_step], dtype=torch.float64, device=dev)
-    if world > 1:
-        dist.all_reduce(t_max, op=dist.ReduceOp.MAX)
-    t_step = float(t_max.item())
+    t_step = channels.max_over_ranks(t_step, device=dev)
     value = world * N / (t_step * 1e-3)
 
     # ---- roofline of the dominant kernel (the fused tile kernel) -----------------------
