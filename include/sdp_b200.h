@@ -424,10 +424,12 @@ int sdp_pipeline_visplan(sdp_pipeline *p, sdp_visplan **plan);
 int sdp_pipeline_destroy(sdp_pipeline *p);
 
 /* Failure-detection self test (no counterpart in the reference): launches
- * nblocks (1..64) blocks that wait at a grid barrier one arrival short of
- * complete.  Each wait gives up after spin_limit sleeps of about 64 ns, so
- * the kernel ends; *status receives SDP_ERR_TIMEOUT when the bounded wait
- * reported the timeout (the expected result), SDP_OK otherwise. */
+ * nblocks (1..64) blocks that each publish a result and wait, with the wait
+ * the persistent CLEAN kernel uses, for one result more than there are
+ * blocks.  Each wait gives up after spin_limit polls (a ~32 ns sleep and an
+ * L2 read each), so the kernel ends; *status receives SDP_ERR_TIMEOUT when
+ * the bounded wait reported the timeout (the expected result), SDP_OK
+ * otherwise. */
 int sdp_selftest_bounded_wait(int nblocks, long long spin_limit, int *status);
 
 #ifdef __cplusplus
