@@ -56,6 +56,7 @@ def parse():
     ap.add_argument("--e2e-steps", type=int, default=3)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-major-cycle", action="store_true")
+    ap.add_argument("--no-c3", action="store_true", help="skip the batched 64-channel pass")
     ap.add_argument("--cpu-sample", type=int, default=200_000, help="visibilities per CPU-baseline step")
     return ap.parse_args()
 
@@ -278,6 +279,80 @@ def snap_host(w):
 # ---------------------------------------------------------------------------
 # B200 arm
 # ---------------------------------------------------------------------------
+def c3_block(S, D, dev, reps: int = 5):
+    """The batched multi-channel workload: the 256-antenna layout at 64
+    channels over 100-200 MHz, seeded per-channel flag fractions of 0-60 %
+    (uneven visibility counts), 32 w-planes of half support 4, OS 16, one
+    2048^2 grid per channel.  All channels' fused passes run in one
+    persistent launch (sdp_visbatch); the same passes as 64 separate plan
+    launches are timed beside it.  Inputs resident in HBM (4+ GB, larger than
+    L2)."""
+    import torch
+
+    nch, f_lo, f_hi = 64, 100e6, 200e6
+    base = synth.make_workload("c3_base", 256, 5000.0, "spiral", 120, 2048, 1, 1e-3, 1.0, 1e-4, 32, 4,
+                               freq_hz=f_hi, seed=3, compute_vis=False)
+    G, OS = base.cfg.grid_size, base.cfg.oversampling
+    n_full = base.num_vis
+    counts = channels.flagged_counts(nch, n_full, seed=11)
+    gk = torch.from_numpy(base.gkernels).to(dev)
+    dk = torch.from_numpy(base.dkernels).to(dev)
+    sup = torch.from_numpy(base.supports).to(dev)
+    wk_g = S.Device.wkernels(gk, sup, base.supports)
+    wk_d = S.Device.wkernels(dk, sup, base.supports)
+    uvw_top = torch.from_numpy(base.uvw).to(dev)
+    plans, resid, keep = [], [], []
+    gen = torch.Generator(device=dev)
+    for c in range(nch):
+        f = f_lo + (f_hi - f_lo) * c / (nch - 1)
+        gen.manual_seed(1000 + c)
+        sel = torch.randperm(n_full, device=dev, generator=gen)[:counts[c]].sort().values
+        uvw = (uvw_top[sel] * (f / f_hi)).contiguous()
+        meas = 0.1 * torch.randn((counts[c], 2), device=dev, generator=gen)
+        pl = D.plan(G, OS, base.cfg.uv_scale, base.cfg.w_scale, uvw, wk_g, wk_d, keep=(uvw, gk, dk, sup))
+        pl.set_measured(meas)
+        plans.append(pl)
+        resid.append(torch.empty((G * G, 2), dtype=torch.float32, device=dev))
+        keep.append(meas)
+    del uvw_top
+    model = (1e-3 * torch.randn((G * G, 2), device=dev, generator=gen)).contiguous()
+    batch = D.batch(plans)
+    batch.set_grids([model] * nch, resid)
+
+    def timed(fn):
+        fn()
+        torch.cuda.synchronize()
+        ts = []
+        for _ in range(reps):
+            a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            a.record()
+            fn()
+            b.record()
+            torch.cuda.synchronize()
+            ts.append(a.elapsed_time(b))
+        return statistics.median(ts)
+
+    def separate():
+        for pl, r in zip(plans, resid):
+            pl.cycle(model, r, S.SDP_DEGRID_CONV)
+
+    t_batch = timed(lambda: batch.cycle(S.SDP_DEGRID_CONV))
+    t_sep = timed(separate)
+    total = int(sum(counts))
+    out = {"workload": "64 channels 100-200 MHz, 256 antennas 10 km spiral, 120 time steps, per-channel flags "
+                       "0-60 %, G=2048 per channel, 32 w-planes hs=4 OS=16",
+           "vis_total": total, "vis_min": int(min(counts)), "vis_max": int(max(counts)),
+           "work_items": batch.num_work_items(),
+           "ms_batched": t_batch, "vis_per_s_batched": total / (t_batch * 1e-3),
+           "ms_64_launches": t_sep, "vis_per_s_64_launches": total / (t_sep * 1e-3)}
+    batch.close()
+    for pl in plans:
+        pl.close()
+    del resid, keep, model
+    torch.cuda.empty_cache()
+    return out
+
+
 def b200_arm(args):
     import torch
     import torch.distributed as dist
@@ -407,6 +482,11 @@ def b200_arm(args):
                  "stages": "image->grid FFT, fused degrid/subtract/grid, grid->image FFT + taper, Hogbom x200"}
         pl.close()
 
+    # ---- the batched multi-channel pass (one GPU only) ---------------------------------
+    c3 = None
+    if world == 1 and not args.no_c3:
+        c3 = c3_block(S, D, dev)
+
     # ---- e2e through the reference-facing C ABI with pinned host buffers ---------------
     uvw_h = torch.empty((N, 3), dtype=torch.float32).pin_memory()
     uvw_h.copy_(uvw.cpu())
@@ -474,6 +554,8 @@ def b200_arm(args):
     }
     if major is not None:
         line["major_cycle"] = major
+    if c3 is not None:
+        line["c3_batched"] = c3
     if cpu is not None:
         line["cpu_baseline"] = cpu
     plan.close()

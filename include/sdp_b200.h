@@ -296,6 +296,23 @@ int sdp_visplan_degrid(sdp_visplan *plan, const sdp_float2 *model_grid, sdp_floa
  * residual_grid = grid(delta).  predicted/delta may be NULL (not stored). */
 int sdp_visplan_cycle(sdp_visplan *plan, const sdp_float2 *model_grid, int degrid_mode, sdp_float2 *predicted,
                       sdp_float2 *delta, sdp_float2 *residual_grid, void *stream);
+
+/* Several frequency channels' fused passes in one persistent launch over a
+ * shared (channel, uv-tile) work queue (the reference runs channels as
+ * separate pipelines: read_ms/joint_nnode_ms/main.c:118-145 distributes them
+ * over MPI ranks).  Each plan is one channel's std_gridding plan with its
+ * measured visibilities set; all plans use one coordinate mode and stay
+ * owned by the caller (they must outlive the batch).  set_grids takes host
+ * arrays of device pointers (one model and one residual grid per channel);
+ * cycle zeroes every residual grid and runs the pass of sdp_visplan_cycle
+ * for all channels at once. */
+typedef struct sdp_visbatch sdp_visbatch;
+int sdp_visbatch_create(sdp_visbatch **batch, sdp_visplan *const *plans, int num_plans, void *stream);
+int sdp_visbatch_set_grids(sdp_visbatch *batch, const sdp_float2 *const *model_grids,
+                           sdp_float2 *const *residual_grids, void *stream);
+int sdp_visbatch_cycle(sdp_visbatch *batch, int degrid_mode, void *stream);
+int sdp_visbatch_num_work_items(const sdp_visbatch *batch, int *count);
+int sdp_visbatch_destroy(sdp_visbatch *batch);
 /* g2g_degridgrid on a plan built with grid_mode SDP_GRID_G2G:
  * out_grid = regrid(nearest_cell(in_grid)) with the plane-0 gridding kernel. */
 enum { SDP_GRID_G2G = 2 };

@@ -26,6 +26,7 @@
 #include <cstring>
 
 #include <algorithm>
+#include <vector>
 
 #include "internal.cuh"
 
@@ -325,6 +326,284 @@ constexpr int kThreads = 256;  // 8 warps per CTA of the tile kernels
 // visibility (grid edges, where the reference mirrors or skips taps, 2 hs + 1
 // taps, differing supports) takes the general path, which evaluates the
 // reference's index arithmetic tap by tap.
+// One work item of the tile kernels (the whole CTA): stage the input-grid
+// tile, walk the item's visibilities, flush the subgrid.  `planes` holds the
+// plan's per-plane constants; `share` / `share_sign` say whether the
+// gridding samples can be taken from the degridding samples.
+template <typename T, int GMODE, int OP, int LG>
+__device__ __forceinline__ void tile_item(const PlanDev &P, const int4 it, float *smem_f, const int4 *planes,
+                                          bool share, float share_sign, const float2 *__restrict__ vis_in,
+                                          const float2 *__restrict__ in_grid, float2 *__restrict__ out_grid,
+                                          float2 *__restrict__ pred_out, float2 *__restrict__ delta_out,
+                                          const float2 *__restrict__ measured)
+{
+    constexpr bool kGrids = (OP != OP_DEGRID);
+    constexpr bool kConv = (OP == OP_DEGRID || OP == OP_CYCLE_CONV);
+    constexpr bool kStageIn = (OP != OP_GRID);
+    constexpr int VPW = 32 / LG;
+    constexpr bool kShareable = (OP == OP_CYCLE_CONV) && LG == 8;
+    const int S = P.S, SS = S * S;
+    float2 *mtile = reinterpret_cast<float2 *>(smem_f);
+    float *sub_re = smem_f + (kStageIn ? 2 * SS : 0);
+    float *sub_im = sub_re + SS;
+    const int lane = threadIdx.x & 31;
+    const int warp = threadIdx.x >> 5;
+    const int grp = lane / LG;
+    const int cl = lane % LG;
+    const T fos = (T)P.OS;
+    const Rec<T> *__restrict__ recs = static_cast<const Rec<T> *>(P.rec);
+    float2 ksr[kShareable ? LG : 1];
+    const int ox = (it.x % P.ntx) * kTile;  // tile origin in grid cells
+    const int oy = (it.x / P.ntx) * kTile;
+    if (kGrids)
+        for (int k = threadIdx.x; k < 2 * SS; k += kThreads) sub_re[k] = 0.f;
+    if (kStageIn)
+        for (int k = threadIdx.x; k < SS; k += kThreads) {
+            const int gy = oy + k / S, gx = ox + k % S;
+            mtile[k] = (gx < P.G && gy < P.G) ? __ldg(&in_grid[(size_t)gy * P.G + gx]) : make_float2(0.f, 0.f);
+        }
+    __syncthreads();
+
+    for (int base = it.y + warp * VPW; base < it.z; base += (kThreads / 32) * VPW) {
+        const int r = base + grp;
+        const bool valid = r < it.z;
+        Rec<T> rec;
+        if (valid) {
+            rec = recs[r];
+        } else {
+            rec.px = (T)0;
+            rec.py = (T)0;
+            rec.meta = 0;
+            rec.idx = 0;
+        }
+        const int plane = rec.meta & 0xffff;
+        const float conj = (rec.meta < 0) ? -1.f : 1.f;
+
+        // ---------------- tap geometry and the fast-path test ----------------
+        const int4 pl = planes[plane];
+        const int hs_d = kConv ? pl.x : 0;
+        const int hs_g = kGrids ? pl.z : 0;
+        const int hs = kGrids ? hs_g : hs_d;
+        const T lox = tceil(tsub(rec.px, (T)hs));
+        const T loy = tceil(tsub(rec.py, (T)hs));
+        int ncols, nrows;
+        if (GMODE == SDP_GRID_SNAPPED) {  // gridding_run.c:84-112: inclusive floor bound
+            ncols = (int)(tfloor(tadd(rec.px, (T)hs)) - lox) + 1;
+            nrows = (int)(tfloor(tadd(rec.py, (T)hs)) - loy) + 1;
+        } else {  // degridgrid.c:93, 103
+            ncols = (int)(tceil(tadd(rec.px, (T)hs)) - lox);
+            nrows = (int)(tceil(tadd(rec.py, (T)hs)) - loy);
+        }
+        const int ix0 = (int)lox + P.gc, iy0 = (int)loy + P.gc;  // grid index of the first tap
+        const int tx0 = ix0 - ox, ty0 = iy0 - oy;                // ... and in the tile
+        const bool fast = valid && (!(kConv && kGrids) || hs_d == hs_g) && ncols <= LG && nrows <= LG &&
+                          ix0 >= 0 && iy0 >= 0 && ix0 + ncols <= P.G && iy0 + nrows <= P.G && tx0 >= 0 &&
+                          ty0 >= 0 && tx0 + ncols <= S && ty0 + nrows <= S;
+        const unsigned fmask = __ballot_sync(0xffffffffu, fast);
+        int colp_d = 0, colp_g = 0, lx = 0, rowpack = 0;
+        bool colok = false;
+        if (fast) {
+            const int A = hs + 1;
+            colok = cl < ncols;
+            const int kc = kcol(P, A, ref_kidx((int)lox + cl, rec.px, fos));
+            if (kConv) colp_d = pl.y + kc;
+            if (kGrids) colp_g = pl.w + kc;
+            lx = tx0 + cl;
+            // row cl of the box: kernel-row offset and tile row, packed
+            rowpack = (krow(P, A, ref_kidx((int)loy + cl, rec.py, fos)) << 6) | (ty0 + cl);
+        }
+
+        // ---------------- degrid (prediction) ----------------
+        float2 value = make_float2(0.f, 0.f);
+        if (kConv) {
+            // sum gv * Re(k) and gv * Im(k) separately; the conjugation of
+            // k for w < 0 (degridgrid.c:143, 175) is applied after the sum
+            float2 a1 = make_float2(0.f, 0.f), a2 = make_float2(0.f, 0.f);
+            float nrm = 0.f;
+            if (fast) {
+#pragma unroll
+                for (int rr = 0; rr < LG; ++rr) {
+                    const int pk = __shfl_sync(fmask, rowpack, grp * LG + rr);
+                    if (rr < nrows && colok) {
+                        const float2 ks = __ldg(&P.dk[colp_d + (pk >> 6)]);
+                        if constexpr (kShareable) ksr[rr] = ks;
+                        const float2 gv = mtile[(pk & 63) * S + lx];
+                        a1.x = fmaf(gv.x, ks.x, a1.x);
+                        a1.y = fmaf(gv.y, ks.x, a1.y);
+                        a2.x = fmaf(gv.x, ks.y, a2.x);
+                        a2.y = fmaf(gv.y, ks.y, a2.y);
+                        nrm = fmaf(ks.x, ks.x, fmaf(ks.y, ks.y, nrm));
+                    }
+                }
+            } else if (valid) {
+                // general path: degridgrid.c:147-186 tap by tap, edges mirrored
+                const int A = hs_d + 1, stride = A * P.OS;
+                const T dlox = tceil(tsub(rec.px, (T)hs_d));
+                const T dloy = tceil(tsub(rec.py, (T)hs_d));
+                const int dnc = (int)(tceil(tadd(rec.px, (T)hs_d)) - dlox);
+                const int dnr = (int)(tceil(tadd(rec.py, (T)hs_d)) - dloy);
+                const int off = pl.y;
+                for (int c = cl; c < dnc; c += LG) {
+                    const int cu = mirror((int)dlox + c, P.gc);
+                    const int kx = ref_kidx(cu, rec.px, fos);
+                    const bool kx_ok = kx < stride;
+                    const int colp = off + kcol(P, A, kx);
+                    const int gx = cu + P.gc;
+                    const int tx = gx - ox;
+                    for (int rr = 0; rr < dnr; ++rr) {
+                        const int cv = mirror((int)dloy + rr, P.gc);
+                        const int ky = ref_kidx(cv, rec.py, fos);
+                        float2 ks = make_float2(0.f, 0.f);
+                        if (kx_ok && ky < stride) ks = __ldg(&P.dk[colp + krow(P, A, ky)]);
+                        const int gy = cv + P.gc;
+                        const int ty = gy - oy;
+                        float2 gv;
+                        if ((unsigned)tx < (unsigned)S && (unsigned)ty < (unsigned)S) {
+                            gv = mtile[ty * S + tx];
+                        } else if (gx >= 0 && gy >= 0 && gx < P.G && gy < P.G) {
+                            gv = __ldg(&in_grid[(size_t)gy * P.G + gx]);
+                        } else {
+                            gv = make_float2(0.f, 0.f);
+                        }
+                        a1.x = fmaf(gv.x, ks.x, a1.x);
+                        a1.y = fmaf(gv.y, ks.x, a1.y);
+                        a2.x = fmaf(gv.x, ks.y, a2.x);
+                        a2.y = fmaf(gv.y, ks.y, a2.y);
+                        nrm = fmaf(ks.x, ks.x, fmaf(ks.y, ks.y, nrm));
+                    }
+                }
+            }
+#pragma unroll
+            for (int o = LG / 2; o > 0; o >>= 1) {
+                a1.x += __shfl_xor_sync(0xffffffffu, a1.x, o);
+                a1.y += __shfl_xor_sync(0xffffffffu, a1.y, o);
+                a2.x += __shfl_xor_sync(0xffffffffu, a2.x, o);
+                a2.y += __shfl_xor_sync(0xffffffffu, a2.y, o);
+                nrm += __shfl_xor_sync(0xffffffffu, nrm, o);
+            }
+            // gv * (kr + i conj ki) summed; then degridgrid.c:188-191
+            // (the .y fallback uses the new .x)
+            const float sx = fmaf(-conj, a2.y, a1.x);
+            const float sy = fmaf(conj, a2.x, a1.y);
+            // (one correctly rounded reciprocal instead of two divides: the
+            // sum's order already differs from the reference's)
+            const float cn = __fsqrt_rn(nrm);
+            const bool tiny = cn < 1e-5f;
+            const float inv = tiny ? 1e5f : __frcp_rn(cn);
+            const float nx = sx * inv;
+            const float ny = tiny ? nx * inv : sy * inv;
+            value = make_float2(nx, ny);
+        } else if (OP == OP_CYCLE_NEAR || OP == OP_G2G) {
+            // degridgrid.c:194-200 / :273-285
+            const int x = ref_nearest(rec.px, P.gc), y = ref_nearest(rec.py, P.gc);
+            const int tx = x - ox, ty = y - oy;
+            if ((unsigned)tx < (unsigned)S && (unsigned)ty < (unsigned)S && x < P.G && y < P.G) {
+                value = mtile[ty * S + tx];
+            } else {
+                const long long gi = (long long)x + (long long)y * P.G;
+                if (gi >= 0 && gi < (long long)P.G * P.G) value = __ldg(&in_grid[gi]);
+            }
+        }
+
+        float2 gval = make_float2(0.f, 0.f);
+        if (OP == OP_GRID) {
+            if (valid) gval = __ldg(&vis_in[rec.idx]);
+        } else if (OP == OP_G2G) {
+            gval = value;
+        } else if (OP == OP_CYCLE_CONV || OP == OP_CYCLE_NEAR) {
+            if (valid) {
+                const float2 m = measured[r];
+                gval = make_float2(__fsub_rn(m.x, value.x), __fsub_rn(m.y, value.y));
+                if (cl == 0) {
+                    if (pred_out) pred_out[rec.idx] = value;
+                    if (delta_out) delta_out[rec.idx] = gval;
+                }
+            }
+        } else {  // OP_DEGRID
+            if (valid && cl == 0) pred_out[rec.idx] = value;
+        }
+
+        // ---------------- grid ----------------
+        if (kGrids) {
+            // vis * (kr + i conj ki): re = vr kr - (conj vi) ki, im = vi kr + (conj vr) ki
+            const float ca = conj * gval.y, cb = conj * gval.x;
+            if (fast) {
+#pragma unroll
+                for (int rr = 0; rr < LG; ++rr) {
+                    const int pk = __shfl_sync(fmask, rowpack, grp * LG + rr);
+                    if (rr < nrows && colok) {
+                        float2 ks;
+                        if constexpr (kShareable) {
+                            ks = share ? make_float2(ksr[rr].x, share_sign * ksr[rr].y)
+                                       : __ldg(&P.gk[colp_g + (pk >> 6)]);
+                        } else {
+                            ks = __ldg(&P.gk[colp_g + (pk >> 6)]);
+                        }
+                        const int cell = (pk & 63) * S + lx;
+                        atomicAdd(sub_re + cell, fmaf(-ca, ks.y, gval.x * ks.x));
+                        atomicAdd(sub_im + cell, fmaf(cb, ks.y, gval.y * ks.x));
+                    }
+                }
+            } else if (valid) {
+                // general path: degridgrid.c:93-122 / gridding_run.c:104-132 tap by tap
+                const int A = hs_g + 1, stride = A * P.OS;
+                const int off = pl.w;
+                for (int c = cl; c < ncols; c += LG) {
+                    const int u = (int)lox + c;
+                    const int gx = u + P.gc;
+                    if (gx < 0 || gx >= P.G) continue;
+                    const int tx = gx - ox;
+                    const int kx = ref_kidx(u, rec.px, fos);
+                    if (kx >= stride || (unsigned)tx >= (unsigned)S) {  // cannot happen for a valid plan
+                        atomicOr(P.flags, FLAG_BOX);
+                        continue;
+                    }
+                    const int colp = off + kcol(P, A, kx);
+                    for (int rr = 0; rr < nrows; ++rr) {
+                        const int v = (int)loy + rr;
+                        const int gy = v + P.gc;
+                        if (gy < 0 || gy >= P.G) continue;
+                        const int ty = gy - oy;
+                        const int ky = ref_kidx(v, rec.py, fos);
+                        if (ky >= stride || (unsigned)ty >= (unsigned)S) {
+                            atomicOr(P.flags, FLAG_BOX);
+                            continue;
+                        }
+                        const float2 ks = __ldg(&P.gk[colp + krow(P, A, ky)]);
+                        const int cell = ty * S + tx;
+                        atomicAdd(sub_re + cell, fmaf(-ca, ks.y, gval.x * ks.x));
+                        atomicAdd(sub_im + cell, fmaf(cb, ks.y, gval.y * ks.x));
+                    }
+                }
+            }
+        }
+    }
+    if (kGrids) {
+        __syncthreads();
+        // flush: one vector atomic per touched cell of the subgrid
+        for (int k = threadIdx.x; k < SS; k += kThreads) {
+            const float2 v = make_float2(sub_re[k], sub_im[k]);
+            if (v.x != 0.f || v.y != 0.f) {
+                const int gy = oy + k / S, gx = ox + k % S;
+                if (gx < P.G && gy < P.G) atomicAdd(&out_grid[(size_t)gy * P.G + gx], v);
+            }
+        }
+    }
+    __syncthreads();
+}
+
+// Per-plane constants {hs_d, degrid offset, hs_g, grid offset} of a plan
+// into shared memory (the whole CTA).
+template <int OP>
+__device__ __forceinline__ void load_planes(const PlanDev &P, int4 *planes)
+{
+    constexpr bool kGrids = (OP != OP_DEGRID);
+    constexpr bool kConv = (OP == OP_DEGRID || OP == OP_CYCLE_CONV);
+    for (int k = threadIdx.x; k < P.nk_g; k += kThreads)
+        planes[k] = make_int4(kConv && k < P.nk_d ? P.ds[k].x : 0, kConv && k < P.nk_d ? P.dpoff[k] : 0,
+                              kGrids ? P.gs[k].x : 0, kGrids ? P.gpoff[k] : 0);
+}
+
 template <typename T, int GMODE, int OP, int LG>
 __global__ void __launch_bounds__(kThreads, 4) k_tiles(PlanDev P, const float2 *__restrict__ vis_in,
                                                    const float2 *__restrict__ in_grid,
@@ -334,277 +613,73 @@ __global__ void __launch_bounds__(kThreads, 4) k_tiles(PlanDev P, const float2 *
 {
     extern __shared__ float smem_f[];
     constexpr bool kGrids = (OP != OP_DEGRID);
-    constexpr bool kConv = (OP == OP_DEGRID || OP == OP_CYCLE_CONV);
     constexpr bool kStageIn = (OP != OP_GRID);
-    constexpr int VPW = 32 / LG;
-    const int S = P.S, SS = S * S;
-    float2 *mtile = reinterpret_cast<float2 *>(smem_f);
-    float *sub_re = smem_f + (kStageIn ? 2 * SS : 0);
-    float *sub_im = sub_re + SS;
-    // per-plane constants {hs_d, degrid offset, hs_g, grid offset}, loaded once
+    const int SS = P.S * P.S;
     int4 *planes = reinterpret_cast<int4 *>(smem_f + (kStageIn ? 2 * SS : 0) + (kGrids ? 2 * SS : 0));
-    for (int k = threadIdx.x; k < P.nk_g; k += kThreads)
-        planes[k] = make_int4(kConv && k < P.nk_d ? P.ds[k].x : 0, kConv && k < P.nk_d ? P.dpoff[k] : 0,
-                              kGrids ? P.gs[k].x : 0, kGrids ? P.gpoff[k] : 0);
-    const int lane = threadIdx.x & 31;
-    const int warp = threadIdx.x >> 5;
-    const int grp = lane / LG;
-    const int cl = lane % LG;
-    const T fos = (T)P.OS;
-    const Rec<T> *__restrict__ recs = static_cast<const Rec<T> *>(P.rec);
+    load_planes<OP>(P, planes);
     __shared__ int s_item;
     // When the degridding set equals the gridding set or its conjugate (bit
     // for bit, checked at plan build), the fast path of a cycle reads each
     // kernel sample once and keeps it in registers for the gridding pass.
-    constexpr bool kShareable = (OP == OP_CYCLE_CONV) && LG == 8;
-    const int kdiff = kShareable ? *P.kdiff : 3;
+    const int kdiff = (OP == OP_CYCLE_CONV && LG == 8) ? *P.kdiff : 3;
     const bool share = (kdiff & 1) == 0 || (kdiff & 2) == 0;
     const float share_sign = (kdiff & 1) == 0 ? 1.f : -1.f;
-    float2 ksr[kShareable ? LG : 1];
-
     for (;;) {
         if (threadIdx.x == 0) s_item = atomicAdd(P.item_counter, 1);
         __syncthreads();
         const int item = s_item;
         if (item >= *P.n_items) break;
-        const int4 it = P.items[item];
-        const int ox = (it.x % P.ntx) * kTile;  // tile origin in grid cells
-        const int oy = (it.x / P.ntx) * kTile;
-        if (kGrids)
-            for (int k = threadIdx.x; k < 2 * SS; k += kThreads) sub_re[k] = 0.f;
-        if (kStageIn)
-            for (int k = threadIdx.x; k < SS; k += kThreads) {
-                const int gy = oy + k / S, gx = ox + k % S;
-                mtile[k] = (gx < P.G && gy < P.G) ? __ldg(&in_grid[(size_t)gy * P.G + gx]) : make_float2(0.f, 0.f);
-            }
+        tile_item<T, GMODE, OP, LG>(P, P.items[item], smem_f, planes, share, share_sign, vis_in, in_grid, out_grid,
+                                    pred_out, delta_out, measured);
+    }
+}
+
+// Several plans (one per frequency channel) in one persistent launch over a
+// shared (channel, tile) work queue: item.w is the channel.  A CTA copies a
+// channel's plan description and per-plane constants to shared memory when
+// its next item belongs to another channel (items are channel-major, so that
+// is rare).
+struct BatchIO {
+    const float2 *in_grid;   // model grid of the channel
+    float2 *out_grid;        // residual grid of the channel
+    const float2 *measured;  // measured visibilities in plan order
+    float2 *pred_out;
+    float2 *delta_out;
+};
+
+template <typename T, int GMODE, int OP, int LG>
+__global__ void __launch_bounds__(kThreads, 4) k_tiles_batch(const PlanDev *__restrict__ plans,
+                                                         const BatchIO *__restrict__ io,
+                                                         const int4 *__restrict__ items, int n_items,
+                                                         int *item_counter, int smem_stride)
+{
+    extern __shared__ float smem_f[];
+    __shared__ PlanDev sP;
+    __shared__ BatchIO sIO;
+    __shared__ int s_item, s_share;
+    int4 *planes = reinterpret_cast<int4 *>(smem_f + smem_stride);
+    int cur = -1;
+    for (;;) {
+        if (threadIdx.x == 0) s_item = atomicAdd(item_counter, 1);
         __syncthreads();
-
-        for (int base = it.y + warp * VPW; base < it.z; base += (kThreads / 32) * VPW) {
-            const int r = base + grp;
-            const bool valid = r < it.z;
-            Rec<T> rec;
-            if (valid) {
-                rec = recs[r];
-            } else {
-                rec.px = (T)0;
-                rec.py = (T)0;
-                rec.meta = 0;
-                rec.idx = 0;
+        const int item = s_item;
+        if (item >= n_items) break;
+        const int4 it = items[item];
+        if (it.w != cur) {
+            if (threadIdx.x == 0) {
+                sP = plans[it.w];
+                sIO = io[it.w];
+                s_share = (OP == OP_CYCLE_CONV && LG == 8) ? *sP.kdiff : 3;
             }
-            const int plane = rec.meta & 0xffff;
-            const float conj = (rec.meta < 0) ? -1.f : 1.f;
-
-            // ---------------- tap geometry and the fast-path test ----------------
-            const int4 pl = planes[plane];
-            const int hs_d = kConv ? pl.x : 0;
-            const int hs_g = kGrids ? pl.z : 0;
-            const int hs = kGrids ? hs_g : hs_d;
-            const T lox = tceil(tsub(rec.px, (T)hs));
-            const T loy = tceil(tsub(rec.py, (T)hs));
-            int ncols, nrows;
-            if (GMODE == SDP_GRID_SNAPPED) {  // gridding_run.c:84-112: inclusive floor bound
-                ncols = (int)(tfloor(tadd(rec.px, (T)hs)) - lox) + 1;
-                nrows = (int)(tfloor(tadd(rec.py, (T)hs)) - loy) + 1;
-            } else {  // degridgrid.c:93, 103
-                ncols = (int)(tceil(tadd(rec.px, (T)hs)) - lox);
-                nrows = (int)(tceil(tadd(rec.py, (T)hs)) - loy);
-            }
-            const int ix0 = (int)lox + P.gc, iy0 = (int)loy + P.gc;  // grid index of the first tap
-            const int tx0 = ix0 - ox, ty0 = iy0 - oy;                // ... and in the tile
-            const bool fast = valid && (!(kConv && kGrids) || hs_d == hs_g) && ncols <= LG && nrows <= LG &&
-                              ix0 >= 0 && iy0 >= 0 && ix0 + ncols <= P.G && iy0 + nrows <= P.G && tx0 >= 0 &&
-                              ty0 >= 0 && tx0 + ncols <= S && ty0 + nrows <= S;
-            const unsigned fmask = __ballot_sync(0xffffffffu, fast);
-            int colp_d = 0, colp_g = 0, lx = 0, rowpack = 0;
-            bool colok = false;
-            if (fast) {
-                const int A = hs + 1;
-                colok = cl < ncols;
-                const int kc = kcol(P, A, ref_kidx((int)lox + cl, rec.px, fos));
-                if (kConv) colp_d = pl.y + kc;
-                if (kGrids) colp_g = pl.w + kc;
-                lx = tx0 + cl;
-                // row cl of the box: kernel-row offset and tile row, packed
-                rowpack = (krow(P, A, ref_kidx((int)loy + cl, rec.py, fos)) << 6) | (ty0 + cl);
-            }
-
-            // ---------------- degrid (prediction) ----------------
-            float2 value = make_float2(0.f, 0.f);
-            if (kConv) {
-                // sum gv * Re(k) and gv * Im(k) separately; the conjugation of
-                // k for w < 0 (degridgrid.c:143, 175) is applied after the sum
-                float2 a1 = make_float2(0.f, 0.f), a2 = make_float2(0.f, 0.f);
-                float nrm = 0.f;
-                if (fast) {
-#pragma unroll
-                    for (int rr = 0; rr < LG; ++rr) {
-                        const int pk = __shfl_sync(fmask, rowpack, grp * LG + rr);
-                        if (rr < nrows && colok) {
-                            const float2 ks = __ldg(&P.dk[colp_d + (pk >> 6)]);
-                            if constexpr (kShareable) ksr[rr] = ks;
-                            const float2 gv = mtile[(pk & 63) * S + lx];
-                            a1.x = fmaf(gv.x, ks.x, a1.x);
-                            a1.y = fmaf(gv.y, ks.x, a1.y);
-                            a2.x = fmaf(gv.x, ks.y, a2.x);
-                            a2.y = fmaf(gv.y, ks.y, a2.y);
-                            nrm = fmaf(ks.x, ks.x, fmaf(ks.y, ks.y, nrm));
-                        }
-                    }
-                } else if (valid) {
-                    // general path: degridgrid.c:147-186 tap by tap, edges mirrored
-                    const int A = hs_d + 1, stride = A * P.OS;
-                    const T dlox = tceil(tsub(rec.px, (T)hs_d));
-                    const T dloy = tceil(tsub(rec.py, (T)hs_d));
-                    const int dnc = (int)(tceil(tadd(rec.px, (T)hs_d)) - dlox);
-                    const int dnr = (int)(tceil(tadd(rec.py, (T)hs_d)) - dloy);
-                    const int off = pl.y;
-                    for (int c = cl; c < dnc; c += LG) {
-                        const int cu = mirror((int)dlox + c, P.gc);
-                        const int kx = ref_kidx(cu, rec.px, fos);
-                        const bool kx_ok = kx < stride;
-                        const int colp = off + kcol(P, A, kx);
-                        const int gx = cu + P.gc;
-                        const int tx = gx - ox;
-                        for (int rr = 0; rr < dnr; ++rr) {
-                            const int cv = mirror((int)dloy + rr, P.gc);
-                            const int ky = ref_kidx(cv, rec.py, fos);
-                            float2 ks = make_float2(0.f, 0.f);
-                            if (kx_ok && ky < stride) ks = __ldg(&P.dk[colp + krow(P, A, ky)]);
-                            const int gy = cv + P.gc;
-                            const int ty = gy - oy;
-                            float2 gv;
-                            if ((unsigned)tx < (unsigned)S && (unsigned)ty < (unsigned)S) {
-                                gv = mtile[ty * S + tx];
-                            } else if (gx >= 0 && gy >= 0 && gx < P.G && gy < P.G) {
-                                gv = __ldg(&in_grid[(size_t)gy * P.G + gx]);
-                            } else {
-                                gv = make_float2(0.f, 0.f);
-                            }
-                            a1.x = fmaf(gv.x, ks.x, a1.x);
-                            a1.y = fmaf(gv.y, ks.x, a1.y);
-                            a2.x = fmaf(gv.x, ks.y, a2.x);
-                            a2.y = fmaf(gv.y, ks.y, a2.y);
-                            nrm = fmaf(ks.x, ks.x, fmaf(ks.y, ks.y, nrm));
-                        }
-                    }
-                }
-#pragma unroll
-                for (int o = LG / 2; o > 0; o >>= 1) {
-                    a1.x += __shfl_xor_sync(0xffffffffu, a1.x, o);
-                    a1.y += __shfl_xor_sync(0xffffffffu, a1.y, o);
-                    a2.x += __shfl_xor_sync(0xffffffffu, a2.x, o);
-                    a2.y += __shfl_xor_sync(0xffffffffu, a2.y, o);
-                    nrm += __shfl_xor_sync(0xffffffffu, nrm, o);
-                }
-                // gv * (kr + i conj ki) summed; then degridgrid.c:188-191
-                // (the .y fallback uses the new .x)
-                const float sx = fmaf(-conj, a2.y, a1.x);
-                const float sy = fmaf(conj, a2.x, a1.y);
-                // (one correctly rounded reciprocal instead of two divides: the
-                // sum's order already differs from the reference's)
-                const float cn = __fsqrt_rn(nrm);
-                const bool tiny = cn < 1e-5f;
-                const float inv = tiny ? 1e5f : __frcp_rn(cn);
-                const float nx = sx * inv;
-                const float ny = tiny ? nx * inv : sy * inv;
-                value = make_float2(nx, ny);
-            } else if (OP == OP_CYCLE_NEAR || OP == OP_G2G) {
-                // degridgrid.c:194-200 / :273-285
-                const int x = ref_nearest(rec.px, P.gc), y = ref_nearest(rec.py, P.gc);
-                const int tx = x - ox, ty = y - oy;
-                if ((unsigned)tx < (unsigned)S && (unsigned)ty < (unsigned)S && x < P.G && y < P.G) {
-                    value = mtile[ty * S + tx];
-                } else {
-                    const long long gi = (long long)x + (long long)y * P.G;
-                    if (gi >= 0 && gi < (long long)P.G * P.G) value = __ldg(&in_grid[gi]);
-                }
-            }
-
-            float2 gval = make_float2(0.f, 0.f);
-            if (OP == OP_GRID) {
-                if (valid) gval = __ldg(&vis_in[rec.idx]);
-            } else if (OP == OP_G2G) {
-                gval = value;
-            } else if (OP == OP_CYCLE_CONV || OP == OP_CYCLE_NEAR) {
-                if (valid) {
-                    const float2 m = measured[r];
-                    gval = make_float2(__fsub_rn(m.x, value.x), __fsub_rn(m.y, value.y));
-                    if (cl == 0) {
-                        if (pred_out) pred_out[rec.idx] = value;
-                        if (delta_out) delta_out[rec.idx] = gval;
-                    }
-                }
-            } else {  // OP_DEGRID
-                if (valid && cl == 0) pred_out[rec.idx] = value;
-            }
-
-            // ---------------- grid ----------------
-            if (kGrids) {
-                // vis * (kr + i conj ki): re = vr kr - (conj vi) ki, im = vi kr + (conj vr) ki
-                const float ca = conj * gval.y, cb = conj * gval.x;
-                if (fast) {
-#pragma unroll
-                    for (int rr = 0; rr < LG; ++rr) {
-                        const int pk = __shfl_sync(fmask, rowpack, grp * LG + rr);
-                        if (rr < nrows && colok) {
-                            float2 ks;
-                            if constexpr (kShareable) {
-                                ks = share ? make_float2(ksr[rr].x, share_sign * ksr[rr].y)
-                                           : __ldg(&P.gk[colp_g + (pk >> 6)]);
-                            } else {
-                                ks = __ldg(&P.gk[colp_g + (pk >> 6)]);
-                            }
-                            const int cell = (pk & 63) * S + lx;
-                            atomicAdd(sub_re + cell, fmaf(-ca, ks.y, gval.x * ks.x));
-                            atomicAdd(sub_im + cell, fmaf(cb, ks.y, gval.y * ks.x));
-                        }
-                    }
-                } else if (valid) {
-                    // general path: degridgrid.c:93-122 / gridding_run.c:104-132 tap by tap
-                    const int A = hs_g + 1, stride = A * P.OS;
-                    const int off = pl.w;
-                    for (int c = cl; c < ncols; c += LG) {
-                        const int u = (int)lox + c;
-                        const int gx = u + P.gc;
-                        if (gx < 0 || gx >= P.G) continue;
-                        const int tx = gx - ox;
-                        const int kx = ref_kidx(u, rec.px, fos);
-                        if (kx >= stride || (unsigned)tx >= (unsigned)S) {  // cannot happen for a valid plan
-                            atomicOr(P.flags, FLAG_BOX);
-                            continue;
-                        }
-                        const int colp = off + kcol(P, A, kx);
-                        for (int rr = 0; rr < nrows; ++rr) {
-                            const int v = (int)loy + rr;
-                            const int gy = v + P.gc;
-                            if (gy < 0 || gy >= P.G) continue;
-                            const int ty = gy - oy;
-                            const int ky = ref_kidx(v, rec.py, fos);
-                            if (ky >= stride || (unsigned)ty >= (unsigned)S) {
-                                atomicOr(P.flags, FLAG_BOX);
-                                continue;
-                            }
-                            const float2 ks = __ldg(&P.gk[colp + krow(P, A, ky)]);
-                            const int cell = ty * S + tx;
-                            atomicAdd(sub_re + cell, fmaf(-ca, ks.y, gval.x * ks.x));
-                            atomicAdd(sub_im + cell, fmaf(cb, ks.y, gval.y * ks.x));
-                        }
-                    }
-                }
-            }
-        }
-        if (kGrids) {
             __syncthreads();
-            // flush: one vector atomic per touched cell of the subgrid
-            for (int k = threadIdx.x; k < SS; k += kThreads) {
-                const float2 v = make_float2(sub_re[k], sub_im[k]);
-                if (v.x != 0.f || v.y != 0.f) {
-                    const int gy = oy + k / S, gx = ox + k % S;
-                    if (gx < P.G && gy < P.G) atomicAdd(&out_grid[(size_t)gy * P.G + gx], v);
-                }
-            }
+            load_planes<OP>(sP, planes);
+            __syncthreads();
+            cur = it.w;
         }
-        __syncthreads();
+        const int kdiff = s_share;
+        tile_item<T, GMODE, OP, LG>(sP, it, smem_f, planes, (kdiff & 1) == 0 || (kdiff & 2) == 0,
+                                    (kdiff & 1) == 0 ? 1.f : -1.f, nullptr, sIO.in_grid, sIO.out_grid,
+                                    sIO.pred_out, sIO.delta_out, sIO.measured);
     }
 }
 
@@ -1114,4 +1189,163 @@ SDP_EXPORT int sdp_visplan_g2g(sdp_visplan *p, const sdp_float2 *in_grid, sdp_fl
     if (p->n == 0) return SDP_OK;
     return launch_tiles(p, OP_G2G, nullptr, reinterpret_cast<const float2 *>(in_grid),
                         reinterpret_cast<float2 *>(out_grid), nullptr, nullptr, st);
+}
+
+// ----------------------------------------------------------------------------
+// Batches of plans (frequency channels) in one launch
+// ----------------------------------------------------------------------------
+struct sdp_visbatch {
+    int n = 0;
+    bool f64 = false;
+    int hs_max = 0, S_max = 0, nk_max = 0, n_items = 0;
+    std::vector<sdp_visplan *> plans;
+    std::vector<sdp::BatchIO> io;
+    sdp::PlanDev *d_plans = nullptr;
+    sdp::BatchIO *d_io = nullptr;
+    int4 *d_items = nullptr;
+    int *d_counter = nullptr;
+    bool io_set = false;
+};
+
+namespace sdp {
+
+template <typename T, int LG>
+static int launch_batch_lg(sdp_visbatch *b, int op, cudaStream_t st)
+{
+    const size_t SS = (size_t)b->S_max * b->S_max;
+    const int stride = (int)(4 * SS);  // floats: model tile (2 SS) + subgrid (2 SS) of the widest channel
+    const size_t smem = sizeof(float) * (size_t)stride + sizeof(int4) * (size_t)b->nk_max;
+    void (*fn)(const PlanDev *, const BatchIO *, const int4 *, int, int *, int) =
+        op == OP_CYCLE_CONV ? k_tiles_batch<T, SDP_GRID_STD, OP_CYCLE_CONV, LG>
+                            : k_tiles_batch<T, SDP_GRID_STD, OP_CYCLE_NEAR, LG>;
+    if (smem > 48 * 1024) SDP_CUDA_TRY(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    int per_sm = 0;
+    SDP_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, kThreads, smem));
+    if (per_sm < 1) return set_error(SDP_ERR_RANGE, "batched tile kernel does not fit (%zu B shared memory)", smem);
+    SDP_CUDA_TRY(cudaMemsetAsync(b->d_counter, 0, sizeof(int), st));
+    fn<<<per_sm * num_sms(), kThreads, smem, st>>>(b->d_plans, b->d_io, b->d_items, b->n_items, b->d_counter,
+                                                   stride);
+    SDP_LAUNCH_CHECK();
+    return SDP_OK;
+}
+
+}  // namespace sdp
+
+static void visbatch_free(sdp_visbatch *b)
+{
+    if (!b) return;
+    cudaFree(b->d_plans);
+    cudaFree(b->d_io);
+    cudaFree(b->d_items);
+    cudaFree(b->d_counter);
+    delete b;
+}
+
+SDP_EXPORT int sdp_visbatch_create(sdp_visbatch **out, sdp_visplan *const *plans, int num_plans, void *stream)
+{
+    SDP_CHECK_ARG(out && plans && num_plans >= 1, "bad argument");
+    *out = nullptr;
+    cudaStream_t st = as_stream(stream);
+    sdp_visbatch *b = new sdp_visbatch();
+    b->n = num_plans;
+    b->f64 = plans[0] && plans[0]->coord_f64;
+    std::vector<PlanDev> devs;
+    std::vector<int4> items;
+    for (int c = 0; c < num_plans; ++c) {
+        sdp_visplan *p = plans[c];
+        if (!p || p->mode != SDP_GRID_STD || p->coord_f64 != b->f64) {
+            visbatch_free(b);
+            return set_error(SDP_ERR_INVALID, "plan %d: a batch holds std_gridding plans of one coordinate mode", c);
+        }
+        b->plans.push_back(p);
+        devs.push_back(plan_dev(p));
+        b->hs_max = std::max(b->hs_max, p->hs_max);
+        b->S_max = std::max(b->S_max, p->S);
+        b->nk_max = std::max(b->nk_max, p->gk.num_kernels);
+        int ni = 0;
+        cudaError_t e = cudaMemcpyAsync(&ni, p->n_items, sizeof(int), cudaMemcpyDeviceToHost, st);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+        if (e != cudaSuccess) {
+            visbatch_free(b);
+            return cuda_error(e, "reading a plan's work-item count");
+        }
+        std::vector<int4> pi((size_t)ni);
+        if (ni > 0) {
+            e = cudaMemcpy(pi.data(), p->items, sizeof(int4) * (size_t)ni, cudaMemcpyDeviceToHost);
+            if (e != cudaSuccess) {
+                visbatch_free(b);
+                return cuda_error(e, "reading a plan's work items");
+            }
+        }
+        for (int4 it : pi) items.push_back(make_int4(it.x, it.y, it.z, c));
+    }
+    b->n_items = (int)items.size();
+    b->io.resize((size_t)num_plans);
+    cudaError_t e = cudaMalloc(&b->d_plans, sizeof(PlanDev) * devs.size());
+    if (e == cudaSuccess) e = cudaMalloc(&b->d_io, sizeof(BatchIO) * (size_t)num_plans);
+    if (e == cudaSuccess) e = cudaMalloc(&b->d_items, sizeof(int4) * std::max<size_t>(items.size(), 1));
+    if (e == cudaSuccess) e = cudaMalloc(&b->d_counter, sizeof(int));
+    if (e == cudaSuccess) e = cudaMemcpy(b->d_plans, devs.data(), sizeof(PlanDev) * devs.size(), cudaMemcpyHostToDevice);
+    if (e == cudaSuccess && !items.empty())
+        e = cudaMemcpy(b->d_items, items.data(), sizeof(int4) * items.size(), cudaMemcpyHostToDevice);
+    if (e != cudaSuccess) {
+        visbatch_free(b);
+        return cuda_error(e, "visibility batch set-up");
+    }
+    *out = b;
+    return SDP_OK;
+}
+
+SDP_EXPORT int sdp_visbatch_set_grids(sdp_visbatch *b, const sdp_float2 *const *model_grids,
+                                      sdp_float2 *const *residual_grids, void *stream)
+{
+    SDP_CHECK_ARG(b && model_grids && residual_grids, "NULL argument");
+    for (int c = 0; c < b->n; ++c) {
+        SDP_CHECK_ARG(model_grids[c] && residual_grids[c], "channel %d: NULL grid", c);
+        b->io[(size_t)c] = BatchIO{reinterpret_cast<const float2 *>(model_grids[c]),
+                                   reinterpret_cast<float2 *>(residual_grids[c]), b->plans[(size_t)c]->measured,
+                                   nullptr, nullptr};
+    }
+    cudaStream_t st = as_stream(stream);
+    SDP_CUDA_TRY(cudaMemcpyAsync(b->d_io, b->io.data(), sizeof(BatchIO) * (size_t)b->n, cudaMemcpyHostToDevice, st));
+    SDP_CUDA_TRY(cudaStreamSynchronize(st));  // the host array may change after return
+    b->io_set = true;
+    return SDP_OK;
+}
+
+SDP_EXPORT int sdp_visbatch_cycle(sdp_visbatch *b, int degrid_mode, void *stream)
+{
+    SDP_CHECK_ARG(b, "batch is NULL");
+    SDP_CHECK_ARG(b->io_set, "sdp_visbatch_set_grids was not called");
+    SDP_CHECK_ARG(degrid_mode == SDP_DEGRID_NEAREST || degrid_mode == SDP_DEGRID_CONV, "degrid mode %d unknown",
+                  degrid_mode);
+    cudaStream_t st = as_stream(stream);
+    for (int c = 0; c < b->n; ++c) {
+        const size_t G2 = (size_t)b->plans[(size_t)c]->geom.grid_size * b->plans[(size_t)c]->geom.grid_size;
+        SDP_CUDA_TRY(cudaMemsetAsync(b->io[(size_t)c].out_grid, 0, sizeof(float2) * G2, st));
+    }
+    if (b->n_items == 0) return SDP_OK;
+    const int op = degrid_mode == SDP_DEGRID_CONV ? OP_CYCLE_CONV : OP_CYCLE_NEAR;
+    const int taps = 2 * b->hs_max;
+    if (b->f64) {
+        if (taps <= 8) return launch_batch_lg<double, 8>(b, op, st);
+        if (taps <= 16) return launch_batch_lg<double, 16>(b, op, st);
+        return launch_batch_lg<double, 32>(b, op, st);
+    }
+    if (taps <= 8) return launch_batch_lg<float, 8>(b, op, st);
+    if (taps <= 16) return launch_batch_lg<float, 16>(b, op, st);
+    return launch_batch_lg<float, 32>(b, op, st);
+}
+
+SDP_EXPORT int sdp_visbatch_num_work_items(const sdp_visbatch *b, int *count)
+{
+    SDP_CHECK_ARG(b && count, "NULL argument");
+    *count = b->n_items;
+    return SDP_OK;
+}
+
+SDP_EXPORT int sdp_visbatch_destroy(sdp_visbatch *b)
+{
+    visbatch_free(b);
+    return SDP_OK;
 }

@@ -453,6 +453,45 @@ class VisPlan:
         check(self.lib.sdp_visplan_check(self.handle, _stream(stream)), self.lib)
 
 
+class VisBatch:
+    """Owns an sdp_visbatch: several channels' plans in one launch.  The plans
+    (VisPlan objects) are kept alive by the batch."""
+
+    def __init__(self, lib, plans, stream=None):
+        self.lib = lib
+        self.plans = list(plans)
+        arr = (_p * len(self.plans))(*[pl.handle for pl in self.plans])
+        self.handle = _p()
+        check(lib.sdp_visbatch_create(C.byref(self.handle), arr, _i(len(self.plans)), _stream(stream)), lib)
+        self._grids = ()
+
+    def set_grids(self, model_grids, residual_grids, stream=None):
+        n = len(self.plans)
+        m = (_p * n)(*[_dp(g) for g in model_grids])
+        r = (_p * n)(*[_dp(g) for g in residual_grids])
+        self._grids = (list(model_grids), list(residual_grids))
+        check(self.lib.sdp_visbatch_set_grids(self.handle, m, r, _stream(stream)), self.lib)
+
+    def cycle(self, mode=SDP_DEGRID_CONV, stream=None):
+        check(self.lib.sdp_visbatch_cycle(self.handle, _i(mode), _stream(stream)), self.lib)
+
+    def num_work_items(self) -> int:
+        c = _i(0)
+        check(self.lib.sdp_visbatch_num_work_items(self.handle, C.byref(c)), self.lib)
+        return c.value
+
+    def close(self):
+        if self.handle:
+            check(self.lib.sdp_visbatch_destroy(self.handle), self.lib)
+            self.handle = _p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
 SDP_COORD_F32 = 0
 SDP_COORD_F64 = 1
 SDP_PLAN_COORD_F64 = 0x100
@@ -529,6 +568,9 @@ class Device:
              mode=SDP_GRID_STD, stream=None, keep=()) -> VisPlan:
         geom = Geometry(grid_size, oversampling, uv_scale, w_scale)
         return VisPlan(self.lib, geom, gk, dk, uvw, mode, stream, keep)
+
+    def batch(self, plans, stream=None) -> VisBatch:
+        return VisBatch(self.lib, plans, stream)
 
     def pipeline(self, cfg: PipelineConfig, uvw, measured, psf, gk: WKernels, dk: WKernels | None = None,
                  stream=None, keep=()) -> Pipeline:
