@@ -12,6 +12,7 @@
 #include <cstring>
 
 #include <algorithm>
+#include <vector>
 
 #include "internal.cuh"
 
@@ -37,6 +38,8 @@ enum Slot {
     S_IMG2,
     S_PROLATE,
     S_PLAN,
+    S_UVW_KEY,  // the uvw the cached plan was built from (device copy)
+    S_FLAG,
     S_PSF,
     S_MODEL,
     S_SRC,
@@ -77,9 +80,29 @@ struct Stage {
         if (count) SDP_CUDA_TRY(cudaMemcpyAsync(host, dev, sizeof(T) * count, cudaMemcpyDeviceToHost, st));
         return SDP_OK;
     }
+    // Upload on the side stream (ordered after the work already queued on
+    // st), so it overlaps what st runs next; join(k) makes st wait for it.
+    template <class T>
+    int up_side(int slot, const void *host, size_t count, T **dev, int k)
+    {
+        void *p = nullptr;
+        SDP_TRY(ctx_buffer(ctx, slot, sizeof(T) * std::max<size_t>(count, 1), &p));
+        SDP_CUDA_TRY(cudaEventRecord(ctx->ev[3], st));
+        SDP_CUDA_TRY(cudaStreamWaitEvent(ctx->side, ctx->ev[3], 0));
+        if (count) SDP_CUDA_TRY(cudaMemcpyAsync(p, host, sizeof(T) * count, cudaMemcpyHostToDevice, ctx->side));
+        SDP_CUDA_TRY(cudaEventRecord(ctx->ev[k], ctx->side));
+        *dev = static_cast<T *>(p);
+        return SDP_OK;
+    }
+    int join(int k)
+    {
+        SDP_CUDA_TRY(cudaStreamWaitEvent(st, ctx->ev[k], 0));
+        return SDP_OK;
+    }
     int sync()
     {
         SDP_CUDA_TRY(cudaStreamSynchronize(st));
+        SDP_CUDA_TRY(cudaStreamSynchronize(ctx->side));
         return SDP_OK;
     }
 };
@@ -96,15 +119,93 @@ int max_half_support(const sdp_int2 *sup, int nk)
         if ((call) != SDP_OK) actor_fail(name); \
     } while (0)
 
+// This thread's cached std plan (see std_plan below).
+struct PlanCache {
+    bool valid = false;
+    int n = 0, G = 0, OS = 0, nk = 0;
+    long long tks = 0;
+    double uv_scale = 0, w_scale = 0;
+    std::vector<sdp_int2> sup;
+    sdp_visplan plan;
+};
+thread_local PlanCache t_cache;
+
 // Builds a transient plan in the thread's buffers for (uvw already on device).
+// It takes the thread's plan arena, so the cached plan is dropped.
 int transient_plan(Stage &s, sdp_visplan *p, const sdp_geometry *geom, const sdp_wkernels *gk,
                    const sdp_wkernels *dk, int n, int mode, const sdp_float3 *d_uvw)
 {
+    t_cache.valid = false;
     SDP_TRY(visplan_setup(p, geom, gk, dk, n, mode));
     void *arena = nullptr;
     SDP_TRY(ctx_buffer(s.ctx, S_PLAN, visplan_arena_bytes(p), &arena));
     p->owns_arena = false;
     return visplan_build(p, arena, reinterpret_cast<const float3 *>(d_uvw), s.st);
+}
+
+// The std_gridding / std_degridding plan of this thread's last call, reused
+// when the next call bins the same visibilities: the same grid size,
+// oversampling, scales, supports and visibility count, and uvw equal word for
+// word to the ones it was built from (compared on the device after the
+// upload the call makes anyway).  A schedule calls std_degridding and
+// std_gridding with the same uvw every major cycle, so one binning serves
+// them all; only the kernel-table copies are rebuilt (visplan_kernels).  Any
+// other plan built in the thread's arena drops the cache.
+__global__ void k_words_differ(const unsigned *__restrict__ a, const unsigned *__restrict__ b, size_t n, int *diff)
+{
+    bool d = false;
+    for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x)
+        d |= a[i] != b[i];
+    if (__syncthreads_or(d) && threadIdx.x == 0) atomicOr(diff, 1);
+}
+
+int std_plan(Stage &s, sdp_visplan **out, const sdp_geometry *geom, const sdp_wkernels *wk, const sdp_int2 *host_sup,
+             int n, const sdp_float3 *d_uvw)
+{
+    PlanCache &c = t_cache;
+    const int NK = wk->num_kernels;
+    bool match = c.valid && c.n == n && c.G == geom->grid_size && c.OS == geom->oversampling &&
+                 c.uv_scale == geom->uv_scale && c.w_scale == geom->w_scale && c.nk == NK &&
+                 c.tks == (long long)wk->total_samples &&
+                 std::memcmp(c.sup.data(), host_sup, sizeof(sdp_int2) * (size_t)NK) == 0;
+    if (match && n > 0) {
+        void *key = nullptr, *flag = nullptr;
+        SDP_TRY(ctx_buffer(s.ctx, S_UVW_KEY, sizeof(sdp_float3) * (size_t)n, &key));
+        SDP_TRY(ctx_buffer(s.ctx, S_FLAG, sizeof(int), &flag));
+        SDP_CUDA_TRY(cudaMemsetAsync(flag, 0, sizeof(int), s.st));
+        k_words_differ<<<4 * num_sms(), 256, 0, s.st>>>(static_cast<const unsigned *>(key),
+                                                       reinterpret_cast<const unsigned *>(d_uvw), (size_t)n * 3,
+                                                       static_cast<int *>(flag));
+        SDP_LAUNCH_CHECK();
+        int differ = 1;
+        SDP_CUDA_TRY(cudaMemcpyAsync(&differ, flag, sizeof(int), cudaMemcpyDeviceToHost, s.st));
+        SDP_CUDA_TRY(cudaStreamSynchronize(s.st));
+        match = differ == 0;
+    }
+    if (match) {
+        c.plan.gk = *wk;
+        c.plan.dk = *wk;
+        SDP_TRY(visplan_kernels(&c.plan, s.st));
+        *out = &c.plan;
+        return SDP_OK;
+    }
+    c.valid = false;
+    SDP_TRY(transient_plan(s, &c.plan, geom, wk, wk, n, SDP_GRID_STD, d_uvw));
+    if (n > 0) {
+        void *key = nullptr;
+        SDP_TRY(ctx_buffer(s.ctx, S_UVW_KEY, sizeof(sdp_float3) * (size_t)n, &key));
+        SDP_CUDA_TRY(cudaMemcpyAsync(key, d_uvw, sizeof(sdp_float3) * (size_t)n, cudaMemcpyDeviceToDevice, s.st));
+    }
+    c.n = n;
+    c.G = geom->grid_size;
+    c.OS = geom->oversampling;
+    c.uv_scale = geom->uv_scale;
+    c.w_scale = geom->w_scale;
+    c.nk = NK;
+    c.tks = (long long)wk->total_samples;
+    c.sup.assign(host_sup, host_sup + NK);
+    *out = &c.plan;
+    return SDP_OK;  // marked valid by the caller once the plan's flags read clean
 }
 
 // ---------------------------------------------------------------------------
@@ -152,16 +253,18 @@ int do_std_gridding(int G, int NV, int NK, int TKS, int OS, int BYPASS, int *maj
     SDP_TRY(s.up(S_GKERN, kernels, TKS, &d_k));
     SDP_TRY(s.up(S_GSUP, sup, NK, &d_sup));
     SDP_TRY(s.up(S_UVW, uvw, n, &d_uvw));
-    SDP_TRY(s.up(S_VIS, vis, n, &d_vis));
+    SDP_TRY(s.up_side(S_VIS, vis, n, &d_vis, 0));  // overlaps the binning
     SDP_TRY(s.buf(S_GRID, G2, &d_grid));
     sdp_geometry geom{G, OS, cfg->uv_scale, cfg->w_scale};
     sdp_wkernels wk{d_k, d_sup, NK, TKS, max_half_support(sup, NK)};
-    sdp_visplan p;
-    SDP_TRY(transient_plan(s, &p, &geom, &wk, &wk, n, SDP_GRID_STD, d_uvw));
-    SDP_TRY(sdp_visplan_grid(&p, d_vis, d_grid, 0, s.st));
+    sdp_visplan *p = nullptr;
+    SDP_TRY(std_plan(s, &p, &geom, &wk, sup, n, d_uvw));
+    SDP_TRY(s.join(0));
+    SDP_TRY(sdp_visplan_grid(p, d_vis, d_grid, 0, s.st));
     SDP_TRY(s.down(out_grid, d_grid, G2));
-    SDP_TRY(visplan_check_flags(&p, s.st));
-    return SDP_OK;
+    SDP_TRY(visplan_check_flags(p, s.st));
+    t_cache.valid = true;
+    return s.sync();
 }
 
 int do_std_degridding(int G, int NV, int NK, int TKS, int OS, sdp_float2 *kernels, sdp_int2 *sup, sdp_float2 *grid,
@@ -176,11 +279,12 @@ int do_std_degridding(int G, int NV, int NK, int TKS, int OS, sdp_float2 *kernel
     sdp_float3 *d_uvw;
     sdp_float2 *d_grid, *d_out;
     SDP_TRY(s.up(S_UVW, uvw, n, &d_uvw));
-    SDP_TRY(s.up(S_GRID, grid, G2, &d_grid));
+    SDP_TRY(s.up_side(S_GRID, grid, G2, &d_grid, 0));  // overlaps the binning
     SDP_TRY(s.buf(S_OUTVIS, std::max(NV, 1), &d_out));
     // degridgrid.c:132: every output entry starts at zero
     SDP_CUDA_TRY(cudaMemsetAsync(d_out, 0, sizeof(sdp_float2) * (size_t)NV, s.st));
     if (g_degrid_mode == SDP_DEGRID_NEAREST) {
+        SDP_TRY(s.join(0));
         SDP_TRY(sdp_degrid_nearest(G, cfg->uv_scale, n, d_uvw, d_grid, d_out, s.st));
         SDP_TRY(s.down(out, d_out, NV));
         SDP_TRY(s.sync());
@@ -193,12 +297,14 @@ int do_std_degridding(int G, int NV, int NK, int TKS, int OS, sdp_float2 *kernel
     SDP_TRY(s.up(S_DSUP, sup, NK, &d_sup));
     sdp_geometry geom{G, OS, cfg->uv_scale, cfg->w_scale};
     sdp_wkernels wk{d_k, d_sup, NK, TKS, max_half_support(sup, NK)};
-    sdp_visplan p;
-    SDP_TRY(transient_plan(s, &p, &geom, &wk, &wk, n, SDP_GRID_STD, d_uvw));
-    SDP_TRY(sdp_visplan_degrid(&p, d_grid, d_out, SDP_DEGRID_CONV, s.st));
+    sdp_visplan *p = nullptr;
+    SDP_TRY(std_plan(s, &p, &geom, &wk, sup, n, d_uvw));
+    SDP_TRY(s.join(0));
+    SDP_TRY(sdp_visplan_degrid(p, d_grid, d_out, SDP_DEGRID_CONV, s.st));
     SDP_TRY(s.down(out, d_out, NV));
-    SDP_TRY(visplan_check_flags(&p, s.st));
-    return SDP_OK;
+    SDP_TRY(visplan_check_flags(p, s.st));
+    t_cache.valid = true;
+    return s.sync();
 }
 
 int do_g2g(int G, int NV, int NGK, int NDK, int TGK, int TDK, int OS, sdp_float2 *gk, sdp_int2 *gs, sdp_float2 *dk,
@@ -290,15 +396,29 @@ int do_vis_binary(int n, const sdp_float2 *a, const sdp_float2 *b, sdp_float2 *o
     Stage s;
     SDP_TRY(s.init());
     sdp_float2 *da, *db, *dout;
-    SDP_TRY(s.up(S_VIS, a, n, &da));
-    SDP_TRY(s.up(S_VIS2, b, n, &db));
+    SDP_TRY(s.buf(S_VIS, n, &da));
+    SDP_TRY(s.buf(S_VIS2, n, &db));
     SDP_TRY(s.buf(S_OUTVIS, n, &dout));
-    if (subtract) {
-        SDP_TRY(sdp_subtract_vis(n, da, db, dout, s.st));
-    } else {
-        SDP_TRY(sdp_add_vis(n, da, db, dout, s.st));
+    // chunks: uploads and the kernel on the thread's stream, each chunk's
+    // download on the side stream, so downloads overlap later uploads (the
+    // two copy directions run concurrently)
+    constexpr int kChunks = 4;
+    const int per = (n + kChunks - 1) / kChunks;
+    SDP_CUDA_TRY(cudaEventRecord(s.ctx->ev[3], s.st));
+    SDP_CUDA_TRY(cudaStreamWaitEvent(s.ctx->side, s.ctx->ev[3], 0));
+    for (int c = 0, b0 = 0; c < kChunks && b0 < n; ++c, b0 += per) {
+        const int m = std::min(per, n - b0);
+        SDP_CUDA_TRY(cudaMemcpyAsync(da + b0, a + b0, sizeof(sdp_float2) * m, cudaMemcpyHostToDevice, s.st));
+        SDP_CUDA_TRY(cudaMemcpyAsync(db + b0, b + b0, sizeof(sdp_float2) * m, cudaMemcpyHostToDevice, s.st));
+        if (subtract) {
+            SDP_TRY(sdp_subtract_vis(m, da + b0, db + b0, dout + b0, s.st));
+        } else {
+            SDP_TRY(sdp_add_vis(m, da + b0, db + b0, dout + b0, s.st));
+        }
+        SDP_CUDA_TRY(cudaEventRecord(s.ctx->ev[c % 3], s.st));
+        SDP_CUDA_TRY(cudaStreamWaitEvent(s.ctx->side, s.ctx->ev[c % 3], 0));
+        SDP_CUDA_TRY(cudaMemcpyAsync(o + b0, dout + b0, sizeof(sdp_float2) * m, cudaMemcpyDeviceToHost, s.ctx->side));
     }
-    SDP_TRY(s.down(o, dout, n));
     return s.sync();
 }
 

@@ -62,6 +62,8 @@ struct DevBuf {
 
 struct ThreadCtx {
     cudaStream_t stream = nullptr;
+    cudaStream_t side = nullptr;  // second stream: uploads that overlap work on `stream`
+    cudaEvent_t ev[4] = {};       // ordering between the two (timing disabled)
     int device = -1;
     DevBuf bufs[24];
     ~ThreadCtx();

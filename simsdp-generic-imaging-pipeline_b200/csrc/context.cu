@@ -55,6 +55,9 @@ ThreadCtx::~ThreadCtx()
     // at process exit the driver reclaims them.
     for (auto &b : bufs)
         if (b.ptr) cudaFree(b.ptr);
+    for (auto &e : ev)
+        if (e) cudaEventDestroy(e);
+    if (side) cudaStreamDestroy(side);
     if (stream) cudaStreamDestroy(stream);
 }
 
@@ -70,10 +73,18 @@ int thread_ctx(ThreadCtx **out)
                 b.ptr = nullptr;
                 b.bytes = 0;
             }
+            for (auto &e : c->ev) {
+                if (e) cudaEventDestroy(e);
+                e = nullptr;
+            }
+            if (c->side) cudaStreamDestroy(c->side);
             cudaStreamDestroy(c->stream);
             c->stream = nullptr;
+            c->side = nullptr;
         }
         SDP_CUDA_TRY(cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking));
+        SDP_CUDA_TRY(cudaStreamCreateWithFlags(&c->side, cudaStreamNonBlocking));
+        for (auto &e : c->ev) SDP_CUDA_TRY(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
         c->device = dev;
     }
     *out = c;
@@ -90,6 +101,7 @@ int ctx_buffer(ThreadCtx *ctx, int slot, size_t bytes, void **out)
         if (b.ptr) {
             // the previous contents may still be in use by queued work
             SDP_CUDA_TRY(cudaStreamSynchronize(ctx->stream));
+            SDP_CUDA_TRY(cudaStreamSynchronize(ctx->side));
             SDP_CUDA_TRY(cudaFree(b.ptr));
             b.ptr = nullptr;
             b.bytes = 0;

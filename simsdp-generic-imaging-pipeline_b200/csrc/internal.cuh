@@ -58,6 +58,9 @@ size_t visplan_arena_bytes(const sdp_visplan *p);
 // Bins the visibilities into the arena (which must hold visplan_arena_bytes).
 int visplan_build(sdp_visplan *p, void *arena, const float3 *uvw, cudaStream_t st);
 size_t visplan_record_bytes(const sdp_visplan *p);
+// Rebuilds the kernel-table copies of a built plan from p->gk / p->dk (same
+// supports as at build time).
+int visplan_kernels(sdp_visplan *p, cudaStream_t st);
 // Reads and clears the device error flags (blocking on st).
 int visplan_check_flags(sdp_visplan *p, cudaStream_t st);
 

@@ -905,35 +905,13 @@ size_t visplan_arena_bytes(const sdp_visplan *p)
     return total;
 }
 
-int visplan_build(sdp_visplan *p, void *arena, const float3 *uvw, cudaStream_t st)
+// (Re)builds the plan's kernel-table copies and the sharing flag from
+// p->gk / p->dk (the binning does not depend on the table contents, only on
+// the supports, so a plan can be reused with other tables of the same
+// supports after this).
+int visplan_kernels(sdp_visplan *p, cudaStream_t st)
 {
-    size_t off[16], total;
-    plan_layout(p, off, &total);
-    char *a = static_cast<char *>(arena);
-    p->arena = arena;
-    p->rec = a + off[0];
-    void *rec_tmp = a + off[1];
-    p->perm = reinterpret_cast<int *>(a + off[2]);
-    int *keys = reinterpret_cast<int *>(a + off[3]);
-    int *counts = reinterpret_cast<int *>(a + off[4]);
-    int *offsets = reinterpret_cast<int *>(a + off[5]);
-    int *item_counts = reinterpret_cast<int *>(a + off[6]);
-    int *item_offsets = reinterpret_cast<int *>(a + off[7]);
-    p->items = reinterpret_cast<int4 *>(a + off[8]);
-    int *scan_scratch = reinterpret_cast<int *>(a + off[9]);
-    int *scalars = reinterpret_cast<int *>(a + off[10]);
-    p->n_items = scalars;
-    p->item_counter = scalars + 1;
-    p->flags = scalars + 2;
-    p->kshare = scalars + 3;
-    p->measured = reinterpret_cast<float2 *>(a + off[11]);
-    p->gpoff = reinterpret_cast<int *>(a + off[12]);
-    p->dpoff = reinterpret_cast<int *>(a + off[13]);
-    p->gk2 = reinterpret_cast<float2 *>(a + off[14]);
-    p->dk2 = reinterpret_cast<float2 *>(a + off[15]);
-    const int n = p->n;
-
-    SDP_CUDA_TRY(cudaMemsetAsync(scalars, 0, sizeof(int) * 4, st));
+    SDP_CUDA_TRY(cudaMemsetAsync(p->kshare, 0, sizeof(int), st));
     // kernel tables: phase-major copies (or the caller's tables as they are)
     {
         const int os = p->geom.oversampling;
@@ -966,6 +944,39 @@ int visplan_build(sdp_visplan *p, void *arena, const float3 *uvw, cudaStream_t s
         SDP_LAUNCH_CHECK();
     }
 
+    return SDP_OK;
+}
+
+int visplan_build(sdp_visplan *p, void *arena, const float3 *uvw, cudaStream_t st)
+{
+    size_t off[16], total;
+    plan_layout(p, off, &total);
+    char *a = static_cast<char *>(arena);
+    p->arena = arena;
+    p->rec = a + off[0];
+    void *rec_tmp = a + off[1];
+    p->perm = reinterpret_cast<int *>(a + off[2]);
+    int *keys = reinterpret_cast<int *>(a + off[3]);
+    int *counts = reinterpret_cast<int *>(a + off[4]);
+    int *offsets = reinterpret_cast<int *>(a + off[5]);
+    int *item_counts = reinterpret_cast<int *>(a + off[6]);
+    int *item_offsets = reinterpret_cast<int *>(a + off[7]);
+    p->items = reinterpret_cast<int4 *>(a + off[8]);
+    int *scan_scratch = reinterpret_cast<int *>(a + off[9]);
+    int *scalars = reinterpret_cast<int *>(a + off[10]);
+    p->n_items = scalars;
+    p->item_counter = scalars + 1;
+    p->flags = scalars + 2;
+    p->kshare = scalars + 3;
+    p->measured = reinterpret_cast<float2 *>(a + off[11]);
+    p->gpoff = reinterpret_cast<int *>(a + off[12]);
+    p->dpoff = reinterpret_cast<int *>(a + off[13]);
+    p->gk2 = reinterpret_cast<float2 *>(a + off[14]);
+    p->dk2 = reinterpret_cast<float2 *>(a + off[15]);
+    const int n = p->n;
+
+    SDP_CUDA_TRY(cudaMemsetAsync(scalars, 0, sizeof(int) * 4, st));
+    SDP_TRY(visplan_kernels(p, st));
     SDP_CUDA_TRY(cudaMemsetAsync(counts, 0, sizeof(int) * ((size_t)p->nbins + 1), st));
     if (n > 0) {
         const int2 *gs = reinterpret_cast<const int2 *>(p->gk.supports);
