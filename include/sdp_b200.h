@@ -117,7 +117,8 @@ enum {
     SDP_ERR_CUDA = 3,     /* CUDA runtime error or no usable device         */
     SDP_ERR_NOMEM = 4,    /* device allocation failed                        */
     SDP_ERR_TIMEOUT = 5,  /* a bounded device-side wait gave up             */
-    SDP_ERR_DATA = 6      /* input data outside the grid / kernel tables     */
+    SDP_ERR_DATA = 6,     /* input data outside the grid / kernel tables     */
+    SDP_ERR_IO = 7        /* an input file could not be opened or read      */
 };
 
 int sdp_last_status(void);           /* status of the calling thread's last failing call */
@@ -225,7 +226,19 @@ void split_uvgrid(int GRID_SIZE, int SLICES, sdp_float2 *input_grid, sdp_float2 
 void subtract_from_measurements_finegrid(int NUM_VISIBILITIES, sdp_float2 *gridded_measured_vis,
                                          sdp_float2 *input_vis, int *num_finegrid_vis, sdp_float2 *delta_vis);
 
-/* top.h:17, 31-41, 43-45 — setup math (file-reading setup actors are not exported). */
+/* top.h:24, 26, 28, 37 — file-reading setup actors (top.c:139-380, 453-510):
+ * the same files, values and float roundings as the reference, parsed by
+ * several host threads instead of one fscanf per number.  Host code only.
+ * A file that cannot be opened sets SDP_ERR_IO (the reference exits). */
+void visibility_host_set_up(int NUM_VISIBILITIES, sdp_config *config, sdp_float3 *vis_uvw_coords,
+                            sdp_float2 *measured_vis);
+void kernel_host_set_up(int NUM_KERNELS, int TOTAL_KERNEL_SAMPLES, sdp_config *config, sdp_int2 *kernel_supports,
+                        sdp_float2 *kernels);
+void degridding_kernel_host_set_up(int NUM_KERNELS, int TOTAL_KERNEL_SAMPLES, sdp_config *config,
+                                   sdp_int2 *degridding_kernel_supports, sdp_float2 *degridding_kernels);
+void psf_host_set_up(int GRID_SIZE, int PSF_GRID_SIZE, sdp_config *config, float *psf, double *psf_max_value);
+
+/* top.h:17, 31-41, 43-45 — setup math. */
 void config_struct_set_up(int GRID_SIZE, int NUM_KERNELS, sdp_config *config);
 void correction_set_up(int GRID_SIZE, float *prolate);
 void create_1D_half_prolate(float *prolate, int grid_size);
