@@ -238,6 +238,20 @@ void degridding_kernel_host_set_up(int NUM_KERNELS, int TOTAL_KERNEL_SAMPLES, sd
                                    sdp_int2 *degridding_kernel_supports, sdp_float2 *degridding_kernels);
 void psf_host_set_up(int GRID_SIZE, int PSF_GRID_SIZE, sdp_config *config, float *psf, double *psf_max_value);
 
+/* major_loop_iter.h:22, 27-30 and major_loop_iter.c:8 — restoring and
+ * writing (major_loop_iter.c:8-46, 168-278): conv2D runs on the GPU with the
+ * reference's products and order of additions (bit-exact); the writers
+ * format "%f, " as the reference does, on all host threads.  The reference
+ * prints an MD5 of every image it saves; these writers do not. */
+void conv2D(float *image, float *filter, float *result, int IMAGE_DIM, sdp_int2 filter_half_dims);
+void save_image_to_file(sdp_config *config, float *image, const char *file_name, int start_x, int start_y,
+                        int range_x, int range_y, int cycle);
+void save_output(int GRID_SIZE, float *residual, float *model, float *clean_psf, sdp_int2 *clean_psf_halfdims,
+                 float *psf, sdp_config *config, int *cycle);
+void save_extracted_sources_actor(int GRID_SIZE, int SAVE_EXTRACTED_SOURCES, int NUM_MAX_SOURCES, int *num_sources,
+                                  sdp_float3 *sources, int *cycle_count, sdp_config *config, float *image_in,
+                                  float *clean_psf, sdp_int2 *clean_psf_halfdims, float *image_out);
+
 /* top.h:17, 31-41, 43-45 — setup math. */
 void config_struct_set_up(int GRID_SIZE, int NUM_KERNELS, sdp_config *config);
 void correction_set_up(int GRID_SIZE, float *prolate);
@@ -353,6 +367,15 @@ int sdp_prolate_table(int grid_size, float *prolate_ext, void *stream); /* G/2 +
 /* top.c:530-595: Gaussian clean beam from the dirty PSF; halfdims_dev: 2 ints. */
 int sdp_clean_psf(int grid_size, double psf_max_value, const float *dirty_psf, float *clean_psf, int *halfdims_dev,
                   void *stream);
+
+/* The model image convolved with the clean PSF window (conv2D,
+ * major_loop_iter.c:8-46), bit-exact with the reference: model pixels >= 1e-5
+ * contribute model * psf[(G/2+1 - fy) G + (G/2+1 - fx)] for (fy, fx) in
+ * [-half_y, half_y) x [-half_x, half_x) inside the image.  Device pointers;
+ * workspace of sdp_restore_workspace_bytes(grid_size). */
+int sdp_restore_workspace_bytes(int grid_size, size_t *bytes);
+int sdp_restore(int grid_size, const float *model, const float *clean_psf, int half_x, int half_y, float *result,
+                void *workspace, size_t workspace_bytes, void *stream);
 
 /* 2-D complex FFT, FFTW sign convention (-1 forward, +1 inverse), unnormalised.
  * Power-of-two grid_size from 16 to 16384; in may equal out. */

@@ -46,6 +46,7 @@ enum Slot {
     S_WS,
     S_COUNT
 };
+static_assert(S_COUNT <= kSlotRestore, "actor buffer slots overlap the restore actors' slots");
 
 struct Stage {
     ThreadCtx *ctx = nullptr;

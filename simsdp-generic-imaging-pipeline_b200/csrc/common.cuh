@@ -69,6 +69,10 @@ struct ThreadCtx {
     ~ThreadCtx();
 };
 
+// Buffer slots 0 .. kSlotRestore-1 belong to the actor layer (actors.cu),
+// kSlotRestore .. +3 to the restore / writer actors (restore.cu).
+constexpr int kSlotRestore = 20;
+
 int thread_ctx(ThreadCtx **out);
 // Returns a device buffer of at least `bytes` for slot `slot` of this thread.
 int ctx_buffer(ThreadCtx *ctx, int slot, size_t bytes, void **out);
