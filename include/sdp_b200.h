@@ -222,6 +222,26 @@ void split_fftdegrid_visibilities(int NUM_VISIBILITIES, int SLICES, int GRID_SIZ
                                   sdp_config *output_configs, int *num_vis, int *maj_iter_out);
 void split_uvgrid(int GRID_SIZE, int SLICES, sdp_float2 *input_grid, sdp_float2 *output_grid);
 
+/* gains_apply_run.h:14, 19, 23, 28 and top.h:19, 22 — gains (gains_apply_run.c:4-120,
+ * top.c:71-136): conj(g)/|g|^2 per receiver, and measured * g_a * conj(g_b)
+ * (minus the prediction) per visibility, baseline = index % NUM_BASELINES;
+ * bit-exact with the float build.  apply_gains_only stores the measured
+ * visibilities unchanged, as the reference does (:117).  A receiver pair
+ * outside [0, NUM_RECEIVERS) sets SDP_ERR_DATA (the reference reads past
+ * gains[]). */
+void reciprocal_transform_actor(int NUM_RECEIVERS, sdp_float2 *gains_in, sdp_config *config, sdp_float2 *gains_out);
+void apply_gains_actor(int CALIBRATION, int NUM_RECEIVERS, int NUM_BASELINES, int NUM_VISIBILITIES,
+                       sdp_float2 *measured_vis, sdp_float2 *visibilities_in, sdp_float2 *gains,
+                       sdp_int2 *receiver_pairs, sdp_config *config, sdp_float2 *visibilities_out);
+void subtract_from_measurements(int NUM_RECEIVERS, int NUM_BASELINES, int NUM_VISIBILITIES, sdp_float2 *measured_vis,
+                                sdp_float2 *visibilities_in, sdp_float2 *gains, sdp_int2 *receiver_pairs,
+                                sdp_config *config, sdp_float2 *visibilities_out);
+void apply_gains_only(int NUM_RECEIVERS, int NUM_BASELINES, int NUM_VISIBILITIES, sdp_float2 *measured_vis,
+                      sdp_float2 *gains, sdp_int2 *receiver_pairs, sdp_config *config, sdp_float2 *visibilities_out);
+void gains_host_set_up(int NUM_RECEIVERS, int NUM_BASELINES, sdp_config *config, sdp_float2 *gains,
+                       sdp_int2 *receiver_pairs);
+void calculate_receiver_pairs(int NUM_BASELINES, int NUM_RECEIVERS, sdp_int2 *receiver_pairs);
+
 /* gains_apply_run.h:31 */
 void subtract_from_measurements_finegrid(int NUM_VISIBILITIES, sdp_float2 *gridded_measured_vis,
                                          sdp_float2 *input_vis, int *num_finegrid_vis, sdp_float2 *delta_vis);
@@ -376,6 +396,15 @@ int sdp_clean_psf(int grid_size, double psf_max_value, const float *dirty_psf, f
 int sdp_restore_workspace_bytes(int grid_size, size_t *bytes);
 int sdp_restore(int grid_size, const float *model, const float *clean_psf, int half_x, int half_y, float *result,
                 void *workspace, size_t workspace_bytes, void *stream);
+
+/* Gains on the device: reciprocal per receiver; per visibility
+ * out = measured * g[pair.x] * conj(g[pair.y]) (- vis_in when subtract),
+ * pair = receiver_pairs[i % num_baselines].  flags_dev (device int, cleared
+ * by the caller) gets 1 when a pair indexes outside the gains. */
+int sdp_gains_reciprocal(int num_receivers, const sdp_float2 *gains_in, sdp_float2 *gains_out, void *stream);
+int sdp_apply_gains(int num_vis, int num_baselines, int num_receivers, const sdp_float2 *measured,
+                    const sdp_float2 *vis_in, const sdp_float2 *gains, const sdp_int2 *receiver_pairs, int subtract,
+                    sdp_float2 *vis_out, int *flags_dev, void *stream);
 
 /* 2-D complex FFT, FFTW sign convention (-1 forward, +1 inverse), unnormalised.
  * Power-of-two grid_size from 16 to 16384; in may equal out. */
