@@ -406,6 +406,28 @@ int sdp_apply_gains(int num_vis, int num_baselines, int num_receivers, const sdp
                     const sdp_float2 *vis_in, const sdp_float2 *gains, const sdp_int2 *receiver_pairs, int subtract,
                     sdp_float2 *vis_out, int *flags_dev, void *stream);
 
+/* Inputs the reference reads from files and never generates (no counterpart
+ * in its code; its kernel files follow the layout of top.c:256-312):
+ * W-projection kernel tables for num_planes planes of the given half
+ * supports, oversampling, maximum |w| and field of view (separable
+ * prolate-tapered w screen, image_samples points across the field), written
+ * in the reference's quarter-plane layout with supports[p] = (hs, offset);
+ * degrid_kernels (may be NULL) receives the conjugates.  Device tables;
+ * supports may be host or device memory; scratch of
+ * sdp_wkernels_generate_scratch_bytes.  Synchronises the stream. */
+int sdp_wkernels_generate_sizes(int num_planes, const int *half_supports, int oversampling, int *total_samples);
+size_t sdp_wkernels_generate_scratch_bytes(int num_planes, const int *half_supports, int oversampling);
+int sdp_wkernels_generate(int num_planes, const int *half_supports, int oversampling, double max_w, double fov_rad,
+                          int image_samples, sdp_float2 *grid_kernels, sdp_float2 *degrid_kernels,
+                          sdp_int2 *supports, void *scratch, size_t scratch_bytes, void *stream);
+/* The dirty PSF of a std_gridding plan: unit visibilities gridded, shifted,
+ * inverse-transformed, taper-corrected (as a major cycle images), then
+ * divided by its maximum, which lands in *psf_max_dev (device double), as
+ * psf_host_set_up normalises the PSF it reads (top.c:481-509).  Scratch:
+ * num_vis complex, two G^2 complex. */
+int sdp_psf_generate(sdp_visplan *plan, const float *prolate_ext, sdp_float2 *unit_vis_scratch,
+                     sdp_float2 *grid_scratch, sdp_float2 *work, float *psf, double *psf_max_dev, void *stream);
+
 /* 2-D complex FFT, FFTW sign convention (-1 forward, +1 inverse), unnormalised.
  * Power-of-two grid_size from 16 to 16384; in may equal out. */
 int sdp_fft2d(int grid_size, const sdp_float2 *in, sdp_float2 *out, int sign, void *stream);

@@ -3,7 +3,7 @@
 // a grid sized to a multiple of the SM count.
 #include <algorithm>
 
-#include "common.cuh"
+#include "internal.cuh"
 
 namespace sdp {
 
@@ -146,40 +146,6 @@ __global__ void k_conv_correction(int G, const float *__restrict__ in, const flo
     }
 }
 
-// top.c:399-451: Schwab's rational approximation of the prolate spheroidal,
-// evaluated in double with the reference's two-interval split at nu = 0.75.
-__device__ double prolate_schwab(double nu)
-{
-    const double p[10] = {0.08203343, -0.3644705, 0.627866, -0.5335581, 0.2312756,
-                          0.004028559, -0.03697768, 0.1021332, -0.1201436, 0.06412774};
-    const double q[6] = {1.0, 0.8212018, 0.2078043, 1.0, 0.9599102, 0.2918724};
-    int part;
-    double nuend;
-    if (nu >= 0.0 && nu < 0.75) {
-        part = 0;
-        nuend = 0.75;
-    } else if (nu >= 0.75 && nu < 1.0) {
-        part = 1;
-        nuend = 1.0;
-    } else {
-        return 0.0;
-    }
-    const double d = nu * nu - nuend * nuend;
-    // powers formed by repeated multiplication (pow(delta, i) for small
-    // integer i is exact to the last bit on glibc only up to rounding; the
-    // table is checked against the reference to 1 ulp)
-    double top = p[part * 5], bot = q[part * 3], dp = 1.0;
-    for (int i = 1; i < 5; ++i) {
-        dp = __dmul_rn(dp, d);
-        top = __dadd_rn(top, __dmul_rn(p[part * 5 + i], dp));
-    }
-    dp = 1.0;
-    for (int i = 1; i < 3; ++i) {
-        dp = __dmul_rn(dp, d);
-        bot = __dadd_rn(bot, __dmul_rn(q[part * 3 + i], dp));
-    }
-    return (bot == 0.0) ? 0.0 : __ddiv_rn(top, bot);
-}
 
 __global__ void k_prolate(int G, float *__restrict__ out)
 {
