@@ -439,7 +439,8 @@ int sdp_grid_to_image(int grid_size, const sdp_float2 *grid, const float *prolat
 int sdp_image_to_grid(int grid_size, const float *image, sdp_float2 *work, sdp_float2 *grid, void *stream);
 
 /* DFT predict: sources (l, m, I); phase argument in FP64 (north-star
- * precision), sin/cos in FP32 after exact range reduction. */
+ * precision), sin/cos in FP32 (hardware approximation) after exact range
+ * reduction to one turn. */
 int sdp_dft(int num_vis, int num_sources, const sdp_float3 *sources, const sdp_float3 *uvw, sdp_float2 *vis,
             void *stream);
 
