@@ -57,6 +57,7 @@ def parse():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-major-cycle", action="store_true")
     ap.add_argument("--no-c3", action="store_true", help="skip the batched 64-channel pass")
+    ap.add_argument("--no-c5", action="store_true", help="skip the 8192^2 single-channel measurement")
     ap.add_argument("--cpu-sample", type=int, default=200_000, help="visibilities per CPU-baseline step")
     return ap.parse_args()
 
@@ -353,6 +354,74 @@ def c3_block(S, D, dev, reps: int = 5):
     return out
 
 
+def c5_block(S, D, dev, reps: int = 3):
+    """One channel of the large g2g-scale workload: 512 antennas on a seeded
+    40 km log spiral, 200 time steps (26,163,200 visibilities), 8192^2 grid,
+    64 w-planes of half support 4 (kernels generated on the GPU), OS 16.
+    Times the plan build, the fused visibility pass and a whole major cycle
+    (graph; 200 Hogbom minor cycles on 8192^2, the one-launch-per-cycle
+    path)."""
+    import torch
+
+    w = synth.make_workload("c5_8192", 512, 20000.0, "spiral", 200, 8192, 1, 1e-3, 1.0, 1e-4, 64, 4,
+                            freq_hz=140e6, seed=5, compute_vis=False)
+    G, OS, N = w.cfg.grid_size, w.cfg.oversampling, w.num_vis
+    fov = w.cfg.cell_size * G
+    gk, dk, sup = D.wkernels_generate([4] * 64, OS, w.cfg.max_w, fov)
+    sup_h = sup.cpu().numpy()
+    wk_g = S.Device.wkernels(gk, sup, sup_h)
+    wk_d = S.Device.wkernels(dk, sup, sup_h)
+    uvw_raw = torch.from_numpy(w.uvw).to(dev)
+    uvw = torch.empty_like(uvw_raw)
+    D.correct_to_finegrid(G, OS, w.cfg.uv_scale, uvw_raw, uvw)
+    del uvw_raw
+    gen = torch.Generator(device=dev).manual_seed(23)
+    meas = 0.1 * torch.randn((N, 2), device=dev, generator=gen)
+
+    def ev_time(fn, n):
+        fn()
+        torch.cuda.synchronize()
+        ts = []
+        for _ in range(n):
+            a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            a.record()
+            fn()
+            b.record()
+            torch.cuda.synchronize()
+            ts.append(a.elapsed_time(b))
+        return statistics.median(ts)
+
+    plans = []
+    t_plan = ev_time(lambda: plans.append(D.plan(G, OS, w.cfg.uv_scale, w.cfg.w_scale, uvw, wk_g, wk_d,
+                                                 keep=(uvw, gk, dk, sup))), 2)
+    for pl in plans[:-1]:
+        pl.close()
+    plan = plans[-1]
+    plan.set_measured(meas)
+    model = (1e-3 * torch.randn((G * G, 2), device=dev, generator=gen)).contiguous()
+    res = torch.empty_like(model)
+    t_pass = ev_time(lambda: plan.cycle(model, res, S.SDP_DEGRID_CONV), reps)
+    prol = torch.empty(G // 2 + 1, dtype=torch.float32, device=dev)
+    D.prolate_table(G, prol)
+    psf = torch.empty(G * G, dtype=torch.float32, device=dev)
+    psf_max = D.psf_generate(plan, prol, psf)
+    del model, res
+    torch.cuda.empty_cache()
+    pcfg = S.PipelineConfig(G, OS, w.cfg.uv_scale, w.cfg.w_scale, w.cfg.cell_size, 200, 200, 0.1, 1.5, 0.0002,
+                            psf_max, S.SDP_DEGRID_CONV, S.SDP_COORD_F32, 0, 1)
+    pipe = D.pipeline(pcfg, uvw, meas, psf, wk_g, wk_d, keep=(uvw, gk, dk, sup))
+    t_cyc = ev_time(pipe.major_cycle, 2)
+    out = {"workload": "512 antennas 40 km spiral, 200 time steps, 26163200 vis, G=8192, 64 w-planes hs=4 "
+                       "OS=16 (kernels generated on the GPU)",
+           "ms_plan_build": t_plan, "ms_fused_pass": t_pass, "vis_per_s_fused_pass": N / (t_pass * 1e-3),
+           "ms_major_cycle": t_cyc, "cuda_graph": pipe.graph_active(), "minor_cycles": 200}
+    pipe.close()
+    plan.close()
+    del psf, meas, uvw
+    torch.cuda.empty_cache()
+    return out
+
+
 def b200_arm(args):
     import torch
     import torch.distributed as dist
@@ -487,6 +556,10 @@ def b200_arm(args):
     if world == 1 and not args.no_c3:
         c3 = c3_block(S, D, dev)
 
+    c5 = None
+    if world == 1 and not args.no_c5:
+        c5 = c5_block(S, D, dev)
+
     # ---- e2e through the reference-facing C ABI with pinned host buffers ---------------
     uvw_h = torch.empty((N, 3), dtype=torch.float32).pin_memory()
     uvw_h.copy_(uvw.cpu())
@@ -556,6 +629,8 @@ def b200_arm(args):
         line["major_cycle"] = major
     if c3 is not None:
         line["c3_batched"] = c3
+    if c5 is not None:
+        line["c5_channel_8192"] = c5
     if cpu is not None:
         line["cpu_baseline"] = cpu
     plan.close()

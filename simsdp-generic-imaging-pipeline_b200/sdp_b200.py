@@ -598,6 +598,39 @@ class Device:
         check(self.lib.sdp_image_to_grid(_i(grid_size), _dp(image), _dp(work), _dp(grid), _stream(stream)),
               self.lib)
 
+    def psf_generate(self, plan: "VisPlan", prolate, psf, stream=None):
+        """Dirty PSF of a plan's uv coverage, normalised to peak 1; returns the
+        peak before normalisation."""
+        import torch
+        G = plan.geom.grid_size
+        dev = psf.device
+        ones = torch.empty((max(plan.n, 1), 2), dtype=torch.float32, device=dev)
+        grid = torch.empty((G * G, 2), dtype=torch.float32, device=dev)
+        work = torch.empty_like(grid)
+        mx = torch.zeros(1, dtype=torch.float64, device=dev)
+        check(self.lib.sdp_psf_generate(plan.handle, _dp(prolate), _dp(ones), _dp(grid), _dp(work), _dp(psf),
+                                        _dp(mx), _stream(stream)), self.lib)
+        return float(mx.item())
+
+    def wkernels_generate(self, half_supports, oversampling, max_w, fov_rad, image_samples=256, stream=None):
+        """W-projection tables on the device: (gridding, degridding, supports)."""
+        import torch
+        planes = len(half_supports)
+        hs = (_i * planes)(*[int(h) for h in half_supports])
+        total = _i(0)
+        check(self.lib.sdp_wkernels_generate_sizes(_i(planes), hs, _i(oversampling), C.byref(total)), self.lib)
+        self.lib.sdp_wkernels_generate_scratch_bytes.restype = C.c_size_t
+        nscr = self.lib.sdp_wkernels_generate_scratch_bytes(_i(planes), hs, _i(oversampling))
+        dev = torch.device("cuda", torch.cuda.current_device())
+        gk = torch.empty((total.value, 2), dtype=torch.float32, device=dev)
+        dk = torch.empty_like(gk)
+        sup = torch.empty((planes, 2), dtype=torch.int32, device=dev)
+        scr = torch.empty(nscr, dtype=torch.uint8, device=dev)
+        check(self.lib.sdp_wkernels_generate(_i(planes), hs, _i(oversampling), _d(max_w), _d(fov_rad),
+                                             _i(image_samples), _dp(gk), _dp(dk), _dp(sup), _dp(scr),
+                                             C.c_size_t(nscr), _stream(stream)), self.lib)
+        return gk, dk, sup
+
     def prolate_table(self, grid_size, out, stream=None):
         check(self.lib.sdp_prolate_table(_i(grid_size), _dp(out), _stream(stream)), self.lib)
 
