@@ -550,6 +550,25 @@ def b200_arm(args):
                  "cuda_graph": pl.graph_active(), "graph_error": pl.graph_error(),
                  "stages": "image->grid FFT, fused degrid/subtract/grid, grid->image FFT + taper, Hogbom x200"}
         pl.close()
+        # time to the target residual RMS (plain Hogbom pipeline): from an empty
+        # model, cycles until the FP64 residual RMS is within 1 % of the lowest
+        # reached in 12 cycles
+        pl = D.pipeline(pcfg, uvw, measured, psf, wk_g, wk_d, keep=(uvw, gk, dk, sup))
+        ms, rms = [], []
+        for _ in range(12):
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            pl.major_cycle()
+            e1.record(stream)
+            torch.cuda.synchronize()
+            ms.append(e0.elapsed_time(e1))
+            rms.append(pl.residual_rms())
+        target = 1.01 * min(rms)
+        k = next(i for i, r in enumerate(rms) if r <= target)
+        major["time_to_rms"] = {"target": "1.01 x the lowest FP64 residual RMS of 12 plain cycles",
+                                "cycles": k + 1, "ms": float(sum(ms[:k + 1])),
+                                "rms_per_cycle": [float(r) for r in rms], "learned": "not built"}
+        pl.close()
 
     # ---- the batched multi-channel pass (one GPU only) ---------------------------------
     c3 = None

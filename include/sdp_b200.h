@@ -428,6 +428,10 @@ int sdp_wkernels_generate(int num_planes, const int *half_supports, int oversamp
 int sdp_psf_generate(sdp_visplan *plan, const float *prolate_ext, sdp_float2 *unit_vis_scratch,
                      sdp_float2 *grid_scratch, sdp_float2 *work, float *psf, double *psf_max_dev, void *stream);
 
+/* RMS of an image, summed in FP64 in a fixed order (the residual level that
+ * decides major-cycle convergence).  *rms_dev is a device double. */
+int sdp_image_rms(int grid_size, const float *image, double *rms_dev, void *stream);
+
 /* 2-D complex FFT, FFTW sign convention (-1 forward, +1 inverse), unnormalised.
  * Power-of-two grid_size from 16 to 16384; in may equal out. */
 int sdp_fft2d(int grid_size, const sdp_float2 *in, sdp_float2 *out, int sign, void *stream);

@@ -134,9 +134,32 @@ __global__ void k_normalise(size_t n, float *x, const double *mx)
     if (i < n) x[i] = (float)((double)x[i] / *mx);
 }
 
+// Sum of x^2 over n floats in FP64 (one block; deterministic order).
+__global__ void k_sum_sq(size_t n, const float *__restrict__ x, double *out)
+{
+    __shared__ double s[1024];
+    double a = 0.0;
+    for (size_t i = threadIdx.x; i < n; i += blockDim.x) a = fma((double)x[i], (double)x[i], a);
+    s[threadIdx.x] = a;
+    __syncthreads();
+    for (int o = blockDim.x / 2; o > 0; o >>= 1) {
+        if ((int)threadIdx.x < o) s[threadIdx.x] += s[threadIdx.x + o];
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) *out = sqrt(s[0] / (double)(n ? n : 1));
+}
+
 }  // namespace sdp
 
 using namespace sdp;
+
+SDP_EXPORT int sdp_image_rms(int grid_size, const float *image, double *rms_dev, void *stream)
+{
+    SDP_CHECK_ARG(grid_size >= 1 && image && rms_dev, "bad argument");
+    k_sum_sq<<<1, 1024, 0, as_stream(stream)>>>((size_t)grid_size * grid_size, image, rms_dev);
+    SDP_LAUNCH_CHECK();
+    return SDP_OK;
+}
 
 SDP_EXPORT int sdp_wkernels_generate_sizes(int num_planes, const int *half_supports, int oversampling,
                                            int *total_samples)

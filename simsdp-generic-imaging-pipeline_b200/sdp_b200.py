@@ -540,6 +540,16 @@ class Pipeline:
                                                  _stream(stream)), self.lib)
         return res, model, src[: max(0, n.value)].copy(), n.value
 
+    def residual_rms(self, stream=None) -> float:
+        """FP64 RMS of the last cycle's residual image (on the device)."""
+        import torch
+        res, model, src, n = _p(), _p(), _p(), _p()
+        check(self.lib.sdp_pipeline_outputs(self.handle, C.byref(res), C.byref(model), C.byref(src), C.byref(n)),
+              self.lib)
+        out = torch.zeros(1, dtype=torch.float64, device=torch.device("cuda", torch.cuda.current_device()))
+        check(self.lib.sdp_image_rms(_i(self.G), res, _dp(out), _stream(stream)), self.lib)
+        return float(out.item())
+
     def close(self):
         if self.handle:
             check(self.lib.sdp_pipeline_destroy(self.handle), self.lib)
@@ -630,6 +640,12 @@ class Device:
                                              _i(image_samples), _dp(gk), _dp(dk), _dp(sup), _dp(scr),
                                              C.c_size_t(nscr), _stream(stream)), self.lib)
         return gk, dk, sup
+
+    def image_rms(self, grid_size, image, stream=None) -> float:
+        import torch
+        out = torch.zeros(1, dtype=torch.float64, device=image.device)
+        check(self.lib.sdp_image_rms(_i(grid_size), _dp(image), _dp(out), _stream(stream)), self.lib)
+        return float(out.item())
 
     def prolate_table(self, grid_size, out, stream=None):
         check(self.lib.sdp_prolate_table(_i(grid_size), _dp(out), _stream(stream)), self.lib)

@@ -88,3 +88,13 @@ def test_psf_generate_matches_oracle(sdp, device, oracle32):
     assert rel_rms(got * t, np.asarray(psf_ref, np.float64) * t) <= 2e-5
     assert got.max() == np.float32(1.0)
     plan.close()
+
+
+def test_image_rms_fp64(sdp, device):
+    import torch
+    rng = np.random.default_rng(3)
+    G = 300
+    img = (rng.standard_normal(G * G) * 10.0 ** rng.integers(-3, 3, G * G)).astype(np.float32)
+    got = device.image_rms(G, torch.from_numpy(img).cuda())
+    ref = float(np.sqrt(np.mean(img.astype(np.float64) ** 2)))
+    assert abs(got - ref) <= 1e-12 * ref
