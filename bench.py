@@ -81,18 +81,23 @@ def algorithmic_flops(n_vis: int, taps: int) -> int:
     return n_vis * taps * 16
 
 
-def read_traffic(kernel: str):
-    """dram bytes per launch from the committed ncu summary, if present."""
+def read_profile_value(kernel: str, key: str):
+    """A per-launch figure ("key: value") from the committed ncu summary."""
     f = PROFILES / f"{kernel}.txt"
     if not f.exists():
         return None
     for line in f.read_text().splitlines():
-        if line.startswith("traffic_bytes_per_launch:"):
+        if line.startswith(key + ":"):
             try:
                 return int(float(line.split(":", 1)[1].split()[0]))
             except ValueError:
                 return None
     return None
+
+
+def read_traffic(kernel: str):
+    """dram bytes per launch from the committed ncu summary, if present."""
+    return read_profile_value(kernel, "traffic_bytes_per_launch")
 
 
 class ClockSampler:
@@ -516,6 +521,11 @@ def b200_arm(args):
     peak = float(peaks.get("hbm_gbs", 6650.0))
     peak_src = "measured" if "hbm_gbs" in peaks else "fallback"
     traffic = read_traffic("k_tiles_cycle_conv_c2_2048")
+    # the unit that binds this kernel: the shared-memory data pipe, one
+    # wavefront per SM per clock (wavefronts per launch from the committed
+    # ncu summary; clock: the median SM clock sampled in the timed region)
+    wf = read_profile_value("k_tiles_cycle_conv_c2_2048", "shared_wavefronts_per_launch")
+    binding = None
 
     # ---- whole major cycle (device pipeline, CUDA graph): image->grid, fused
     #      vis pass, grid->image, 200 Hogbom minor cycles ---------------------------------
@@ -626,6 +636,16 @@ def b200_arm(args):
         cpu = {"value": sample / t_cpu, "unit": UNIT, "cores": threads, "kind": kind,
                "sample": f"{sample} visibilities of the workload, {threads} slices on {threads} threads"}
 
+    csum = clocks.summary()
+    if wf is not None and csum.get("sm_mhz"):
+        sms = torch.cuda.get_device_properties(dev).multi_processor_count
+        peak_wf = sms * float(csum["sm_mhz"]) * 1e6
+        ach_wf = wf / (t_step * 1e-3)
+        binding = {"unit": "shared-memory wavefronts/s", "achieved": ach_wf, "peak": peak_wf,
+                   "frac": ach_wf / peak_wf, "per_launch": wf,
+                   "peak_source": f"{sms} SMs x 1 wavefront/clock x median SM clock in the timed region",
+                   "note": "the fused pass is bound by the L1/shared-memory pipe (emulated float atomics, "
+                           "bank conflicts), not HBM; see profiles/k_tiles_cycle_conv_c2_2048.txt"}
     line = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
         "warmup": max(3, args.warmup), "ms_per_step": t_step, "higher_is_better": True, "scaling": "weak",
@@ -639,10 +659,11 @@ def b200_arm(args):
                      "kernel": "k_tiles<STD, OP_CYCLE_CONV>",
                      "algorithmic_bytes_per_launch": alg_bytes,
                      "fp32_flops_per_launch": algorithmic_flops(N, taps)},
+        "roofline_binding": binding,
         "e2e": {"value": world * N / t_e2e, "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
                 "path": "std_degridding + subtract_from_measurements_finegrid + std_gridding (host buffers)"},
         "gpu_launches": args.steps,
-        "clocks": clocks.summary(),
+        "clocks": csum,
     }
     if major is not None:
         line["major_cycle"] = major
