@@ -58,6 +58,8 @@ def parse():
     ap.add_argument("--no-major-cycle", action="store_true")
     ap.add_argument("--no-c3", action="store_true", help="skip the batched 64-channel pass")
     ap.add_argument("--no-c5", action="store_true", help="skip the 8192^2 single-channel measurement")
+    ap.add_argument("--no-c4", action="store_true", help="skip the learned-proposal comparison")
+    ap.add_argument("--c4-skies", type=int, default=16, help="held-out skies of the learned-proposal comparison")
     ap.add_argument("--cpu-sample", type=int, default=200_000, help="visibilities per CPU-baseline step")
     return ap.parse_args()
 
@@ -427,6 +429,100 @@ def c5_block(S, D, dev, reps: int = 3):
     return out
 
 
+def unet_flops(n: int, h: int, w: int, base: int = 32, backward: bool = False) -> int:
+    """Tensor FLOPs (2 per multiply-add) of the U-Net's 3x3 convolutions and
+    head for n images of h x w; backward: the data gradients (all but the
+    first layer) plus the weight gradients."""
+    shapes = []
+    for lv in range(4):
+        shapes += [(lv, 32 if lv == 0 else base << (lv - 1), base << lv), (lv, base << lv, base << lv)]
+    for lv in range(2, -1, -1):
+        shapes += [(lv, (base << lv) + (base << (lv + 1)), base << lv), (lv, base << lv, base << lv)]
+    fwd = sum(2 * 9 * ci * co * n * (h >> lv) * (w >> lv) for lv, ci, co in shapes) + 2 * base * n * h * w
+    if not backward:
+        return fwd
+    dgrad = sum(2 * 9 * ci * co * n * (h >> lv) * (w >> lv) for lv, ci, co in shapes[1:])
+    return dgrad + (fwd - 2 * base * n * h * w) + 4 * base * n * h * w
+
+
+def c4_learned_block(S, D, dev, skies: int):
+    """Learned CLEAN proposals against plain Hogbom on held-out skies: one
+    channel of the 256-antenna spiral layout (3,916,800 visibilities) imaged
+    at 1024^2 (17 w-planes hs=4, kernels generated on the GPU); skies of
+    10-500 points and 0-20 Gaussians (seed never used in training).  The
+    plain pipeline runs 10 major cycles (200 Hogbom minor cycles, DFT
+    predict); the learned one runs until it reaches the plain final FP64
+    residual RMS x 1.01.  Also times the network: forward at 1024^2 and one
+    training step (16 crops of 256^2)."""
+    import torch
+    import learned as L
+
+    img = L.Imaging(D, L.spiral_layout(1024))
+    params = L.load_weights()
+    rows = L.evaluate(img, params, skies, seed=777)
+    sp = [r["plain_s"] / r["learned_s"] for r in rows if r["learned_s"]]
+
+    def ev(fn, n=7):
+        fn()
+        torch.cuda.synchronize()
+        ts = []
+        for _ in range(n):
+            a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            a.record()
+            fn()
+            b.record()
+            torch.cuda.synchronize()
+            ts.append(a.elapsed_time(b))
+        return statistics.median(ts)
+
+    net = S.UNet(D.lib, L.IN_CHANNELS, 1, 1024, 1024, training=False)
+    net.set_params(params)
+    x = torch.randn((1, L.IN_CHANNELS, 1024, 1024), device=dev)
+    out = torch.empty((1, 1024, 1024), device=dev)
+    t_fwd = ev(lambda: net.forward(x, out))
+    net.close()
+    tn = S.UNet(D.lib, L.IN_CHANNELS, 16, 256, 256, training=True)
+    tn.set_params(params)
+    xb = torch.randn((16, L.IN_CHANNELS, 256, 256), device=dev)
+    ob = torch.empty((16, 256, 256), device=dev)
+    gb = 1e-6 * torch.randn_like(ob)
+
+    def step():
+        tn.forward(xb, ob)
+        tn.zero_grads()
+        tn.backward(gb)
+        tn.adam_step(0.0)
+
+    t_train = ev(step)
+    tn.close()
+    f_fwd = unet_flops(1, 1024, 1024)
+    f_train = f_fwd + unet_flops(16, 256, 256, backward=True)
+    peaks = {}
+    try:
+        peaks = json.loads((ROOT / "MEASURED_PEAKS.json").read_text())
+    except (OSError, ValueError):
+        pass
+    bf16 = peaks.get("bf16_tflops") or 1590.0
+    img.close()
+    med = lambda xs: float(statistics.median(xs)) if xs else None  # noqa: E731
+    return {
+        "workload": "256 antennas 10 km spiral, 3916800 vis, G=1024, 17 w-planes hs=4; held-out skies of 10-500 "
+                    "points + 0-20 Gaussians (FWHM 2-10 px)",
+        "skies": len(rows), "plain": "10 major cycles x 200 Hogbom minor cycles (gain 0.1), DFT predict",
+        "target": "plain final FP64 residual RMS x 1.01",
+        "speedup_median": med(sp), "speedup_geomean": float(np.exp(np.mean(np.log(sp)))) if sp else None,
+        "speedup_min": min(sp) if sp else None, "speedup_max": max(sp) if sp else None,
+        "reached": sum(1 for r in rows if r["learned_s"]),
+        "plain_ms_median": med([r["plain_s"] * 1e3 for r in rows]),
+        "learned_ms_median": med([r["learned_s"] * 1e3 for r in rows if r["learned_s"]]),
+        "learned_cycles": [r["learned_cycles"] for r in rows], "learned_kinds": [r["learned_kinds"] for r in rows],
+        "unet_forward_ms_1024": t_fwd, "unet_forward_tflops": f_fwd / (t_fwd * 1e-3) / 1e12,
+        "unet_train_step_ms_16x256": t_train, "unet_train_tflops": f_train / (t_train * 1e-3) / 1e12,
+        "unet_frac_of_bf16_peak": f_fwd / (t_fwd * 1e-3) / 1e12 / bf16,
+        "tensor_path": "mma.sync m16n8k16 BF16 -> FP32 (ldmatrix, cp.async)",
+    }
+
+
 def b200_arm(args):
     import torch
     import torch.distributed as dist
@@ -577,7 +673,9 @@ def b200_arm(args):
         k = next(i for i, r in enumerate(rms) if r <= target)
         major["time_to_rms"] = {"target": "1.01 x the lowest FP64 residual RMS of 12 plain cycles",
                                 "cycles": k + 1, "ms": float(sum(ms[:k + 1])),
-                                "rms_per_cycle": [float(r) for r in rms], "learned": "not built"}
+                                "rms_per_cycle": [float(r) for r in rms],
+                                "learned": "c4_learned (the reference's FFT-pipeline prediction does not converge; "
+                                           "the learned comparison runs on the DFT-predict major cycle)"}
         pl.close()
 
     # ---- the batched multi-channel pass (one GPU only) ---------------------------------
@@ -588,6 +686,10 @@ def b200_arm(args):
     c5 = None
     if world == 1 and not args.no_c5:
         c5 = c5_block(S, D, dev)
+
+    c4 = None
+    if world == 1 and not args.no_c4:
+        c4 = c4_learned_block(S, D, dev, args.c4_skies)
 
     # ---- e2e through the reference-facing C ABI with pinned host buffers ---------------
     uvw_h = torch.empty((N, 3), dtype=torch.float32).pin_memory()
@@ -671,6 +773,8 @@ def b200_arm(args):
         line["c3_batched"] = c3
     if c5 is not None:
         line["c5_channel_8192"] = c5
+    if c4 is not None:
+        line["c4_learned"] = c4
     if cpu is not None:
         line["cpu_baseline"] = cpu
     plan.close()

@@ -44,6 +44,7 @@ extern "C" {
 typedef struct { int x, y; } sdp_int2;
 typedef struct { float x, y; } sdp_float2;
 typedef struct { float x, y, z; } sdp_float3;
+typedef struct { float x, y, z, w; } sdp_float4;
 
 typedef struct sdp_config {
     bool retain_device_mem;
@@ -531,6 +532,84 @@ int sdp_pipeline_graph_active(const sdp_pipeline *p);
 const char *sdp_pipeline_graph_error(const sdp_pipeline *p);
 int sdp_pipeline_visplan(sdp_pipeline *p, sdp_visplan **plan);
 int sdp_pipeline_destroy(sdp_pipeline *p);
+
+/* ---------------------------------------------------------------------------
+ * Learned CLEAN proposals (no counterpart in the reference, whose only
+ * deconvolution is Hogbom, deconvolution_run.c:197-311).  A 4-level U-Net
+ * (base 32 channels, 3x3 convolutions, 2x2 mean pooling, nearest
+ * upsampling, skip concatenations, one-channel 1x1 output head) maps the
+ * residual image and the PSF to a sky map; its largest values become a batch
+ * of components, which the caller verifies through an exact major cycle and
+ * rejects in favour of Hogbom when the residual RMS does not fall.
+ * BF16 weights and activations, FP32 accumulation, FP32 master weights,
+ * forward and backward passes and Adam on the device.
+ * ------------------------------------------------------------------------- */
+typedef struct sdp_unet sdp_unet;
+/* Images up to max_batch x max_height x max_width (sides multiples of 8);
+ * in_channels 1..32; base_channels 32; training = 0 allocates no gradient
+ * or optimiser buffers.  Parameters start at zero (see sdp_unet_set_params). */
+int sdp_unet_create(sdp_unet **net, int base_channels, int in_channels, int max_batch, int max_height,
+                    int max_width, int training);
+int sdp_unet_destroy(sdp_unet *net);
+/* Flat FP32 parameter vector: for each 3x3 layer (0..13: e0a e0 e1a e1 e2a
+ * e2 e3a e3 d2a d2 d1a d1 d0a d0) the weights [9][out][in] (tap = 3 (dy+1) +
+ * (dx+1); layer 0's input is padded to 32 channels) then the bias [out];
+ * then the head (layer 14): weights [base], bias [1]. */
+int sdp_unet_num_params(const sdp_unet *net, size_t *count);
+int sdp_unet_layer(const sdp_unet *net, int layer, int *in_channels, int *out_channels, size_t *weight_offset,
+                   size_t *bias_offset);
+/* Host or device pointers (cudaMemcpyDefault); set resets the Adam state. */
+int sdp_unet_set_params(sdp_unet *net, const float *params, void *stream);
+int sdp_unet_get_params(const sdp_unet *net, float *params, void *stream);
+int sdp_unet_get_grads(const sdp_unet *net, float *grads, void *stream);
+int sdp_unet_zero_grads(sdp_unet *net, void *stream);
+/* input [batch][in_channels][height][width] FP32 (device); scale (device,
+ * [batch], or NULL): every input channel is divided and the output
+ * multiplied by it; output [batch][height][width] FP32 (device).  Keeps the
+ * activations for sdp_unet_backward. */
+int sdp_unet_forward(sdp_unet *net, int batch, int height, int width, const float *input, const float *scale,
+                     float *output, void *stream);
+/* Adds d(loss)/d(params) for d(loss)/d(output) = grad_output (the last
+ * forward's shape; scale NULL) to the gradient vector. */
+int sdp_unet_backward(sdp_unet *net, const float *grad_output, void *stream);
+/* One Adam step on the master weights (bias-corrected moments). */
+int sdp_unet_adam_step(sdp_unet *net, float lr, float beta1, float beta2, float eps, void *stream);
+/* loss = mean over pixels of (b * (pred - target))^2, b the 3x3 binomial
+ * blur (zero padding per image); grad (may be NULL) = d(loss)/d(pred);
+ * diff_scratch holds 2 x batch x height x width floats; loss a device double. */
+int sdp_blur_mse(int batch, int height, int width, const float *pred, const float *target, float *diff_scratch,
+                 float *grad, double *loss, void *stream);
+/* The network's input planes from a residual image (all device, G^2 each):
+ * r / s, sign(r) sqrt(|r| / s), psf, with s = max |r| written to scale_dev. */
+int sdp_unet_input_planes(int grid_size, const float *residual, const float *psf, float *planes, float *scale_dev,
+                          void *stream);
+/* Components from a proposal image: the largest values (signed_values = 0:
+ * positive values; 1: largest |value|, either sign) at or above
+ * rel_threshold x the maximum, at most max_count of them (whole histogram
+ * bins from the top), as (l, m, value x scale, 0) with l = (x - G/2) cell,
+ * m = (y - G/2) cell; *count_dev receives their number; delta_image (may be
+ * NULL) receives them as an image.  workspace: sdp_select_workspace_bytes. */
+int sdp_select_workspace_bytes(size_t *bytes);
+int sdp_select_components(int grid_size, double cell_size, const float *proposal, const float *scale_dev,
+                          int signed_values, float rel_threshold, int max_count, sdp_float4 *components,
+                          int *count_dev, float *delta_image, void *workspace, void *stream);
+/* dots_dev[0] = <a, b>, dots_dev[1] = <b, b>, summed in FP64. */
+int sdp_dots(long long n, const float *a, const float *b, double *dots_dev, void *stream);
+/* y += sign x alpha x with alpha = clamp(dots[0] / dots[1], 0, alpha_max)
+ * (the least-squares step of a proposal); alpha_dev (may be NULL) receives
+ * alpha. */
+int sdp_axpy_ratio(long long n, const double *dots_dev, double alpha_max, float sign, const float *x, float *y,
+                   float *alpha_dev, void *stream);
+int sdp_scale(long long n, float *x, float factor, void *stream);
+/* Adds components (l, m, flux, sigma) to a G x G image: points (sigma = 0)
+ * at the nearest pixel, circular Gaussians of standard deviation sigma
+ * (direction cosines) sampled over +-4 sigma. */
+int sdp_sky_render(int grid_size, double cell_size, int num, const sdp_float4 *components, float *image,
+                   void *stream);
+/* DFT predict of points and circular Gaussians (l, m, flux, sigma): the
+ * sdp_dft term times exp(-2 pi^2 sigma^2 (u^2 + v^2)). */
+int sdp_dft_gauss(int num_vis, int num_sources, const sdp_float4 *sources, const sdp_float3 *uvw, sdp_float2 *vis,
+                  void *stream);
 
 /* Failure-detection self test (no counterpart in the reference): launches
  * nblocks (1..64) blocks that each publish a result and wait, with the wait

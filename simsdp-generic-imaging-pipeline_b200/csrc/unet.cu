@@ -1,0 +1,1137 @@
+// U-Net that proposes CLEAN components from a residual image: BF16
+// tensor-core convolutions with FP32 accumulation (forward, data gradient,
+// weight gradient), the pooling / upsampling / output-head kernels around
+// them, the blurred squared-error loss and the Adam optimiser.
+//
+// No counterpart in the reference (its deconvolution is Hogbom only,
+// deconvolution_run.c:197-311); the network proposes components that the
+// major cycle verifies, with Hogbom as the fallback.
+//
+// Network (levels 0..3, c_l = base * 2^l channels, level l at H/2^l x W/2^l):
+//   e0a = relu(conv(x)),            e0 = relu(conv(e0a))
+//   e1a = relu(conv(pool(e0))),     e1 = relu(conv(e1a))
+//   e2a = relu(conv(pool(e1))),     e2 = relu(conv(e2a))
+//   e3a = relu(conv(pool(e2))),     e3 = relu(conv(e3a))
+//   d2a = relu(conv([e2, up(e3)])), d2 = relu(conv(d2a))
+//   d1a = relu(conv([e1, up(d2)])), d1 = relu(conv(d1a))
+//   d0a = relu(conv([e0, up(d1)])), d0 = relu(conv(d0a))
+//   out = head(d0)   (1x1 convolution to one channel, FP32 output)
+// conv = 3x3, zero padding; pool = 2x2 mean; up = nearest (2x2 repeat);
+// [a, b] = channel concatenation.  The concatenation and the upsampling are
+// never materialised: the convolution's loader reads channels below c_a
+// from a and the rest from b at (y/2, x/2).
+//
+// Layouts: activations and their gradients are BF16, NHWC (channels
+// innermost; every channel count is a multiple of 32, the network input is
+// padded to 32 channels).  Weights: FP32 master copy [tap][cout][cin]
+// (tap = 3 * (dy + 1) + (dx + 1)) followed by the FP32 bias; the BF16 copy
+// in the same order feeds the forward pass and a transposed, tap-flipped
+// copy [8 - tap][cin][cout] the data gradient.
+//
+// Tensor-core path: mma.sync m16n8k16 BF16 -> FP32, operands loaded from
+// shared memory with ldmatrix (conflict-free: every 8-channel group is a
+// 16-byte row of its own plane), tiles staged by cp.async with zero fill
+// outside the image, double buffered.
+#include <cuda_bf16.h>
+
+#include <cmath>
+#include <cstring>
+
+#include "common.cuh"
+
+namespace sdp {
+namespace unet {
+
+typedef __nv_bfloat16 bf16;
+
+constexpr int kTH = 8, kTW = 16;              // output tile: 8 rows x 16 columns
+constexpr int kHH = kTH + 2, kHW = kTW + 2;   // input halo of the tile
+constexpr int kHalo = kHH * kHW;              // 180 pixels
+constexpr int kInPad = 32;                    // network input channels padded to 32
+constexpr int kLayers = 14;                   // 3x3 convolutions
+constexpr int kLevels = 4;
+
+__device__ __forceinline__ uint32_t smem_u32(const void *p) { return (uint32_t)__cvta_generic_to_shared(p); }
+
+__device__ __forceinline__ void cp_async16(uint32_t dst, const void *src, int bytes)
+{
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;\n" ::"r"(dst), "l"(src), "r"(bytes));
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait()
+{
+    asm volatile("cp.async.wait_group %0;\n" ::"n"(N));
+}
+
+__device__ __forceinline__ void ldsm4(uint32_t (&r)[4], uint32_t addr)
+{
+    asm volatile("ldmatrix.sync.aligned.m8n8.x4.shared.b16 {%0,%1,%2,%3}, [%4];\n"
+                 : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3])
+                 : "r"(addr));
+}
+__device__ __forceinline__ void ldsm4t(uint32_t (&r)[4], uint32_t addr)
+{
+    asm volatile("ldmatrix.sync.aligned.m8n8.x4.trans.shared.b16 {%0,%1,%2,%3}, [%4];\n"
+                 : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3])
+                 : "r"(addr));
+}
+// D += A (16x16, row) * B (16x8, col), BF16 inputs, FP32 accumulators
+__device__ __forceinline__ void mma16816(float (&d)[4], const uint32_t (&a)[4], uint32_t b0, uint32_t b1)
+{
+    asm volatile(
+        "mma.sync.aligned.m16n8k16.row.col.f32.bf16.bf16.f32 {%0,%1,%2,%3}, {%4,%5,%6,%7}, {%8,%9}, "
+        "{%0,%1,%2,%3};\n"
+        : "+f"(d[0]), "+f"(d[1]), "+f"(d[2]), "+f"(d[3])
+        : "r"(a[0]), "r"(a[1]), "r"(a[2]), "r"(a[3]), "r"(b0), "r"(b1));
+}
+
+// Source of one 8-channel group of the (virtual) convolution input at image
+// pixel (yy, xx) of image img: channels [c, c + 8) of [a, up(b)].
+struct VIn {
+    const bf16 *a;
+    const bf16 *b;
+    int ca, cb, h, w;
+    __device__ __forceinline__ const bf16 *at(int img, int yy, int xx, int c) const
+    {
+        if (c < ca) return a + (((size_t)img * h + yy) * w + xx) * ca + c;
+        return b + (((size_t)img * (h >> 1) + (yy >> 1)) * (w >> 1) + (xx >> 1)) * cb + (c - ca);
+    }
+};
+
+// ----------------------------------------------------------------------------
+// 3x3 convolution, implicit GEMM: out[p][o] = sum_tap sum_i in[p + off(tap)][i]
+// * wk[tap][o][i] (+ bias, relu, mask).  One CTA: an 8 x 16 pixel tile and
+// BN output channels; warp w owns tile rows 2w, 2w + 1 (two m16 tiles) and
+// all BN channels.  K runs over 16-channel chunks, each chunk over 9 taps.
+// Used for the forward pass (wk = W) and the data gradient (wk = flipped
+// transpose, no bias; mask = the forward activation whose relu gates it).
+// ----------------------------------------------------------------------------
+struct ConvArgs {
+    VIn in;
+    const bf16 *wk;      // [9][cout][cin]
+    const float *bias;   // [cout] or null
+    const bf16 *mask;    // [n][h][w][cout] or null: out = 0 where mask <= 0
+    bf16 *out;           // [n][h][w][cout]
+    int cout, relu;
+    int tiles_x, tiles_y;
+};
+
+template <int BN>
+struct ConvSmem {
+    static constexpr int kHaloBytes = 2 * kHalo * 16;
+    static constexpr int kWBytes = 9 * 2 * BN * 16;
+    static constexpr int kStage = kHaloBytes + kWBytes;
+    static constexpr int kBytes = 2 * kStage;
+};
+
+template <int BN>
+__global__ void __launch_bounds__(128) k_conv3x3(ConvArgs p)
+{
+    extern __shared__ __align__(16) unsigned char smem[];
+    using SM = ConvSmem<BN>;
+    const int cin = p.in.ca + p.in.cb;
+    const int nchunks = cin >> 4;
+    int t = blockIdx.x;
+    const int tx = t % p.tiles_x;
+    t /= p.tiles_x;
+    const int ty = t % p.tiles_y;
+    const int img = t / p.tiles_y;
+    const int y0 = ty * kTH, x0 = tx * kTW;
+    const int co0 = blockIdx.y * BN;
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const int H = p.in.h, W = p.in.w;
+
+    auto load_chunk = [&](int k, int s) {
+        unsigned char *base = smem + s * SM::kStage;
+        const uint32_t hs = smem_u32(base), ws = smem_u32(base + SM::kHaloBytes);
+        const int c0 = k << 4;
+        for (int i = tid; i < 2 * kHalo; i += 128) {
+            const int half = i >= kHalo;
+            const int hidx = i - half * kHalo;
+            const int yy = y0 - 1 + hidx / kHW, xx = x0 - 1 + hidx % kHW;
+            const bool inside = yy >= 0 && yy < H && xx >= 0 && xx < W;
+            const bf16 *src = inside ? p.in.at(img, yy, xx, c0 + 8 * half) : p.in.a;
+            cp_async16(hs + i * 16, src, inside ? 16 : 0);
+        }
+        for (int i = tid; i < 9 * 2 * BN; i += 128) {
+            const int co = i % BN, th = i / BN;  // th = 2 * tap + half
+            const bf16 *src = p.wk + ((size_t)(th >> 1) * p.cout + co0 + co) * cin + c0 + 8 * (th & 1);
+            cp_async16(ws + i * 16, src, 16);
+        }
+    };
+
+    float acc[2][BN / 8][4];
+#pragma unroll
+    for (int a = 0; a < 2; ++a)
+#pragma unroll
+        for (int b = 0; b < BN / 8; ++b)
+#pragma unroll
+            for (int c = 0; c < 4; ++c) acc[a][b][c] = 0.f;
+
+    load_chunk(0, 0);
+    cp_async_commit();
+    const int q = lane >> 3, i8 = lane & 7;
+    for (int k = 0; k < nchunks; ++k) {
+        if (k + 1 < nchunks) load_chunk(k + 1, (k + 1) & 1);
+        cp_async_commit();
+        cp_async_wait<1>();
+        __syncthreads();
+        const unsigned char *base = smem + (k & 1) * SM::kStage;
+        const uint32_t hs = smem_u32(base), ws = smem_u32(base + SM::kHaloBytes);
+#pragma unroll 1
+        for (int tap = 0; tap < 9; ++tap) {
+            const int dy = tap / 3, dx = tap - 3 * (tap / 3);
+            uint32_t af[2][4];
+#pragma unroll
+            for (int mt = 0; mt < 2; ++mt) {
+                // matrix q: pixels (q & 1) * 8 + 0..7 of tile row r, channel half q >> 1
+                const int r = warp * 2 + mt;
+                const int hidx = (r + dy) * kHW + (q & 1) * 8 + i8 + dx;
+                ldsm4(af[mt], hs + ((q >> 1) * kHalo + hidx) * 16);
+            }
+#pragma unroll
+            for (int j = 0; j < BN / 8; j += 2) {
+                // matrix q: output channels of n-tile j + (q >> 1), channel half q & 1
+                uint32_t bfr[4];
+                const int co = (j + (q >> 1)) * 8 + i8;
+                ldsm4(bfr, ws + ((tap * 2 + (q & 1)) * BN + co) * 16);
+#pragma unroll
+                for (int mt = 0; mt < 2; ++mt) {
+                    mma16816(acc[mt][j], af[mt], bfr[0], bfr[1]);
+                    mma16816(acc[mt][j + 1], af[mt], bfr[2], bfr[3]);
+                }
+            }
+        }
+        __syncthreads();
+    }
+
+    const int g = lane >> 2, tq = lane & 3;
+#pragma unroll
+    for (int mt = 0; mt < 2; ++mt) {
+        const int y = y0 + warp * 2 + mt;
+#pragma unroll
+        for (int hr = 0; hr < 2; ++hr) {
+            const int x = x0 + g + hr * 8;
+            if (y >= H || x >= W) continue;
+            const size_t pix = ((size_t)img * H + y) * W + x;
+#pragma unroll
+            for (int j = 0; j < BN / 8; ++j) {
+                const int co = co0 + j * 8 + tq * 2;
+                float v0 = acc[mt][j][hr * 2], v1 = acc[mt][j][hr * 2 + 1];
+                if (p.bias) {
+                    v0 += p.bias[co];
+                    v1 += p.bias[co + 1];
+                }
+                if (p.relu) {
+                    v0 = v0 > 0.f ? v0 : 0.f;
+                    v1 = v1 > 0.f ? v1 : 0.f;
+                }
+                if (p.mask) {
+                    const __nv_bfloat162 m = *reinterpret_cast<const __nv_bfloat162 *>(p.mask + pix * p.cout + co);
+                    if (!(__low2float(m) > 0.f)) v0 = 0.f;
+                    if (!(__high2float(m) > 0.f)) v1 = 0.f;
+                }
+                *reinterpret_cast<__nv_bfloat162 *>(p.out + pix * p.cout + co) = __floats2bfloat162_rn(v0, v1);
+            }
+        }
+    }
+}
+
+// ----------------------------------------------------------------------------
+// Weight gradient: dw[tap][o][i] += sum_p dz[p][o] * in[p + off(tap)][i].
+// One CTA: 32 output x 32 input channels, all 9 taps (warp = tap), over a
+// strided set of pixel tiles; per tile and tile row one k16 step of
+// m = output channel, n = input channel, k = pixel.  Partial sums are added
+// to the FP32 gradient with atomics once per CTA.
+// ----------------------------------------------------------------------------
+struct WgradArgs {
+    const bf16 *dz;  // [n][h][w][cout]
+    int cout;
+    VIn in;
+    float *dw;       // [9][cout][cin]
+    int n, tiles_x, tiles_y, ntiles;
+};
+
+constexpr int kWgDz = 4 * (kTH * kTW) * 16;  // dz tile: 4 planes x 128 pixels
+constexpr int kWgX = 4 * kHalo * 16;         // input halo: 4 planes x 180 pixels
+constexpr int kWgStage = kWgDz + kWgX;
+constexpr int kWgBytes = 2 * kWgStage;
+
+__global__ void __launch_bounds__(288) k_wgrad3x3(WgradArgs p)
+{
+    extern __shared__ __align__(16) unsigned char smem[];
+    const int co0 = blockIdx.x * 32, ci0 = blockIdx.y * 32;
+    const int cin = p.in.ca + p.in.cb;
+    const int tid = threadIdx.x, lane = tid & 31, tap = tid >> 5;
+    const int dy = tap / 3, dx = tap - 3 * (tap / 3);
+    const int H = p.in.h, W = p.in.w;
+
+    auto load_tile = [&](int t, int s) {
+        const int tx = t % p.tiles_x;
+        const int ty = (t / p.tiles_x) % p.tiles_y;
+        const int img = t / (p.tiles_x * p.tiles_y);
+        const int y0 = ty * kTH, x0 = tx * kTW;
+        unsigned char *base = smem + s * kWgStage;
+        const uint32_t ds = smem_u32(base), xs = smem_u32(base + kWgDz);
+        for (int i = tid; i < 4 * kTH * kTW; i += 288) {
+            const int pl = i >> 7, px = i & 127;
+            const int yy = y0 + (px >> 4), xx = x0 + (px & 15);
+            const bool inside = yy < H && xx < W;
+            const bf16 *src = inside ? p.dz + (((size_t)img * H + yy) * W + xx) * p.cout + co0 + 8 * pl : p.dz;
+            cp_async16(ds + i * 16, src, inside ? 16 : 0);
+        }
+        for (int i = tid; i < 4 * kHalo; i += 288) {
+            const int pl = i / kHalo, hidx = i - pl * kHalo;
+            const int yy = y0 - 1 + hidx / kHW, xx = x0 - 1 + hidx % kHW;
+            const bool inside = yy >= 0 && yy < H && xx >= 0 && xx < W;
+            const bf16 *src = inside ? p.in.at(img, yy, xx, ci0 + 8 * pl) : p.in.a;
+            cp_async16(xs + i * 16, src, inside ? 16 : 0);
+        }
+    };
+
+    float acc[2][4][4];
+#pragma unroll
+    for (int a = 0; a < 2; ++a)
+#pragma unroll
+        for (int b = 0; b < 4; ++b)
+#pragma unroll
+            for (int c = 0; c < 4; ++c) acc[a][b][c] = 0.f;
+
+    int t = blockIdx.z;
+    if (t < p.ntiles) {
+        load_tile(t, 0);
+        cp_async_commit();
+        const int q = lane >> 3, i8 = lane & 7;
+        for (int s = 0; t < p.ntiles; t += gridDim.z, s ^= 1) {
+            if (t + (int)gridDim.z < p.ntiles) load_tile(t + gridDim.z, s ^ 1);
+            cp_async_commit();
+            cp_async_wait<1>();
+            __syncthreads();
+            const unsigned char *base = smem + s * kWgStage;
+            const uint32_t ds = smem_u32(base), xs = smem_u32(base + kWgDz);
+#pragma unroll 1
+            for (int r = 0; r < kTH; ++r) {
+                uint32_t af[2][4];
+#pragma unroll
+                for (int mt = 0; mt < 2; ++mt) {
+                    // transposed: matrix q = (channel half q & 1, pixel half q >> 1)
+                    const int pl = 2 * mt + (q & 1);
+                    const int px = r * kTW + (q >> 1) * 8 + i8;
+                    ldsm4t(af[mt], ds + (pl * (kTH * kTW) + px) * 16);
+                }
+#pragma unroll
+                for (int j = 0; j < 4; j += 2) {
+                    // transposed: matrix q = (pixel half q & 1, input plane j + (q >> 1))
+                    uint32_t bfr[4];
+                    const int pl = j + (q >> 1);
+                    const int hidx = (r + dy) * kHW + (q & 1) * 8 + i8 + dx;
+                    ldsm4t(bfr, xs + (pl * kHalo + hidx) * 16);
+#pragma unroll
+                    for (int mt = 0; mt < 2; ++mt) {
+                        mma16816(acc[mt][j], af[mt], bfr[0], bfr[1]);
+                        mma16816(acc[mt][j + 1], af[mt], bfr[2], bfr[3]);
+                    }
+                }
+            }
+            __syncthreads();
+        }
+    }
+    const int g = lane >> 2, tq = lane & 3;
+#pragma unroll
+    for (int mt = 0; mt < 2; ++mt)
+#pragma unroll
+        for (int j = 0; j < 4; ++j)
+#pragma unroll
+            for (int e = 0; e < 4; ++e) {
+                const int co = co0 + mt * 16 + g + (e >> 1) * 8;
+                const int ci = ci0 + j * 8 + tq * 2 + (e & 1);
+                atomicAdd(p.dw + ((size_t)tap * p.cout + co) * cin + ci, acc[mt][j][e]);
+            }
+}
+
+// db[c] += sum_p dz[p][c]; c divides 256 (32 .. 256 channels).
+__global__ void __launch_bounds__(256) k_bias_grad(const bf16 *__restrict__ dz, long long npix, int c,
+                                                  float *__restrict__ db)
+{
+    const int rows = 256 / c;
+    const int ch = threadIdx.x % c, r0 = threadIdx.x / c;
+    float s = 0.f;
+    for (long long p = (long long)blockIdx.x * rows + r0; p < npix; p += (long long)gridDim.x * rows)
+        s += __bfloat162float(dz[p * c + ch]);
+    atomicAdd(db + ch, s);
+}
+
+// ----------------------------------------------------------------------------
+// Element-wise kernels (8 channels = one 16-byte vector per thread)
+// ----------------------------------------------------------------------------
+union V8 {
+    uint4 u;
+    __nv_bfloat162 h[4];
+};
+
+__device__ __forceinline__ void unpack8(const uint4 &u, float (&f)[8])
+{
+    V8 v;
+    v.u = u;
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+        f[2 * k] = __low2float(v.h[k]);
+        f[2 * k + 1] = __high2float(v.h[k]);
+    }
+}
+__device__ __forceinline__ uint4 pack8(const float (&f)[8])
+{
+    V8 v;
+#pragma unroll
+    for (int k = 0; k < 4; ++k) v.h[k] = __floats2bfloat162_rn(f[2 * k], f[2 * k + 1]);
+    return v.u;
+}
+
+// x[n][y][x][0..31] = in[n][c][y][x] / scale[n] (c < cin), 0 above.
+__global__ void k_pack_input(int n, int cin, int h, int w, const float *__restrict__ in,
+                             const float *__restrict__ scale, bf16 *__restrict__ x)
+{
+    const long long npix = (long long)n * h * w;
+    for (long long p = blockIdx.x * (long long)blockDim.x + threadIdx.x; p < npix;
+         p += (long long)gridDim.x * blockDim.x) {
+        const long long img = p / ((long long)h * w), yx = p - img * h * w;
+        const float inv = scale ? 1.0f / scale[img] : 1.0f;
+        float f[kInPad];
+#pragma unroll
+        for (int c = 0; c < kInPad; ++c) f[c] = 0.f;
+        for (int c = 0; c < cin; ++c) f[c] = in[(img * cin + c) * h * w + yx] * inv;
+        uint4 *dst = reinterpret_cast<uint4 *>(x + p * kInPad);
+#pragma unroll
+        for (int k = 0; k < kInPad / 8; ++k) {
+            float g[8];
+#pragma unroll
+            for (int e = 0; e < 8; ++e) g[e] = f[8 * k + e];
+            dst[k] = pack8(g);
+        }
+    }
+}
+
+// out[n][y][x][c] = mean of in over the 2x2 block (h, w of the input).
+__global__ void k_pool2(int n, int h, int w, int c, const bf16 *__restrict__ in, bf16 *__restrict__ out)
+{
+    const int h2 = h >> 1, w2 = w >> 1, cg = c >> 3;
+    const long long total = (long long)n * h2 * w2 * cg;
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < total;
+         i += (long long)gridDim.x * blockDim.x) {
+        const int g = (int)(i % cg);
+        const long long pix = i / cg;
+        const int x = (int)(pix % w2), y = (int)((pix / w2) % h2);
+        const long long img = pix / ((long long)w2 * h2);
+        float s[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+#pragma unroll
+        for (int d = 0; d < 4; ++d) {
+            const long long q = (img * h + 2 * y + (d >> 1)) * w + 2 * x + (d & 1);
+            float f[8];
+            unpack8(*reinterpret_cast<const uint4 *>(in + q * c + 8 * g), f);
+#pragma unroll
+            for (int e = 0; e < 8; ++e) s[e] += f[e];
+        }
+#pragma unroll
+        for (int e = 0; e < 8; ++e) s[e] *= 0.25f;
+        *reinterpret_cast<uint4 *>(out + pix * c + 8 * g) = pack8(s);
+    }
+}
+
+// de[p][c] = (dp[p/2][c] / 4 + dcat[p][c]) * (e[p][c] > 0): the gradient of
+// an encoder output e used by the pool below it and by the decoder's
+// concatenation (first c of its ctot channels).
+__global__ void k_pool_bwd_add(int n, int h, int w, int c, const bf16 *__restrict__ dp, const bf16 *__restrict__ dcat,
+                               int ctot, const bf16 *__restrict__ e, bf16 *__restrict__ de)
+{
+    const int cg = c >> 3, w2 = w >> 1, h2 = h >> 1;
+    const long long total = (long long)n * h * w * cg;
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < total;
+         i += (long long)gridDim.x * blockDim.x) {
+        const int g = (int)(i % cg);
+        const long long pix = i / cg;
+        const int x = (int)(pix % w), y = (int)((pix / w) % h);
+        const long long img = pix / ((long long)w * h);
+        float a[8], b[8], m[8];
+        unpack8(*reinterpret_cast<const uint4 *>(dp + ((img * h2 + (y >> 1)) * w2 + (x >> 1)) * c + 8 * g), a);
+        unpack8(*reinterpret_cast<const uint4 *>(dcat + pix * ctot + 8 * g), b);
+        unpack8(*reinterpret_cast<const uint4 *>(e + pix * c + 8 * g), m);
+        float o[8];
+#pragma unroll
+        for (int k = 0; k < 8; ++k) o[k] = (m[k] > 0.f) ? (a[k] * 0.25f + b[k]) : 0.f;
+        *reinterpret_cast<uint4 *>(de + pix * c + 8 * g) = pack8(o);
+    }
+}
+
+// dlow[q][c] = sum over the 2x2 block of dcat[p][coff + c], times
+// (ylow[q][c] > 0); h, w of the full-resolution dcat.
+__global__ void k_up_bwd(int n, int h, int w, int ctot, int coff, int c, const bf16 *__restrict__ dcat,
+                         const bf16 *__restrict__ ylow, bf16 *__restrict__ dlow)
+{
+    const int h2 = h >> 1, w2 = w >> 1, cg = c >> 3;
+    const long long total = (long long)n * h2 * w2 * cg;
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < total;
+         i += (long long)gridDim.x * blockDim.x) {
+        const int g = (int)(i % cg);
+        const long long pix = i / cg;
+        const int x = (int)(pix % w2), y = (int)((pix / w2) % h2);
+        const long long img = pix / ((long long)w2 * h2);
+        float s[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+#pragma unroll
+        for (int d = 0; d < 4; ++d) {
+            const long long q = (img * h + 2 * y + (d >> 1)) * w + 2 * x + (d & 1);
+            float f[8];
+            unpack8(*reinterpret_cast<const uint4 *>(dcat + q * ctot + coff + 8 * g), f);
+#pragma unroll
+            for (int e = 0; e < 8; ++e) s[e] += f[e];
+        }
+        float m[8];
+        unpack8(*reinterpret_cast<const uint4 *>(ylow + pix * c + 8 * g), m);
+#pragma unroll
+        for (int e = 0; e < 8; ++e) s[e] = (m[e] > 0.f) ? s[e] : 0.f;
+        *reinterpret_cast<uint4 *>(dlow + pix * c + 8 * g) = pack8(s);
+    }
+}
+
+// out[p] = sum_c d0[p][c] * bf16(hw[c]) + hb, times scale[img] when given.
+__global__ void k_head_fwd(long long npix, long long pix_per_img, int c, const bf16 *__restrict__ d0,
+                           const float *__restrict__ hw, const float *__restrict__ hb,
+                           const float *__restrict__ scale, float *__restrict__ out)
+{
+    for (long long p = blockIdx.x * (long long)blockDim.x + threadIdx.x; p < npix;
+         p += (long long)gridDim.x * blockDim.x) {
+        float s = 0.f;
+        for (int g = 0; g < c / 8; ++g) {
+            float f[8];
+            unpack8(*reinterpret_cast<const uint4 *>(d0 + p * c + 8 * g), f);
+#pragma unroll
+            for (int e = 0; e < 8; ++e) s += f[e] * __bfloat162float(__float2bfloat16_rn(hw[8 * g + e]));
+        }
+        s += hb[0];
+        if (scale) s *= scale[p / pix_per_img];
+        out[p] = s;
+    }
+}
+
+// dd0[p][c] = go[p] * bf16(hw[c]) * (d0[p][c] > 0); dhw[c] += sum_p go[p] d0[p][c];
+// dhb += sum_p go[p].  c <= 64.
+__global__ void __launch_bounds__(256) k_head_bwd(long long npix, int c, const bf16 *__restrict__ d0,
+                                                 const float *__restrict__ hw, const float *__restrict__ go,
+                                                 bf16 *__restrict__ dd0, float *__restrict__ dhw,
+                                                 float *__restrict__ dhb)
+{
+    __shared__ float s_dw[65];
+    for (int i = threadIdx.x; i < 65; i += blockDim.x) s_dw[i] = 0.f;
+    __syncthreads();
+    float part[64];
+    for (int k = 0; k < 64; ++k) part[k] = 0.f;
+    float pb = 0.f;
+    for (long long p = blockIdx.x * (long long)blockDim.x + threadIdx.x; p < npix;
+         p += (long long)gridDim.x * blockDim.x) {
+        const float g = go[p];
+        pb += g;
+        for (int gi = 0; gi < c / 8; ++gi) {
+            float f[8], o[8];
+            unpack8(*reinterpret_cast<const uint4 *>(d0 + p * c + 8 * gi), f);
+#pragma unroll
+            for (int e = 0; e < 8; ++e) {
+                const float wv = __bfloat162float(__float2bfloat16_rn(hw[8 * gi + e]));
+                o[e] = (f[e] > 0.f) ? g * wv : 0.f;
+                part[8 * gi + e] += g * f[e];
+            }
+            *reinterpret_cast<uint4 *>(dd0 + p * c + 8 * gi) = pack8(o);
+        }
+    }
+    for (int k = 0; k < c; ++k) {
+        float v = part[k];
+        for (int off = 16; off; off >>= 1) v += __shfl_xor_sync(0xffffffffu, v, off);
+        if ((threadIdx.x & 31) == 0) atomicAdd(&s_dw[k], v);
+    }
+    for (int off = 16; off; off >>= 1) pb += __shfl_xor_sync(0xffffffffu, pb, off);
+    if ((threadIdx.x & 31) == 0) atomicAdd(&s_dw[64], pb);
+    __syncthreads();
+    for (int k = threadIdx.x; k < c; k += blockDim.x) atomicAdd(dhw + k, s_dw[k]);
+    if (threadIdx.x == 0) atomicAdd(dhb, s_dw[64]);
+}
+
+// BF16 copies of one layer's FP32 weights: w[tap][o][i] and the data-gradient
+// form wt[8 - tap][i][o].
+__global__ void k_layer_weights(int cout, int cin, const float *__restrict__ master, bf16 *__restrict__ w,
+                                bf16 *__restrict__ wt)
+{
+    const int total = 9 * cout * cin;
+    for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < total; k += gridDim.x * blockDim.x) {
+        const int ci = k % cin, co = (k / cin) % cout, tap = k / (cin * cout);
+        const bf16 v = __float2bfloat16_rn(master[k]);
+        w[k] = v;
+        wt[((size_t)(8 - tap) * cin + ci) * cout + co] = v;
+    }
+}
+
+// Adam (Kingma & Ba 2015) on the FP32 master weights; c1 = 1 - beta1^t,
+// c2 = 1 - beta2^t.
+__global__ void k_adam(long long n, float *__restrict__ w, const float *__restrict__ g, float *__restrict__ m,
+                       float *__restrict__ v, float lr, float b1, float b2, float eps, float c1, float c2)
+{
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
+         i += (long long)gridDim.x * blockDim.x) {
+        const float gi = g[i];
+        const float mi = b1 * m[i] + (1.f - b1) * gi;
+        const float vi = b2 * v[i] + (1.f - b2) * gi * gi;
+        m[i] = mi;
+        v[i] = vi;
+        w[i] -= lr * (mi / c1) / (sqrtf(vi / c2) + eps);
+    }
+}
+
+// ----------------------------------------------------------------------------
+// Loss: L = mean over pixels of (g * (pred - target))^2 with g the 3x3
+// binomial kernel (1 2 1)^T (1 2 1) / 16, zero padding per image, so a
+// component one pixel off costs little; grad = 2/npix * g * (g * (pred - target)).
+// ----------------------------------------------------------------------------
+__device__ __forceinline__ float binom3(const float *a, int h, int w, int y, int x)
+{
+    float s = 0.f;
+#pragma unroll
+    for (int dy = -1; dy <= 1; ++dy) {
+        const int yy = y + dy;
+        if (yy < 0 || yy >= h) continue;
+#pragma unroll
+        for (int dx = -1; dx <= 1; ++dx) {
+            const int xx = x + dx;
+            if (xx < 0 || xx >= w) continue;
+            s += a[(size_t)yy * w + xx] * (float)((2 - (dy < 0 ? -dy : dy)) * (2 - (dx < 0 ? -dx : dx)));
+        }
+    }
+    return s * (1.f / 16.f);
+}
+
+__global__ void k_diff(long long n, const float *__restrict__ a, const float *__restrict__ b, float *__restrict__ d)
+{
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
+         i += (long long)gridDim.x * blockDim.x)
+        d[i] = a[i] - b[i];
+}
+
+__global__ void __launch_bounds__(256) k_blur_sq(int n, int h, int w, const float *__restrict__ d,
+                                                float *__restrict__ bd, double *__restrict__ loss_sum)
+{
+    __shared__ double s_part[8];
+    const long long total = (long long)n * h * w;
+    double acc = 0.0;
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < total;
+         i += (long long)gridDim.x * blockDim.x) {
+        const long long img = i / ((long long)h * w);
+        const int yx = (int)(i - img * h * w);
+        const float v = binom3(d + img * h * w, h, w, yx / w, yx % w);
+        bd[i] = v;
+        acc += (double)v * v;
+    }
+    for (int off = 16; off; off >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, off);
+    if ((threadIdx.x & 31) == 0) s_part[threadIdx.x >> 5] = acc;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double s = 0.0;
+        for (int k = 0; k < (int)(blockDim.x >> 5); ++k) s += s_part[k];
+        atomicAdd(loss_sum, s);
+    }
+}
+
+__global__ void k_blur_grad(int n, int h, int w, const float *__restrict__ bd, float scale, float *__restrict__ grad)
+{
+    const long long total = (long long)n * h * w;
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < total;
+         i += (long long)gridDim.x * blockDim.x) {
+        const long long img = i / ((long long)h * w);
+        const int yx = (int)(i - img * h * w);
+        grad[i] = scale * binom3(bd + img * h * w, h, w, yx / w, yx % w);
+    }
+}
+
+__global__ void k_scale_loss(double *loss_sum, double inv_n) { loss_sum[0] *= inv_n; }
+
+inline int grid_for(long long n, int threads = 256)
+{
+    long long b = (n + threads - 1) / threads;
+    const long long cap = (long long)num_sms() * 16;
+    return (int)(b < 1 ? 1 : (b > cap ? cap : b));
+}
+
+}  // namespace unet
+}  // namespace sdp
+
+// ============================================================================
+// Host object
+// ============================================================================
+using namespace sdp;
+using namespace sdp::unet;
+
+namespace {
+struct Layer {
+    int cin, cout;
+    size_t woff, boff;  // into the FP32 parameter vector
+    bf16 *w = nullptr, *wt = nullptr;
+};
+struct Act {  // one activation tensor (and its gradient scratch)
+    bf16 *p = nullptr;
+    int level = 0, c = 0;
+};
+}  // namespace
+
+struct sdp_unet {
+    int base = 32, in_ch = 1, max_n = 1, max_h = 8, max_w = 8, training = 0;
+    Layer layer[kLayers];
+    size_t nparams = 0, head_off = 0;
+    float *master = nullptr, *grad = nullptr, *adam_m = nullptr, *adam_v = nullptr;
+    bf16 *wbuf = nullptr;  // BF16 weights (forward and transposed) of all layers
+    long long step = 0;
+    // forward activations
+    bf16 *x = nullptr;
+    bf16 *e[kLevels][2] = {};  // e[l][0] = e_l a, e[l][1] = e_l
+    bf16 *pool[kLevels] = {};  // pool[l] = pool(e_{l-1}), l >= 1
+    bf16 *d[kLevels - 1][2] = {};
+    // gradient scratch (training)
+    bf16 *gz[kLevels][2] = {};
+    bf16 *dcat[kLevels - 1] = {};
+    // shape of the last forward pass
+    int n = 0, h = 0, w = 0;
+    bool have_forward = false;
+    void *arena = nullptr;
+};
+
+namespace {
+
+int ch(const sdp_unet *u, int l) { return u->base << l; }
+
+size_t pix(const sdp_unet *u, int l) { return (size_t)u->max_n * (u->max_h >> l) * (u->max_w >> l); }
+
+// Layer table in parameter order: e0a e0 e1a e1 e2a e2 e3a e3 d2a d2 d1a d1 d0a d0.
+void layer_shapes(sdp_unet *u)
+{
+    int k = 0;
+    for (int l = 0; l < kLevels; ++l) {
+        u->layer[k].cin = l == 0 ? kInPad : ch(u, l - 1);
+        u->layer[k++].cout = ch(u, l);
+        u->layer[k].cin = ch(u, l);
+        u->layer[k++].cout = ch(u, l);
+    }
+    for (int l = kLevels - 2; l >= 0; --l) {
+        u->layer[k].cin = ch(u, l) + ch(u, l + 1);
+        u->layer[k++].cout = ch(u, l);
+        u->layer[k].cin = ch(u, l);
+        u->layer[k++].cout = ch(u, l);
+    }
+    size_t off = 0;
+    for (auto &L : u->layer) {
+        L.woff = off;
+        off += (size_t)9 * L.cin * L.cout;
+        L.boff = off;
+        off += L.cout;
+    }
+    u->head_off = off;
+    u->nparams = off + ch(u, 0) + 1;
+}
+
+int enc_layer(int l, int second) { return 2 * l + second; }
+int dec_layer(int l, int second) { return 8 + 2 * (kLevels - 2 - l) + second; }
+
+size_t tiles(int n, int h, int w) { return (size_t)n * ((h + kTH - 1) / kTH) * ((w + kTW - 1) / kTW); }
+
+int conv(const Layer &L, VIn in, const bf16 *wk, const float *bias, const bf16 *mask, bf16 *out, int cout, int relu,
+         int n, cudaStream_t st)
+{
+    ConvArgs a;
+    a.in = in;
+    a.wk = wk;
+    a.bias = bias;
+    a.mask = mask;
+    a.out = out;
+    a.cout = cout;
+    a.relu = relu;
+    a.tiles_x = (in.w + kTW - 1) / kTW;
+    a.tiles_y = (in.h + kTH - 1) / kTH;
+    const size_t nt = tiles(n, in.h, in.w);
+    (void)L;
+    if (cout % 64 == 0 && nt * (cout / 64) >= (size_t)2 * num_sms()) {
+        k_conv3x3<64><<<dim3((unsigned)nt, cout / 64), 128, ConvSmem<64>::kBytes, st>>>(a);
+    } else {
+        k_conv3x3<32><<<dim3((unsigned)nt, cout / 32), 128, ConvSmem<32>::kBytes, st>>>(a);
+    }
+    SDP_LAUNCH_CHECK();
+    return SDP_OK;
+}
+
+int wgrad(const bf16 *dz, int cout, VIn in, float *dw, float *db, int n, cudaStream_t st)
+{
+    WgradArgs a;
+    a.dz = dz;
+    a.cout = cout;
+    a.in = in;
+    a.dw = dw;
+    a.n = n;
+    a.tiles_x = (in.w + kTW - 1) / kTW;
+    a.tiles_y = (in.h + kTH - 1) / kTH;
+    a.ntiles = (int)tiles(n, in.h, in.w);
+    const int cin = in.ca + in.cb;
+    const int blocks_xy = (cout / 32) * (cin / 32);
+    int z = (4 * num_sms() + blocks_xy - 1) / blocks_xy;
+    if (z > a.ntiles) z = a.ntiles;
+    if (z < 1) z = 1;
+    k_wgrad3x3<<<dim3(cout / 32, cin / 32, z), 288, kWgBytes, st>>>(a);
+    SDP_LAUNCH_CHECK();
+    const long long np = (long long)n * in.h * in.w;
+    k_bias_grad<<<grid_for(np / (256 / cout) + 1), 256, 0, st>>>(dz, np, cout, db);
+    SDP_LAUNCH_CHECK();
+    return SDP_OK;
+}
+
+VIn vin(const bf16 *a, int ca, const bf16 *b, int cb, int h, int w)
+{
+    VIn v;
+    v.a = a;
+    v.b = b;
+    v.ca = ca;
+    v.cb = cb;
+    v.h = h;
+    v.w = w;
+    return v;
+}
+
+int set_attrs()
+{
+    static bool done = false;
+    if (done) return SDP_OK;
+    SDP_CUDA_TRY(cudaFuncSetAttribute(k_conv3x3<32>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                      ConvSmem<32>::kBytes));
+    SDP_CUDA_TRY(cudaFuncSetAttribute(k_conv3x3<64>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                      ConvSmem<64>::kBytes));
+    SDP_CUDA_TRY(cudaFuncSetAttribute(k_wgrad3x3, cudaFuncAttributeMaxDynamicSharedMemorySize, kWgBytes));
+    done = true;
+    return SDP_OK;
+}
+
+int refresh_weights(sdp_unet *u, cudaStream_t st)
+{
+    for (auto &L : u->layer) {
+        const int total = 9 * L.cin * L.cout;
+        k_layer_weights<<<grid_for(total), 256, 0, st>>>(L.cout, L.cin, u->master + L.woff, L.w, L.wt);
+        SDP_LAUNCH_CHECK();
+    }
+    return SDP_OK;
+}
+
+}  // namespace
+
+SDP_EXPORT int sdp_unet_create(sdp_unet **out, int base_channels, int in_channels, int max_batch, int max_height,
+                               int max_width, int training)
+{
+    SDP_CHECK_ARG(out, "NULL handle");
+    *out = nullptr;
+    SDP_CHECK_ARG(base_channels == 32, "base_channels must be 32");
+    SDP_CHECK_ARG(in_channels >= 1 && in_channels <= kInPad, "in_channels must be 1..%d", kInPad);
+    SDP_CHECK_ARG(max_batch >= 1 && max_height >= 8 && max_width >= 8, "sizes must be positive, images >= 8 x 8");
+    SDP_CHECK_ARG(max_height % 8 == 0 && max_width % 8 == 0, "image sides must be multiples of 8");
+    SDP_CHECK_ARG((long long)max_batch * max_height * max_width <= (1LL << 31) / 2,
+                  "batch x height x width too large");
+    SDP_TRY(set_attrs());
+    sdp_unet *u = new sdp_unet();
+    u->base = base_channels;
+    u->in_ch = in_channels;
+    u->max_n = max_batch;
+    u->max_h = max_height;
+    u->max_w = max_width;
+    u->training = training ? 1 : 0;
+    layer_shapes(u);
+
+    // one arena: FP32 parameters (+ gradient and Adam moments when training),
+    // BF16 weights, activations and gradient scratch
+    size_t bytes = 0;
+    auto take = [&](size_t b) {
+        const size_t at = bytes;
+        bytes += (b + 255) & ~(size_t)255;
+        return at;
+    };
+    const size_t o_master = take(u->nparams * 4);
+    const size_t o_grad = u->training ? take(u->nparams * 4) : 0;
+    const size_t o_m = u->training ? take(u->nparams * 4) : 0;
+    const size_t o_v = u->training ? take(u->nparams * 4) : 0;
+    size_t o_w[kLayers], o_wt[kLayers];
+    for (int k = 0; k < kLayers; ++k) {
+        o_w[k] = take((size_t)9 * u->layer[k].cin * u->layer[k].cout * 2);
+        o_wt[k] = take((size_t)9 * u->layer[k].cin * u->layer[k].cout * 2);
+    }
+    const size_t o_x = take(pix(u, 0) * kInPad * 2);
+    size_t o_e[kLevels][2], o_pool[kLevels] = {}, o_d[kLevels - 1][2], o_gz[kLevels][2] = {}, o_dcat[kLevels - 1] = {};
+    for (int l = 0; l < kLevels; ++l) {
+        o_e[l][0] = take(pix(u, l) * ch(u, l) * 2);
+        o_e[l][1] = take(pix(u, l) * ch(u, l) * 2);
+        if (l > 0) o_pool[l] = take(pix(u, l) * ch(u, l - 1) * 2);
+    }
+    for (int l = 0; l < kLevels - 1; ++l) {
+        o_d[l][0] = take(pix(u, l) * ch(u, l) * 2);
+        o_d[l][1] = take(pix(u, l) * ch(u, l) * 2);
+    }
+    if (u->training) {
+        for (int l = 0; l < kLevels; ++l) {
+            o_gz[l][0] = take(pix(u, l) * ch(u, l) * 2);
+            o_gz[l][1] = take(pix(u, l) * ch(u, l) * 2);
+        }
+        for (int l = 0; l < kLevels - 1; ++l) o_dcat[l] = take(pix(u, l) * (ch(u, l) + ch(u, l + 1)) * 2);
+    }
+    void *arena = nullptr;
+    cudaError_t e = cudaMalloc(&arena, bytes);
+    if (e != cudaSuccess) {
+        delete u;
+        return cuda_error(e, "cudaMalloc(unet arena)");
+    }
+    u->arena = arena;
+    char *A = static_cast<char *>(arena);
+    u->master = reinterpret_cast<float *>(A + o_master);
+    if (u->training) {
+        u->grad = reinterpret_cast<float *>(A + o_grad);
+        u->adam_m = reinterpret_cast<float *>(A + o_m);
+        u->adam_v = reinterpret_cast<float *>(A + o_v);
+    }
+    for (int k = 0; k < kLayers; ++k) {
+        u->layer[k].w = reinterpret_cast<bf16 *>(A + o_w[k]);
+        u->layer[k].wt = reinterpret_cast<bf16 *>(A + o_wt[k]);
+    }
+    u->x = reinterpret_cast<bf16 *>(A + o_x);
+    for (int l = 0; l < kLevels; ++l) {
+        u->e[l][0] = reinterpret_cast<bf16 *>(A + o_e[l][0]);
+        u->e[l][1] = reinterpret_cast<bf16 *>(A + o_e[l][1]);
+        if (l > 0) u->pool[l] = reinterpret_cast<bf16 *>(A + o_pool[l]);
+        if (u->training) {
+            u->gz[l][0] = reinterpret_cast<bf16 *>(A + o_gz[l][0]);
+            u->gz[l][1] = reinterpret_cast<bf16 *>(A + o_gz[l][1]);
+        }
+    }
+    for (int l = 0; l < kLevels - 1; ++l) {
+        u->d[l][0] = reinterpret_cast<bf16 *>(A + o_d[l][0]);
+        u->d[l][1] = reinterpret_cast<bf16 *>(A + o_d[l][1]);
+        if (u->training) u->dcat[l] = reinterpret_cast<bf16 *>(A + o_dcat[l]);
+    }
+    e = cudaMemset(arena, 0, bytes);
+    if (e != cudaSuccess) {
+        cudaFree(arena);
+        delete u;
+        return cuda_error(e, "cudaMemset(unet arena)");
+    }
+    *out = u;
+    return SDP_OK;
+}
+
+SDP_EXPORT int sdp_unet_destroy(sdp_unet *u)
+{
+    if (!u) return SDP_OK;
+    cudaDeviceSynchronize();
+    if (u->arena) cudaFree(u->arena);
+    delete u;
+    return SDP_OK;
+}
+
+SDP_EXPORT int sdp_unet_num_params(const sdp_unet *u, size_t *count)
+{
+    SDP_CHECK_ARG(u && count, "NULL argument");
+    *count = u->nparams;
+    return SDP_OK;
+}
+
+SDP_EXPORT int sdp_unet_layer(const sdp_unet *u, int layer, int *in_channels, int *out_channels,
+                              size_t *weight_offset, size_t *bias_offset)
+{
+    SDP_CHECK_ARG(u, "NULL handle");
+    SDP_CHECK_ARG(layer >= 0 && layer <= kLayers, "layer must be 0..%d (%d = output head)", kLayers, kLayers);
+    if (layer == kLayers) {
+        if (in_channels) *in_channels = ch(u, 0);
+        if (out_channels) *out_channels = 1;
+        if (weight_offset) *weight_offset = u->head_off;
+        if (bias_offset) *bias_offset = u->head_off + ch(u, 0);
+        return SDP_OK;
+    }
+    const Layer &L = u->layer[layer];
+    if (in_channels) *in_channels = L.cin;
+    if (out_channels) *out_channels = L.cout;
+    if (weight_offset) *weight_offset = L.woff;
+    if (bias_offset) *bias_offset = L.boff;
+    return SDP_OK;
+}
+
+SDP_EXPORT int sdp_unet_set_params(sdp_unet *u, const float *params, void *stream)
+{
+    SDP_CHECK_ARG(u && params, "NULL argument");
+    cudaStream_t st = as_stream(stream);
+    SDP_CUDA_TRY(cudaMemcpyAsync(u->master, params, u->nparams * 4, cudaMemcpyDefault, st));
+    SDP_TRY(refresh_weights(u, st));
+    if (u->training) {
+        SDP_CUDA_TRY(cudaMemsetAsync(u->adam_m, 0, u->nparams * 4, st));
+        SDP_CUDA_TRY(cudaMemsetAsync(u->adam_v, 0, u->nparams * 4, st));
+        u->step = 0;
+    }
+    return SDP_OK;
+}
+
+SDP_EXPORT int sdp_unet_get_params(const sdp_unet *u, float *params, void *stream)
+{
+    SDP_CHECK_ARG(u && params, "NULL argument");
+    SDP_CUDA_TRY(cudaMemcpyAsync(params, u->master, u->nparams * 4, cudaMemcpyDefault, as_stream(stream)));
+    return SDP_OK;
+}
+
+SDP_EXPORT int sdp_unet_get_grads(const sdp_unet *u, float *grads, void *stream)
+{
+    SDP_CHECK_ARG(u && grads, "NULL argument");
+    if (!u->training) return set_error(SDP_ERR_INVALID, "network created without training buffers");
+    SDP_CUDA_TRY(cudaMemcpyAsync(grads, u->grad, u->nparams * 4, cudaMemcpyDefault, as_stream(stream)));
+    return SDP_OK;
+}
+
+SDP_EXPORT int sdp_unet_zero_grads(sdp_unet *u, void *stream)
+{
+    SDP_CHECK_ARG(u, "NULL handle");
+    if (!u->training) return set_error(SDP_ERR_INVALID, "network created without training buffers");
+    SDP_CUDA_TRY(cudaMemsetAsync(u->grad, 0, u->nparams * 4, as_stream(stream)));
+    return SDP_OK;
+}
+
+SDP_EXPORT int sdp_unet_forward(sdp_unet *u, int n, int h, int w, const float *input, const float *scale,
+                                float *output, void *stream)
+{
+    SDP_CHECK_ARG(u && input && output, "NULL argument");
+    SDP_CHECK_ARG(n >= 1 && n <= u->max_n && h >= 8 && h <= u->max_h && w >= 8 && w <= u->max_w,
+                  "batch %d x %d x %d outside the network's capacity %d x %d x %d", n, h, w, u->max_n, u->max_h,
+                  u->max_w);
+    SDP_CHECK_ARG(h % 8 == 0 && w % 8 == 0, "image sides must be multiples of 8");
+    cudaStream_t st = as_stream(stream);
+    const long long np = (long long)n * h * w;
+    k_pack_input<<<grid_for(np), 256, 0, st>>>(n, u->in_ch, h, w, input, scale, u->x);
+    SDP_LAUNCH_CHECK();
+    const float *P = u->master;
+    // encoder
+    for (int l = 0; l < kLevels; ++l) {
+        const int hl = h >> l, wl = w >> l, c = ch(u, l);
+        const bf16 *src = l == 0 ? u->x : u->pool[l];
+        const int cs = l == 0 ? kInPad : ch(u, l - 1);
+        if (l > 0) {
+            const int cp = ch(u, l - 1);
+            k_pool2<<<grid_for((long long)n * hl * wl * (cp / 8)), 256, 0, st>>>(n, h >> (l - 1), w >> (l - 1), cp,
+                                                                              u->e[l - 1][1], u->pool[l]);
+            SDP_LAUNCH_CHECK();
+        }
+        const Layer &La = u->layer[enc_layer(l, 0)], &Lb = u->layer[enc_layer(l, 1)];
+        SDP_TRY(conv(La, vin(src, cs, nullptr, 0, hl, wl), La.w, P + La.boff, nullptr, u->e[l][0], c, 1, n, st));
+        SDP_TRY(conv(Lb, vin(u->e[l][0], c, nullptr, 0, hl, wl), Lb.w, P + Lb.boff, nullptr, u->e[l][1], c, 1, n,
+                     st));
+    }
+    // decoder
+    for (int l = kLevels - 2; l >= 0; --l) {
+        const int hl = h >> l, wl = w >> l, c = ch(u, l), c1 = ch(u, l + 1);
+        const bf16 *low = (l == kLevels - 2) ? u->e[l + 1][1] : u->d[l + 1][1];
+        const Layer &La = u->layer[dec_layer(l, 0)], &Lb = u->layer[dec_layer(l, 1)];
+        SDP_TRY(conv(La, vin(u->e[l][1], c, low, c1, hl, wl), La.w, P + La.boff, nullptr, u->d[l][0], c, 1, n, st));
+        SDP_TRY(conv(Lb, vin(u->d[l][0], c, nullptr, 0, hl, wl), Lb.w, P + Lb.boff, nullptr, u->d[l][1], c, 1, n,
+                     st));
+    }
+    k_head_fwd<<<grid_for(np), 256, 0, st>>>(np, (long long)h * w, ch(u, 0), u->d[0][1], P + u->head_off,
+                                             P + u->head_off + ch(u, 0), scale, output);
+    SDP_LAUNCH_CHECK();
+    u->n = n;
+    u->h = h;
+    u->w = w;
+    u->have_forward = true;
+    return SDP_OK;
+}
+
+SDP_EXPORT int sdp_unet_backward(sdp_unet *u, const float *grad_output, void *stream)
+{
+    SDP_CHECK_ARG(u && grad_output, "NULL argument");
+    if (!u->training) return set_error(SDP_ERR_INVALID, "network created without training buffers");
+    if (!u->have_forward) return set_error(SDP_ERR_INVALID, "backward before forward");
+    cudaStream_t st = as_stream(stream);
+    const int n = u->n, h = u->h, w = u->w;
+    const long long np = (long long)n * h * w;
+    float *G = u->grad;
+    const int c0 = ch(u, 0);
+    // head: dZ(d0) -> gz[0][0]
+    k_head_bwd<<<grid_for(np), 256, 0, st>>>(np, c0, u->d[0][1], u->master + u->head_off, grad_output, u->gz[0][0],
+                                             G + u->head_off, G + u->head_off + c0);
+    SDP_LAUNCH_CHECK();
+    // decoder, top (level 0) down to level kLevels - 2; gz[l][0] holds dZ of d_l on entry
+    for (int l = 0; l <= kLevels - 2; ++l) {
+        const int hl = h >> l, wl = w >> l, c = ch(u, l), c1 = ch(u, l + 1);
+        const Layer &La = u->layer[dec_layer(l, 0)], &Lb = u->layer[dec_layer(l, 1)];
+        // second conv: d_l = conv(d_l a)
+        SDP_TRY(wgrad(u->gz[l][0], c, vin(u->d[l][0], c, nullptr, 0, hl, wl), G + Lb.woff, G + Lb.boff, n, st));
+        SDP_TRY(conv(Lb, vin(u->gz[l][0], c, nullptr, 0, hl, wl), Lb.wt, nullptr, u->d[l][0], u->gz[l][1], c, 0, n,
+                     st));
+        // first conv: d_l a = conv([e_l, up(low)])
+        const bf16 *low = (l == kLevels - 2) ? u->e[l + 1][1] : u->d[l + 1][1];
+        SDP_TRY(wgrad(u->gz[l][1], c, vin(u->e[l][1], c, low, c1, hl, wl), G + La.woff, G + La.boff, n, st));
+        SDP_TRY(conv(La, vin(u->gz[l][1], c, nullptr, 0, hl, wl), La.wt, nullptr, nullptr, u->dcat[l], c + c1, 0, n,
+                     st));
+        // up-sampled part -> dZ of the lower tensor (d_{l+1} or e_3)
+        k_up_bwd<<<grid_for((long long)n * (hl / 2) * (wl / 2) * (c1 / 8)), 256, 0, st>>>(
+            n, hl, wl, c + c1, c, c1, u->dcat[l], low, u->gz[l + 1][0]);
+        SDP_LAUNCH_CHECK();
+    }
+    // encoder, bottom (level kLevels - 1) up to level 0; gz[l][0] holds dZ of e_l on entry
+    for (int l = kLevels - 1; l >= 0; --l) {
+        const int hl = h >> l, wl = w >> l, c = ch(u, l);
+        const Layer &La = u->layer[enc_layer(l, 0)], &Lb = u->layer[enc_layer(l, 1)];
+        SDP_TRY(wgrad(u->gz[l][0], c, vin(u->e[l][0], c, nullptr, 0, hl, wl), G + Lb.woff, G + Lb.boff, n, st));
+        SDP_TRY(conv(Lb, vin(u->gz[l][0], c, nullptr, 0, hl, wl), Lb.wt, nullptr, u->e[l][0], u->gz[l][1], c, 0, n,
+                     st));
+        const bf16 *src = l == 0 ? u->x : u->pool[l];
+        const int cs = l == 0 ? kInPad : ch(u, l - 1);
+        SDP_TRY(wgrad(u->gz[l][1], c, vin(src, cs, nullptr, 0, hl, wl), G + La.woff, G + La.boff, n, st));
+        if (l == 0) break;
+        // data gradient of the pooled input (cs channels at level l), into gz[l][0]
+        SDP_TRY(conv(La, vin(u->gz[l][1], c, nullptr, 0, hl, wl), La.wt, nullptr, nullptr, u->gz[l][0], cs, 0, n,
+                     st));
+        // dZ(e_{l-1}) = (pool backward + concatenation part) * relu'
+        const int hu = h >> (l - 1), wu = w >> (l - 1);
+        k_pool_bwd_add<<<grid_for((long long)n * hu * wu * (cs / 8)), 256, 0, st>>>(
+            n, hu, wu, cs, u->gz[l][0], u->dcat[l - 1], cs + c, u->e[l - 1][1], u->gz[l - 1][0]);
+        SDP_LAUNCH_CHECK();
+    }
+    return SDP_OK;
+}
+
+SDP_EXPORT int sdp_unet_adam_step(sdp_unet *u, float lr, float beta1, float beta2, float eps, void *stream)
+{
+    SDP_CHECK_ARG(u, "NULL handle");
+    if (!u->training) return set_error(SDP_ERR_INVALID, "network created without training buffers");
+    SDP_CHECK_ARG(lr >= 0.f && beta1 >= 0.f && beta1 < 1.f && beta2 >= 0.f && beta2 < 1.f && eps > 0.f,
+                  "invalid Adam hyper-parameters");
+    cudaStream_t st = as_stream(stream);
+    u->step += 1;
+    const float c1 = (float)(1.0 - std::pow((double)beta1, (double)u->step));
+    const float c2 = (float)(1.0 - std::pow((double)beta2, (double)u->step));
+    k_adam<<<grid_for((long long)u->nparams), 256, 0, st>>>((long long)u->nparams, u->master, u->grad, u->adam_m,
+                                                           u->adam_v, lr, beta1, beta2, eps, c1, c2);
+    SDP_LAUNCH_CHECK();
+    return refresh_weights(u, st);
+}
+
+SDP_EXPORT int sdp_blur_mse(int n, int h, int w, const float *pred, const float *target, float *diff_scratch,
+                            float *grad, double *loss, void *stream)
+{
+    SDP_CHECK_ARG(n >= 1 && h >= 1 && w >= 1, "empty images");
+    SDP_CHECK_ARG(pred && target && diff_scratch && loss, "NULL argument");
+    cudaStream_t st = as_stream(stream);
+    const long long np = (long long)n * h * w;
+    // diff_scratch holds 2 * np floats: the difference, then its blur
+    float *d = diff_scratch, *bd = diff_scratch + np;
+    k_diff<<<grid_for(np), 256, 0, st>>>(np, pred, target, d);
+    SDP_LAUNCH_CHECK();
+    SDP_CUDA_TRY(cudaMemsetAsync(loss, 0, sizeof(double), st));
+    k_blur_sq<<<grid_for(np), 256, 0, st>>>(n, h, w, d, bd, loss);
+    SDP_LAUNCH_CHECK();
+    k_scale_loss<<<1, 1, 0, st>>>(loss, 1.0 / (double)np);
+    SDP_LAUNCH_CHECK();
+    if (grad) {
+        k_blur_grad<<<grid_for(np), 256, 0, st>>>(n, h, w, bd, (float)(2.0 / (double)np), grad);
+        SDP_LAUNCH_CHECK();
+    }
+    return SDP_OK;
+}

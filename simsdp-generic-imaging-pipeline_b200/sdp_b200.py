@@ -669,3 +669,127 @@ class Device:
         check(self.lib.sdp_hogbom(C.byref(params), _dp(residual), _dp(psf), _dp(model), _dp(sources), _dp(count),
                                   _dp(workspace), _sz(workspace.numel() * workspace.element_size()),
                                   _stream(stream)), self.lib)
+
+    # -- learned major cycle ------------------------------------------------------------
+    def unet_input_planes(self, grid_size, residual, psf, planes, scale, stream=None):
+        """planes (3 G^2): r / s, sign(r) sqrt(|r| / s), psf; scale[0] = s = max |r|."""
+        check(self.lib.sdp_unet_input_planes(_i(grid_size), _dp(residual), _dp(psf), _dp(planes), _dp(scale),
+                                             _stream(stream)), self.lib)
+
+    def select_workspace(self):
+        import torch
+        b = _sz(0)
+        check(self.lib.sdp_select_workspace_bytes(C.byref(b)), self.lib)
+        return torch.empty(b.value, dtype=torch.uint8, device=torch.device("cuda", torch.cuda.current_device()))
+
+    def select_components(self, grid_size, cell, proposal, scale, rel_threshold, max_count, comps, count,
+                          delta_image, workspace, signed=False, stream=None):
+        check(self.lib.sdp_select_components(_i(grid_size), _d(cell), _dp(proposal), _dp(scale),
+                                             _i(1 if signed else 0), C.c_float(rel_threshold), _i(max_count),
+                                             _dp(comps), _dp(count), _dp(delta_image), _dp(workspace),
+                                             _stream(stream)), self.lib)
+
+    def dots(self, a, b, out, stream=None):
+        check(self.lib.sdp_dots(C.c_longlong(a.numel()), _dp(a), _dp(b), _dp(out), _stream(stream)), self.lib)
+
+    def axpy_ratio(self, dots, alpha_max, x, y, alpha=None, sign=1.0, stream=None):
+        """y += sign * alpha * x, alpha = clamp(dots[0] / dots[1], 0, alpha_max)."""
+        check(self.lib.sdp_axpy_ratio(C.c_longlong(x.numel()), _dp(dots), _d(alpha_max), C.c_float(sign), _dp(x),
+                                      _dp(y), _dp(alpha), _stream(stream)), self.lib)
+
+    def scale(self, x, factor, stream=None):
+        check(self.lib.sdp_scale(C.c_longlong(x.numel()), _dp(x), C.c_float(factor), _stream(stream)), self.lib)
+
+    def sky_render(self, grid_size, cell, comps, image, stream=None):
+        check(self.lib.sdp_sky_render(_i(grid_size), _d(cell), _i(comps.shape[0]), _dp(comps), _dp(image),
+                                      _stream(stream)), self.lib)
+
+    def dft_gauss(self, sources, uvw, vis, stream=None):
+        check(self.lib.sdp_dft_gauss(_i(uvw.shape[0]), _i(sources.shape[0]), _dp(sources), _dp(uvw), _dp(vis),
+                                     _stream(stream)), self.lib)
+
+    def add_vis(self, a, b, out, stream=None):
+        check(self.lib.sdp_add_vis(_i(a.shape[0]), _dp(a), _dp(b), _dp(out), _stream(stream)), self.lib)
+
+    def blur_mse(self, pred, target, scratch, grad, loss, stream=None):
+        """loss[0] (device double) = mean((b * (pred - target))^2); grad = d loss / d pred
+        (may be None); pred/target [n][h][w]; scratch 2 n h w floats."""
+        n, h, w = pred.shape
+        check(self.lib.sdp_blur_mse(_i(n), _i(h), _i(w), _dp(pred), _dp(target), _dp(scratch), _dp(grad),
+                                    _dp(loss), _stream(stream)), self.lib)
+
+
+class UNet:
+    """The learned-proposal U-Net on the device (sdp_unet_*): 4 levels, base
+    32 channels, BF16 weights and activations with FP32 accumulation."""
+
+    def __init__(self, lib, in_channels: int, max_batch: int, max_height: int, max_width: int,
+                 training: bool = True, base: int = 32):
+        self.lib = lib
+        self.in_channels = in_channels
+        self.handle = _p()
+        check(lib.sdp_unet_create(C.byref(self.handle), _i(base), _i(in_channels), _i(max_batch), _i(max_height),
+                                  _i(max_width), _i(1 if training else 0)), lib)
+        n = _sz(0)
+        check(lib.sdp_unet_num_params(self.handle, C.byref(n)), lib)
+        self.num_params = n.value
+
+    def close(self):
+        if self.handle:
+            check(self.lib.sdp_unet_destroy(self.handle), self.lib)
+            self.handle = _p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def layer(self, k: int):
+        ci, co, wo, bo = _i(0), _i(0), _sz(0), _sz(0)
+        check(self.lib.sdp_unet_layer(self.handle, _i(k), C.byref(ci), C.byref(co), C.byref(wo), C.byref(bo)),
+              self.lib)
+        return ci.value, co.value, wo.value, bo.value
+
+    def set_params(self, params, stream=None):
+        """params: float32 numpy array (host) or CUDA tensor of num_params."""
+        if isinstance(params, np.ndarray):
+            a = np.ascontiguousarray(params, dtype=np.float32)
+            assert a.size == self.num_params
+            check(self.lib.sdp_unet_set_params(self.handle, a.ctypes.data_as(_p), _stream(stream)), self.lib)
+            import torch
+            torch.cuda.synchronize()  # the host array may go away
+        else:
+            assert params.numel() == self.num_params
+            check(self.lib.sdp_unet_set_params(self.handle, _dp(params), _stream(stream)), self.lib)
+
+    def get_params(self, stream=None) -> np.ndarray:
+        import torch
+        out = np.empty(self.num_params, np.float32)
+        check(self.lib.sdp_unet_get_params(self.handle, out.ctypes.data_as(_p), _stream(stream)), self.lib)
+        torch.cuda.synchronize()
+        return out
+
+    def get_grads(self, stream=None) -> np.ndarray:
+        import torch
+        out = np.empty(self.num_params, np.float32)
+        check(self.lib.sdp_unet_get_grads(self.handle, out.ctypes.data_as(_p), _stream(stream)), self.lib)
+        torch.cuda.synchronize()
+        return out
+
+    def zero_grads(self, stream=None):
+        check(self.lib.sdp_unet_zero_grads(self.handle, _stream(stream)), self.lib)
+
+    def forward(self, x, out, scale=None, stream=None):
+        """x [n][in_channels][h][w] -> out [n][h][w] (CUDA float32 tensors)."""
+        n, c, h, w = x.shape
+        assert c == self.in_channels
+        check(self.lib.sdp_unet_forward(self.handle, _i(n), _i(h), _i(w), _dp(x), _dp(scale), _dp(out),
+                                        _stream(stream)), self.lib)
+
+    def backward(self, grad_out, stream=None):
+        check(self.lib.sdp_unet_backward(self.handle, _dp(grad_out), _stream(stream)), self.lib)
+
+    def adam_step(self, lr, beta1=0.9, beta2=0.999, eps=1e-8, stream=None):
+        check(self.lib.sdp_unet_adam_step(self.handle, C.c_float(lr), C.c_float(beta1), C.c_float(beta2),
+                                          C.c_float(eps), _stream(stream)), self.lib)
