@@ -606,6 +606,14 @@ int sdp_scale(long long n, float *x, float factor, void *stream);
  * (direction cosines) sampled over +-4 sigma. */
 int sdp_sky_render(int grid_size, double cell_size, int num, const sdp_float4 *components, float *image,
                    void *stream);
+/* DFT predict of components on the pixel grid (CLEAN components, network
+ * proposals): component k = (l, m, flux, ...) at components + k * stride
+ * floats, l and m multiples of cell_size (rounded to the nearest pixel
+ * offset); the sdp_dft formula with the phase reduced modulo one cycle in
+ * fixed point (error below 1e-6 rad for offsets up to 2048 pixels).
+ * accumulate = 1 adds to vis. */
+int sdp_dft_pixels(int num_vis, int num_components, const float *components, int stride, double cell_size,
+                   const sdp_float3 *uvw, sdp_float2 *vis, int accumulate, void *stream);
 /* DFT predict of points and circular Gaussians (l, m, flux, sigma): the
  * sdp_dft term times exp(-2 pi^2 sigma^2 (u^2 + v^2)). */
 int sdp_dft_gauss(int num_vis, int num_sources, const sdp_float4 *sources, const sdp_float3 *uvw, sdp_float2 *vis,

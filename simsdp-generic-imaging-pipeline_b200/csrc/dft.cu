@@ -134,9 +134,106 @@ __global__ void __launch_bounds__(kDftThreads) k_dft_gauss(int n, int ns, const 
     if (i < n) vis[i] = make_float2(sx, sy);
 }
 
+// Components on the image's pixel grid (CLEAN components and network
+// proposals; no counterpart in the reference, whose dft_actor takes any
+// (l, m)): component k at pixel offset (X, Y) from the centre, l = X cell,
+// m = Y cell.  The phase u l + v m - w (l^2 + m^2)/2 = U X + V Y - W R2 with
+// U = u cell, V = v cell, W = w cell^2 / 2 (formed in FP64 per visibility)
+// and R2 = X^2 + Y^2 is reduced modulo one cycle exactly in fixed point:
+// frac(U) and frac(V) as 32-bit fractions (integer products wrap modulo 2^32,
+// i.e. modulo one cycle; error <= |X| 2^-33 cycles) and W as a 44-bit
+// fraction multiplied by R2 in 64 bits (error <= R2 2^-45 cycles).  The
+// reduced phase (23 bits) becomes a float in [-1/2, 1/2) cycles by its bit
+// pattern, so the only special-function work per term is the sine and the
+// cosine (__sincosf on [-pi, pi)).
+struct PixTerm {
+    int x, y;
+    unsigned r2;
+    float amp;
+};
+
+constexpr int kPixTile = 1024;
+
+__global__ void __launch_bounds__(kDftThreads) k_dft_pixels(int n, int ns, const float *__restrict__ comps, int stride,
+                                                           double cell, const float3 *__restrict__ uvw,
+                                                           float2 *__restrict__ vis, int accumulate)
+{
+    __shared__ PixTerm tile[kPixTile];
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    unsigned ufx = 0, vfx = 0;
+    unsigned long long wfx = 0;
+    bool wneg = false;
+    if (i < n) {
+        const float3 c = uvw[i];
+        const double U = (double)c.x * cell, V = (double)c.y * cell;
+        const double W = (double)c.z * cell * cell * 0.5;
+        ufx = (unsigned)(long long)llrint((U - floor(U)) * 4294967296.0);
+        vfx = (unsigned)(long long)llrint((V - floor(V)) * 4294967296.0);
+        wneg = W < 0.0;
+        wfx = (unsigned long long)llrint(fabs(W) * 17592186044416.0);  // 2^44
+    }
+    float sx = 0.f, sy = 0.f;
+    const double inv_cell = 1.0 / cell;
+    for (int base = 0; base < ns; base += kPixTile) {
+        const int cnt = min(kPixTile, ns - base);
+        __syncthreads();
+        for (int k = threadIdx.x; k < cnt; k += blockDim.x) {
+            const float *s = comps + (size_t)(base + k) * stride;
+            PixTerm t;
+            t.x = (int)llrint((double)s[0] * inv_cell);
+            t.y = (int)llrint((double)s[1] * inv_cell);
+            t.r2 = (unsigned)(t.x * t.x + t.y * t.y);
+            const double h = 0.5 * (double)t.r2 * cell * cell;
+            t.amp = (float)((double)s[2] / (1.0 - h));
+            tile[k] = t;
+        }
+        __syncthreads();
+        if (i < n) {
+            for (int k = 0; k < cnt; ++k) {
+                const PixTerm t = tile[k];
+                // w term: frac(W R2) in units of 2^-32 cycles
+                const unsigned long long wp = wfx * (unsigned long long)t.r2;
+                unsigned wq = (unsigned)(wp >> 12);
+                if (wneg) wq = 0u - wq;
+                // phase U X + V Y - W R2 modulo 1, as a 32-bit fraction
+                const unsigned p = ufx * (unsigned)t.x + vfx * (unsigned)t.y - wq;
+                // [-1/2, 1/2) cycles from the top 23 bits (rounded): 1.5 + f as a float
+                const float f = __uint_as_float(0x3F800000u | ((p + 0x80000100u) >> 9)) - 1.5f;
+                float sn, cs;
+                __sincosf(6.28318530717958647692f * f, &sn, &cs);
+                sx = fmaf(cs, t.amp, sx);
+                sy = fmaf(-sn, t.amp, sy);
+            }
+        }
+    }
+    if (i < n) {
+        if (accumulate) {
+            const float2 o = vis[i];
+            vis[i] = make_float2(o.x + sx, o.y + sy);
+        } else {
+            vis[i] = make_float2(sx, sy);
+        }
+    }
+}
+
 }  // namespace sdp
 
 using namespace sdp;
+
+SDP_EXPORT int sdp_dft_pixels(int num_vis, int num_components, const float *components, int stride, double cell_size,
+                              const sdp_float3 *uvw, sdp_float2 *vis, int accumulate, void *stream)
+{
+    SDP_CHECK_ARG(num_vis >= 0 && num_components >= 0, "negative size");
+    SDP_CHECK_ARG(stride >= 3, "stride must be >= 3 floats (l, m, flux, ...)");
+    SDP_CHECK_ARG(cell_size > 0.0, "cell_size must be positive");
+    if (num_vis == 0) return SDP_OK;
+    SDP_CHECK_ARG(uvw && vis && (components || num_components == 0), "NULL argument");
+    k_dft_pixels<<<(num_vis + kDftThreads - 1) / kDftThreads, kDftThreads, 0, as_stream(stream)>>>(
+        num_vis, num_components, components, stride, cell_size, reinterpret_cast<const float3 *>(uvw),
+        reinterpret_cast<float2 *>(vis), accumulate ? 1 : 0);
+    SDP_LAUNCH_CHECK();
+    return SDP_OK;
+}
 
 SDP_EXPORT int sdp_dft_gauss(int num_vis, int num_sources, const sdp_float4 *sources, const sdp_float3 *uvw,
                              sdp_float2 *vis, void *stream)

@@ -134,13 +134,39 @@ __global__ void k_normalise(size_t n, float *x, const double *mx)
     if (i < n) x[i] = (float)((double)x[i] / *mx);
 }
 
-// Sum of x^2 over n floats in FP64 (one block; deterministic order).
-__global__ void k_sum_sq(size_t n, const float *__restrict__ x, double *out)
+// Sum of x^2 over n floats in FP64 (one block; deterministic order): each
+// thread keeps four accumulators over 16-byte loads (memory-level
+// parallelism for a single SM), then a fixed tree.
+__global__ void __launch_bounds__(1024) k_sum_sq(size_t n, const float *__restrict__ x, double *out)
 {
     __shared__ double s[1024];
-    double a = 0.0;
-    for (size_t i = threadIdx.x; i < n; i += blockDim.x) a = fma((double)x[i], (double)x[i], a);
-    s[threadIdx.x] = a;
+    double a0 = 0.0, a1 = 0.0, a2 = 0.0, a3 = 0.0;
+    size_t head = 0;
+    if ((reinterpret_cast<uintptr_t>(x) & 15) == 0) {
+        const size_t n4 = n / 4;
+        const float4 *x4 = reinterpret_cast<const float4 *>(x);
+        size_t i = threadIdx.x;
+        for (; i + 3 * blockDim.x < n4; i += 4 * blockDim.x) {
+            const float4 p = __ldg(x4 + i), q = __ldg(x4 + i + blockDim.x);
+            const float4 r = __ldg(x4 + i + 2 * blockDim.x), t = __ldg(x4 + i + 3 * blockDim.x);
+            a0 = fma((double)p.x, (double)p.x, fma((double)p.y, (double)p.y, a0));
+            a1 = fma((double)p.z, (double)p.z, fma((double)p.w, (double)p.w, a1));
+            a2 = fma((double)q.x, (double)q.x, fma((double)q.y, (double)q.y, a2));
+            a3 = fma((double)q.z, (double)q.z, fma((double)q.w, (double)q.w, a3));
+            a0 = fma((double)r.x, (double)r.x, fma((double)r.y, (double)r.y, a0));
+            a1 = fma((double)r.z, (double)r.z, fma((double)r.w, (double)r.w, a1));
+            a2 = fma((double)t.x, (double)t.x, fma((double)t.y, (double)t.y, a2));
+            a3 = fma((double)t.z, (double)t.z, fma((double)t.w, (double)t.w, a3));
+        }
+        for (; i < n4; i += blockDim.x) {
+            const float4 p = __ldg(x4 + i);
+            a0 = fma((double)p.x, (double)p.x, fma((double)p.y, (double)p.y, a0));
+            a1 = fma((double)p.z, (double)p.z, fma((double)p.w, (double)p.w, a1));
+        }
+        head = n4 * 4;
+    }
+    for (size_t i = head + threadIdx.x; i < n; i += blockDim.x) a0 = fma((double)x[i], (double)x[i], a0);
+    s[threadIdx.x] = (a0 + a1) + (a2 + a3);
     __syncthreads();
     for (int o = blockDim.x / 2; o > 0; o >>= 1) {
         if ((int)threadIdx.x < o) s[threadIdx.x] += s[threadIdx.x + o];

@@ -16,7 +16,8 @@ computes runs as libsdp_b200 kernels on the device; torch owns the memory.
   blurred squared error and Adam, all on the device.
 * ``Deconvolver``: the major cycle, plain (Hogbom components, DFT predict)
   or learned: the network proposes up to max_components components from the
-  residual; their visibilities are gridded to an image, the least-squares
+  residual; their visibilities (DFT of pixel components, phase reduced
+  exactly in fixed point) are gridded to an image, the least-squares
   step alpha = <R, I>/<I, I> scales them, and the candidate residual is
   recomputed from the visibilities (measured - model - alpha x proposal),
   i.e. one exact degrid/grid major cycle.  The proposal is kept only when
@@ -244,7 +245,7 @@ class _Proposer:
         n = int(self.count.item())
         if n == 0:
             return False
-        D.dft_gauss(self.comps[:n], self.img.uvw_raw, self.vis)
+        D.dft_pixels(self.comps[:n], self.img.layout.cell, self.img.uvw_raw, self.vis)
         self.img.image(self.vis, self.pimg)
         D.dots(dirty, self.pimg, self.dots)
         D.axpy_ratio(self.dots, cfg.alpha_max, self.pimg, dirty, sign=-1.0)
@@ -431,8 +432,7 @@ class Deconvolver:
         D.hogbom(self.params, self.clean_img, self.img.psf, self.model_img, self.sources, self.nsrc, self.clean_ws)
         n = int(self.nsrc.item())
         if n > 0:
-            D.dft(self.sources[:n], self.img.uvw_raw, self.prop_vis)
-            D.add_vis(self.model_vis, self.prop_vis, self.model_vis)
+            D.dft_pixels(self.sources[:n], self.img.layout.cell, self.img.uvw_raw, self.model_vis, accumulate=True)
         return self._residual(measured), n
 
     def _propose(self, rms) -> tuple[bool, float, float, int]:
@@ -444,7 +444,7 @@ class Deconvolver:
         n = int(self.count.item())
         if n == 0:
             return False, rms, 0.0, 0
-        D.dft_gauss(self.comps[:n], self.img.uvw_raw, self.prop_vis)
+        D.dft_pixels(self.comps[:n], self.img.layout.cell, self.img.uvw_raw, self.prop_vis)
         self.img.image(self.prop_vis, self.prop_img)
         D.dots(self.residual, self.prop_img, self.dots)
         self.cand.copy_(self.residual)
@@ -457,10 +457,12 @@ class Deconvolver:
             return True, new, a, n
         return False, rms, a, n
 
-    def exact_rms(self, measured) -> float:
-        """RMS of the residual imaged afresh from measured - model visibilities
-        (the state a run left)."""
-        return self._residual(measured)
+    def exact_residual(self, measured):
+        """(tracked residual image, residual imaged afresh from measured -
+        model visibilities, RMS of the latter) for the state a run left."""
+        tracked = self.residual.clone()
+        rms = self._residual(measured)
+        return tracked, self.residual.clone(), rms
 
     def run(self, measured, max_cycles: int, learned: bool, target_rms: float | None = None):
         """Runs up to max_cycles major cycles from an empty model (stops early

@@ -708,6 +708,12 @@ class Device:
         check(self.lib.sdp_dft_gauss(_i(uvw.shape[0]), _i(sources.shape[0]), _dp(sources), _dp(uvw), _dp(vis),
                                      _stream(stream)), self.lib)
 
+    def dft_pixels(self, comps, cell, uvw, vis, accumulate=False, stream=None):
+        """comps [k][3 or 4] (l, m, flux[, ...]) on the pixel grid of cell."""
+        check(self.lib.sdp_dft_pixels(_i(uvw.shape[0]), _i(comps.shape[0]), _dp(comps), _i(comps.shape[1]),
+                                      _d(cell), _dp(uvw), _dp(vis), _i(1 if accumulate else 0), _stream(stream)),
+              self.lib)
+
     def add_vis(self, a, b, out, stream=None):
         check(self.lib.sdp_add_vis(_i(a.shape[0]), _dp(a), _dp(b), _dp(out), _stream(stream)), self.lib)
 
