@@ -572,6 +572,13 @@ int sdp_unet_forward(sdp_unet *net, int batch, int height, int width, const floa
 /* Adds d(loss)/d(params) for d(loss)/d(output) = grad_output (the last
  * forward's shape; scale NULL) to the gradient vector. */
 int sdp_unet_backward(sdp_unet *net, const float *grad_output, void *stream);
+/* Convolution engine: 1 (default) tcgen05 tensor cores with the accumulator
+ * in tensor memory (TMA-fed, warp-specialised); 0 the mma.sync kernel (kept
+ * for comparison). */
+int sdp_unet_set_tensor_path(sdp_unet *net, int tcgen05);
+/* Blocking: SDP_ERR_TIMEOUT when a tensor-core convolution gave up a bounded
+ * wait since the last check (its outputs are then incomplete), else SDP_OK. */
+int sdp_unet_check(sdp_unet *net, void *stream);
 /* One Adam step on the master weights (bias-corrected moments). */
 int sdp_unet_adam_step(sdp_unet *net, float lr, float beta1, float beta2, float eps, void *stream);
 /* loss = mean over pixels of (b * (pred - target))^2, b the 3x3 binomial

@@ -32,7 +32,9 @@
 // shared memory with ldmatrix (conflict-free: every 8-channel group is a
 // 16-byte row of its own plane), tiles staged by cp.async with zero fill
 // outside the image, double buffered.
+#include <cuda.h>
 #include <cuda_bf16.h>
+#include <cudaTypedefs.h>
 
 #include <cmath>
 #include <cstring>
@@ -86,6 +88,30 @@ __device__ __forceinline__ void mma16816(float (&d)[4], const uint32_t (&a)[4], 
         : "r"(a[0]), "r"(a[1]), "r"(a[2]), "r"(a[3]), "r"(b0), "r"(b1));
 }
 
+// 8 BF16 channels = one 16-byte vector
+union V8 {
+    uint4 u;
+    __nv_bfloat162 h[4];
+};
+
+__device__ __forceinline__ void unpack8(const uint4 &u, float (&f)[8])
+{
+    V8 v;
+    v.u = u;
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+        f[2 * k] = __low2float(v.h[k]);
+        f[2 * k + 1] = __high2float(v.h[k]);
+    }
+}
+__device__ __forceinline__ uint4 pack8(const float (&f)[8])
+{
+    V8 v;
+#pragma unroll
+    for (int k = 0; k < 4; ++k) v.h[k] = __floats2bfloat162_rn(f[2 * k], f[2 * k + 1]);
+    return v.u;
+}
+
 // Source of one 8-channel group of the (virtual) convolution input at image
 // pixel (yy, xx) of image img: channels [c, c + 8) of [a, up(b)].
 struct VIn {
@@ -128,7 +154,7 @@ struct ConvSmem {
 template <int BN>
 __global__ void __launch_bounds__(128) k_conv3x3(ConvArgs p)
 {
-    extern __shared__ __align__(16) unsigned char smem[];
+    extern __shared__ __align__(128) unsigned char smem[];
     using SM = ConvSmem<BN>;
     const int cin = p.in.ca + p.in.cb;
     const int nchunks = cin >> 4;
@@ -239,6 +265,354 @@ __global__ void __launch_bounds__(128) k_conv3x3(ConvArgs p)
 }
 
 // ----------------------------------------------------------------------------
+// The same convolution on the 5th-generation tensor cores (tcgen05), as a
+// persistent warp-specialised kernel.  Tile = R consecutive image rows
+// (R = 1, 2, 4 or 8; each a 128-pixel segment, M = 128 per row) x nt output
+// channels (nt <= 256, a multiple of 32), R accumulators in tensor memory.
+// K = 9 taps x Cin, walked as (chunk of KC = 32 or 64 channels, tap) pairs;
+// one pair = one pipeline stage:
+//   A: the R x 128 input pixels the tap reads (rows y0 + dy - 1 .., columns
+//      x0 + dx - 1 ..), KC channels each, by one 4-D TMA box {KC, 128, R, 1}
+//      (reads outside the image return zero);
+//   B: the pair's nt x KC weights, pre-arranged in global memory as the
+//      shared-memory image, by one bulk copy;
+// both in the K-major canonical layout with the 128-byte (KC = 64) or
+// 64-byte (KC = 32) swizzle, which the TMA writes and the MMA reads (rows of
+// KC channels; 8-row atoms of 1024 / 512 bytes; K advanced 16 channels = 32
+// bytes inside the row).  A stage is R x KC / 16 tcgen05.mma (M128 x nt x
+// K16, BF16 -> FP32 in tensor memory); each row's A starts on an atom.
+//   warp 0 (one thread): loads, through an S-stage ring (full/empty
+//     mbarriers, transaction counts);
+//   warp 1 (one thread): MMAs; commits free a stage (empty) and, after a
+//     tile's last stage, hand its accumulator to the epilogue;
+//   warps 2-5: epilogue, tcgen05.ld of the accumulator (warp w reads lanes
+//     32 (w % 4) ..), bias, relu or the gradient mask, BF16 stores; then
+//     free the accumulator.  Two accumulators in tensor memory let the
+//     epilogue of one tile overlap the MMAs of the next.
+// Every wait is bounded: on timeout the CTA records the error and each role
+// leaves its loop (its later waits are bounded too).
+// ----------------------------------------------------------------------------
+constexpr int kTcM = 128;                       // pixels per tile
+constexpr int kTcMaxStages = 16;
+constexpr int kTcSmemBudget = 200 * 1024;       // stages; +1 KB for the 1024-byte alignment
+constexpr long long kTcSpins = 1LL << 20;       // bounded mbarrier polls
+
+inline int tc_kc(int cin) { return cin % 64 == 0 ? 64 : 32; }
+__host__ __device__ constexpr int tc_a_bytes(int kc, int rows) { return rows * kTcM * kc * 2; }
+__host__ __device__ constexpr int tc_b_bytes(int nt, int kc) { return nt * kc * 2; }
+__host__ __device__ constexpr int tc_stage_bytes(int nt, int kc, int rows)
+{
+    return (tc_a_bytes(kc, rows) + tc_b_bytes(nt, kc) + 1023) & ~1023;
+}
+inline int tc_stages(int nt, int kc, int rows)
+{
+    int s = kTcSmemBudget / tc_stage_bytes(nt, kc, rows);
+    return s > kTcMaxStages ? kTcMaxStages : s;
+}
+__host__ __device__ constexpr uint32_t tc_ncols(int nt) { return nt <= 32 ? 32u : (nt <= 64 ? 64u : (nt <= 128 ? 128u : 256u)); }
+
+struct TcArgs {
+    int n, h, w;         // image batch and size (input = output)
+    int cin, cout, nt;   // nt: output channels per slice (blockIdx.y)
+    int kc, nchunks;     // channels per chunk (32 or 64), cin / kc
+    int rows;            // image rows per tile (R)
+    int tiles_x, tiles_y, ntiles; // tiles per slice
+    int stages;
+    const bf16 *wtc;     // [slice][chunk][tap] blocks of nt x kc, swizzled as in shared memory
+    const float *bias;   // [cout] or null
+    const bf16 *mask;    // [n][h][w][cout] or null
+    bf16 *out;           // [n][h][w][cout]
+    int relu;
+    int *err;            // set to 1 when a bounded wait gave up
+};
+
+// K-major operand descriptor with the 128-byte (layout 2) or 64-byte
+// (layout 4) swizzle: SBO = one 8-row atom, LBO unused (1).
+__device__ __forceinline__ uint64_t umma_desc_sw(uint32_t saddr, int kc)
+{
+    const uint32_t sbo = (uint32_t)(8 * kc * 2);
+    uint64_t d = (uint64_t)((saddr >> 4) & 0x3FFFu);
+    d |= (uint64_t)1 << 16;
+    d |= (uint64_t)((sbo >> 4) & 0x3FFFu) << 32;
+    d |= (uint64_t)1 << 46;  // descriptor version of sm_100
+    d |= (uint64_t)(kc == 64 ? 2 : 4) << 61;
+    return d;
+}
+
+__device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity)
+{
+    for (long long i = 0; i < kTcSpins; ++i) {
+        uint32_t done;
+        asm volatile(
+            "{\n\t.reg .pred P1;\n\t"
+            "mbarrier.try_wait.parity.shared::cta.b64 P1, [%1], %2;\n\t"
+            "selp.b32 %0, 1, 0, P1;\n\t}"
+            : "=r"(done)
+            : "r"(bar), "r"(parity)
+            : "memory");
+        if (done) return true;
+    }
+    return false;
+}
+
+__device__ __forceinline__ void mbar_init(uint32_t bar, uint32_t count)
+{
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(bar), "r"(count));
+}
+
+__device__ __forceinline__ void mbar_arrive(uint32_t bar)
+{
+    asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(bar) : "memory");
+}
+
+__device__ __forceinline__ void mbar_expect_tx(uint32_t bar, uint32_t bytes)
+{
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar), "r"(bytes) : "memory");
+}
+
+__global__ void __launch_bounds__(192, 1) k_conv3x3_tc(const __grid_constant__ CUtensorMap tin, TcArgs p)
+{
+    extern __shared__ __align__(128) unsigned char smem[];
+    __shared__ __align__(8) uint64_t s_full[kTcMaxStages], s_empty[kTcMaxStages], s_tfull[2], s_tempty[2];
+    __shared__ uint32_t s_tmem;
+    __shared__ int s_fail;
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    const int nt = p.nt, S = p.stages, kc = p.kc, R = p.rows;
+    const int slice = blockIdx.y;
+    const uint32_t ncols = tc_ncols(nt);
+    const uint32_t acc_cols = (uint32_t)R * ncols;  // one accumulator set (R rows)
+    const int stage_bytes = tc_stage_bytes(nt, kc, R);
+    // stages start on 1024-byte boundaries (the swizzle atoms)
+    const uint32_t sbase = (smem_u32(smem) + 1023u) & ~1023u;
+    const int per_tile = 9 * p.nchunks;
+
+    if (warp == 0) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(&s_tmem)),
+                     "r"(2 * acc_cols));
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::);
+    }
+    if (tid == 32) {
+        for (int i = 0; i < S; ++i) {
+            mbar_init(smem_u32(&s_full[i]), 1);
+            mbar_init(smem_u32(&s_empty[i]), 1);
+        }
+        for (int i = 0; i < 2; ++i) {
+            mbar_init(smem_u32(&s_tfull[i]), 1);
+            mbar_init(smem_u32(&s_tempty[i]), 4);
+        }
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+        s_fail = 0;
+    }
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+    __syncthreads();
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+    const uint32_t tmem = s_tmem;
+    const int first = blockIdx.x, step = gridDim.x;
+    volatile int *fail = &s_fail;  // read afresh in every loop condition
+
+    if (warp == 0) {
+        if (lane == 0) {
+            // ---------------- loads ----------------
+            const uint32_t a_bytes = (uint32_t)tc_a_bytes(kc, R), b_bytes = (uint32_t)tc_b_bytes(nt, kc);
+            long long g = 0;
+            for (int t = first; t < p.ntiles && !*fail; t += step) {
+                const int tx = t % p.tiles_x, trow = t / p.tiles_x;
+                const int img = trow / p.tiles_y, y = (trow - img * p.tiles_y) * R;
+                for (int k = 0; k < per_tile; ++k, ++g) {
+                    const int chunk = k / 9, tap = k - 9 * chunk;
+                    const int dy = tap / 3, dx = tap - 3 * dy;
+                    const int s = (int)(g % S);
+                    const long long use = g / S;
+                    if (use > 0 && !mbar_wait(smem_u32(&s_empty[s]), (uint32_t)((use - 1) & 1))) {
+                        *fail = 1;
+                        break;
+                    }
+                    const uint32_t st = sbase + (uint32_t)(s * stage_bytes);
+                    const uint32_t bar = smem_u32(&s_full[s]);
+                    mbar_expect_tx(bar, a_bytes + b_bytes);
+                    asm volatile(
+                        "cp.async.bulk.tensor.4d.shared::cluster.global.tile.mbarrier::complete_tx::bytes "
+                        "[%0], [%1, {%2, %3, %4, %5}], [%6];" ::"r"(st),
+                        "l"(reinterpret_cast<uint64_t>(&tin)), "r"(kc * chunk), "r"(tx * kTcM + dx - 1),
+                        "r"(y + dy - 1), "r"(img), "r"(bar)
+                        : "memory");
+                    const bf16 *wsrc = p.wtc + (((size_t)slice * p.nchunks + chunk) * 9 + tap) * (size_t)(nt * kc);
+                    asm volatile(
+                        "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+                            st + a_bytes),
+                        "l"(wsrc), "r"(b_bytes), "r"(bar)
+                        : "memory");
+                }
+            }
+        }
+    } else if (warp == 1) {
+        if (lane == 0) {
+            // ---------------- MMAs ----------------
+            const uint32_t idesc = (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(nt >> 3) << 17) |
+                                   ((uint32_t)(kTcM >> 4) << 24);
+            const uint32_t a_bytes = (uint32_t)tc_a_bytes(kc, R), row_bytes = (uint32_t)tc_a_bytes(kc, 1);
+            long long g = 0;
+            int j = 0;
+            for (int t = first; t < p.ntiles && !*fail; t += step, ++j) {
+                const int acc = j & 1, use = j >> 1;
+                if (use > 0 && !mbar_wait(smem_u32(&s_tempty[acc]), (uint32_t)((use - 1) & 1))) {
+                    *fail = 1;
+                    break;
+                }
+                asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+                const uint32_t d = tmem + (uint32_t)acc * acc_cols;
+                bool ok = true;
+                for (int k = 0; k < per_tile; ++k, ++g) {
+                    const int s = (int)(g % S);
+                    if (!mbar_wait(smem_u32(&s_full[s]), (uint32_t)((g / S) & 1))) {
+                        ok = false;
+                        break;
+                    }
+                    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+                    const uint32_t as = sbase + (uint32_t)(s * stage_bytes), bs = as + a_bytes;
+                    for (int kk = 0; kk < kc / 16; ++kk) {
+                        const uint64_t bd = umma_desc_sw(bs + (uint32_t)(kk * 32), kc);
+                        const uint32_t accum = (k > 0 || kk > 0) ? 1u : 0u;
+                        for (int r = 0; r < R; ++r) {
+                            const uint64_t ad = umma_desc_sw(as + (uint32_t)r * row_bytes + (uint32_t)(kk * 32), kc);
+                            asm volatile(
+                                "{\n\t.reg .pred p;\n\t"
+                                "setp.ne.b32 p, %4, 0;\n\t"
+                                "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, {%5, %6, %7, %8}, p;\n\t}"
+                                :
+                                : "r"(d + (uint32_t)r * ncols), "l"(ad), "l"(bd), "r"(idesc), "r"(accum), "r"(0u),
+                                  "r"(0u), "r"(0u), "r"(0u));
+                        }
+                    }
+                    asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
+                                     smem_u32(&s_empty[s]))
+                                 : "memory");
+                }
+                if (!ok) {
+                    *fail = 1;
+                    break;
+                }
+                asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
+                                 smem_u32(&s_tfull[acc]))
+                             : "memory");
+            }
+        }
+    } else {
+        // ---------------- epilogue (warps 2..5) ----------------
+        const int q = warp & 3;  // tensor-memory lane quarter this warp may read
+        int j = 0;
+        for (int t = first; t < p.ntiles; t += step, ++j) {
+            const int acc = j & 1, use = j >> 1;
+            if (__any_sync(0xffffffffu, *fail != 0)) break;
+            bool ok = mbar_wait(smem_u32(&s_tfull[acc]), (uint32_t)(use & 1));
+            ok = __all_sync(0xffffffffu, ok);
+            if (!ok) {
+                if (lane == 0) *fail = 1;
+                break;
+            }
+            asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+            const int tx = t % p.tiles_x, trow = t / p.tiles_x;
+            const int img = trow / p.tiles_y, y0 = (trow - img * p.tiles_y) * R;
+            const int x = tx * kTcM + q * 32 + lane;
+            const int cbase = slice * nt;
+            for (int rr = 0; rr < R; ++rr)
+            for (int c = 0; c < nt; c += 32) {
+                const int y = y0 + rr;
+                const bool store = x < p.w && y < p.h;
+                const size_t pix = ((size_t)img * p.h + (store ? y : 0)) * p.w + (store ? x : 0);
+                uint32_t r[32];
+                const uint32_t taddr = tmem + (uint32_t)acc * acc_cols + (uint32_t)rr * ncols +
+                                       ((uint32_t)(q * 32) << 16) + (uint32_t)c;
+                asm volatile(
+                    "tcgen05.ld.sync.aligned.32x32b.x32.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15,"
+                    "%16,%17,%18,%19,%20,%21,%22,%23,%24,%25,%26,%27,%28,%29,%30,%31}, [%32];"
+                    : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]),
+                      "=r"(r[7]), "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]),
+                      "=r"(r[14]), "=r"(r[15]), "=r"(r[16]), "=r"(r[17]), "=r"(r[18]), "=r"(r[19]), "=r"(r[20]),
+                      "=r"(r[21]), "=r"(r[22]), "=r"(r[23]), "=r"(r[24]), "=r"(r[25]), "=r"(r[26]), "=r"(r[27]),
+                      "=r"(r[28]), "=r"(r[29]), "=r"(r[30]), "=r"(r[31])
+                    : "r"(taddr));
+                asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+                if (!store) continue;
+                const int cg = cbase + c;
+#pragma unroll
+                for (int gi = 0; gi < 4; ++gi) {
+                    float v[8];
+#pragma unroll
+                    for (int e = 0; e < 8; ++e) {
+                        float f = __uint_as_float(r[8 * gi + e]);
+                        if (p.bias) f += __ldg(p.bias + cg + 8 * gi + e);
+                        if (p.relu) f = f > 0.f ? f : 0.f;
+                        v[e] = f;
+                    }
+                    if (p.mask) {
+                        float m[8];
+                        unpack8(*reinterpret_cast<const uint4 *>(p.mask + pix * p.cout + cg + 8 * gi), m);
+#pragma unroll
+                        for (int e = 0; e < 8; ++e)
+                            if (!(m[e] > 0.f)) v[e] = 0.f;
+                    }
+                    *reinterpret_cast<uint4 *>(p.out + pix * p.cout + cg + 8 * gi) = pack8(v);
+                }
+            }
+            asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+            __syncwarp();
+            if (lane == 0) mbar_arrive(smem_u32(&s_tempty[acc]));
+        }
+    }
+    __syncthreads();
+    if (*fail && tid == 0 && p.err) atomicExch(p.err, 1);
+    if (warp == 0) {
+        asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(2 * acc_cols));
+    }
+}
+
+// Weights in the tensor-core kernel's staging order: one block of nt x kc
+// per (slice, chunk, tap), row co = output channel, kc input channels, the
+// 16-byte groups of row co stored at group ^ swizzle(co) (128-byte swizzle:
+// co & 7; 64-byte swizzle: (co >> 1) & 3), i.e. the shared-memory image.
+__global__ void k_weights_tc(int cout, int cin, int nt, int kc, const bf16 *__restrict__ wk, bf16 *__restrict__ wtc)
+{
+    const long long total = 9LL * cout * cin;
+    const int nch = cin / kc;
+    for (long long k = blockIdx.x * (long long)blockDim.x + threadIdx.x; k < total;
+         k += (long long)gridDim.x * blockDim.x) {
+        // source index: tap, output channel, input channel
+        const int ci = (int)(k % cin);
+        const long long r = k / cin;
+        const int co_all = (int)(r % cout);
+        const int tap = (int)(r / cout);
+        const int slice = co_all / nt, co = co_all - slice * nt;
+        const int chunk = ci / kc, cl = ci - chunk * kc;
+        const int grp = cl >> 3;
+        const int swz = kc == 64 ? (co & 7) : ((co >> 1) & 3);
+        const size_t block = (((size_t)slice * nch + chunk) * 9 + tap) * (size_t)(nt * kc);
+        wtc[block + (size_t)co * kc + (size_t)(((grp ^ swz) << 3) + (cl & 7))] = wk[k];
+    }
+}
+
+// out[p] = [a[p], b[p / 2]] (nearest upsampling of b, then concatenation).
+__global__ void k_concat_up(int n, int h, int w, int ca, int cb, const bf16 *__restrict__ a,
+                            const bf16 *__restrict__ b, bf16 *__restrict__ out)
+{
+    const int ct = ca + cb, g8 = ct >> 3;
+    const long long total = (long long)n * h * w * g8;
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < total;
+         i += (long long)gridDim.x * blockDim.x) {
+        const int g = (int)(i % g8);
+        const long long pix = i / g8;
+        const int x = (int)(pix % w), y = (int)((pix / w) % h);
+        const long long img = pix / ((long long)w * h);
+        const int c = 8 * g;
+        const uint4 v = c < ca ? *reinterpret_cast<const uint4 *>(a + pix * ca + c)
+                               : *reinterpret_cast<const uint4 *>(
+                                     b + ((img * (h >> 1) + (y >> 1)) * (w >> 1) + (x >> 1)) * cb + (c - ca));
+        *reinterpret_cast<uint4 *>(out + pix * ct + c) = v;
+    }
+}
+
+// ----------------------------------------------------------------------------
 // Weight gradient: dw[tap][o][i] += sum_p dz[p][o] * in[p + off(tap)][i].
 // One CTA: 32 output x 32 input channels, all 9 taps (warp = tap), over a
 // strided set of pixel tiles; per tile and tile row one k16 step of
@@ -260,7 +634,7 @@ constexpr int kWgBytes = 2 * kWgStage;
 
 __global__ void __launch_bounds__(288) k_wgrad3x3(WgradArgs p)
 {
-    extern __shared__ __align__(16) unsigned char smem[];
+    extern __shared__ __align__(128) unsigned char smem[];
     const int co0 = blockIdx.x * 32, ci0 = blockIdx.y * 32;
     const int cin = p.in.ca + p.in.cb;
     const int tid = threadIdx.x, lane = tid & 31, tap = tid >> 5;
@@ -365,29 +739,6 @@ __global__ void __launch_bounds__(256) k_bias_grad(const bf16 *__restrict__ dz, 
 // ----------------------------------------------------------------------------
 // Element-wise kernels (8 channels = one 16-byte vector per thread)
 // ----------------------------------------------------------------------------
-union V8 {
-    uint4 u;
-    __nv_bfloat162 h[4];
-};
-
-__device__ __forceinline__ void unpack8(const uint4 &u, float (&f)[8])
-{
-    V8 v;
-    v.u = u;
-#pragma unroll
-    for (int k = 0; k < 4; ++k) {
-        f[2 * k] = __low2float(v.h[k]);
-        f[2 * k + 1] = __high2float(v.h[k]);
-    }
-}
-__device__ __forceinline__ uint4 pack8(const float (&f)[8])
-{
-    V8 v;
-#pragma unroll
-    for (int k = 0; k < 4; ++k) v.h[k] = __floats2bfloat162_rn(f[2 * k], f[2 * k + 1]);
-    return v.u;
-}
-
 // x[n][y][x][0..31] = in[n][c][y][x] / scale[n] (c < cin), 0 above.
 __global__ void k_pack_input(int n, int cin, int h, int w, const float *__restrict__ in,
                              const float *__restrict__ scale, bf16 *__restrict__ x)
@@ -671,6 +1022,7 @@ struct Layer {
     int cin, cout;
     size_t woff, boff;  // into the FP32 parameter vector
     bf16 *w = nullptr, *wt = nullptr;
+    bf16 *wtc = nullptr, *wttc = nullptr;  // the two in the tensor-core kernel's staging order
 };
 struct Act {  // one activation tensor (and its gradient scratch)
     bf16 *p = nullptr;
@@ -693,9 +1045,12 @@ struct sdp_unet {
     // gradient scratch (training)
     bf16 *gz[kLevels][2] = {};
     bf16 *dcat[kLevels - 1] = {};
+    bf16 *cat[kLevels - 1] = {};  // [e_l, up(low)] materialised for the tensor-core path
     // shape of the last forward pass
     int n = 0, h = 0, w = 0;
     bool have_forward = false;
+    int tensor_path = 1;    // 1: tcgen05 convolutions, 0: mma.sync
+    int *err = nullptr;     // device flag: a bounded wait gave up
     void *arena = nullptr;
 };
 
@@ -737,9 +1092,93 @@ int dec_layer(int l, int second) { return 8 + 2 * (kLevels - 2 - l) + second; }
 
 size_t tiles(int n, int h, int w) { return (size_t)n * ((h + kTH - 1) / kTH) * ((w + kTW - 1) / kTW); }
 
-int conv(const Layer &L, VIn in, const bf16 *wk, const float *bias, const bf16 *mask, bf16 *out, int cout, int relu,
-         int n, cudaStream_t st)
+// Output-channel slices of a tensor-core convolution: nt = cout / slices <= 256,
+// a multiple of 32.
+int tc_slices(int cout)
 {
+    int ny = (cout + 255) / 256;
+    while (cout % ny != 0 || (cout / ny) % 32 != 0) ++ny;
+    return ny;
+}
+
+PFN_cuTensorMapEncodeTiled_v12000 tensor_map_encoder()
+{
+    static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
+    if (!fn) {
+        void *f = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &f, cudaEnableDefault, &q) == cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            fn = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(f);
+    }
+    return fn;
+}
+
+int conv_tc(const bf16 *in, int cin, int h, int w, int n, const bf16 *wtc, const float *bias, const bf16 *mask,
+            bf16 *out, int cout, int relu, int *err, cudaStream_t st)
+{
+    SDP_CHECK_ARG(cin % 32 == 0 && cout % 32 == 0, "tensor-core convolution: channels %d -> %d", cin, cout);
+    auto enc = tensor_map_encoder();
+    if (!enc) return set_error(SDP_ERR_CUDA, "cuTensorMapEncodeTiled unavailable");
+    const int kc = tc_kc(cin);
+    const int ny = tc_slices(cout);
+    const int nt = cout / ny;
+    const int tiles_x = (w + kTcM - 1) / kTcM;
+    // rows per tile: as many as tensor memory holds (two sets of R
+    // accumulators) while the tiles still cover the SMs
+    // and at least three stages fit in shared memory
+    int R = 8;
+    while (R > 1 && (2u * (uint32_t)R * tc_ncols(nt) > 512u || tc_stages(nt, kc, R) < 3 ||
+                     (long long)n * ((h + R - 1) / R) * tiles_x * ny < num_sms()))
+        R >>= 1;
+    CUtensorMap tmap;
+    const cuuint64_t dims[4] = {(cuuint64_t)cin, (cuuint64_t)w, (cuuint64_t)h, (cuuint64_t)n};
+    const cuuint64_t strides[3] = {(cuuint64_t)cin * 2, (cuuint64_t)w * cin * 2, (cuuint64_t)h * w * cin * 2};
+    const cuuint32_t box[4] = {(cuuint32_t)kc, (cuuint32_t)kTcM, (cuuint32_t)R, 1};
+    const cuuint32_t estr[4] = {1, 1, 1, 1};
+    const CUresult r = enc(&tmap, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 4, const_cast<bf16 *>(in), dims, strides, box,
+                           estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
+                           kc == 64 ? CU_TENSOR_MAP_SWIZZLE_128B : CU_TENSOR_MAP_SWIZZLE_64B,
+                           CU_TENSOR_MAP_L2_PROMOTION_L2_128B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    if (r != CUDA_SUCCESS) return set_error(SDP_ERR_CUDA, "cuTensorMapEncodeTiled failed (%d)", (int)r);
+    TcArgs a;
+    a.n = n;
+    a.h = h;
+    a.w = w;
+    a.cin = cin;
+    a.cout = cout;
+    a.nt = nt;
+    a.kc = kc;
+    a.nchunks = cin / kc;
+    a.rows = R;
+    a.tiles_x = tiles_x;
+    a.tiles_y = (h + R - 1) / R;
+    a.ntiles = n * a.tiles_y * tiles_x;
+    a.stages = tc_stages(nt, kc, R);
+    a.wtc = wtc;
+    a.bias = bias;
+    a.mask = mask;
+    a.out = out;
+    a.relu = relu;
+    a.err = err;
+    int per_slice = num_sms() / ny;
+    if (per_slice < 1) per_slice = 1;
+    if (per_slice > a.ntiles) per_slice = a.ntiles;
+    const size_t smem = (size_t)a.stages * tc_stage_bytes(nt, kc, R) + 1024;
+    k_conv3x3_tc<<<dim3((unsigned)per_slice, ny), 192, smem, st>>>(tmap, a);
+    SDP_LAUNCH_CHECK();
+    return SDP_OK;
+}
+
+// wk: [9][cout][cin] for the mma.sync kernel; wtc: the same weights in the
+// tensor-core staging order (the tensor-core path reads a plain input, in.cb == 0).
+int conv(const sdp_unet *u, VIn in, const bf16 *wk, const bf16 *wtc, const float *bias, const bf16 *mask, bf16 *out,
+         int cout, int relu, int n, cudaStream_t st)
+{
+    if (u->tensor_path) {
+        SDP_CHECK_ARG(in.cb == 0, "tensor-core convolution reads a materialised input");
+        return conv_tc(in.a, in.ca, in.h, in.w, n, wtc, bias, mask, out, cout, relu, u->err, st);
+    }
     ConvArgs a;
     a.in = in;
     a.wk = wk;
@@ -751,7 +1190,6 @@ int conv(const Layer &L, VIn in, const bf16 *wk, const float *bias, const bf16 *
     a.tiles_x = (in.w + kTW - 1) / kTW;
     a.tiles_y = (in.h + kTH - 1) / kTH;
     const size_t nt = tiles(n, in.h, in.w);
-    (void)L;
     if (cout % 64 == 0 && nt * (cout / 64) >= (size_t)2 * num_sms()) {
         k_conv3x3<64><<<dim3((unsigned)nt, cout / 64), 128, ConvSmem<64>::kBytes, st>>>(a);
     } else {
@@ -806,6 +1244,8 @@ int set_attrs()
     SDP_CUDA_TRY(cudaFuncSetAttribute(k_conv3x3<64>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                       ConvSmem<64>::kBytes));
     SDP_CUDA_TRY(cudaFuncSetAttribute(k_wgrad3x3, cudaFuncAttributeMaxDynamicSharedMemorySize, kWgBytes));
+    SDP_CUDA_TRY(cudaFuncSetAttribute(k_conv3x3_tc, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                      kTcSmemBudget + 1024));
     done = true;
     return SDP_OK;
 }
@@ -815,6 +1255,12 @@ int refresh_weights(sdp_unet *u, cudaStream_t st)
     for (auto &L : u->layer) {
         const int total = 9 * L.cin * L.cout;
         k_layer_weights<<<grid_for(total), 256, 0, st>>>(L.cout, L.cin, u->master + L.woff, L.w, L.wt);
+        SDP_LAUNCH_CHECK();
+        k_weights_tc<<<grid_for(total), 256, 0, st>>>(L.cout, L.cin, L.cout / tc_slices(L.cout), tc_kc(L.cin), L.w,
+                                                      L.wtc);
+        SDP_LAUNCH_CHECK();
+        k_weights_tc<<<grid_for(total), 256, 0, st>>>(L.cin, L.cout, L.cin / tc_slices(L.cin), tc_kc(L.cout), L.wt,
+                                                      L.wttc);
         SDP_LAUNCH_CHECK();
     }
     return SDP_OK;
@@ -851,14 +1297,18 @@ SDP_EXPORT int sdp_unet_create(sdp_unet **out, int base_channels, int in_channel
         bytes += (b + 255) & ~(size_t)255;
         return at;
     };
+    const size_t o_err = take(sizeof(int));
     const size_t o_master = take(u->nparams * 4);
     const size_t o_grad = u->training ? take(u->nparams * 4) : 0;
     const size_t o_m = u->training ? take(u->nparams * 4) : 0;
     const size_t o_v = u->training ? take(u->nparams * 4) : 0;
-    size_t o_w[kLayers], o_wt[kLayers];
+    size_t o_w[kLayers], o_wt[kLayers], o_wtc[kLayers], o_wttc[kLayers];
     for (int k = 0; k < kLayers; ++k) {
-        o_w[k] = take((size_t)9 * u->layer[k].cin * u->layer[k].cout * 2);
-        o_wt[k] = take((size_t)9 * u->layer[k].cin * u->layer[k].cout * 2);
+        const size_t wb = (size_t)9 * u->layer[k].cin * u->layer[k].cout * 2;
+        o_w[k] = take(wb);
+        o_wt[k] = take(wb);
+        o_wtc[k] = take(wb);
+        o_wttc[k] = take(wb);
     }
     const size_t o_x = take(pix(u, 0) * kInPad * 2);
     size_t o_e[kLevels][2], o_pool[kLevels] = {}, o_d[kLevels - 1][2], o_gz[kLevels][2] = {}, o_dcat[kLevels - 1] = {};
@@ -867,9 +1317,11 @@ SDP_EXPORT int sdp_unet_create(sdp_unet **out, int base_channels, int in_channel
         o_e[l][1] = take(pix(u, l) * ch(u, l) * 2);
         if (l > 0) o_pool[l] = take(pix(u, l) * ch(u, l - 1) * 2);
     }
+    size_t o_cat[kLevels - 1];
     for (int l = 0; l < kLevels - 1; ++l) {
         o_d[l][0] = take(pix(u, l) * ch(u, l) * 2);
         o_d[l][1] = take(pix(u, l) * ch(u, l) * 2);
+        o_cat[l] = take(pix(u, l) * (ch(u, l) + ch(u, l + 1)) * 2);
     }
     if (u->training) {
         for (int l = 0; l < kLevels; ++l) {
@@ -886,6 +1338,7 @@ SDP_EXPORT int sdp_unet_create(sdp_unet **out, int base_channels, int in_channel
     }
     u->arena = arena;
     char *A = static_cast<char *>(arena);
+    u->err = reinterpret_cast<int *>(A + o_err);
     u->master = reinterpret_cast<float *>(A + o_master);
     if (u->training) {
         u->grad = reinterpret_cast<float *>(A + o_grad);
@@ -895,6 +1348,8 @@ SDP_EXPORT int sdp_unet_create(sdp_unet **out, int base_channels, int in_channel
     for (int k = 0; k < kLayers; ++k) {
         u->layer[k].w = reinterpret_cast<bf16 *>(A + o_w[k]);
         u->layer[k].wt = reinterpret_cast<bf16 *>(A + o_wt[k]);
+        u->layer[k].wtc = reinterpret_cast<bf16 *>(A + o_wtc[k]);
+        u->layer[k].wttc = reinterpret_cast<bf16 *>(A + o_wttc[k]);
     }
     u->x = reinterpret_cast<bf16 *>(A + o_x);
     for (int l = 0; l < kLevels; ++l) {
@@ -909,6 +1364,7 @@ SDP_EXPORT int sdp_unet_create(sdp_unet **out, int base_channels, int in_channel
     for (int l = 0; l < kLevels - 1; ++l) {
         u->d[l][0] = reinterpret_cast<bf16 *>(A + o_d[l][0]);
         u->d[l][1] = reinterpret_cast<bf16 *>(A + o_d[l][1]);
+        u->cat[l] = reinterpret_cast<bf16 *>(A + o_cat[l]);
         if (u->training) u->dcat[l] = reinterpret_cast<bf16 *>(A + o_dcat[l]);
     }
     e = cudaMemset(arena, 0, bytes);
@@ -927,6 +1383,26 @@ SDP_EXPORT int sdp_unet_destroy(sdp_unet *u)
     cudaDeviceSynchronize();
     if (u->arena) cudaFree(u->arena);
     delete u;
+    return SDP_OK;
+}
+
+SDP_EXPORT int sdp_unet_set_tensor_path(sdp_unet *u, int tcgen05)
+{
+    SDP_CHECK_ARG(u, "NULL handle");
+    u->tensor_path = tcgen05 ? 1 : 0;
+    return SDP_OK;
+}
+
+SDP_EXPORT int sdp_unet_check(sdp_unet *u, void *stream)
+{
+    SDP_CHECK_ARG(u, "NULL handle");
+    int h = 0;
+    SDP_CUDA_TRY(cudaMemcpyAsync(&h, u->err, sizeof(int), cudaMemcpyDeviceToHost, as_stream(stream)));
+    SDP_CUDA_TRY(cudaStreamSynchronize(as_stream(stream)));
+    if (h) {
+        SDP_CUDA_TRY(cudaMemsetAsync(u->err, 0, sizeof(int), as_stream(stream)));
+        return set_error(SDP_ERR_TIMEOUT, "a tensor-core convolution gave up waiting for its MMAs");
+    }
     return SDP_OK;
 }
 
@@ -1019,8 +1495,10 @@ SDP_EXPORT int sdp_unet_forward(sdp_unet *u, int n, int h, int w, const float *i
             SDP_LAUNCH_CHECK();
         }
         const Layer &La = u->layer[enc_layer(l, 0)], &Lb = u->layer[enc_layer(l, 1)];
-        SDP_TRY(conv(La, vin(src, cs, nullptr, 0, hl, wl), La.w, P + La.boff, nullptr, u->e[l][0], c, 1, n, st));
-        SDP_TRY(conv(Lb, vin(u->e[l][0], c, nullptr, 0, hl, wl), Lb.w, P + Lb.boff, nullptr, u->e[l][1], c, 1, n,
+        SDP_TRY(conv(u, vin(src, cs, nullptr, 0, hl, wl), La.w, La.wtc, P + La.boff, nullptr, u->e[l][0], c, 1, n,
+                     st));
+        SDP_TRY(conv(u, vin(u->e[l][0], c, nullptr, 0, hl, wl), Lb.w, Lb.wtc, P + Lb.boff, nullptr, u->e[l][1], c,
+                     1, n,
                      st));
     }
     // decoder
@@ -1028,8 +1506,16 @@ SDP_EXPORT int sdp_unet_forward(sdp_unet *u, int n, int h, int w, const float *i
         const int hl = h >> l, wl = w >> l, c = ch(u, l), c1 = ch(u, l + 1);
         const bf16 *low = (l == kLevels - 2) ? u->e[l + 1][1] : u->d[l + 1][1];
         const Layer &La = u->layer[dec_layer(l, 0)], &Lb = u->layer[dec_layer(l, 1)];
-        SDP_TRY(conv(La, vin(u->e[l][1], c, low, c1, hl, wl), La.w, P + La.boff, nullptr, u->d[l][0], c, 1, n, st));
-        SDP_TRY(conv(Lb, vin(u->d[l][0], c, nullptr, 0, hl, wl), Lb.w, P + Lb.boff, nullptr, u->d[l][1], c, 1, n,
+        VIn cat_in = vin(u->e[l][1], c, low, c1, hl, wl);
+        if (u->tensor_path) {
+            k_concat_up<<<grid_for((long long)n * hl * wl * ((c + c1) / 8)), 256, 0, st>>>(n, hl, wl, c, c1,
+                                                                                           u->e[l][1], low, u->cat[l]);
+            SDP_LAUNCH_CHECK();
+            cat_in = vin(u->cat[l], c + c1, nullptr, 0, hl, wl);
+        }
+        SDP_TRY(conv(u, cat_in, La.w, La.wtc, P + La.boff, nullptr, u->d[l][0], c, 1, n, st));
+        SDP_TRY(conv(u, vin(u->d[l][0], c, nullptr, 0, hl, wl), Lb.w, Lb.wtc, P + Lb.boff, nullptr, u->d[l][1], c,
+                     1, n,
                      st));
     }
     k_head_fwd<<<grid_for(np), 256, 0, st>>>(np, (long long)h * w, ch(u, 0), u->d[0][1], P + u->head_off,
@@ -1062,12 +1548,14 @@ SDP_EXPORT int sdp_unet_backward(sdp_unet *u, const float *grad_output, void *st
         const Layer &La = u->layer[dec_layer(l, 0)], &Lb = u->layer[dec_layer(l, 1)];
         // second conv: d_l = conv(d_l a)
         SDP_TRY(wgrad(u->gz[l][0], c, vin(u->d[l][0], c, nullptr, 0, hl, wl), G + Lb.woff, G + Lb.boff, n, st));
-        SDP_TRY(conv(Lb, vin(u->gz[l][0], c, nullptr, 0, hl, wl), Lb.wt, nullptr, u->d[l][0], u->gz[l][1], c, 0, n,
+        SDP_TRY(conv(u, vin(u->gz[l][0], c, nullptr, 0, hl, wl), Lb.wt, Lb.wttc, nullptr, u->d[l][0], u->gz[l][1],
+                     c, 0, n,
                      st));
         // first conv: d_l a = conv([e_l, up(low)])
         const bf16 *low = (l == kLevels - 2) ? u->e[l + 1][1] : u->d[l + 1][1];
         SDP_TRY(wgrad(u->gz[l][1], c, vin(u->e[l][1], c, low, c1, hl, wl), G + La.woff, G + La.boff, n, st));
-        SDP_TRY(conv(La, vin(u->gz[l][1], c, nullptr, 0, hl, wl), La.wt, nullptr, nullptr, u->dcat[l], c + c1, 0, n,
+        SDP_TRY(conv(u, vin(u->gz[l][1], c, nullptr, 0, hl, wl), La.wt, La.wttc, nullptr, nullptr, u->dcat[l],
+                     c + c1, 0, n,
                      st));
         // up-sampled part -> dZ of the lower tensor (d_{l+1} or e_3)
         k_up_bwd<<<grid_for((long long)n * (hl / 2) * (wl / 2) * (c1 / 8)), 256, 0, st>>>(
@@ -1079,14 +1567,16 @@ SDP_EXPORT int sdp_unet_backward(sdp_unet *u, const float *grad_output, void *st
         const int hl = h >> l, wl = w >> l, c = ch(u, l);
         const Layer &La = u->layer[enc_layer(l, 0)], &Lb = u->layer[enc_layer(l, 1)];
         SDP_TRY(wgrad(u->gz[l][0], c, vin(u->e[l][0], c, nullptr, 0, hl, wl), G + Lb.woff, G + Lb.boff, n, st));
-        SDP_TRY(conv(Lb, vin(u->gz[l][0], c, nullptr, 0, hl, wl), Lb.wt, nullptr, u->e[l][0], u->gz[l][1], c, 0, n,
+        SDP_TRY(conv(u, vin(u->gz[l][0], c, nullptr, 0, hl, wl), Lb.wt, Lb.wttc, nullptr, u->e[l][0], u->gz[l][1],
+                     c, 0, n,
                      st));
         const bf16 *src = l == 0 ? u->x : u->pool[l];
         const int cs = l == 0 ? kInPad : ch(u, l - 1);
         SDP_TRY(wgrad(u->gz[l][1], c, vin(src, cs, nullptr, 0, hl, wl), G + La.woff, G + La.boff, n, st));
         if (l == 0) break;
         // data gradient of the pooled input (cs channels at level l), into gz[l][0]
-        SDP_TRY(conv(La, vin(u->gz[l][1], c, nullptr, 0, hl, wl), La.wt, nullptr, nullptr, u->gz[l][0], cs, 0, n,
+        SDP_TRY(conv(u, vin(u->gz[l][1], c, nullptr, 0, hl, wl), La.wt, La.wttc, nullptr, nullptr, u->gz[l][0],
+                     cs, 0, n,
                      st));
         // dZ(e_{l-1}) = (pool backward + concatenation part) * relu'
         const int hu = h >> (l - 1), wu = w >> (l - 1);

@@ -796,6 +796,13 @@ class UNet:
     def backward(self, grad_out, stream=None):
         check(self.lib.sdp_unet_backward(self.handle, _dp(grad_out), _stream(stream)), self.lib)
 
+    def set_tensor_path(self, tcgen05: bool):
+        check(self.lib.sdp_unet_set_tensor_path(self.handle, _i(1 if tcgen05 else 0)), self.lib)
+
+    def check(self, stream=None):
+        """Raises when a tensor-core convolution gave up a bounded wait."""
+        check(self.lib.sdp_unet_check(self.handle, _stream(stream)), self.lib)
+
     def adam_step(self, lr, beta1=0.9, beta2=0.999, eps=1e-8, stream=None):
         check(self.lib.sdp_unet_adam_step(self.handle, C.c_float(lr), C.c_float(beta1), C.c_float(beta2),
                                           C.c_float(eps), _stream(stream)), self.lib)

@@ -12,8 +12,11 @@
 * Adam against a float32 restatement, over two steps;
 * a few optimiser steps on one batch lower the loss (the training path runs
   end to end).
-Sizes cover partial 8 x 16 tiles at every level (24 x 40: the deepest level
-is 3 x 5) and, at 3 x 256 x 256, the 64-channel tile variant.
+The convolutions run on the tcgen05 path (the default); the mma.sync path
+is compared with it.  Sizes cover partial tiles at every level (24 x 40:
+the deepest level is 3 x 5) and, at 3 x 256 x 256, several tiles per row,
+64-channel chunks and the two output-channel slices of the 384-channel data
+gradient.
 """
 from __future__ import annotations
 
@@ -50,6 +53,7 @@ def test_forward_matches_oracle(sdp, device, n, c, h, w):
     net, p, x, xd, rng = _setup(sdp, n, c, h, w, 11 + h)
     out = torch.empty((n, h, w), dtype=torch.float32, device="cuda")
     net.forward(xd, out)
+    net.check()
     ref = U.UNetRef(p, 32, c).forward(x).detach().numpy()
     assert rel_rms(out.cpu().numpy(), ref) <= 5e-3
     scale = np.array([2.5, 0.125][:n], np.float32)
@@ -80,6 +84,7 @@ def _grad_check(sdp, n, c, h, w, seed, margin):
     gout = rng.standard_normal((n, h, w)).astype(np.float32)
     net.zero_grads()
     net.backward(torch.from_numpy(gout).cuda())
+    net.check()
     g = net.get_grads()
     gr = ref_net.grads(ref_out, gout)
     errs = {}
@@ -172,4 +177,28 @@ def test_training_lowers_loss(sdp, device):
         net.adam_step(1e-3)
     assert np.isfinite(losses).all()
     assert losses[-1] < 0.3 * losses[0], losses[::10]
+    net.close()
+
+
+@pytest.mark.parametrize("n,c,h,w", [(2, 3, 24, 40), (1, 3, 128, 256)])
+def test_tensor_paths_agree(sdp, device, n, c, h, w):
+    """tcgen05 (tensor memory, TMA) and mma.sync convolutions: the same network
+    gives the same outputs and gradients up to BF16 rounding of
+    intermediate activations (different FP32 summation orders)."""
+    import torch
+    net, p, x, xd, rng = _setup(sdp, n, c, h, w, 51)
+    gout = torch.from_numpy(rng.standard_normal((n, h, w)).astype(np.float32)).cuda()
+    res = {}
+    for tc in (True, False):
+        net.set_tensor_path(tc)
+        out = torch.empty((n, h, w), dtype=torch.float32, device="cuda")
+        net.forward(xd, out)
+        net.zero_grads()
+        net.backward(gout)
+        net.check()
+        res[tc] = (out.cpu().numpy(), net.get_grads())
+    assert rel_rms(res[True][0], res[False][0]) <= 5e-3
+    cos = float(res[True][1].astype(np.float64) @ res[False][1] /
+                (np.linalg.norm(res[True][1]) * np.linalg.norm(res[False][1])))
+    assert cos >= 0.99
     net.close()
