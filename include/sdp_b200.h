@@ -331,6 +331,31 @@ int sdp_visplan_create(sdp_visplan **plan, const sdp_geometry *geom, const sdp_w
                        const sdp_wkernels *degrid_kernels, int num_vis, const sdp_float3 *uvw, int grid_mode,
                        void *stream);
 int sdp_visplan_destroy(sdp_visplan *plan);
+/* Plan shape (no counterpart in the reference): uv tile side (power of two,
+ * 8..128, default 32), visibilities per work item (64..65536, default 1024),
+ * lanes per visibility of the tile kernels (0: the fewest the support needs,
+ * or 8 / 16 / 32).  Zero fields take the defaults.  Results are the same for
+ * every shape up to the order of the floating-point sums. */
+typedef struct sdp_plan_options {
+    int tile;
+    int chunk;
+    int lanes;
+} sdp_plan_options;
+int sdp_visplan_create_opt(sdp_visplan **plan, const sdp_geometry *geom, const sdp_wkernels *grid_kernels,
+                           const sdp_wkernels *degrid_kernels, int num_vis, const sdp_float3 *uvw, int grid_mode,
+                           const sdp_plan_options *options, void *stream);
+int sdp_visplan_options(const sdp_visplan *plan, sdp_plan_options *options);
+/* Autotuner: builds a plan for each candidate shape (tiles 16 / 32 / 64,
+ * work items of 512 / 1024 / 2048 visibilities, lanes from the support or
+ * 16), times reps fused major-cycle passes (sdp_visplan_cycle on model_grid,
+ * residual_grid as scratch) with CUDA events on the stream, and returns the
+ * fastest shape, its time per pass (ms) and the number of shapes timed.
+ * Blocking; allocates and frees one plan at a time. */
+int sdp_visplan_autotune(const sdp_geometry *geom, const sdp_wkernels *grid_kernels,
+                         const sdp_wkernels *degrid_kernels, int num_vis, const sdp_float3 *uvw, int grid_mode,
+                         const sdp_float2 *measured, const sdp_float2 *model_grid, sdp_float2 *residual_grid,
+                         int degrid_mode, int reps, sdp_plan_options *best, float *best_ms, int *candidates,
+                         void *stream);
 int sdp_visplan_num_work_items(const sdp_visplan *plan, int *count); /* blocking read */
 /* Measured visibilities (original order) copied into plan order. */
 int sdp_visplan_set_measured(sdp_visplan *plan, const sdp_float2 *measured, void *stream);

@@ -29,6 +29,9 @@ struct sdp_visplan {
     int mode;
     int n;
     int ntx, nty, nk, nbins, ntiles, hs_max, W, S;
+    int tile = 32;                // uv tile side (grid cells)
+    int chunk = 1024;             // visibilities per work item (at most)
+    int lanes = 0;                // lanes per visibility of the tile kernels (0: from the support)
     void *rec = nullptr;          // Rec<float> or Rec<double>
     int coord_f64 = 0;            // index arithmetic of the double build
     int snap = 0;                 // correct_to_finegrid applied to the uvw at plan build

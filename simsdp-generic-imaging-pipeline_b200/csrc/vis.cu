@@ -32,8 +32,8 @@
 
 namespace sdp {
 
-constexpr int kTile = 32;
-constexpr int kChunk = 1024;
+constexpr int kTile = 32;    // default uv tile side
+constexpr int kChunk = 1024;  // default visibilities per work item
 constexpr int kMaxHalfSupport = 15;
 
 enum : int {
@@ -48,7 +48,7 @@ enum : int {
 enum : int { FLAG_PLANE = 1, FLAG_SUPPORT = 2, FLAG_BOX = 4 };
 
 struct PlanDev {
-    int G, gc, OS, nk_g, nk_d, ntx, nty, W, S;
+    int G, gc, OS, nk_g, nk_d, ntx, nty, W, S, tile;
     int phase_major, os_mask, os_shift;
     double uv_scale, w_scale;
     const float2 *gk;   // gridding kernels (phase-major copy when phase_major)
@@ -190,7 +190,8 @@ __device__ __forceinline__ int floor_div(int a, int b) { return (a >= 0) ? a / b
 template <typename T>
 __global__ void k_bin(const float3 *__restrict__ uvw, int n, int mode, int snap, int G, int OS, double uv_scale,
                       double w_scale, const int2 *__restrict__ sup, const int2 *__restrict__ dsup, int nk, int nkd,
-                      long long ntot_g, long long ntot_d, int hs_max, int ntx, int nty, Rec<T> *__restrict__ rec_tmp,
+                      long long ntot_g, long long ntot_d, int hs_max, int ntx, int nty, int tile,
+                      Rec<T> *__restrict__ rec_tmp,
                       int *__restrict__ keys, int *__restrict__ counts, int *__restrict__ flags)
 {
     int i = blockIdx.x * blockDim.x + threadIdx.x;
@@ -233,8 +234,8 @@ __global__ void k_bin(const float3 *__restrict__ uvw, int n, int mode, int snap,
         } else {
             int lox = (int)tceil(tsub(r.px, (T)hs)) + G / 2;
             int loy = (int)tceil(tsub(r.py, (T)hs)) + G / 2;
-            int tx = min(max(floor_div(lox, kTile), 0), ntx - 1);
-            int ty = min(max(floor_div(loy, kTile), 0), nty - 1);
+            int tx = min(max(floor_div(lox, tile), 0), ntx - 1);
+            int ty = min(max(floor_div(loy, tile), 0), nty - 1);
             key = (ty * ntx + tx) * nk + plane;
             atomicAdd(&counts[key], 1);
         }
@@ -257,22 +258,23 @@ __global__ void k_scatter(const Rec<T> *__restrict__ rec_tmp, const int *__restr
     perm[pos] = i;
 }
 
-__global__ void k_item_counts(const int *__restrict__ offsets, int ntiles, int nk, int *__restrict__ item_counts)
+__global__ void k_item_counts(const int *__restrict__ offsets, int ntiles, int nk, int chunk,
+                              int *__restrict__ item_counts)
 {
     int t = blockIdx.x * blockDim.x + threadIdx.x;
     if (t >= ntiles) return;
     int b = offsets[t * nk], e = offsets[(t + 1) * nk];
-    item_counts[t] = (e - b + kChunk - 1) / kChunk;
+    item_counts[t] = (e - b + chunk - 1) / chunk;
 }
 
 __global__ void k_item_fill(const int *__restrict__ offsets, const int *__restrict__ item_offsets, int ntiles,
-                            int nk, int4 *__restrict__ items)
+                            int nk, int chunk, int4 *__restrict__ items)
 {
     int t = blockIdx.x * blockDim.x + threadIdx.x;
     if (t >= ntiles) return;
     int b = offsets[t * nk], e = offsets[(t + 1) * nk];
     int o = item_offsets[t];
-    for (int s = b; s < e; s += kChunk) items[o++] = make_int4(t, s, min(e, s + kChunk), 0);
+    for (int s = b; s < e; s += chunk) items[o++] = make_int4(t, s, min(e, s + chunk), 0);
 }
 
 // ----------------------------------------------------------------------------
@@ -353,8 +355,8 @@ __device__ __forceinline__ void tile_item(const PlanDev &P, const int4 it, float
     const T fos = (T)P.OS;
     const Rec<T> *__restrict__ recs = static_cast<const Rec<T> *>(P.rec);
     float2 ksr[kShareable ? LG : 1];
-    const int ox = (it.x % P.ntx) * kTile;  // tile origin in grid cells
-    const int oy = (it.x / P.ntx) * kTile;
+    const int ox = (it.x % P.ntx) * P.tile;  // tile origin in grid cells
+    const int oy = (it.x / P.ntx) * P.tile;
     if (kGrids)
         for (int k = threadIdx.x; k < 2 * SS; k += kThreads) sub_re[k] = 0.f;
     if (kStageIn)
@@ -409,8 +411,8 @@ __device__ __forceinline__ void tile_item(const PlanDev &P, const int4 it, float
             if (kConv) colp_d = pl.y + kc;
             if (kGrids) colp_g = pl.w + kc;
             lx = tx0 + cl;
-            // row cl of the box: kernel-row offset and tile row, packed
-            rowpack = (krow(P, A, ref_kidx((int)loy + cl, rec.py, fos)) << 6) | (ty0 + cl);
+            // row cl of the box: kernel-row offset and tile row (8 bits: S <= 256), packed
+            rowpack = (krow(P, A, ref_kidx((int)loy + cl, rec.py, fos)) << 8) | (ty0 + cl);
         }
 
         // ---------------- degrid (prediction) ----------------
@@ -425,9 +427,9 @@ __device__ __forceinline__ void tile_item(const PlanDev &P, const int4 it, float
                 for (int rr = 0; rr < LG; ++rr) {
                     const int pk = __shfl_sync(fmask, rowpack, grp * LG + rr);
                     if (rr < nrows && colok) {
-                        const float2 ks = __ldg(&P.dk[colp_d + (pk >> 6)]);
+                        const float2 ks = __ldg(&P.dk[colp_d + (pk >> 8)]);
                         if constexpr (kShareable) ksr[rr] = ks;
-                        const float2 gv = mtile[(pk & 63) * S + lx];
+                        const float2 gv = mtile[(pk & 255) * S + lx];
                         a1.x = fmaf(gv.x, ks.x, a1.x);
                         a1.y = fmaf(gv.y, ks.x, a1.y);
                         a2.x = fmaf(gv.x, ks.y, a2.x);
@@ -535,11 +537,11 @@ __device__ __forceinline__ void tile_item(const PlanDev &P, const int4 it, float
                         float2 ks;
                         if constexpr (kShareable) {
                             ks = share ? make_float2(ksr[rr].x, share_sign * ksr[rr].y)
-                                       : __ldg(&P.gk[colp_g + (pk >> 6)]);
+                                       : __ldg(&P.gk[colp_g + (pk >> 8)]);
                         } else {
-                            ks = __ldg(&P.gk[colp_g + (pk >> 6)]);
+                            ks = __ldg(&P.gk[colp_g + (pk >> 8)]);
                         }
-                        const int cell = (pk & 63) * S + lx;
+                        const int cell = (pk & 255) * S + lx;
                         atomicAdd(sub_re + cell, fmaf(-ca, ks.y, gval.x * ks.x));
                         atomicAdd(sub_im + cell, fmaf(cb, ks.y, gval.y * ks.x));
                     }
@@ -790,6 +792,7 @@ static PlanDev plan_dev(const sdp_visplan *p)
     d.nk_g = p->gk.num_kernels;
     d.nk_d = p->dk.num_kernels;
     d.ntx = p->ntx;
+    d.tile = p->tile;
     d.nty = p->nty;
     d.W = p->W;
     d.S = p->S;
@@ -848,7 +851,7 @@ static void plan_layout(const sdp_visplan *p, size_t *off, size_t *total)
     off[5] = o; o = align_up(o + sizeof(int) * ((size_t)p->nbins + 1), 256);              // offsets
     off[6] = o; o = align_up(o + sizeof(int) * ((size_t)p->ntiles + 1), 256);             // item counts
     off[7] = o; o = align_up(o + sizeof(int) * ((size_t)p->ntiles + 1), 256);             // item offsets
-    off[8] = o; o = align_up(o + sizeof(int4) * ((size_t)n / kChunk + p->ntiles + 1), 256);// items
+    off[8] = o; o = align_up(o + sizeof(int4) * ((size_t)n / p->chunk + p->ntiles + 1), 256);// items
     off[9] = o; o = align_up(o + sizeof(int) * nb_scan, 256);                             // scan scratch
     off[10] = o; o = align_up(o + sizeof(int) * 4, 256);                                  // scalars
     off[11] = o; o = align_up(o + sizeof(float2) * (size_t)std::max(n, 1), 256);          // measured
@@ -885,14 +888,14 @@ int visplan_setup(sdp_visplan *p, const sdp_geometry *geom, const sdp_wkernels *
     p->mode = mode;
     p->n = n;
     const int G = geom->grid_size;
-    p->ntx = (G + kTile - 1) / kTile;
+    p->ntx = (G + p->tile - 1) / p->tile;
     p->nty = p->ntx;
     p->ntiles = p->ntx * p->nty;
     p->nk = gk->num_kernels;
     p->nbins = p->ntiles * p->nk;
     p->hs_max = std::max(gk->max_half_support, dk->max_half_support);
     p->W = 2 * p->hs_max + 1;
-    p->S = kTile + 2 * p->hs_max;
+    p->S = p->tile + 2 * p->hs_max;
     const int os = geom->oversampling;
     p->phase_major = (os & (os - 1)) == 0 ? 1 : 0;
     return SDP_OK;
@@ -985,13 +988,13 @@ int visplan_build(sdp_visplan *p, void *arena, const float3 *uvw, cudaStream_t s
             k_bin<double><<<(n + 255) / 256, 256, 0, st>>>(
                 uvw, n, p->mode, p->snap, p->geom.grid_size, p->geom.oversampling, p->geom.uv_scale, p->geom.w_scale,
                 gs, ds, p->gk.num_kernels, p->dk.num_kernels, (long long)p->gk.total_samples,
-                (long long)p->dk.total_samples, p->hs_max, p->ntx, p->nty, static_cast<Rec<double> *>(rec_tmp), keys,
+                (long long)p->dk.total_samples, p->hs_max, p->ntx, p->nty, p->tile, static_cast<Rec<double> *>(rec_tmp), keys,
                 counts, p->flags);
         } else {
             k_bin<float><<<(n + 255) / 256, 256, 0, st>>>(
                 uvw, n, p->mode, p->snap, p->geom.grid_size, p->geom.oversampling, p->geom.uv_scale, p->geom.w_scale,
                 gs, ds, p->gk.num_kernels, p->dk.num_kernels, (long long)p->gk.total_samples,
-                (long long)p->dk.total_samples, p->hs_max, p->ntx, p->nty, static_cast<Rec<float> *>(rec_tmp), keys,
+                (long long)p->dk.total_samples, p->hs_max, p->ntx, p->nty, p->tile, static_cast<Rec<float> *>(rec_tmp), keys,
                 counts, p->flags);
         }
         SDP_LAUNCH_CHECK();
@@ -1010,10 +1013,11 @@ int visplan_build(sdp_visplan *p, void *arena, const float3 *uvw, cudaStream_t s
                                                               p->perm);
         SDP_LAUNCH_CHECK();
     }
-    k_item_counts<<<(p->ntiles + 255) / 256, 256, 0, st>>>(offsets, p->ntiles, p->nk, item_counts);
+    k_item_counts<<<(p->ntiles + 255) / 256, 256, 0, st>>>(offsets, p->ntiles, p->nk, p->chunk, item_counts);
     SDP_LAUNCH_CHECK();
     SDP_TRY(exclusive_scan(item_counts, item_offsets, p->ntiles, scan_scratch, st));
-    k_item_fill<<<(p->ntiles + 255) / 256, 256, 0, st>>>(offsets, item_offsets, p->ntiles, p->nk, p->items);
+    k_item_fill<<<(p->ntiles + 255) / 256, 256, 0, st>>>(offsets, item_offsets, p->ntiles, p->nk, p->chunk,
+                                                          p->items);
     SDP_LAUNCH_CHECK();
     SDP_CUDA_TRY(cudaMemcpyAsync(p->n_items, item_offsets + p->ntiles, sizeof(int), cudaMemcpyDeviceToDevice, st));
     return SDP_OK;
@@ -1065,6 +1069,125 @@ SDP_EXPORT int sdp_visplan_create(sdp_visplan **out, const sdp_geometry *geom, c
         return status;
     }
     *out = p;
+    return SDP_OK;
+}
+
+SDP_EXPORT int sdp_visplan_create_opt(sdp_visplan **out, const sdp_geometry *geom, const sdp_wkernels *gk,
+                                      const sdp_wkernels *dk, int num_vis, const sdp_float3 *uvw, int grid_mode,
+                                      const sdp_plan_options *opt, void *stream)
+{
+    SDP_CHECK_ARG(out != nullptr, "plan output pointer is NULL");
+    *out = nullptr;
+    SDP_CHECK_ARG(num_vis == 0 || uvw != nullptr, "uvw is NULL");
+    const int tile = (opt && opt->tile) ? opt->tile : kTile;
+    const int chunk = (opt && opt->chunk) ? opt->chunk : kChunk;
+    const int lanes = opt ? opt->lanes : 0;
+    SDP_CHECK_ARG(tile >= 8 && tile <= 128 && (tile & (tile - 1)) == 0, "tile %d: a power of two in 8..128", tile);
+    SDP_CHECK_ARG(chunk >= 64 && chunk <= (1 << 16), "chunk %d: 64..65536 visibilities", chunk);
+    SDP_CHECK_ARG(lanes == 0 || lanes == 8 || lanes == 16 || lanes == 32, "lanes %d: 0, 8, 16 or 32", lanes);
+    sdp_visplan *p = new sdp_visplan();
+    p->tile = tile;
+    p->chunk = chunk;
+    p->lanes = lanes;
+    int status = visplan_setup(p, geom, gk, dk, num_vis, grid_mode);
+    if (status == SDP_OK && lanes != 0 && 2 * p->hs_max > lanes)
+        status = set_error(SDP_ERR_INVALID, "lanes %d below the %d tap columns of the support", lanes,
+                           2 * p->hs_max);
+    if (status != SDP_OK) {
+        delete p;
+        return status;
+    }
+    void *arena = nullptr;
+    cudaError_t e = cudaMalloc(&arena, visplan_arena_bytes(p));
+    if (e != cudaSuccess) {
+        delete p;
+        return cuda_error(e, "cudaMalloc(visibility plan)");
+    }
+    p->owns_arena = true;
+    status = visplan_build(p, arena, reinterpret_cast<const float3 *>(uvw), as_stream(stream));
+    if (status != SDP_OK) {
+        cudaFree(arena);
+        delete p;
+        return status;
+    }
+    *out = p;
+    return SDP_OK;
+}
+
+SDP_EXPORT int sdp_visplan_options(const sdp_visplan *p, sdp_plan_options *opt)
+{
+    SDP_CHECK_ARG(p && opt, "NULL argument");
+    opt->tile = p->tile;
+    opt->chunk = p->chunk;
+    opt->lanes = p->lanes;
+    return SDP_OK;
+}
+
+SDP_EXPORT int sdp_visplan_autotune(const sdp_geometry *geom, const sdp_wkernels *gk, const sdp_wkernels *dk,
+                                    int num_vis, const sdp_float3 *uvw, int grid_mode, const sdp_float2 *measured,
+                                    const sdp_float2 *model_grid, sdp_float2 *residual_grid, int degrid_mode,
+                                    int reps, sdp_plan_options *best, float *best_ms, int *candidates,
+                                    void *stream)
+{
+    SDP_CHECK_ARG(best && best_ms && measured && model_grid && residual_grid, "NULL argument");
+    SDP_CHECK_ARG(reps >= 1 && reps <= 100, "reps %d: 1..100", reps);
+    cudaStream_t st = as_stream(stream);
+    static const int tiles[] = {16, 32, 64};
+    static const int chunks[] = {512, 1024, 2048};
+    static const int lanes_c[] = {0, 16};
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    SDP_CUDA_TRY(cudaEventCreate(&e0));
+    cudaError_t ce = cudaEventCreate(&e1);
+    if (ce != cudaSuccess) {
+        cudaEventDestroy(e0);
+        return cuda_error(ce, "cudaEventCreate");
+    }
+    float best_t = 0.f;
+    int tried = 0;
+    bool have = false;
+    int status = SDP_OK;
+    for (int ti : tiles)
+        for (int ch : chunks)
+            for (int ln : lanes_c) {
+                if (status != SDP_OK) break;
+                sdp_plan_options o{ti, ch, ln};
+                sdp_visplan *p = nullptr;
+                // candidates the device cannot hold (shared memory, lanes) are skipped
+                if (sdp_visplan_create_opt(&p, geom, gk, dk, num_vis, uvw, grid_mode, &o, stream) != SDP_OK) continue;
+                int s = sdp_visplan_set_measured(p, measured, stream);
+                if (s == SDP_OK)
+                    s = sdp_visplan_cycle(p, model_grid, degrid_mode, nullptr, nullptr, residual_grid, stream);  // warm
+                float ms = 0.f;
+                if (s == SDP_OK) {
+                    cudaEventRecord(e0, st);
+                    for (int r = 0; r < reps && s == SDP_OK; ++r)
+                        s = sdp_visplan_cycle(p, model_grid, degrid_mode, nullptr, nullptr, residual_grid, stream);
+                    cudaEventRecord(e1, st);
+                    if (cudaEventSynchronize(e1) != cudaSuccess || cudaEventElapsedTime(&ms, e0, e1) != cudaSuccess)
+                        s = SDP_ERR_CUDA;
+                }
+                if (s == SDP_OK) s = visplan_check_flags(p, st);
+                sdp_visplan_destroy(p);
+                if (s == SDP_ERR_RANGE) continue;  // the tile kernel does not fit this configuration
+                if (s != SDP_OK) {
+                    status = s;  // a failing pass is an error, not a slow candidate
+                    break;
+                }
+                ms /= (float)reps;
+                ++tried;
+                if (!have || ms < best_t) {
+                    have = true;
+                    best_t = ms;
+                    *best = o;
+                }
+            }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    if (status != SDP_OK) return status;
+    if (!have) return set_error(SDP_ERR_RANGE, "no plan configuration fits this device");
+    sdp_clear_error();
+    *best_ms = best_t;
+    if (candidates) *candidates = tried;
     return SDP_OK;
 }
 
@@ -1133,7 +1256,16 @@ static int launch_tiles_lg(sdp_visplan *p, int op, const float2 *vis_in, const f
 static int launch_tiles(sdp_visplan *p, int op, const float2 *vis_in, const float2 *in_grid, float2 *out_grid,
                         float2 *pred, float2 *delta, cudaStream_t st)
 {
-    // lanes per visibility: the tap columns (2 hs + 1 at most) in at most two passes
+    // lanes per visibility: the tap columns (2 hs + 1 at most) in at most two
+    // passes; a plan may ask for more lanes than its support needs
+    if (p->lanes == 16 && 2 * p->hs_max <= 16) {
+        if (p->coord_f64) return launch_tiles_lg<double, 16>(p, op, vis_in, in_grid, out_grid, pred, delta, st);
+        return launch_tiles_lg<float, 16>(p, op, vis_in, in_grid, out_grid, pred, delta, st);
+    }
+    if (p->lanes == 32) {
+        if (p->coord_f64) return launch_tiles_lg<double, 32>(p, op, vis_in, in_grid, out_grid, pred, delta, st);
+        return launch_tiles_lg<float, 32>(p, op, vis_in, in_grid, out_grid, pred, delta, st);
+    }
     if (p->coord_f64) {
         if (2 * p->hs_max <= 8) return launch_tiles_lg<double, 8>(p, op, vis_in, in_grid, out_grid, pred, delta, st);
         if (2 * p->hs_max <= 16) return launch_tiles_lg<double, 16>(p, op, vis_in, in_grid, out_grid, pred, delta, st);

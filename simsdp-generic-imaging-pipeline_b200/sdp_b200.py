@@ -400,11 +400,17 @@ def _stream(s=None):
     return _p(s.cuda_stream)
 
 
+class PlanOptions(C.Structure):
+    """Plan shape: uv tile side, visibilities per work item, lanes per
+    visibility (0 = default)."""
+    _fields_ = [("tile", _i), ("chunk", _i), ("lanes", _i)]
+
+
 class VisPlan:
     """Owns an sdp_visplan (visibilities binned by uv tile and w-plane)."""
 
     def __init__(self, lib, geom: Geometry, gk: WKernels, dk: WKernels | None, uvw, mode: int, stream=None,
-                 keep=()):
+                 keep=(), options: PlanOptions | None = None):
         self.lib = lib
         self.geom = geom
         self._keep = keep  # tensors the plan points at
@@ -412,8 +418,18 @@ class VisPlan:
         self.dk = dk or gk
         self.n = int(uvw.shape[0])
         self.handle = _p()
-        check(lib.sdp_visplan_create(C.byref(self.handle), C.byref(geom), C.byref(self.gk), C.byref(self.dk),
-                                     _i(self.n), _dp(uvw), _i(mode), _stream(stream)), lib)
+        if options is None:
+            check(lib.sdp_visplan_create(C.byref(self.handle), C.byref(geom), C.byref(self.gk), C.byref(self.dk),
+                                         _i(self.n), _dp(uvw), _i(mode), _stream(stream)), lib)
+        else:
+            check(lib.sdp_visplan_create_opt(C.byref(self.handle), C.byref(geom), C.byref(self.gk),
+                                             C.byref(self.dk), _i(self.n), _dp(uvw), _i(mode), C.byref(options),
+                                             _stream(stream)), lib)
+
+    def options(self) -> PlanOptions:
+        o = PlanOptions()
+        check(self.lib.sdp_visplan_options(self.handle, C.byref(o)), self.lib)
+        return o
 
     def close(self):
         if self.handle:
@@ -575,9 +591,25 @@ class Device:
                         int(sh[:, 0].max()))
 
     def plan(self, grid_size, oversampling, uv_scale, w_scale, uvw, gk: WKernels, dk: WKernels | None = None,
-             mode=SDP_GRID_STD, stream=None, keep=()) -> VisPlan:
+             mode=SDP_GRID_STD, stream=None, keep=(), options: PlanOptions | None = None) -> VisPlan:
         geom = Geometry(grid_size, oversampling, uv_scale, w_scale)
-        return VisPlan(self.lib, geom, gk, dk, uvw, mode, stream, keep)
+        return VisPlan(self.lib, geom, gk, dk, uvw, mode, stream, keep, options)
+
+    def autotune(self, grid_size, oversampling, uv_scale, w_scale, uvw, gk: WKernels, dk: WKernels | None,
+                 measured, model_grid, residual_grid, degrid_mode=SDP_DEGRID_CONV, reps=3, mode=SDP_GRID_STD,
+                 stream=None):
+        """Fastest plan shape for this visibility set (sdp_visplan_autotune):
+        (PlanOptions, ms per fused pass, shapes timed)."""
+        geom = Geometry(grid_size, oversampling, uv_scale, w_scale)
+        best = PlanOptions()
+        ms = C.c_float(0)
+        cand = _i(0)
+        dk = dk or gk
+        check(self.lib.sdp_visplan_autotune(C.byref(geom), C.byref(gk), C.byref(dk), _i(uvw.shape[0]), _dp(uvw),
+                                            _i(mode), _dp(measured), _dp(model_grid), _dp(residual_grid),
+                                            _i(degrid_mode), _i(reps), C.byref(best), C.byref(ms), C.byref(cand),
+                                            _stream(stream)), self.lib)
+        return best, float(ms.value), cand.value
 
     def batch(self, plans, stream=None) -> VisBatch:
         return VisBatch(self.lib, plans, stream)
