@@ -480,6 +480,9 @@ def c4_learned_block(S, D, dev, skies: int):
     x = torch.randn((1, L.IN_CHANNELS, 1024, 1024), device=dev)
     out = torch.empty((1, 1024, 1024), device=dev)
     t_fwd = ev(lambda: net.forward(x, out))
+    net.check()
+    net.set_tensor_path(False)
+    t_fwd_legacy = ev(lambda: net.forward(x, out))
     net.close()
     tn = S.UNet(D.lib, L.IN_CHANNELS, 16, 256, 256, training=True)
     tn.set_params(params)
@@ -494,6 +497,7 @@ def c4_learned_block(S, D, dev, skies: int):
         tn.adam_step(0.0)
 
     t_train = ev(step)
+    tn.check()
     tn.close()
     f_fwd = unet_flops(1, 1024, 1024)
     f_train = f_fwd + unet_flops(16, 256, 256, backward=True)
@@ -519,7 +523,8 @@ def c4_learned_block(S, D, dev, skies: int):
         "unet_forward_ms_1024": t_fwd, "unet_forward_tflops": f_fwd / (t_fwd * 1e-3) / 1e12,
         "unet_train_step_ms_16x256": t_train, "unet_train_tflops": f_train / (t_train * 1e-3) / 1e12,
         "unet_frac_of_bf16_peak": f_fwd / (t_fwd * 1e-3) / 1e12 / bf16,
-        "tensor_path": "mma.sync m16n8k16 BF16 -> FP32 (ldmatrix, cp.async)",
+        "tensor_path": "tcgen05.mma (TMEM accumulators, TMA loads, warp-specialised)",
+        "unet_forward_ms_1024_mma_sync": t_fwd_legacy,
     }
 
 
@@ -570,7 +575,15 @@ def b200_arm(args):
     model_grid = torch.empty((G * G, 2), dtype=torch.float32, device=dev)
     D.image_to_grid(G, model_img, work, model_grid)
     residual = torch.empty((G * G, 2), dtype=torch.float32, device=dev)
-    plan = D.plan(G, OS, w.cfg.uv_scale, w.cfg.w_scale, uvw, wk_g, wk_d, keep=(uvw, gk, dk, sup))
+    # plan shape from the autotuner (tile side, visibilities per work item,
+    # lanes per visibility), timed on this workload's own fused pass
+    t_tune = time.perf_counter()
+    shape, tuned_ms, n_shapes = D.autotune(G, OS, w.cfg.uv_scale, w.cfg.w_scale, uvw, wk_g, wk_d, measured,
+                                          model_grid, residual, reps=5)
+    tune = {"tile": shape.tile, "chunk": shape.chunk, "lanes": shape.lanes or "from support",
+            "ms_per_pass": tuned_ms, "shapes_timed": n_shapes, "seconds": time.perf_counter() - t_tune,
+            "default": {"tile": 32, "chunk": 1024}}
+    plan = D.plan(G, OS, w.cfg.uv_scale, w.cfg.w_scale, uvw, wk_g, wk_d, keep=(uvw, gk, dk, sup), options=shape)
     plan.set_measured(measured)
     plan.check_flags()
     n_items = plan.num_work_items()
@@ -755,7 +768,8 @@ def b200_arm(args):
         "config": {"workload": f"{w.name}: 256 antennas, 10 km log spiral, 120 time steps, {N} vis per channel, "
                                f"G=2048, 17 w-planes hs=4 OS=16, one channel per GPU",
                    "degrid": "convolutional (normalised, degridgrid.c:147-191)",
-                   "l2": "flushed between timed steps (256 MB write)", "work_items": n_items},
+                   "l2": "flushed between timed steps (256 MB write)", "work_items": n_items,
+                   "plan_shape": tune},
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                      "frac": achieved / peak, "traffic": traffic, "peak_source": peak_src,
                      "kernel": "k_tiles<STD, OP_CYCLE_CONV>",
