@@ -537,12 +537,15 @@ def evaluate(img: Imaging, params: np.ndarray, skies: int, seed: int = 777, plai
 
 
 def main(argv=None) -> int:
-    """python learned.py train|eval [--skies N] [--out PATH] [--grid G]"""
+    """python learned.py train|eval|forward [--skies N] [--out PATH] [--grid G]
+
+    forward: two forward passes of the committed network on a random
+    3 x G x G input (the second timed with CUDA events)."""
     import argparse
     import json
     torch = _torch()
     ap = argparse.ArgumentParser()
-    ap.add_argument("cmd", choices=["train", "eval"])
+    ap.add_argument("cmd", choices=["train", "eval", "forward"])
     ap.add_argument("--skies", type=int, default=20000)
     ap.add_argument("--grid", type=int, default=1024)
     ap.add_argument("--out", type=Path, default=WEIGHTS)
@@ -552,6 +555,21 @@ def main(argv=None) -> int:
     a = ap.parse_args(argv)
     torch.cuda.init()
     D = S.Device()
+    if a.cmd == "forward":
+        net = S.UNet(D.lib, IN_CHANNELS, 1, a.grid, a.grid, training=False)
+        net.set_params(load_weights(a.weights))
+        x = torch.randn((1, IN_CHANNELS, a.grid, a.grid), device="cuda")
+        out = torch.empty((1, a.grid, a.grid), device="cuda")
+        net.forward(x, out)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        net.forward(x, out)
+        e1.record()
+        torch.cuda.synchronize()
+        net.check()
+        print(f"forward {a.grid}^2: {e0.elapsed_time(e1):.3f} ms")
+        net.close()
+        return 0
     img = Imaging(D, spiral_layout(a.grid))
     if a.cmd == "train":
         params, log = train(img, TrainConfig(skies=a.skies))
