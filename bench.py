@@ -445,6 +445,41 @@ def unet_flops(n: int, h: int, w: int, base: int = 32, backward: bool = False) -
     return dgrad + (fwd - 2 * base * n * h * w) + 4 * base * n * h * w
 
 
+def fft_block(S, D, dev, G: int = 2048, reps: int = 20):
+    """The 2-D FFT of a G x G complex grid (seeded normal values): the FP32
+    Stockham transform and the tensor-core transform (BF16 split hi/lo,
+    FP32 accumulation), time per transform (CUDA events, median) and error
+    against numpy's complex128 FFT."""
+    import torch
+    rng = np.random.default_rng(11)
+    x = rng.standard_normal((G * G, 2)).astype(np.float32)
+    xd = torch.from_numpy(x).to(dev)
+    out, work = torch.empty_like(xd), torch.empty_like(xd)
+
+    def ev(fn):
+        fn()
+        torch.cuda.synchronize()
+        ts = []
+        for _ in range(reps):
+            a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            a.record()
+            fn()
+            b.record()
+            torch.cuda.synchronize()
+            ts.append(a.elapsed_time(b))
+        return statistics.median(ts)
+
+    ref = np.fft.fft2((x[:, 0] + 1j * x[:, 1]).astype(np.complex128).reshape(G, G)).reshape(-1)
+    res = {"grid": G}
+    for name, fn in (("fp32", lambda: D.fft2d(G, xd, out, -1)), ("tensor_bf16x3", lambda: D.fft2d_tc(G, xd, out, -1,
+                                                                                                      work))):
+        t = ev(fn)
+        o = out.cpu().numpy().astype(np.float64)
+        err = float(np.linalg.norm((o[:, 0] + 1j * o[:, 1]) - ref) / np.linalg.norm(ref))
+        res[name] = {"ms": t, "rel_rms_vs_fp64": err}
+    return res
+
+
 def c4_learned_block(S, D, dev, skies: int):
     """Learned CLEAN proposals against plain Hogbom on held-out skies: one
     channel of the 256-antenna spiral layout (3,916,800 visibilities) imaged
@@ -703,6 +738,7 @@ def b200_arm(args):
     c4 = None
     if world == 1 and not args.no_c4:
         c4 = c4_learned_block(S, D, dev, args.c4_skies)
+    fftc = fft_block(S, D, dev) if world == 1 and not args.no_c4 else None
 
     # ---- e2e through the reference-facing C ABI with pinned host buffers ---------------
     uvw_h = torch.empty((N, 3), dtype=torch.float32).pin_memory()
@@ -789,6 +825,8 @@ def b200_arm(args):
         line["c5_channel_8192"] = c5
     if c4 is not None:
         line["c4_learned"] = c4
+    if fftc is not None:
+        line["fft_2048"] = fftc
     if cpu is not None:
         line["cpu_baseline"] = cpu
     plan.close()

@@ -632,6 +632,11 @@ class Device:
     def fft2d(self, grid_size, x, out, sign, stream=None):
         check(self.lib.sdp_fft2d(_i(grid_size), _dp(x), _dp(out), _i(sign), _stream(stream)), self.lib)
 
+    def fft2d_tc(self, grid_size, x, out, sign, work, stream=None):
+        """Tensor-core (BF16 split hi/lo) 2-D FFT, G = 1024 / 2048 / 4096."""
+        check(self.lib.sdp_fft2d_tc(_i(grid_size), _dp(x), _dp(out), _i(sign), _dp(work), _stream(stream)),
+              self.lib)
+
     def grid_to_image(self, grid_size, grid, prolate_ext, work, image, stream=None):
         check(self.lib.sdp_grid_to_image(_i(grid_size), _dp(grid), _dp(prolate_ext), _dp(work), _dp(image),
                                          _stream(stream)), self.lib)
