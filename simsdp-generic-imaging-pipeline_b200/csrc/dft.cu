@@ -189,10 +189,14 @@ __global__ void __launch_bounds__(kDftThreads) k_dft_pixels(int n, int ns, const
         }
         __syncthreads();
         if (i < n) {
+            // |W| 2^44 below 2^32 (|W| < 2^-12, the usual case): one 32 x 32 -> 64-bit product
+            const bool w32 = (wfx >> 32) == 0ull;
+            const unsigned wlo = (unsigned)wfx;
             for (int k = 0; k < cnt; ++k) {
                 const PixTerm t = tile[k];
                 // w term: frac(W R2) in units of 2^-32 cycles
-                const unsigned long long wp = wfx * (unsigned long long)t.r2;
+                const unsigned long long wp =
+                    w32 ? (unsigned long long)wlo * (unsigned long long)t.r2 : wfx * (unsigned long long)t.r2;
                 unsigned wq = (unsigned)(wp >> 12);
                 if (wneg) wq = 0u - wq;
                 // phase U X + V Y - W R2 modulo 1, as a 32-bit fraction

@@ -269,18 +269,19 @@ __global__ void __launch_bounds__(128) k_conv3x3(ConvArgs p)
 // persistent warp-specialised kernel.  Tile = R consecutive image rows
 // (R = 1, 2, 4 or 8; each a 128-pixel segment, M = 128 per row) x nt output
 // channels (nt <= 256, a multiple of 32), R accumulators in tensor memory.
-// K = 9 taps x Cin, walked as (chunk of KC = 32 or 64 channels, tap) pairs;
-// one pair = one pipeline stage:
-//   A: the R x 128 input pixels the tap reads (rows y0 + dy - 1 .., columns
-//      x0 + dx - 1 ..), KC channels each, by one 4-D TMA box {KC, 128, R, 1}
-//      (reads outside the image return zero);
-//   B: the pair's nt x KC weights, pre-arranged in global memory as the
-//      shared-memory image, by one bulk copy;
+// K = 9 taps x Cin, walked as (chunk of KC = 32 or 64 channels, column tap
+// dx) pairs; one pair = one pipeline stage:
+//   A: the (R + 2) x 128 input pixels the three row taps of dx read (rows
+//      y0 - 1 .. y0 + R, columns x0 + dx - 1 ..), KC channels each, by one
+//      4-D TMA box {KC, 128, R + 2, 1} (reads outside the image return zero);
+//      row tap dy of output row r is box row r + dy;
+//   B: the pair's 3 x nt x KC weights (dy = 0, 1, 2), pre-arranged in global
+//      memory as the shared-memory image, by one bulk copy;
 // both in the K-major canonical layout with the 128-byte (KC = 64) or
 // 64-byte (KC = 32) swizzle, which the TMA writes and the MMA reads (rows of
 // KC channels; 8-row atoms of 1024 / 512 bytes; K advanced 16 channels = 32
-// bytes inside the row).  A stage is R x KC / 16 tcgen05.mma (M128 x nt x
-// K16, BF16 -> FP32 in tensor memory); each row's A starts on an atom.
+// bytes inside the row).  A stage is 3 x R x KC / 16 tcgen05.mma (M128 x nt
+// x K16, BF16 -> FP32 in tensor memory); each row's A starts on an atom.
 //   warp 0 (one thread): loads, through an S-stage ring (full/empty
 //     mbarriers, transaction counts);
 //   warp 1 (one thread): MMAs; commits free a stage (empty) and, after a
@@ -297,9 +298,10 @@ constexpr int kTcMaxStages = 16;
 constexpr int kTcSmemBudget = 200 * 1024;       // stages; +1 KB for the 1024-byte alignment
 constexpr long long kTcSpins = 1LL << 20;       // bounded mbarrier polls
 
-inline int tc_kc(int cin) { return cin % 64 == 0 ? 64 : 32; }
-__host__ __device__ constexpr int tc_a_bytes(int kc, int rows) { return rows * kTcM * kc * 2; }
-__host__ __device__ constexpr int tc_b_bytes(int nt, int kc) { return nt * kc * 2; }
+inline int tc_kc(int) { return 32; }  // 32-channel chunks (64-byte swizzle) for every layer
+__host__ __device__ constexpr int tc_row_bytes(int kc) { return kTcM * kc * 2; }
+__host__ __device__ constexpr int tc_a_bytes(int kc, int rows) { return (rows + 2) * tc_row_bytes(kc); }
+__host__ __device__ constexpr int tc_b_bytes(int nt, int kc) { return 3 * nt * kc * 2; }
 __host__ __device__ constexpr int tc_stage_bytes(int nt, int kc, int rows)
 {
     return (tc_a_bytes(kc, rows) + tc_b_bytes(nt, kc) + 1023) & ~1023;
@@ -376,15 +378,17 @@ __global__ void __launch_bounds__(192, 1) k_conv3x3_tc(const __grid_constant__ C
     __shared__ __align__(8) uint64_t s_full[kTcMaxStages], s_empty[kTcMaxStages], s_tfull[2], s_tempty[2];
     __shared__ uint32_t s_tmem;
     __shared__ int s_fail;
+    __shared__ float s_bias[256];
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
     const int nt = p.nt, S = p.stages, kc = p.kc, R = p.rows;
+    for (int i = tid; i < nt; i += blockDim.x) s_bias[i] = p.bias ? p.bias[blockIdx.y * nt + i] : 0.f;
     const int slice = blockIdx.y;
     const uint32_t ncols = tc_ncols(nt);
     const uint32_t acc_cols = (uint32_t)R * ncols;  // one accumulator set (R rows)
     const int stage_bytes = tc_stage_bytes(nt, kc, R);
     // stages start on 1024-byte boundaries (the swizzle atoms)
     const uint32_t sbase = (smem_u32(smem) + 1023u) & ~1023u;
-    const int per_tile = 9 * p.nchunks;
+    const int per_tile = 3 * p.nchunks;
 
     if (warp == 0) {
         asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(&s_tmem)),
@@ -419,8 +423,7 @@ __global__ void __launch_bounds__(192, 1) k_conv3x3_tc(const __grid_constant__ C
                 const int tx = t % p.tiles_x, trow = t / p.tiles_x;
                 const int img = trow / p.tiles_y, y = (trow - img * p.tiles_y) * R;
                 for (int k = 0; k < per_tile; ++k, ++g) {
-                    const int chunk = k / 9, tap = k - 9 * chunk;
-                    const int dy = tap / 3, dx = tap - 3 * dy;
+                    const int chunk = k / 3, dx = k - 3 * chunk;
                     const int s = (int)(g % S);
                     const long long use = g / S;
                     if (use > 0 && !mbar_wait(smem_u32(&s_empty[s]), (uint32_t)((use - 1) & 1))) {
@@ -434,9 +437,10 @@ __global__ void __launch_bounds__(192, 1) k_conv3x3_tc(const __grid_constant__ C
                         "cp.async.bulk.tensor.4d.shared::cluster.global.tile.mbarrier::complete_tx::bytes "
                         "[%0], [%1, {%2, %3, %4, %5}], [%6];" ::"r"(st),
                         "l"(reinterpret_cast<uint64_t>(&tin)), "r"(kc * chunk), "r"(tx * kTcM + dx - 1),
-                        "r"(y + dy - 1), "r"(img), "r"(bar)
+                        "r"(y - 1), "r"(img), "r"(bar)
                         : "memory");
-                    const bf16 *wsrc = p.wtc + (((size_t)slice * p.nchunks + chunk) * 9 + tap) * (size_t)(nt * kc);
+                    const bf16 *wsrc =
+                        p.wtc + (((size_t)slice * p.nchunks + chunk) * 3 + dx) * (size_t)(3 * nt * kc);
                     asm volatile(
                         "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
                             st + a_bytes),
@@ -450,7 +454,8 @@ __global__ void __launch_bounds__(192, 1) k_conv3x3_tc(const __grid_constant__ C
             // ---------------- MMAs ----------------
             const uint32_t idesc = (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(nt >> 3) << 17) |
                                    ((uint32_t)(kTcM >> 4) << 24);
-            const uint32_t a_bytes = (uint32_t)tc_a_bytes(kc, R), row_bytes = (uint32_t)tc_a_bytes(kc, 1);
+            const uint32_t a_bytes = (uint32_t)tc_a_bytes(kc, R), row_bytes = (uint32_t)tc_row_bytes(kc);
+            const uint32_t tap_bytes = (uint32_t)(nt * kc * 2);
             long long g = 0;
             int j = 0;
             for (int t = first; t < p.ntiles && !*fail; t += step, ++j) {
@@ -470,11 +475,13 @@ __global__ void __launch_bounds__(192, 1) k_conv3x3_tc(const __grid_constant__ C
                     }
                     asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
                     const uint32_t as = sbase + (uint32_t)(s * stage_bytes), bs = as + a_bytes;
+                    for (int dy = 0; dy < 3; ++dy)
                     for (int kk = 0; kk < kc / 16; ++kk) {
-                        const uint64_t bd = umma_desc_sw(bs + (uint32_t)(kk * 32), kc);
-                        const uint32_t accum = (k > 0 || kk > 0) ? 1u : 0u;
+                        const uint64_t bd = umma_desc_sw(bs + (uint32_t)dy * tap_bytes + (uint32_t)(kk * 32), kc);
+                        const uint32_t accum = (k > 0 || dy > 0 || kk > 0) ? 1u : 0u;
                         for (int r = 0; r < R; ++r) {
-                            const uint64_t ad = umma_desc_sw(as + (uint32_t)r * row_bytes + (uint32_t)(kk * 32), kc);
+                            const uint64_t ad =
+                                umma_desc_sw(as + (uint32_t)(r + dy) * row_bytes + (uint32_t)(kk * 32), kc);
                             asm volatile(
                                 "{\n\t.reg .pred p;\n\t"
                                 "setp.ne.b32 p, %4, 0;\n\t"
@@ -500,6 +507,31 @@ __global__ void __launch_bounds__(192, 1) k_conv3x3_tc(const __grid_constant__ C
     } else {
         // ---------------- epilogue (warps 2..5) ----------------
         const int q = warp & 3;  // tensor-memory lane quarter this warp may read
+        const int per_row = nt / 32, nslices = R * per_row;
+        uint32_t ra[32], rb[32];
+        auto tld = [&](uint32_t (&r)[32], uint32_t taddr) {
+            asm volatile(
+                "tcgen05.ld.sync.aligned.32x32b.x32.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15,"
+                "%16,%17,%18,%19,%20,%21,%22,%23,%24,%25,%26,%27,%28,%29,%30,%31}, [%32];"
+                : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
+                  "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]),
+                  "=r"(r[15]), "=r"(r[16]), "=r"(r[17]), "=r"(r[18]), "=r"(r[19]), "=r"(r[20]), "=r"(r[21]),
+                  "=r"(r[22]), "=r"(r[23]), "=r"(r[24]), "=r"(r[25]), "=r"(r[26]), "=r"(r[27]), "=r"(r[28]),
+                  "=r"(r[29]), "=r"(r[30]), "=r"(r[31])
+                : "r"(taddr));
+        };
+        // waits for every outstanding tcgen05.ld; the registers pass through
+        // it so no use of them is scheduled before the wait
+        auto twait = [&](uint32_t (&r)[32]) {
+            asm volatile("tcgen05.wait::ld.sync.aligned;"
+                         : "+r"(r[0]), "+r"(r[1]), "+r"(r[2]), "+r"(r[3]), "+r"(r[4]), "+r"(r[5]), "+r"(r[6]),
+                           "+r"(r[7]), "+r"(r[8]), "+r"(r[9]), "+r"(r[10]), "+r"(r[11]), "+r"(r[12]), "+r"(r[13]),
+                           "+r"(r[14]), "+r"(r[15]), "+r"(r[16]), "+r"(r[17]), "+r"(r[18]), "+r"(r[19]),
+                           "+r"(r[20]), "+r"(r[21]), "+r"(r[22]), "+r"(r[23]), "+r"(r[24]), "+r"(r[25]),
+                           "+r"(r[26]), "+r"(r[27]), "+r"(r[28]), "+r"(r[29]), "+r"(r[30]), "+r"(r[31])
+                         :
+                         : "memory");
+        };
         int j = 0;
         for (int t = first; t < p.ntiles; t += step, ++j) {
             const int acc = j & 1, use = j >> 1;
@@ -515,25 +547,14 @@ __global__ void __launch_bounds__(192, 1) k_conv3x3_tc(const __grid_constant__ C
             const int img = trow / p.tiles_y, y0 = (trow - img * p.tiles_y) * R;
             const int x = tx * kTcM + q * 32 + lane;
             const int cbase = slice * nt;
-            for (int rr = 0; rr < R; ++rr)
-            for (int c = 0; c < nt; c += 32) {
+            const uint32_t tbase = tmem + (uint32_t)acc * acc_cols + ((uint32_t)(q * 32) << 16);
+            // slice i: row i / per_row, columns 32 (i % per_row) ..
+            auto taddr = [&](int i) { return tbase + (uint32_t)(i / per_row) * ncols + (uint32_t)(32 * (i % per_row)); };
+            auto process = [&](const uint32_t (&r)[32], int i) {
+                const int rr = i / per_row, c = 32 * (i % per_row);
                 const int y = y0 + rr;
-                const bool store = x < p.w && y < p.h;
-                const size_t pix = ((size_t)img * p.h + (store ? y : 0)) * p.w + (store ? x : 0);
-                uint32_t r[32];
-                const uint32_t taddr = tmem + (uint32_t)acc * acc_cols + (uint32_t)rr * ncols +
-                                       ((uint32_t)(q * 32) << 16) + (uint32_t)c;
-                asm volatile(
-                    "tcgen05.ld.sync.aligned.32x32b.x32.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15,"
-                    "%16,%17,%18,%19,%20,%21,%22,%23,%24,%25,%26,%27,%28,%29,%30,%31}, [%32];"
-                    : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]),
-                      "=r"(r[7]), "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]),
-                      "=r"(r[14]), "=r"(r[15]), "=r"(r[16]), "=r"(r[17]), "=r"(r[18]), "=r"(r[19]), "=r"(r[20]),
-                      "=r"(r[21]), "=r"(r[22]), "=r"(r[23]), "=r"(r[24]), "=r"(r[25]), "=r"(r[26]), "=r"(r[27]),
-                      "=r"(r[28]), "=r"(r[29]), "=r"(r[30]), "=r"(r[31])
-                    : "r"(taddr));
-                asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
-                if (!store) continue;
+                if (!(x < p.w && y < p.h)) return;
+                const size_t pix = ((size_t)img * p.h + y) * p.w + x;
                 const int cg = cbase + c;
 #pragma unroll
                 for (int gi = 0; gi < 4; ++gi) {
@@ -541,7 +562,7 @@ __global__ void __launch_bounds__(192, 1) k_conv3x3_tc(const __grid_constant__ C
 #pragma unroll
                     for (int e = 0; e < 8; ++e) {
                         float f = __uint_as_float(r[8 * gi + e]);
-                        if (p.bias) f += __ldg(p.bias + cg + 8 * gi + e);
+                        if (p.bias) f += s_bias[c + 8 * gi + e];
                         if (p.relu) f = f > 0.f ? f : 0.f;
                         v[e] = f;
                     }
@@ -553,6 +574,18 @@ __global__ void __launch_bounds__(192, 1) k_conv3x3_tc(const __grid_constant__ C
                             if (!(m[e] > 0.f)) v[e] = 0.f;
                     }
                     *reinterpret_cast<uint4 *>(p.out + pix * p.cout + cg + 8 * gi) = pack8(v);
+                }
+            };
+            // two register sets: the next slice's load overlaps this slice's stores
+            tld(ra, taddr(0));
+            for (int i = 0; i < nslices; i += 2) {
+                twait(ra);
+                if (i + 1 < nslices) tld(rb, taddr(i + 1));
+                process(ra, i);
+                if (i + 1 < nslices) {
+                    twait(rb);
+                    if (i + 2 < nslices) tld(ra, taddr(i + 2));
+                    process(rb, i + 1);
                 }
             }
             asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
@@ -569,7 +602,7 @@ __global__ void __launch_bounds__(192, 1) k_conv3x3_tc(const __grid_constant__ C
 }
 
 // Weights in the tensor-core kernel's staging order: one block of nt x kc
-// per (slice, chunk, tap), row co = output channel, kc input channels, the
+// per (slice, chunk, dx, dy), row co = output channel, kc input channels, the
 // 16-byte groups of row co stored at group ^ swizzle(co) (128-byte swizzle:
 // co & 7; 64-byte swizzle: (co >> 1) & 3), i.e. the shared-memory image.
 __global__ void k_weights_tc(int cout, int cin, int nt, int kc, const bf16 *__restrict__ wk, bf16 *__restrict__ wtc)
@@ -587,7 +620,8 @@ __global__ void k_weights_tc(int cout, int cin, int nt, int kc, const bf16 *__re
         const int chunk = ci / kc, cl = ci - chunk * kc;
         const int grp = cl >> 3;
         const int swz = kc == 64 ? (co & 7) : ((co >> 1) & 3);
-        const size_t block = (((size_t)slice * nch + chunk) * 9 + tap) * (size_t)(nt * kc);
+        const int dy = tap / 3, dx = tap - 3 * dy;
+        const size_t block = ((((size_t)slice * nch + chunk) * 3 + dx) * 3 + dy) * (size_t)(nt * kc);
         wtc[block + (size_t)co * kc + (size_t)(((grp ^ swz) << 3) + (cl & 7))] = wk[k];
     }
 }
@@ -1120,21 +1154,22 @@ int conv_tc(const bf16 *in, int cin, int h, int w, int n, const bf16 *wtc, const
     SDP_CHECK_ARG(cin % 32 == 0 && cout % 32 == 0, "tensor-core convolution: channels %d -> %d", cin, cout);
     auto enc = tensor_map_encoder();
     if (!enc) return set_error(SDP_ERR_CUDA, "cuTensorMapEncodeTiled unavailable");
-    const int kc = tc_kc(cin);
     const int ny = tc_slices(cout);
     const int nt = cout / ny;
     const int tiles_x = (w + kTcM - 1) / kTcM;
     // rows per tile: as many as tensor memory holds (two sets of R
-    // accumulators) while the tiles still cover the SMs
-    // and at least three stages fit in shared memory
+    // accumulators) while the tiles still cover the SMs and at least three
+    // stages fit in shared memory
+    const int kc = tc_kc(cin);
     int R = 8;
     while (R > 1 && (2u * (uint32_t)R * tc_ncols(nt) > 512u || tc_stages(nt, kc, R) < 3 ||
                      (long long)n * ((h + R - 1) / R) * tiles_x * ny < num_sms()))
         R >>= 1;
+    SDP_CHECK_ARG(tc_stages(nt, kc, R) >= 2, "tensor-core convolution: %d output channels do not fit", nt);
     CUtensorMap tmap;
     const cuuint64_t dims[4] = {(cuuint64_t)cin, (cuuint64_t)w, (cuuint64_t)h, (cuuint64_t)n};
     const cuuint64_t strides[3] = {(cuuint64_t)cin * 2, (cuuint64_t)w * cin * 2, (cuuint64_t)h * w * cin * 2};
-    const cuuint32_t box[4] = {(cuuint32_t)kc, (cuuint32_t)kTcM, (cuuint32_t)R, 1};
+    const cuuint32_t box[4] = {(cuuint32_t)kc, (cuuint32_t)kTcM, (cuuint32_t)(R + 2), 1};
     const cuuint32_t estr[4] = {1, 1, 1, 1};
     const CUresult r = enc(&tmap, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 4, const_cast<bf16 *>(in), dims, strides, box,
                            estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
