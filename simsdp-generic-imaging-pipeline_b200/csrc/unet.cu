@@ -284,11 +284,13 @@ __global__ void __launch_bounds__(128) k_conv3x3(ConvArgs p)
 // x K16, BF16 -> FP32 in tensor memory); each row's A starts on an atom.
 //   warp 0 (one thread): loads, through an S-stage ring (full/empty
 //     mbarriers, transaction counts);
-//   warp 1 (one thread): MMAs; commits free a stage (empty) and, after a
-//     tile's last stage, hand its accumulator to the epilogue;
-//   warps 2-5: epilogue, tcgen05.ld of the accumulator (warp w reads lanes
-//     32 (w % 4) ..), bias, relu or the gradient mask, BF16 stores; then
-//     free the accumulator.  Two accumulators in tensor memory let the
+//   warp 1: MMAs, issued by lane 0 while the whole warp walks the loop (the
+//     descriptors stay warp-uniform); commits free a stage (empty) and, after
+//     a tile's last stage, hand its accumulator to the epilogue;
+//   warps 2-9: epilogue, tcgen05.ld of the accumulator (warp w reads lanes
+//     32 (w % 4) .., the two warps of a quarter alternate over the 32-column
+//     slices), bias, relu or the gradient mask, BF16 stores; then free the
+//     accumulator.  Two accumulators in tensor memory let the
 //     epilogue of one tile overlap the MMAs of the next.
 // Every wait is bounded: on timeout the CTA records the error and each role
 // leaves its loop (its later waits are bounded too).
@@ -297,6 +299,8 @@ constexpr int kTcM = 128;                       // pixels per tile
 constexpr int kTcMaxStages = 16;
 constexpr int kTcSmemBudget = 200 * 1024;       // stages; +1 KB for the 1024-byte alignment
 constexpr long long kTcSpins = 1LL << 20;       // bounded mbarrier polls
+constexpr int kTcEpiWarps = 8;                  // two epilogue warps per tensor-memory lane quarter
+constexpr int kTcThreads = 32 * (2 + kTcEpiWarps);
 
 inline int tc_kc(int) { return 32; }  // 32-channel chunks (64-byte swizzle) for every layer
 __host__ __device__ constexpr int tc_row_bytes(int kc) { return kTcM * kc * 2; }
@@ -372,7 +376,7 @@ __device__ __forceinline__ void mbar_expect_tx(uint32_t bar, uint32_t bytes)
     asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar), "r"(bytes) : "memory");
 }
 
-__global__ void __launch_bounds__(192, 1) k_conv3x3_tc(const __grid_constant__ CUtensorMap tin, TcArgs p)
+__global__ void __launch_bounds__(kTcThreads, 1) k_conv3x3_tc(const __grid_constant__ CUtensorMap tin, TcArgs p)
 {
     extern __shared__ __align__(128) unsigned char smem[];
     __shared__ __align__(8) uint64_t s_full[kTcMaxStages], s_empty[kTcMaxStages], s_tfull[2], s_tempty[2];
@@ -402,7 +406,7 @@ __global__ void __launch_bounds__(192, 1) k_conv3x3_tc(const __grid_constant__ C
         }
         for (int i = 0; i < 2; ++i) {
             mbar_init(smem_u32(&s_tfull[i]), 1);
-            mbar_init(smem_u32(&s_tempty[i]), 4);
+            mbar_init(smem_u32(&s_tempty[i]), kTcEpiWarps);
         }
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
         s_fail = 0;
@@ -418,15 +422,15 @@ __global__ void __launch_bounds__(192, 1) k_conv3x3_tc(const __grid_constant__ C
         if (lane == 0) {
             // ---------------- loads ----------------
             const uint32_t a_bytes = (uint32_t)tc_a_bytes(kc, R), b_bytes = (uint32_t)tc_b_bytes(nt, kc);
-            long long g = 0;
+            int s = 0;
+            uint32_t phase = 0;
+            bool first_lap = true;
             for (int t = first; t < p.ntiles && !*fail; t += step) {
                 const int tx = t % p.tiles_x, trow = t / p.tiles_x;
                 const int img = trow / p.tiles_y, y = (trow - img * p.tiles_y) * R;
-                for (int k = 0; k < per_tile; ++k, ++g) {
+                for (int k = 0; k < per_tile; ++k) {
                     const int chunk = k / 3, dx = k - 3 * chunk;
-                    const int s = (int)(g % S);
-                    const long long use = g / S;
-                    if (use > 0 && !mbar_wait(smem_u32(&s_empty[s]), (uint32_t)((use - 1) & 1))) {
+                    if (!first_lap && !mbar_wait(smem_u32(&s_empty[s]), phase ^ 1u)) {
                         *fail = 1;
                         break;
                     }
@@ -446,67 +450,87 @@ __global__ void __launch_bounds__(192, 1) k_conv3x3_tc(const __grid_constant__ C
                             st + a_bytes),
                         "l"(wsrc), "r"(b_bytes), "r"(bar)
                         : "memory");
+                    if (++s == S) {
+                        s = 0;
+                        phase ^= 1u;
+                        first_lap = false;
+                    }
                 }
             }
         }
     } else if (warp == 1) {
-        if (lane == 0) {
-            // ---------------- MMAs ----------------
-            const uint32_t idesc = (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(nt >> 3) << 17) |
-                                   ((uint32_t)(kTcM >> 4) << 24);
-            const uint32_t a_bytes = (uint32_t)tc_a_bytes(kc, R), row_bytes = (uint32_t)tc_row_bytes(kc);
-            const uint32_t tap_bytes = (uint32_t)(nt * kc * 2);
-            long long g = 0;
-            int j = 0;
-            for (int t = first; t < p.ntiles && !*fail; t += step, ++j) {
-                const int acc = j & 1, use = j >> 1;
-                if (use > 0 && !mbar_wait(smem_u32(&s_tempty[acc]), (uint32_t)((use - 1) & 1))) {
-                    *fail = 1;
+        // ---------------- MMAs ----------------
+        // The whole warp walks the loop, so the descriptors are warp-uniform
+        // values; lane 0 issues.  Descriptors advance by adding (bytes >> 4)
+        // to the start-address field (shared addresses stay below 2^18).
+        const uint32_t idesc = (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(nt >> 3) << 17) |
+                               ((uint32_t)(kTcM >> 4) << 24);
+        const uint64_t desc0 = umma_desc_sw(sbase, kc);
+        const uint32_t a16 = (uint32_t)tc_a_bytes(kc, R) >> 4, row16 = (uint32_t)tc_row_bytes(kc) >> 4;
+        const uint32_t tap16 = (uint32_t)(nt * kc * 2) >> 4, stage16 = (uint32_t)stage_bytes >> 4;
+        const uint32_t leader = lane == 0 ? 1u : 0u;
+        int s = 0;
+        uint32_t phase = 0;
+        int j = 0;
+        for (int t = first; t < p.ntiles && !*fail; t += step, ++j) {
+            const int acc = j & 1, use = j >> 1;
+            if (use > 0 && !__all_sync(0xffffffffu, mbar_wait(smem_u32(&s_tempty[acc]), (uint32_t)((use - 1) & 1)))) {
+                if (leader) *fail = 1;
+                break;
+            }
+            asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+            const uint32_t d = tmem + (uint32_t)acc * acc_cols;
+            bool ok = true;
+            for (int k = 0; k < per_tile; ++k) {
+                if (!__all_sync(0xffffffffu, mbar_wait(smem_u32(&s_full[s]), phase))) {
+                    ok = false;
                     break;
                 }
                 asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-                const uint32_t d = tmem + (uint32_t)acc * acc_cols;
-                bool ok = true;
-                for (int k = 0; k < per_tile; ++k, ++g) {
-                    const int s = (int)(g % S);
-                    if (!mbar_wait(smem_u32(&s_full[s]), (uint32_t)((g / S) & 1))) {
-                        ok = false;
-                        break;
-                    }
-                    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-                    const uint32_t as = sbase + (uint32_t)(s * stage_bytes), bs = as + a_bytes;
-                    for (int dy = 0; dy < 3; ++dy)
-                    for (int kk = 0; kk < kc / 16; ++kk) {
-                        const uint64_t bd = umma_desc_sw(bs + (uint32_t)dy * tap_bytes + (uint32_t)(kk * 32), kc);
+                const uint64_t ad0 = desc0 + (uint64_t)((uint32_t)s * stage16);
+                const uint64_t bd0 = ad0 + a16;
+#pragma unroll 1
+                for (int dy = 0; dy < 3; ++dy)
+#pragma unroll
+                    for (int kk = 0; kk < 2; ++kk) {  // kc = 32: two K16 steps
+                        const uint64_t bd = bd0 + (uint32_t)dy * tap16 + (uint32_t)(2 * kk);
                         const uint32_t accum = (k > 0 || dy > 0 || kk > 0) ? 1u : 0u;
                         for (int r = 0; r < R; ++r) {
-                            const uint64_t ad =
-                                umma_desc_sw(as + (uint32_t)(r + dy) * row_bytes + (uint32_t)(kk * 32), kc);
+                            const uint64_t ad = ad0 + (uint32_t)(r + dy) * row16 + (uint32_t)(2 * kk);
                             asm volatile(
-                                "{\n\t.reg .pred p;\n\t"
+                                "{\n\t.reg .pred p, e;\n\t"
+                                "setp.ne.b32 e, %9, 0;\n\t"
                                 "setp.ne.b32 p, %4, 0;\n\t"
-                                "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, {%5, %6, %7, %8}, p;\n\t}"
+                                "@e tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, {%5, %6, %7, %8}, p;\n\t}"
                                 :
                                 : "r"(d + (uint32_t)r * ncols), "l"(ad), "l"(bd), "r"(idesc), "r"(accum), "r"(0u),
-                                  "r"(0u), "r"(0u), "r"(0u));
+                                  "r"(0u), "r"(0u), "r"(0u), "r"(leader));
                         }
                     }
+                if (leader)
                     asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
                                      smem_u32(&s_empty[s]))
                                  : "memory");
+                __syncwarp();
+                if (++s == S) {
+                    s = 0;
+                    phase ^= 1u;
                 }
-                if (!ok) {
-                    *fail = 1;
-                    break;
-                }
+            }
+            if (!ok) {
+                if (leader) *fail = 1;
+                break;
+            }
+            if (leader)
                 asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
                                  smem_u32(&s_tfull[acc]))
                              : "memory");
-            }
+            __syncwarp();
         }
     } else {
-        // ---------------- epilogue (warps 2..5) ----------------
-        const int q = warp & 3;  // tensor-memory lane quarter this warp may read
+        // ---------------- epilogue (warps 2..9) ----------------
+        const int q = warp & 3;           // tensor-memory lane quarter this warp may read
+        const int half = (warp - 2) >> 2; // the two warps of a quarter take alternate slices
         const int per_row = nt / 32, nslices = R * per_row;
         uint32_t ra[32], rb[32];
         auto tld = [&](uint32_t (&r)[32], uint32_t taddr) {
@@ -576,16 +600,17 @@ __global__ void __launch_bounds__(192, 1) k_conv3x3_tc(const __grid_constant__ C
                     *reinterpret_cast<uint4 *>(p.out + pix * p.cout + cg + 8 * gi) = pack8(v);
                 }
             };
-            // two register sets: the next slice's load overlaps this slice's stores
-            tld(ra, taddr(0));
-            for (int i = 0; i < nslices; i += 2) {
+            // slices half, half + 2, ...; two register sets: the next slice's
+            // load overlaps this slice's stores
+            if (half < nslices) tld(ra, taddr(half));
+            for (int i = half; i < nslices; i += 4) {
                 twait(ra);
-                if (i + 1 < nslices) tld(rb, taddr(i + 1));
+                if (i + 2 < nslices) tld(rb, taddr(i + 2));
                 process(ra, i);
-                if (i + 1 < nslices) {
+                if (i + 2 < nslices) {
                     twait(rb);
-                    if (i + 2 < nslices) tld(ra, taddr(i + 2));
-                    process(rb, i + 1);
+                    if (i + 4 < nslices) tld(ra, taddr(i + 4));
+                    process(rb, i + 2);
                 }
             }
             asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
@@ -1200,7 +1225,7 @@ int conv_tc(const bf16 *in, int cin, int h, int w, int n, const bf16 *wtc, const
     if (per_slice < 1) per_slice = 1;
     if (per_slice > a.ntiles) per_slice = a.ntiles;
     const size_t smem = (size_t)a.stages * tc_stage_bytes(nt, kc, R) + 1024;
-    k_conv3x3_tc<<<dim3((unsigned)per_slice, ny), 192, smem, st>>>(tmap, a);
+    k_conv3x3_tc<<<dim3((unsigned)per_slice, ny), kTcThreads, smem, st>>>(tmap, a);
     SDP_LAUNCH_CHECK();
     return SDP_OK;
 }
