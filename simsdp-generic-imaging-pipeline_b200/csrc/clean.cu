@@ -312,7 +312,7 @@ struct CleanBar {
 constexpr int kPersistThreads = 1024;
 constexpr int kPersistSlice = 51200;           // floats of residual per block (200 KB)
 constexpr int kBatch = 8;                      // pixels per thread whose PSF loads are in flight together
-constexpr long long kBarrierSpins = 4000000;   // polls of ~32 ns sleep + an L2 read: one to two seconds
+constexpr long long kBarrierSpins = 4000000;   // polling rounds of ~32 ns sleep + an L2 read: one to two seconds
 
 __device__ __forceinline__ void better3(float &v, int &i, float &sv, float v2, int i2, float sv2)
 {
@@ -324,24 +324,37 @@ __device__ __forceinline__ void better3(float &v, int &i, float &sv, float v2, i
 }
 
 // Waits (one warp) until the results of blocks 0..nb-1 in buf carry flag
-// `target`.  Bounded: after spin_limit polls of one flag, or once another
-// block has timed out, it sets bar->err and returns false.
+// `target`.  Lane l watches blocks l, l + 32, ...: each polling round issues
+// all of its flag loads at once (relaxed, so they are in flight together and
+// a round costs one L2 round trip, not one per block), and one acquire fence
+// after the last round orders the result reads behind the flags.  Bounded:
+// after spin_limit rounds, or once another block has timed out, it sets
+// bar->err and returns false.  nb <= 32 * kWaitPerLane.
+constexpr int kWaitPerLane = 8;
+
 __device__ bool wait_results(PPart *buf, int nb, int target, CleanBar *bar, long long spin_limit)
 {
     cuda::atomic_ref<int, cuda::thread_scope_device> err(bar->err);
+    const int lane = (int)(threadIdx.x & 31);
     int fail = 0;
-    for (int b = (int)(threadIdx.x & 31); b < nb && !fail; b += 32) {
-        cuda::atomic_ref<int, cuda::thread_scope_device> flag(buf[b].flag);
-        long long spins = 0;
-        while (flag.load(cuda::memory_order_acquire) != target) {
-            if (err.load(cuda::memory_order_relaxed) != 0 || ++spins > spin_limit) {
-                err.store(1, cuda::memory_order_relaxed);
-                fail = 1;
-                break;
-            }
-            __nanosleep(32);
+    for (long long spins = 0;;) {
+        bool ready = true;
+#pragma unroll
+        for (int j = 0; j < kWaitPerLane; ++j) {
+            const int b = lane + 32 * j;
+            if (b < nb)
+                ready &= cuda::atomic_ref<int, cuda::thread_scope_device>(buf[b].flag).load(
+                             cuda::memory_order_relaxed) == target;
         }
+        if (ready) break;
+        if (err.load(cuda::memory_order_relaxed) != 0 || ++spins > spin_limit) {
+            err.store(1, cuda::memory_order_relaxed);
+            fail = 1;
+            break;
+        }
+        __nanosleep(32);
     }
+    cuda::atomic_thread_fence(cuda::memory_order_acquire, cuda::thread_scope_device);
     return !__any_sync(0xffffffffu, fail);
 }
 
@@ -688,7 +701,7 @@ int sdp::hogbom_launch(const sdp_clean_params *p, float *residual, const float *
     float3 *src = reinterpret_cast<float3 *>(sources);
 
     int pnb = 0;
-    if (allow_persistent && persistent_fits(G, &pnb)) {
+    if (allow_persistent && persistent_fits(G, &pnb) && pnb <= 32 * kWaitPerLane) {
         size_t off[4], base, bar_off, parts_off, total;
         clean_layout(clean_blocks(), off, &base);
         persist_layout(pnb, base, &bar_off, &parts_off, &total);
