@@ -282,6 +282,18 @@ __global__ void __launch_bounds__(128) k_conv3x3(ConvArgs p)
 // KC channels; 8-row atoms of 1024 / 512 bytes; K advanced 16 channels = 32
 // bytes inside the row).  A stage is 3 x R x KC / 16 tcgen05.mma (M128 x nt
 // x K16, BF16 -> FP32 in tensor memory); each row's A starts on an atom.
+// Packed row taps (nt = 32, where an N = 32 MMA would leave most of the
+// tensor core idle: any N <= 128 costs about the same time per K16 step):
+// one MMA per box row i and K16 step takes the three dy weight blocks as one
+// N = 96 operand (they are contiguous in the staged B), and writes them to
+// three consecutive 32-column accumulator blocks.  Output row r lives at
+// columns 32 (R + 1 - r), so block dy of box row i (output row i - dy) is at
+// 32 (R + 1 - i) + 32 dy for every dy: the MMAs of rows i and i + 1 overlap
+// by two blocks and accumulate into the same rows.  One set is 32 (R + 4)
+// columns (two blocks above and below the R real rows take contributions
+// that belong to neighbouring tiles and are discarded); every MMA
+// accumulates, so the epilogue stores zeros to the set after reading it.
+// (R + 2) x KC / 16 MMAs per stage instead of 3 R KC / 16.
 //   warp 0 (one thread): loads, through an S-stage ring (full/empty
 //     mbarriers, transaction counts);
 //   warp 1: MMAs, issued by lane 0 while the whole warp walks the loop (the
@@ -330,7 +342,17 @@ struct TcArgs {
     bf16 *out;           // [n][h][w][cout]
     int relu;
     int *err;            // set to 1 when a bounded wait gave up
+    int pack;            // packed row taps (nt = 32)
 };
+
+__host__ __device__ constexpr uint32_t tc_acc_cols(int pack, int rows, int nt)
+{
+    return pack ? 32u * (uint32_t)(rows + 4) : (uint32_t)rows * tc_ncols(nt);
+}
+__host__ __device__ constexpr uint32_t tc_tmem_cols(uint32_t need)
+{
+    return need <= 32u ? 32u : need <= 64u ? 64u : need <= 128u ? 128u : need <= 256u ? 256u : 512u;
+}
 
 // K-major operand descriptor with the 128-byte (layout 2) or 64-byte
 // (layout 4) swizzle: SBO = one 8-row atom, LBO unused (1).
@@ -343,6 +365,17 @@ __device__ __forceinline__ uint64_t umma_desc_sw(uint32_t saddr, int kc)
     d |= (uint64_t)1 << 46;  // descriptor version of sm_100
     d |= (uint64_t)(kc == 64 ? 2 : 4) << 61;
     return d;
+}
+
+// Zeros 32 consecutive tensor-memory columns of the warp's 32 lanes.
+__device__ __forceinline__ void tmem_zero32(uint32_t taddr)
+{
+    const uint32_t z = 0u;
+    asm volatile(
+        "tcgen05.st.sync.aligned.32x32b.x32.b32 [%0], {%1,%1,%1,%1,%1,%1,%1,%1,%1,%1,%1,%1,%1,%1,%1,%1,"
+        "%1,%1,%1,%1,%1,%1,%1,%1,%1,%1,%1,%1,%1,%1,%1,%1};" ::"r"(taddr),
+        "r"(z)
+        : "memory");
 }
 
 __device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity)
@@ -388,7 +421,9 @@ __global__ void __launch_bounds__(kTcThreads, 1) k_conv3x3_tc(const __grid_const
     for (int i = tid; i < nt; i += blockDim.x) s_bias[i] = p.bias ? p.bias[blockIdx.y * nt + i] : 0.f;
     const int slice = blockIdx.y;
     const uint32_t ncols = tc_ncols(nt);
-    const uint32_t acc_cols = (uint32_t)R * ncols;  // one accumulator set (R rows)
+    const int pack = p.pack;
+    const uint32_t acc_cols = tc_acc_cols(pack, R, nt);  // one accumulator set
+    const uint32_t tmem_cols = tc_tmem_cols(2 * acc_cols);
     const int stage_bytes = tc_stage_bytes(nt, kc, R);
     // stages start on 1024-byte boundaries (the swizzle atoms)
     const uint32_t sbase = (smem_u32(smem) + 1023u) & ~1023u;
@@ -396,7 +431,7 @@ __global__ void __launch_bounds__(kTcThreads, 1) k_conv3x3_tc(const __grid_const
 
     if (warp == 0) {
         asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(&s_tmem)),
-                     "r"(2 * acc_cols));
+                     "r"(tmem_cols));
         asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::);
     }
     if (tid == 32) {
@@ -417,6 +452,18 @@ __global__ void __launch_bounds__(kTcThreads, 1) k_conv3x3_tc(const __grid_const
     const uint32_t tmem = s_tmem;
     const int first = blockIdx.x, step = gridDim.x;
     volatile int *fail = &s_fail;  // read afresh in every loop condition
+    if (pack) {
+        // packed row taps: every MMA accumulates, so both sets start at zero
+        if (warp >= 2) {
+            const uint32_t lanes = (uint32_t)((warp & 3) * 32) << 16;
+            for (uint32_t c = 32u * (uint32_t)((warp - 2) >> 2); c < 2 * acc_cols; c += 64u)
+                tmem_zero32(tmem + lanes + c);
+            asm volatile("tcgen05.wait::st.sync.aligned;" ::: "memory");
+        }
+        asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+        __syncthreads();
+        asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+    }
 
     if (warp == 0) {
         if (lane == 0) {
@@ -465,6 +512,8 @@ __global__ void __launch_bounds__(kTcThreads, 1) k_conv3x3_tc(const __grid_const
         // to the start-address field (shared addresses stay below 2^18).
         const uint32_t idesc = (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(nt >> 3) << 17) |
                                ((uint32_t)(kTcM >> 4) << 24);
+        const uint32_t idesc_pack = (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(96 >> 3) << 17) |
+                                    ((uint32_t)(kTcM >> 4) << 24);
         const uint64_t desc0 = umma_desc_sw(sbase, kc);
         const uint32_t a16 = (uint32_t)tc_a_bytes(kc, R) >> 4, row16 = (uint32_t)tc_row_bytes(kc) >> 4;
         const uint32_t tap16 = (uint32_t)(nt * kc * 2) >> 4, stage16 = (uint32_t)stage_bytes >> 4;
@@ -489,8 +538,26 @@ __global__ void __launch_bounds__(kTcThreads, 1) k_conv3x3_tc(const __grid_const
                 asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
                 const uint64_t ad0 = desc0 + (uint64_t)((uint32_t)s * stage16);
                 const uint64_t bd0 = ad0 + a16;
+                if (pack) {
+                    // box row i, all three row taps: N = 96 at columns 32 (R + 1 - i)
 #pragma unroll 1
-                for (int dy = 0; dy < 3; ++dy)
+                    for (int i = 0; i < R + 2; ++i)
+#pragma unroll
+                        for (int kk = 0; kk < 2; ++kk) {
+                            const uint64_t ad = ad0 + (uint32_t)i * row16 + (uint32_t)(2 * kk);
+                            const uint64_t bd = bd0 + (uint32_t)(2 * kk);
+                            asm volatile(
+                                "{\n\t.reg .pred p, e;\n\t"
+                                "setp.ne.b32 e, %9, 0;\n\t"
+                                "setp.ne.b32 p, %4, 0;\n\t"
+                                "@e tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, {%5, %6, %7, %8}, p;\n\t}"
+                                :
+                                : "r"(d + 32u * (uint32_t)(R + 1 - i)), "l"(ad), "l"(bd), "r"(idesc_pack), "r"(1u),
+                                  "r"(0u), "r"(0u), "r"(0u), "r"(0u), "r"(leader));
+                        }
+                }
+#pragma unroll 1
+                for (int dy = 0; dy < 3 && !pack; ++dy)
 #pragma unroll
                     for (int kk = 0; kk < 2; ++kk) {  // kc = 32: two K16 steps
                         const uint64_t bd = bd0 + (uint32_t)dy * tap16 + (uint32_t)(2 * kk);
@@ -573,7 +640,10 @@ __global__ void __launch_bounds__(kTcThreads, 1) k_conv3x3_tc(const __grid_const
             const int cbase = slice * nt;
             const uint32_t tbase = tmem + (uint32_t)acc * acc_cols + ((uint32_t)(q * 32) << 16);
             // slice i: row i / per_row, columns 32 (i % per_row) ..
-            auto taddr = [&](int i) { return tbase + (uint32_t)(i / per_row) * ncols + (uint32_t)(32 * (i % per_row)); };
+            auto taddr = [&](int i) {
+                return pack ? tbase + 32u * (uint32_t)(R + 1 - i)
+                            : tbase + (uint32_t)(i / per_row) * ncols + (uint32_t)(32 * (i % per_row));
+            };
             auto process = [&](const uint32_t (&r)[32], int i) {
                 const int rr = i / per_row, c = 32 * (i % per_row);
                 const int y = y0 + rr;
@@ -613,6 +683,10 @@ __global__ void __launch_bounds__(kTcThreads, 1) k_conv3x3_tc(const __grid_const
                     process(rb, i + 2);
                 }
             }
+            if (pack) {
+                for (uint32_t c = 32u * (uint32_t)half; c < acc_cols; c += 64u) tmem_zero32(tbase + c);
+                asm volatile("tcgen05.wait::st.sync.aligned;" ::: "memory");
+            }
             asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
             __syncwarp();
             if (lane == 0) mbar_arrive(smem_u32(&s_tempty[acc]));
@@ -622,7 +696,7 @@ __global__ void __launch_bounds__(kTcThreads, 1) k_conv3x3_tc(const __grid_const
     if (*fail && tid == 0 && p.err) atomicExch(p.err, 1);
     if (warp == 0) {
         asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(2 * acc_cols));
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(tmem_cols));
     }
 }
 
@@ -1186,8 +1260,9 @@ int conv_tc(const bf16 *in, int cin, int h, int w, int n, const bf16 *wtc, const
     // accumulators) while the tiles still cover the SMs and at least three
     // stages fit in shared memory
     const int kc = tc_kc(cin);
+    const int pack = nt == 32 ? 1 : 0;
     int R = 8;
-    while (R > 1 && (2u * (uint32_t)R * tc_ncols(nt) > 512u || tc_stages(nt, kc, R) < 3 ||
+    while (R > 1 && (2u * tc_acc_cols(pack, R, nt) > 512u || tc_stages(nt, kc, R) < 3 ||
                      (long long)n * ((h + R - 1) / R) * tiles_x * ny < num_sms()))
         R >>= 1;
     SDP_CHECK_ARG(tc_stages(nt, kc, R) >= 2, "tensor-core convolution: %d output channels do not fit", nt);
@@ -1221,6 +1296,7 @@ int conv_tc(const bf16 *in, int cin, int h, int w, int n, const bf16 *wtc, const
     a.out = out;
     a.relu = relu;
     a.err = err;
+    a.pack = pack;
     int per_slice = num_sms() / ny;
     if (per_slice < 1) per_slice = 1;
     if (per_slice > a.ntiles) per_slice = a.ntiles;
