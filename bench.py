@@ -487,8 +487,10 @@ def c4_learned_block(S, D, dev, skies: int):
     10-500 points and 0-20 Gaussians (seed never used in training).  The
     plain pipeline runs 10 major cycles (200 Hogbom minor cycles, DFT
     predict); the learned one runs until it reaches the plain final FP64
-    residual RMS x 1.01.  Also times the network: forward at 1024^2 and one
-    training step (16 crops of 256^2)."""
+    residual RMS x 1.01.  The same comparison on 8 skies at 2048^2 (same
+    layout and cell, twice the field; the network is the one trained at
+    1024^2).  Also times the network: forward at 1024^2 and one training
+    step (16 crops of 256^2)."""
     import torch
     import learned as L
 
@@ -496,6 +498,10 @@ def c4_learned_block(S, D, dev, skies: int):
     params = L.load_weights()
     rows = L.evaluate(img, params, skies, seed=777)
     sp = [r["plain_s"] / r["learned_s"] for r in rows if r["learned_s"]]
+    img2 = L.Imaging(D, L.spiral_layout(2048))
+    rows2 = L.evaluate(img2, params, max(1, skies // 2), seed=777)
+    img2.close()
+    sp2 = [r["plain_s"] / r["learned_s"] for r in rows2 if r["learned_s"]]
 
     def ev(fn, n=7):
         fn()
@@ -555,6 +561,13 @@ def c4_learned_block(S, D, dev, skies: int):
         "plain_ms_median": med([r["plain_s"] * 1e3 for r in rows]),
         "learned_ms_median": med([r["learned_s"] * 1e3 for r in rows if r["learned_s"]]),
         "learned_cycles": [r["learned_cycles"] for r in rows], "learned_kinds": [r["learned_kinds"] for r in rows],
+        "at_2048": {"skies": len(rows2), "reached": sum(1 for r in rows2 if r["learned_s"]),
+                    "speedup_median": med(sp2),
+                    "speedup_geomean": float(np.exp(np.mean(np.log(sp2)))) if sp2 else None,
+                    "speedup_min": min(sp2) if sp2 else None,
+                    "plain_ms_median": med([r["plain_s"] * 1e3 for r in rows2]),
+                    "learned_ms_median": med([r["learned_s"] * 1e3 for r in rows2 if r["learned_s"]]),
+                    "learned_kinds": [r["learned_kinds"] for r in rows2]},
         "unet_forward_ms_1024": t_fwd, "unet_forward_tflops": f_fwd / (t_fwd * 1e-3) / 1e12,
         "unet_train_step_ms_16x256": t_train, "unet_train_tflops": f_train / (t_train * 1e-3) / 1e12,
         "unet_frac_of_bf16_peak": f_fwd / (t_fwd * 1e-3) / 1e12 / bf16,

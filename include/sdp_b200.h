@@ -639,6 +639,10 @@ int sdp_dots(long long n, const float *a, const float *b, double *dots_dev, void
 int sdp_axpy_ratio(long long n, const double *dots_dev, double alpha_max, float sign, const float *x, float *y,
                    float *alpha_dev, void *stream);
 int sdp_scale(long long n, float *x, float factor, void *stream);
+/* Zeroes the pixels within `border` of the edges of a G x G image (the
+ * proposal window of the learned cycle: the outer band of the image carries
+ * the taper correction's amplified imaging errors, not sources). */
+int sdp_zero_border(int grid_size, int border, float *image, void *stream);
 /* Adds components (l, m, flux, sigma) to a G x G image: points (sigma = 0)
  * at the nearest pixel, circular Gaussians of standard deviation sigma
  * (direction cosines) sampled over +-4 sigma. */

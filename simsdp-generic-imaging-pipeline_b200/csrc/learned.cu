@@ -229,10 +229,44 @@ __global__ void k_render(int G, double cell, int num, const float4 *__restrict__
     }
 }
 
+// Zeroes the pixels within `border` of the edge of a G x G image (only the
+// border band is visited: 4 strips of border x G).
+__global__ void k_zero_border(int G, int border, float *__restrict__ image)
+{
+    const long long strip = (long long)border * G;
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < 4 * strip;
+         i += (long long)gridDim.x * blockDim.x) {
+        const int which = (int)(i / strip);
+        const long long k = i - which * strip;
+        const int a = (int)(k / G), b = (int)(k - (long long)a * G);  // a: 0..border-1, b: 0..G-1
+        long long px;
+        if (which == 0) px = (long long)a * G + b;                    // top rows
+        else if (which == 1) px = (long long)(G - 1 - a) * G + b;     // bottom rows
+        else if (which == 2) px = (long long)b * G + a;               // left columns
+        else px = (long long)b * G + (G - 1 - a);                     // right columns
+        image[px] = 0.f;
+    }
+}
+
 }  // namespace
 }  // namespace sdp
 
 using namespace sdp;
+
+SDP_EXPORT int sdp_zero_border(int grid_size, int border, float *image, void *stream)
+{
+    SDP_CHECK_ARG(grid_size > 0 && border >= 0, "invalid size");
+    SDP_CHECK_ARG(image, "NULL argument");
+    if (border == 0) return SDP_OK;
+    if (2 * border >= grid_size) {
+        SDP_CUDA_TRY(cudaMemsetAsync(image, 0, sizeof(float) * (size_t)grid_size * grid_size, as_stream(stream)));
+        return SDP_OK;
+    }
+    const long long n = 4LL * border * grid_size;
+    k_zero_border<<<blocks_for(n), kThreads, 0, as_stream(stream)>>>(grid_size, border, image);
+    SDP_LAUNCH_CHECK();
+    return SDP_OK;
+}
 
 SDP_EXPORT int sdp_unet_input_planes(int grid_size, const float *residual, const float *psf, float *planes,
                                      float *scale_dev, void *stream)

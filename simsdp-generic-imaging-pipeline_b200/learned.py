@@ -377,18 +377,23 @@ class Deconvolver:
     gridding and imaging is the image of measured - (model + alpha x
     proposal) visibilities.  The proposal is kept when the residual RMS
     (FP64) falls by more than min_gain (relative); otherwise the cycle runs
-    Hogbom, and after give_up rejections the network is not asked again."""
+    Hogbom, and after give_up rejections the network is not asked again.
+    Proposals come from the central window (fraction `window` of each axis):
+    the outer band of the image holds the taper correction's amplified
+    imaging errors (w-term truncation, aliasing), which the network, trained
+    on 1024^2 images, reads as sources at 2048^2."""
 
     def __init__(self, img: Imaging, params: np.ndarray | None, num_minor: int = 200, loop_gain: float = 0.1,
                  max_components: int = 1024, rel_threshold: float = 0.05, alpha_max: float = 2.0,
                  min_gain: float = 0.05, give_up: int = 1, noise_factor: float = 1.5,
-                 weak_source_percent: float = 0.0002, signed: bool = True):
+                 weak_source_percent: float = 0.0002, signed: bool = True, window: float = 0.75):
         torch = _torch()
         self.img, self.D = img, img.D
         G, dev, n = img.G, img.dev, img.n
         self.num_minor, self.max_components = num_minor, max_components
         self.rel_threshold, self.alpha_max, self.min_gain, self.give_up = rel_threshold, alpha_max, min_gain, give_up
         self.signed = signed
+        self.border = int(round(G * (1.0 - window) / 2.0))
         self.params = S.CleanParams(G, num_minor, num_minor, loop_gain, noise_factor, weak_source_percent, 1.0,
                                     img.layout.cell)
         self.net = None
@@ -439,6 +444,7 @@ class Deconvolver:
         D, G = self.D, self.img.G
         D.unet_input_planes(G, self.residual, self.img.psf, self.planes, self.scale)
         self.net.forward(self.planes, self.out)
+        D.zero_border(G, self.border, self.out)
         D.select_components(G, self.img.layout.cell, self.out, self.scale, self.rel_threshold,
                             self.max_components, self.comps, self.count, None, self.sel_ws, signed=self.signed)
         n = int(self.count.item())

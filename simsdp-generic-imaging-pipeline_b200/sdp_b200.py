@@ -737,6 +737,9 @@ class Device:
     def scale(self, x, factor, stream=None):
         check(self.lib.sdp_scale(C.c_longlong(x.numel()), _dp(x), C.c_float(factor), _stream(stream)), self.lib)
 
+    def zero_border(self, grid_size, border, image, stream=None):
+        check(self.lib.sdp_zero_border(_i(grid_size), _i(border), _dp(image), _stream(stream)), self.lib)
+
     def sky_render(self, grid_size, cell, comps, image, stream=None):
         check(self.lib.sdp_sky_render(_i(grid_size), _d(cell), _i(comps.shape[0]), _dp(comps), _dp(image),
                                       _stream(stream)), self.lib)

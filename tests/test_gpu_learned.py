@@ -37,6 +37,39 @@ def test_learned_reaches_plain_rms_in_fewer_cycles(imaging):
     assert t_learned * 1.5 < t_plain, (t_learned, t_plain, rows)
 
 
+def test_learned_at_twice_the_field(device):
+    """The same network on 2048^2 images of the layout (same cell, twice the
+    field): with the proposal window (the image's outer eighth on each side
+    excluded) every sky reaches the plain RMS in fewer cycles, and no
+    component is proposed in the outer band.  (Without the window the
+    network put about two thirds of its components and half of its flux in
+    that band, which holds the taper correction's amplified imaging errors,
+    and no sky of 8 reached the target.)"""
+    import torch
+    import learned as L
+    img = L.Imaging(device, L.spiral_layout(2048))
+    try:
+        rows = L.evaluate(img, L.load_weights(), skies=2, seed=4243)
+        for r in rows:
+            assert r["learned_cycles"] is not None and r["learned_cycles"] < r["plain_cycles"], r
+        dec = L.Deconvolver(img, L.load_weights())
+        comps = torch.from_numpy(L.SkySampler(img.G, img.layout.cell, 98).sample()).to(img.dev)
+        meas = torch.empty((img.n, 2), dtype=torch.float32, device=img.dev)
+        L.measured_vis(img, comps, meas, 1e-4, torch.Generator(device=img.dev).manual_seed(5))
+        rms = dec._residual(meas)
+        ok, _, _, n = dec._propose(rms)
+        assert ok and n > 0
+        G, cell = img.G, img.layout.cell
+        c = dec.comps[:n].cpu().numpy()
+        X, Y = np.rint(c[:, 0] / cell) + G // 2, np.rint(c[:, 1] / cell) + G // 2
+        lo, hi = dec.border, G - dec.border
+        assert dec.border == G // 8
+        assert ((X >= lo) & (X < hi) & (Y >= lo) & (Y < hi)).all()
+        dec.close()
+    finally:
+        img.close()
+
+
 def test_accepted_proposals_are_exact_major_cycles(imaging):
     import torch
     import learned as L

@@ -160,3 +160,19 @@ def test_dft_pixels(sdp, device):
     c3 = torch.from_numpy(np.ascontiguousarray(comps[:, :3])).cuda()
     device.dft_pixels(c3, cell, uvw_d, vis, accumulate=True)
     assert rel_rms(vis.cpu().numpy(), 2 * np.stack([ref.real, ref.imag], axis=1)) <= 3e-6
+
+
+@pytest.mark.parametrize("G,border", [(64, 0), (64, 5), (96, 12), (10, 5), (10, 7)])
+def test_zero_border(sdp, device, G, border):
+    import torch
+    rng = np.random.default_rng(G + border)
+    img = rng.standard_normal((G, G)).astype(np.float32)
+    d = torch.from_numpy(img).cuda()
+    device.zero_border(G, border, d)
+    exp = img.copy()
+    if border > 0:
+        exp[:border] = 0
+        exp[G - border:] = 0
+        exp[:, :border] = 0
+        exp[:, G - border:] = 0
+    np.testing.assert_array_equal(d.cpu().numpy(), exp)
