@@ -330,6 +330,40 @@ def test_hogbom_persistent_sidelobes_vs_oracle(sdp, device, oracle32, G, psf_off
     np.testing.assert_array_equal(r.cpu().numpy(), r1)
 
 
+def test_hogbom_general_path_vs_oracle(sdp, device, oracle32):
+    """G = 2816: the image no longer fits in shared memory over all SMs, so
+    CLEAN runs as one launch per minor cycle (the general path, also the
+    pipeline's fallback when a capture of the cooperative launch is refused);
+    components, model and final residual bit for bit against the oracle,
+    with a PSF whose sidelobes are nonzero everywhere."""
+    import torch
+    dev = torch.device("cuda", 0)
+    G, minor = 2816, 60
+    rng = np.random.default_rng(G)
+    yy, xx = np.mgrid[0:G, 0:G]
+    psf = np.exp(-((xx - G // 2) ** 2 + (yy - G // 2) ** 2) / 8.0) + 2e-3 * rng.standard_normal((G, G))
+    psf = (psf / psf.max()).astype(np.float32)
+    res = 0.01 * rng.standard_normal((G, G))
+    for _ in range(20):
+        x0, y0 = rng.integers(0, G, 2)
+        res += rng.uniform(0.1, 1.0) * np.roll(np.roll(psf, y0 - G // 2, 0), x0 - G // 2, 1)
+    res, psf = res.astype(np.float32).reshape(-1), psf.reshape(-1)
+    n1, s1, m1, r1 = oracle32.hogbom(G, minor, minor, res, psf, 1.0, 1e-5)
+    params = sdp.CleanParams(G, minor, minor, 0.1, 1.5, 0.0002, 1.0, 1e-5)
+    r = torch.from_numpy(res.copy()).to(dev)
+    m = torch.zeros(G * G, dtype=torch.float32, device=dev)
+    s = torch.zeros((minor, 3), dtype=torch.float32, device=dev)
+    c = torch.zeros(1, dtype=torch.int32, device=dev)
+    ws = torch.empty(device.hogbom_workspace_bytes(G), dtype=torch.uint8, device=dev)
+    device.hogbom(params, r, torch.from_numpy(psf).to(dev), m, s, c, ws)
+    torch.cuda.synchronize()
+    n2 = int(c.item())
+    assert n1 == n2 > 20
+    np.testing.assert_array_equal(s[:n2].cpu().numpy(), s1)
+    np.testing.assert_array_equal(m.cpu().numpy(), m1)
+    np.testing.assert_array_equal(r.cpu().numpy(), r1)
+
+
 def test_bounded_wait_reports_timeout(sdp):
     """Failure detection without a GPU fault: a grid barrier that one arrival
     short of complete gives up after its bounded wait and reports
