@@ -480,6 +480,104 @@ def fft_block(S, D, dev, G: int = 2048, reps: int = 20):
     return res
 
 
+def calibration_block(S, D, dev, cpu_baseline: bool, nrx: int = 256, reps: int = 5):
+    """One gain-calibration cycle (gains_calibration_run.c: normal equations,
+    SVD, SUQ product, gain update) for nrx receivers, one sample per
+    baseline (nrx (nrx - 1) / 2 baselines; 512 x 512 normal matrix at 256):
+    the device path (CUDA events, median), the actor path with host buffers
+    (wall clock), and the reference's compiled actors on the host with
+    numpy's SVD in place of LAPACK's (the reference build has no LAPACK here),
+    with the error of the device step's gains against that chain."""
+    import ctypes as C
+    import torch
+    rng = np.random.default_rng(5)
+    pairs = np.array([(a, b) for a in range(nrx) for b in range(a + 1, nrx)], np.int32)
+    nbl, n = pairs.shape[0], 2 * nrx
+    g_true = (1.0 + 0.1 * rng.standard_normal(nrx)) * np.exp(1j * 0.3 * rng.standard_normal(nrx))
+    pred = rng.standard_normal(nbl) + 1j * rng.standard_normal(nbl)
+    meas = pred * g_true[pairs[:, 0]] * np.conj(g_true[pairs[:, 1]])
+    c2 = lambda z: np.ascontiguousarray(np.stack([z.real, z.imag], 1).astype(np.float32))  # noqa: E731
+    m2, p2, g0 = c2(meas), c2(pred), c2(np.ones(nrx, complex))
+    f32 = dict(dtype=torch.float32, device=dev)
+    dm, dp, dg = (torch.from_numpy(a).to(dev) for a in (m2, p2, g0))
+    dpairs = torch.from_numpy(pairs).to(dev)
+    A, Q, Sv, U, VT, suq = (torch.empty(n * n, **f32), torch.empty(n, **f32), torch.empty(n, **f32),
+                            torch.empty(n * n, **f32), torch.empty(n * n, **f32), torch.empty(n, **f32))
+    gout = torch.empty_like(dg)
+    flags = torch.zeros(1, dtype=torch.int32, device=dev)
+    ws = torch.empty(D.svd_workspace_bytes(n), dtype=torch.uint8, device=dev)
+
+    def cycle():
+        D.gaincal_normal_equations(dpairs, dm, dp, dg, A, Q, flags)
+        D.svd(n, A, Sv, U, VT, ws)
+        D.gaincal_suq(n, Sv, U, Q, suq)
+        D.gaincal_update(n, suq, VT, dg, gout)
+
+    cycle()
+    torch.cuda.synchronize()
+    sweeps = D.svd_check(ws)
+    ts = []
+    for _ in range(reps):
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record()
+        cycle()
+        b.record()
+        torch.cuda.synchronize()
+        ts.append(a.elapsed_time(b))
+    g_dev = gout.cpu().numpy()
+    lib = D.lib
+    cfg = S.make_config(64, 1.0, 1.0, 8)
+    _i, _p = C.c_int, C.c_void_p
+    ptr = lambda a: a.ctypes.data_as(_p)  # noqa: E731
+
+    def actor_chain(l, svd_fn=None):
+        Ah, Qh = np.zeros((n, n), np.float32), np.zeros(n, np.float32)
+        tok = _i(1)
+        l.update_gain_calibration_actor(_i(nbl), _i(nrx), _i(nbl), C.byref(tok), ptr(m2), ptr(p2), ptr(g0),
+                                        ptr(pairs), C.byref(cfg), ptr(Ah), ptr(Qh))
+        if svd_fn is None:
+            Sh, Uh, Vh = np.zeros(n, np.float32), np.zeros((n, n), np.float32), np.zeros((n, n), np.float32)
+            l.execute_calibration_SVD_actor(_i(n), _i(n), ptr(Ah), ptr(Sh), ptr(Uh), ptr(Vh))
+        else:
+            Sh, Uh, Vh = svd_fn(Ah)
+        sq = np.zeros(n, np.float32)
+        l.calculate_SUQ_product_actor(_i(n), _i(n), ptr(Sh), ptr(Uh), ptr(Qh), C.byref(cfg), ptr(sq))
+        go = np.zeros((nrx, 2), np.float32)
+        l.calculate_delta_update_gains_actor(_i(n), _i(nrx), ptr(sq), ptr(Vh), C.byref(cfg), ptr(g0), ptr(go))
+        return go
+
+    def numpy_svd(Ah):
+        u, sv, vt = np.linalg.svd(Ah.astype(np.float64).T)
+        return (sv.astype(np.float32), np.ascontiguousarray(u.T).astype(np.float32),
+                np.ascontiguousarray(vt.T).astype(np.float32))
+
+    actor_chain(lib)
+    t0 = time.perf_counter()
+    for _ in range(reps):
+        actor_chain(lib)
+    t_actor = (time.perf_counter() - t0) / reps * 1e3
+    res = {"workload": f"{nrx} receivers, {nbl} baselines, {n} x {n} normal matrix",
+           "device_ms": float(statistics.median(ts)), "actor_ms": t_actor, "svd_sweeps": sweeps}
+    sys.path.insert(0, str(ROOT / "oracle"))
+    import oracle as O
+    if cpu_baseline and O.RefLib.available("f32"):
+        ref = O.RefLib("f32").lib
+        t0 = time.perf_counter()
+        g_ref = actor_chain(ref, numpy_svd)
+        try:
+            from threadpoolctl import threadpool_info
+            blas_threads = max([t.get("num_threads", 1) for t in threadpool_info()] or [1])
+        except Exception:
+            blas_threads = 1
+        res["cpu_baseline"] = {"ms": (time.perf_counter() - t0) * 1e3, "kind": "reference", "cores": blas_threads,
+                               "sample": "one cycle: the reference's compiled actors (oracle/_ref, one thread) "
+                                         "with numpy.linalg.svd (LAPACK, FP64, the BLAS threads) in place of gesvd"}
+        z1, z2 = g_dev[:, 0] + 1j * g_dev[:, 1], g_ref[:, 0] + 1j * g_ref[:, 1]
+        z1 = z1 * np.exp(-1j * np.angle(np.vdot(z2, z1)))  # the free common phase
+        res["gains_rel_err_vs_reference"] = float(np.abs(z1 - z2).max() / np.abs(z2).max())
+    return res
+
+
 def c4_learned_block(S, D, dev, skies: int):
     """Learned CLEAN proposals against plain Hogbom on held-out skies: one
     channel of the 256-antenna spiral layout (3,916,800 visibilities) imaged
@@ -752,6 +850,7 @@ def b200_arm(args):
     if world == 1 and not args.no_c4:
         c4 = c4_learned_block(S, D, dev, args.c4_skies)
     fftc = fft_block(S, D, dev) if world == 1 and not args.no_c4 else None
+    calib = calibration_block(S, D, dev, not args.no_cpu_baseline) if world == 1 and not args.no_c4 else None
 
     # ---- e2e through the reference-facing C ABI with pinned host buffers ---------------
     uvw_h = torch.empty((N, 3), dtype=torch.float32).pin_memory()
@@ -840,6 +939,8 @@ def b200_arm(args):
         line["c4_learned"] = c4
     if fftc is not None:
         line["fft_2048"] = fftc
+    if calib is not None:
+        line["gain_calibration"] = calib
     if cpu is not None:
         line["cpu_baseline"] = cpu
     plan.close()

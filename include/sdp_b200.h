@@ -243,6 +243,25 @@ void gains_host_set_up(int NUM_RECEIVERS, int NUM_BASELINES, sdp_config *config,
                        sdp_int2 *receiver_pairs);
 void calculate_receiver_pairs(int NUM_BASELINES, int NUM_RECEIVERS, sdp_int2 *receiver_pairs);
 
+/* gains_calibration_run.h:25-35 — gain calibration (gains_calibration_run.c):
+ * the normal equations A (2R x 2R, row-major) and Q (2R) of one Gauss-Newton
+ * step from measured and predicted visibilities per baseline (:20-252), the
+ * SVD A = U S V^T (:254-298; LAPACK's column-major U and V^T, S decreasing),
+ * SUQ = S^-1 U^T Q with |S| <= 1e-6 dropped (:439-455), and gains += V SUQ
+ * (:457-476).  The first, third and fourth are bit-exact with the float
+ * build.  The SVD is a one-sided Jacobi method in FP64 (singular vectors
+ * agree with LAPACK's up to sign); it takes square matrices (the
+ * calibration's) and leaves A_array unchanged. */
+void update_gain_calibration_actor(int NUM_BASELINES, int NUM_RECEIVERS, int NUM_VISIBILITIES, int *loop_cycle_token,
+                                   sdp_float2 *measured_vis, sdp_float2 *visibilities, sdp_float2 *gains,
+                                   sdp_int2 *receiver_pairs, sdp_config *config, float *A_array, float *Q_array);
+void execute_calibration_SVD_actor(int NUM_COLS, int NUM_ROWS, float *A_array, float *S_array, float *U_array,
+                                   float *V_array);
+void calculate_SUQ_product_actor(int NUM_COLS, int NUM_ROWS, float *S_array, float *U_array, float *Q_array,
+                                 sdp_config *config, float *SUQ_array);
+void calculate_delta_update_gains_actor(int NUM_COLS, int NUM_RECEIVERS, float *SUQ_array, float *V_array,
+                                        sdp_config *config, sdp_float2 *gains_in, sdp_float2 *gains_out);
+
 /* gains_apply_run.h:31 */
 void subtract_from_measurements_finegrid(int NUM_VISIBILITIES, sdp_float2 *gridded_measured_vis,
                                          sdp_float2 *input_vis, int *num_finegrid_vis, sdp_float2 *delta_vis);
@@ -431,6 +450,23 @@ int sdp_gains_reciprocal(int num_receivers, const sdp_float2 *gains_in, sdp_floa
 int sdp_apply_gains(int num_vis, int num_baselines, int num_receivers, const sdp_float2 *measured,
                     const sdp_float2 *vis_in, const sdp_float2 *gains, const sdp_int2 *receiver_pairs, int subtract,
                     sdp_float2 *vis_out, int *flags_dev, void *stream);
+
+/* Gain calibration on the device (the actors above, device pointers).
+ * flags_dev (device int, cleared by the caller) gets 1 when a receiver pair
+ * indexes outside the gains.  sdp_svd: square n x n A (column-major, n <= 2048), S (n),
+ * U and VT (n x n, column-major); workspace of sdp_svd_workspace_bytes(n);
+ * one cooperative launch whose grid barriers are bounded (sdp_svd_check
+ * reports SDP_ERR_TIMEOUT when one gave up, and the sweeps run). */
+int sdp_gaincal_normal_equations(int num_baselines, int num_receivers, const sdp_float2 *measured,
+                                 const sdp_float2 *predicted, const sdp_float2 *gains, const sdp_int2 *receiver_pairs,
+                                 float *A, float *Q, int *flags_dev, void *stream);
+int sdp_svd_workspace_bytes(int n, size_t *bytes);
+int sdp_svd(int n, const float *A, float *S, float *U, float *VT, void *workspace, size_t workspace_bytes,
+            void *stream);
+int sdp_svd_check(const void *workspace, int *sweeps, void *stream);
+int sdp_gaincal_suq(int n, const float *S, const float *U, const float *Q, float *SUQ, void *stream);
+int sdp_gaincal_update(int n, int num_receivers, const float *SUQ, const float *VT, const sdp_float2 *gains_in,
+                       sdp_float2 *gains_out, void *stream);
 
 /* Inputs the reference reads from files and never generates (no counterpart
  * in its code; its kernel files follow the layout of top.c:256-312):

@@ -737,6 +737,34 @@ class Device:
     def scale(self, x, factor, stream=None):
         check(self.lib.sdp_scale(C.c_longlong(x.numel()), _dp(x), C.c_float(factor), _stream(stream)), self.lib)
 
+    # ---- gain calibration (device layer) ----
+    def gaincal_normal_equations(self, receiver_pairs, measured, predicted, gains, A, Q, flags, stream=None):
+        check(self.lib.sdp_gaincal_normal_equations(_i(receiver_pairs.shape[0]), _i(gains.shape[0]), _dp(measured),
+                                                    _dp(predicted), _dp(gains), _dp(receiver_pairs), _dp(A), _dp(Q),
+                                                    _dp(flags), _stream(stream)), self.lib)
+
+    def svd_workspace_bytes(self, n) -> int:
+        b = _sz(0)
+        check(self.lib.sdp_svd_workspace_bytes(_i(n), C.byref(b)), self.lib)
+        return b.value
+
+    def svd(self, n, A, S, U, VT, workspace, stream=None):
+        check(self.lib.sdp_svd(_i(n), _dp(A), _dp(S), _dp(U), _dp(VT), _dp(workspace), _sz(workspace.numel()),
+                               _stream(stream)), self.lib)
+
+    def svd_check(self, workspace, stream=None) -> int:
+        """Raises when the last sdp_svd's barrier wait gave up; returns its sweeps."""
+        sw = _i(0)
+        check(self.lib.sdp_svd_check(_dp(workspace), C.byref(sw), _stream(stream)), self.lib)
+        return sw.value
+
+    def gaincal_suq(self, n, S, U, Q, SUQ, stream=None):
+        check(self.lib.sdp_gaincal_suq(_i(n), _dp(S), _dp(U), _dp(Q), _dp(SUQ), _stream(stream)), self.lib)
+
+    def gaincal_update(self, n, SUQ, VT, gains_in, gains_out, stream=None):
+        check(self.lib.sdp_gaincal_update(_i(n), _i(gains_in.shape[0]), _dp(SUQ), _dp(VT), _dp(gains_in),
+                                          _dp(gains_out), _stream(stream)), self.lib)
+
     def zero_border(self, grid_size, border, image, stream=None):
         check(self.lib.sdp_zero_border(_i(grid_size), _i(border), _dp(image), _stream(stream)), self.lib)
 

@@ -90,3 +90,44 @@ def test_reciprocal_and_apply_bit_exact(sdp):
                            pairs.ctypes.data_as(_p), C.byref(cfg), o.ctypes.data_as(_p))
     np.testing.assert_array_equal(out, rout)
     assert lib.sdp_last_status() == 0, lib.sdp_last_error()
+
+
+def test_calibration_oracle_chain_recovers_gains():
+    """Pins the oracle for gain calibration: the reference's compiled normal
+    equations, SUQ product and gain update (gains_calibration_run.c), with
+    numpy's SVD in place of LAPACK's gesvd, recover known gains up to the
+    free common phase within a few cycles."""
+    ref = _ref()
+    cfg = O.make_config(64, 1.0, 1.0, 8)
+    rng = np.random.default_rng(3)
+    nrx = 16
+    pairs = np.array([(a, b) for a in range(nrx) for b in range(a + 1, nrx)] * 2, np.int32)
+    nbl, n = pairs.shape[0], 2 * nrx
+    g_true = (1.0 + 0.1 * rng.standard_normal(nrx)) * np.exp(1j * 0.3 * rng.standard_normal(nrx))
+    pred = rng.standard_normal(nbl) + 1j * rng.standard_normal(nbl)
+    meas = pred * g_true[pairs[:, 0]] * np.conj(g_true[pairs[:, 1]])
+    c2 = lambda z: np.ascontiguousarray(np.stack([z.real, z.imag], 1).astype(np.float32))  # noqa: E731
+    m2, p2 = c2(meas), c2(pred)
+    g = c2(np.ones(nrx, complex))
+    tok = _i(1)
+    for _ in range(8):
+        A = np.zeros((n, n), np.float32)
+        Q = np.zeros(n, np.float32)
+        ref.update_gain_calibration_actor(_i(nbl), _i(nrx), _i(nbl), C.byref(tok), m2.ctypes.data_as(_p),
+                                          p2.ctypes.data_as(_p), g.ctypes.data_as(_p), pairs.ctypes.data_as(_p),
+                                          C.byref(cfg), A.ctypes.data_as(_p), Q.ctypes.data_as(_p))
+        assert np.array_equal(A, A.T)
+        u, s, vt = np.linalg.svd(A.astype(np.float64).T)
+        S = s.astype(np.float32)
+        U = np.ascontiguousarray(u.T).astype(np.float32)    # LAPACK's column-major U
+        VT = np.ascontiguousarray(vt.T).astype(np.float32)  # and V^T
+        suq = np.zeros(n, np.float32)
+        ref.calculate_SUQ_product_actor(_i(n), _i(n), S.ctypes.data_as(_p), U.ctypes.data_as(_p),
+                                        Q.ctypes.data_as(_p), C.byref(cfg), suq.ctypes.data_as(_p))
+        out = np.zeros((nrx, 2), np.float32)
+        ref.calculate_delta_update_gains_actor(_i(n), _i(nrx), suq.ctypes.data_as(_p), VT.ctypes.data_as(_p),
+                                               C.byref(cfg), g.ctypes.data_as(_p), out.ctypes.data_as(_p))
+        g = out
+    est = g[:, 0] + 1j * g[:, 1]
+    est = est * np.exp(-1j * np.angle(np.vdot(g_true, est)))
+    assert np.abs(est - g_true).max() <= 2e-3

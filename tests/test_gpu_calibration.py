@@ -1,0 +1,194 @@
+"""Gain calibration (gains_calibration_run.c) through the actor ABI against
+the reference's own compiled actors (oracle/_ref).
+
+* normal equations A, Q: bit for bit, with repeated baselines (several time
+  samples), autocorrelation pairs (both receivers equal) and random gains;
+* SUQ product and gain update: bit for bit on the same S, U, V^T, Q;
+* SVD (one-sided Jacobi, FP64): singular values within 1e-5 (relative to
+  the largest) of numpy's LAPACK SVD, U S V^T reproduces A, U and V
+  orthonormal, S decreasing; odd and even sizes, and the calibration's own
+  rank-deficient normal matrix (one free phase);
+* the whole step: from unit gains, a few calibration cycles recover the true
+  gains up to the free global phase, and one step agrees with the
+  reference's chain (numpy's SVD in place of LAPACK's) to float rounding.
+"""
+from __future__ import annotations
+
+import ctypes as C
+
+import numpy as np
+import pytest
+
+import oracle as O
+
+pytestmark = pytest.mark.gpu
+
+_i, _p = C.c_int, C.c_void_p
+
+
+def _ptr(a):
+    return a.ctypes.data_as(_p)
+
+
+def _ref():
+    if not O.RefLib.available("f32"):
+        pytest.skip("reference build oracle/_ref not present")
+    return O.RefLib("f32").lib
+
+
+def _problem(nrx, times, seed, autocorr=False):
+    rng = np.random.default_rng(seed)
+    pairs = [(a, b) for a in range(nrx) for b in range(a + 1, nrx)]
+    if autocorr:
+        pairs += [(a, a) for a in range(0, nrx, 3)]
+    pairs = np.array(pairs * times, np.int32)
+    nbl = pairs.shape[0]
+    g_true = (1.0 + 0.1 * rng.standard_normal(nrx)) * np.exp(1j * 0.3 * rng.standard_normal(nrx))
+    pred = rng.standard_normal(nbl) + 1j * rng.standard_normal(nbl)
+    meas = pred * g_true[pairs[:, 0]] * np.conj(g_true[pairs[:, 1]])
+    c2 = lambda z: np.ascontiguousarray(np.stack([z.real, z.imag], 1).astype(np.float32))  # noqa: E731
+    return pairs, c2(meas), c2(pred), g_true, c2
+
+
+def _normal(lib, cfg, pairs, meas, pred, gains, nrx):
+    n = 2 * nrx
+    A = np.full((n, n), np.nan, np.float32)
+    Q = np.full(n, np.nan, np.float32)
+    tok = _i(1)
+    lib.update_gain_calibration_actor(_i(pairs.shape[0]), _i(nrx), _i(pairs.shape[0]), C.byref(tok), _ptr(meas),
+                                      _ptr(pred), _ptr(gains), _ptr(pairs), C.byref(cfg), _ptr(A), _ptr(Q))
+    return A, Q
+
+
+@pytest.mark.parametrize("nrx,times,autocorr", [(24, 1, False), (24, 3, True), (64, 2, False)])
+def test_normal_equations_bit_exact(sdp, nrx, times, autocorr):
+    lib, ref = sdp.load(), _ref()
+    cfg = O.make_config(64, 1.0, 1.0, 8)
+    pairs, meas, pred, g_true, c2 = _problem(nrx, times, nrx + times, autocorr)
+    rng = np.random.default_rng(7)
+    gains = c2(g_true * (1 + 0.05 * (rng.standard_normal(nrx) + 1j * rng.standard_normal(nrx))))
+    A1, Q1 = _normal(lib, cfg, pairs, meas, pred, gains, nrx)
+    A2, Q2 = _normal(ref, cfg, pairs, meas, pred, gains, nrx)
+    np.testing.assert_array_equal(Q1, Q2)
+    np.testing.assert_array_equal(A1, A2)
+    assert np.abs(A1).max() > 0
+
+
+def test_suq_and_gain_update_bit_exact(sdp):
+    lib, ref = sdp.load(), _ref()
+    cfg = O.make_config(64, 1.0, 1.0, 8)
+    rng = np.random.default_rng(11)
+    nrx = 40
+    n = 2 * nrx
+    S = np.abs(rng.standard_normal(n)).astype(np.float32)
+    S[[3, 17]] = [5e-7, 0.0]  # dropped by the 1e-6 rule
+    U = rng.standard_normal((n, n)).astype(np.float32)
+    VT = rng.standard_normal((n, n)).astype(np.float32)
+    Q = rng.standard_normal(n).astype(np.float32)
+    gin = rng.standard_normal((nrx, 2)).astype(np.float32)
+    outs = []
+    for l in (lib, ref):
+        suq = np.full(n, np.nan, np.float32)
+        l.calculate_SUQ_product_actor(_i(n), _i(n), _ptr(S), _ptr(U), _ptr(Q), C.byref(cfg), _ptr(suq))
+        gout = np.full((nrx, 2), np.nan, np.float32)
+        l.calculate_delta_update_gains_actor(_i(n), _i(nrx), _ptr(suq), _ptr(VT), C.byref(cfg), _ptr(gin), _ptr(gout))
+        outs.append((suq, gout))
+    np.testing.assert_array_equal(outs[0][0], outs[1][0])
+    np.testing.assert_array_equal(outs[0][1], outs[1][1])
+
+
+def _svd(lib, A):
+    n = A.shape[0]
+    S = np.zeros(n, np.float32)
+    U = np.zeros((n, n), np.float32)
+    VT = np.zeros((n, n), np.float32)
+    a = np.asfortranarray(A.astype(np.float32))
+    a_before = a.copy()
+    lib.execute_calibration_SVD_actor(_i(n), _i(n), _ptr(a), _ptr(S), _ptr(U), _ptr(VT))
+    np.testing.assert_array_equal(a, a_before)  # A is left as it was
+    # LAPACK's column-major layout: U[:, k] is stored at U_flat[k n : (k + 1) n]
+    return S, U.reshape(n, n).T.astype(np.float64), VT.reshape(n, n).T.astype(np.float64)
+
+
+def _check_svd(A, S, U, VT, tol=1e-5):
+    A = A.astype(np.float64)
+    s_ref = np.linalg.svd(A, compute_uv=False)
+    smax = s_ref[0]
+    assert np.all(np.diff(S) <= 0)
+    assert np.abs(S - s_ref).max() <= tol * smax, np.abs(S - s_ref).max() / smax
+    rec = (U * S.astype(np.float64)) @ VT
+    assert np.linalg.norm(rec - A) <= tol * np.linalg.norm(A)
+    keep = S > 1e-4 * smax
+    Uk, Vk = U[:, keep], VT[keep, :]
+    assert np.abs(Uk.T @ Uk - np.eye(keep.sum())).max() <= 1e-5
+    assert np.abs(VT @ VT.T - np.eye(A.shape[0])).max() <= 1e-5
+    assert np.abs(Vk @ Vk.T - np.eye(keep.sum())).max() <= 1e-5
+
+
+@pytest.mark.parametrize("n", [1, 2, 37, 64, 130])
+def test_svd_random(sdp, n):
+    rng = np.random.default_rng(n)
+    A = rng.standard_normal((n, n)).astype(np.float32)
+    S, U, VT = _svd(sdp.load(), A)
+    _check_svd(A, S, U, VT)
+
+
+def test_svd_of_calibration_normal_matrix(sdp):
+    """The normal matrix is symmetric positive semi-definite with one null
+    direction (a common phase rotation of all gains changes nothing)."""
+    lib = sdp.load()
+    cfg = O.make_config(64, 1.0, 1.0, 8)
+    nrx = 96
+    pairs, meas, pred, g_true, c2 = _problem(nrx, 1, 5)
+    gains = c2(np.ones(nrx, complex))
+    A, _ = _normal(lib, cfg, pairs, meas, pred, gains, nrx)
+    S, U, VT = _svd(lib, A)
+    _check_svd(A, S, U, VT)
+    assert S[-1] <= 1e-5 * S[0]  # the free phase
+    assert S[-2] > 1e-3 * S[0]
+
+
+def _step(lib, cfg, pairs, meas, pred, gains, nrx, svd=None):
+    n = 2 * nrx
+    A, Q = _normal(lib, cfg, pairs, meas, pred, gains, nrx)
+    if svd is None:
+        S, U, VT = (np.zeros(n, np.float32), np.zeros((n, n), np.float32), np.zeros((n, n), np.float32))
+        lib.execute_calibration_SVD_actor(_i(n), _i(n), _ptr(A), _ptr(S), _ptr(U), _ptr(VT))
+    else:
+        S, U, VT = svd(A)
+    suq = np.zeros(n, np.float32)
+    lib.calculate_SUQ_product_actor(_i(n), _i(n), _ptr(S), _ptr(U), _ptr(Q), C.byref(cfg), _ptr(suq))
+    gout = np.zeros((nrx, 2), np.float32)
+    lib.calculate_delta_update_gains_actor(_i(n), _i(nrx), _ptr(suq), _ptr(VT), C.byref(cfg), _ptr(gains),
+                                           _ptr(gout))
+    return gout
+
+
+def _numpy_svd(A):
+    """LAPACK's outputs (column-major) from numpy's SVD of the float matrix."""
+    u, s, vt = np.linalg.svd(A.astype(np.float64).T)  # the actor reads A column-major
+    return (s.astype(np.float32), np.ascontiguousarray(u.T).astype(np.float32),
+            np.ascontiguousarray(vt.T).astype(np.float32))
+
+
+def test_calibration_recovers_gains(sdp):
+    lib, ref = sdp.load(), _ref()
+    cfg = O.make_config(64, 1.0, 1.0, 8)
+    nrx = 48
+    pairs, meas, pred, g_true, c2 = _problem(nrx, 2, 21)
+    g = c2(np.ones(nrx, complex))
+    # one step against the reference's chain with numpy's SVD
+    # (the free phase's singular value is rounding noise, above the 1e-6
+    # cut, so both chains add a different small common phase: compare after
+    # removing it)
+    g1 = _step(lib, cfg, pairs, meas, pred, g, nrx)
+    g1_ref = _step(ref, cfg, pairs, meas, pred, g, nrx, svd=_numpy_svd)
+    z1, z2 = g1[:, 0] + 1j * g1[:, 1], g1_ref[:, 0] + 1j * g1_ref[:, 1]
+    z1 = z1 * np.exp(-1j * np.angle(np.vdot(z2, z1)))
+    assert np.abs(z1 - z2).max() <= 1e-4 * np.abs(z2).max()
+    for _ in range(8):
+        g = _step(lib, cfg, pairs, meas, pred, g, nrx)
+    est = g[:, 0] + 1j * g[:, 1]
+    # the gains are determined up to one common phase
+    ph = np.angle(np.vdot(g_true, est))
+    assert np.abs(est * np.exp(-1j * ph) - g_true).max() <= 2e-3
