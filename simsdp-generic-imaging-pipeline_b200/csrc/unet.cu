@@ -269,18 +269,19 @@ __global__ void __launch_bounds__(128) k_conv3x3(ConvArgs p)
 // persistent warp-specialised kernel.  Tile = R consecutive image rows
 // (R = 1, 2, 4 or 8; each a 128-pixel segment, M = 128 per row) x nt output
 // channels (nt <= 256, a multiple of 32), R accumulators in tensor memory.
-// K = 9 taps x Cin, walked as (chunk of KC = 32 or 64 channels, column tap
-// dx) pairs; one pair = one pipeline stage:
+// K = 9 taps x Cin, walked as (chunk of KC = 32 channels, column tap dx)
+// pairs; one pair = one pipeline stage:
 //   A: the (R + 2) x 128 input pixels the three row taps of dx read (rows
 //      y0 - 1 .. y0 + R, columns x0 + dx - 1 ..), KC channels each, by one
 //      4-D TMA box {KC, 128, R + 2, 1} (reads outside the image return zero);
 //      row tap dy of output row r is box row r + dy;
 //   B: the pair's 3 x nt x KC weights (dy = 0, 1, 2), pre-arranged in global
 //      memory as the shared-memory image, by one bulk copy;
-// both in the K-major canonical layout with the 128-byte (KC = 64) or
-// 64-byte (KC = 32) swizzle, which the TMA writes and the MMA reads (rows of
-// KC channels; 8-row atoms of 1024 / 512 bytes; K advanced 16 channels = 32
-// bytes inside the row).  A stage is 3 x R x KC / 16 tcgen05.mma (M128 x nt
+// both in the K-major canonical layout with the 64-byte swizzle, which the
+// TMA writes and the MMA reads (rows of 32 channels; 8-row atoms of 512
+// bytes; K advanced 16 channels = 32 bytes inside the row; the descriptor
+// helper also knows the 128-byte form for 64-channel rows).  A stage is
+// 3 x R x KC / 16 tcgen05.mma (M128 x nt
 // x K16, BF16 -> FP32 in tensor memory); each row's A starts on an atom.
 // Packed row taps (nt = 32, where an N = 32 MMA would leave most of the
 // tensor core idle: any N <= 128 costs about the same time per K16 step):
