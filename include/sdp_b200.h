@@ -705,6 +705,9 @@ int sdp_dft_gauss(int num_vis, int num_sources, const sdp_float4 *sources, const
  * the bounded wait reported the timeout (the expected result), SDP_OK
  * otherwise. */
 int sdp_selftest_bounded_wait(int nblocks, long long spin_limit, int *status);
+/* The same for the SVD's grid barrier (sdp_svd): a barrier expecting one CTA
+ * more than launched; *status = SDP_ERR_TIMEOUT when its waits ran out. */
+int sdp_selftest_svd_barrier(int nblocks, long long spin_limit, int *status);
 
 #ifdef __cplusplus
 }

@@ -175,12 +175,12 @@ constexpr int kJacobiMaxSweeps = 60;
 
 // Grid barrier: an arrival counter and a generation word; the last CTA to
 // arrive resets the counter and advances the generation (release), the others
-// poll the generation (acquire).  Bounded: after kJacobiSpins polls, or once
+// poll the generation (acquire).  Bounded: after `spins` polls, or once
 // another CTA gave up, a CTA records the error and returns false.  (Measured
 // alternatives, one 512 x 512 SVD: a two-level counter tree, the same time;
 // every CTA polling all CTAs' flags, as the persistent CLEAN kernel does,
 // 1.6x slower with 256 CTAs.)
-__device__ bool jacobi_barrier(JacobiBar *bar, unsigned nblocks)
+__device__ bool jacobi_barrier(JacobiBar *bar, unsigned nblocks, long long spin_limit = kJacobiSpins)
 {
     __shared__ int s_ok;
     __threadfence();
@@ -196,7 +196,7 @@ __device__ bool jacobi_barrier(JacobiBar *bar, unsigned nblocks)
         } else {
             long long spins = 0;
             while (gen.load(cuda::memory_order_acquire) == g) {
-                if (err.load(cuda::memory_order_relaxed) != 0 || ++spins > kJacobiSpins) {
+                if (err.load(cuda::memory_order_relaxed) != 0 || ++spins > spin_limit) {
                     err.store(1, cuda::memory_order_relaxed);
                     ok = 0;
                     break;
@@ -359,6 +359,15 @@ __global__ void __launch_bounds__(kJacobiThreads) k_jacobi_svd(int n, const floa
     }
 }
 
+// Bounded-wait self test of the grid barrier: the barrier is told to expect
+// one CTA more than the launch has, so every CTA's wait runs out after
+// spin_limit polls and the error flag is set; nothing faults and the kernel
+// ends.
+__global__ void k_jacobi_barrier_probe(JacobiBar *bar, long long spin_limit)
+{
+    jacobi_barrier(bar, gridDim.x + 1, spin_limit);
+}
+
 }  // namespace
 
 // [JacobiBar | W | V | sigma]
@@ -442,6 +451,26 @@ SDP_EXPORT int sdp_svd_check(const void *workspace, int *sweeps, void *stream)
     SDP_CUDA_TRY(cudaStreamSynchronize(st));
     if (sweeps) *sweeps = b.sweeps;
     return b.err ? set_error(SDP_ERR_TIMEOUT, "svd: a grid barrier wait gave up") : SDP_OK;
+}
+
+SDP_EXPORT int sdp_selftest_svd_barrier(int nblocks, long long spin_limit, int *status)
+{
+    SDP_CHECK_ARG(status != nullptr && nblocks >= 1 && nblocks <= 64 && spin_limit >= 1, "bad argument");
+    *status = SDP_OK;
+    JacobiBar *bar = nullptr;
+    SDP_CUDA_TRY(cudaMalloc(&bar, sizeof(JacobiBar)));
+    int err = 0;
+    cudaError_t e = cudaMemset(bar, 0, sizeof(JacobiBar));
+    if (e == cudaSuccess) {
+        k_jacobi_barrier_probe<<<nblocks, 32>>>(bar, spin_limit);
+        e = cudaGetLastError();
+    }
+    if (e == cudaSuccess) e = cudaDeviceSynchronize();
+    if (e == cudaSuccess) e = cudaMemcpy(&err, &bar->err, sizeof(int), cudaMemcpyDeviceToHost);
+    cudaFree(bar);
+    if (e != cudaSuccess) return cuda_error(e, "svd barrier self test");
+    *status = err ? SDP_ERR_TIMEOUT : SDP_OK;
+    return SDP_OK;
 }
 
 SDP_EXPORT int sdp_gaincal_suq(int n, const float *S, const float *U, const float *Q, float *SUQ, void *stream)

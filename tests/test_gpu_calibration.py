@@ -192,3 +192,16 @@ def test_calibration_recovers_gains(sdp):
     # the gains are determined up to one common phase
     ph = np.angle(np.vdot(g_true, est))
     assert np.abs(est * np.exp(-1j * ph) - g_true).max() <= 2e-3
+
+
+def test_svd_barrier_wait_is_bounded(sdp):
+    """Failure detection without a GPU fault: a grid barrier one arrival
+    short gives up after its bounded wait and reports SDP_ERR_TIMEOUT; the
+    context stays usable (an SVD runs afterwards)."""
+    lib = sdp.load()
+    st = C.c_int(-1)
+    sdp.check(lib.sdp_selftest_svd_barrier(C.c_int(4), C.c_longlong(100_000), C.byref(st)), lib)
+    assert st.value == 5  # SDP_ERR_TIMEOUT
+    A = np.random.default_rng(0).standard_normal((16, 16)).astype(np.float32)
+    S, U, VT = _svd(lib, A)
+    _check_svd(A, S, U, VT)
