@@ -317,15 +317,20 @@ constexpr int kTcThreads = 32 * (2 + kTcEpiWarps);
 
 inline int tc_kc(int) { return 32; }  // 32-channel chunks (64-byte swizzle) for every layer
 __host__ __device__ constexpr int tc_row_bytes(int kc) { return kTcM * kc * 2; }
-__host__ __device__ constexpr int tc_a_bytes(int kc, int rows) { return (rows + 2) * tc_row_bytes(kc); }
-__host__ __device__ constexpr int tc_b_bytes(int nt, int kc) { return 3 * nt * kc * 2; }
-__host__ __device__ constexpr int tc_stage_bytes(int nt, int kc, int rows)
+// sa: shared A (the column taps read one buffer of 18 slabs; see below)
+__host__ __device__ constexpr int tc_slab_bytes(int kc, int rows) { return (rows + 2) * 8 * kc * 2; }
+__host__ __device__ constexpr int tc_a_bytes(int kc, int rows, int sa = 0)
 {
-    return (tc_a_bytes(kc, rows) + tc_b_bytes(nt, kc) + 1023) & ~1023;
+    return sa ? 18 * tc_slab_bytes(kc, rows) : (rows + 2) * tc_row_bytes(kc);
 }
-inline int tc_stages(int nt, int kc, int rows)
+__host__ __device__ constexpr int tc_b_bytes(int nt, int kc, int sa = 0) { return (sa ? 9 : 3) * nt * kc * 2; }
+__host__ __device__ constexpr int tc_stage_bytes(int nt, int kc, int rows, int sa = 0)
 {
-    int s = kTcSmemBudget / tc_stage_bytes(nt, kc, rows);
+    return (tc_a_bytes(kc, rows, sa) + tc_b_bytes(nt, kc, sa) + 1023) & ~1023;
+}
+inline int tc_stages(int nt, int kc, int rows, int sa = 0)
+{
+    int s = kTcSmemBudget / tc_stage_bytes(nt, kc, rows, sa);
     return s > kTcMaxStages ? kTcMaxStages : s;
 }
 __host__ __device__ constexpr uint32_t tc_ncols(int nt) { return nt <= 32 ? 32u : (nt <= 64 ? 64u : (nt <= 128 ? 128u : 256u)); }
@@ -344,6 +349,7 @@ struct TcArgs {
     int relu;
     int *err;            // set to 1 when a bounded wait gave up
     int pack;            // packed row taps (nt = 32)
+    int sa;              // shared A: one stage per chunk, pixels in slab order
 };
 
 __host__ __device__ constexpr uint32_t tc_acc_cols(int pack, int rows, int nt)
@@ -353,6 +359,18 @@ __host__ __device__ constexpr uint32_t tc_acc_cols(int pack, int rows, int nt)
 __host__ __device__ constexpr uint32_t tc_tmem_cols(uint32_t need)
 {
     return need <= 32u ? 32u : need <= 64u ? 64u : need <= 128u ? 128u : need <= 256u ? 256u : 512u;
+}
+
+// K-major operand descriptor with the 64-byte swizzle (layout 4) and a
+// given stride between 8-row groups (the shared-A slabs).
+__device__ __forceinline__ uint64_t umma_desc_sw64_sbo(uint32_t saddr, uint32_t sbo)
+{
+    uint64_t d = (uint64_t)((saddr >> 4) & 0x3FFFu);
+    d |= (uint64_t)1 << 16;
+    d |= (uint64_t)((sbo >> 4) & 0x3FFFu) << 32;
+    d |= (uint64_t)1 << 46;
+    d |= (uint64_t)4 << 61;
+    return d;
 }
 
 // K-major operand descriptor with the 128-byte (layout 2) or 64-byte
@@ -410,7 +428,9 @@ __device__ __forceinline__ void mbar_expect_tx(uint32_t bar, uint32_t bytes)
     asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar), "r"(bytes) : "memory");
 }
 
-__global__ void __launch_bounds__(kTcThreads, 1) k_conv3x3_tc(const __grid_constant__ CUtensorMap tin, TcArgs p)
+__global__ void __launch_bounds__(kTcThreads, 1) k_conv3x3_tc(const __grid_constant__ CUtensorMap tin,
+                                                           const __grid_constant__ CUtensorMap tslab,
+                                                           const __grid_constant__ CUtensorMap thalo, TcArgs p)
 {
     extern __shared__ __align__(128) unsigned char smem[];
     __shared__ __align__(8) uint64_t s_full[kTcMaxStages], s_empty[kTcMaxStages], s_tfull[2], s_tempty[2];
@@ -425,10 +445,11 @@ __global__ void __launch_bounds__(kTcThreads, 1) k_conv3x3_tc(const __grid_const
     const int pack = p.pack;
     const uint32_t acc_cols = tc_acc_cols(pack, R, nt);  // one accumulator set
     const uint32_t tmem_cols = tc_tmem_cols(2 * acc_cols);
-    const int stage_bytes = tc_stage_bytes(nt, kc, R);
+    const int sa = p.sa;
+    const int stage_bytes = tc_stage_bytes(nt, kc, R, sa);
     // stages start on 1024-byte boundaries (the swizzle atoms)
     const uint32_t sbase = (smem_u32(smem) + 1023u) & ~1023u;
-    const int per_tile = 3 * p.nchunks;
+    const int per_tile = sa ? p.nchunks : 3 * p.nchunks;
 
     if (warp == 0) {
         asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(&s_tmem)),
@@ -469,7 +490,8 @@ __global__ void __launch_bounds__(kTcThreads, 1) k_conv3x3_tc(const __grid_const
     if (warp == 0) {
         if (lane == 0) {
             // ---------------- loads ----------------
-            const uint32_t a_bytes = (uint32_t)tc_a_bytes(kc, R), b_bytes = (uint32_t)tc_b_bytes(nt, kc);
+            const uint32_t a_bytes = (uint32_t)tc_a_bytes(kc, R, sa), b_bytes = (uint32_t)tc_b_bytes(nt, kc, sa);
+            const uint32_t slab = (uint32_t)tc_slab_bytes(kc, R);
             int s = 0;
             uint32_t phase = 0;
             bool first_lap = true;
@@ -485,14 +507,39 @@ __global__ void __launch_bounds__(kTcThreads, 1) k_conv3x3_tc(const __grid_const
                     const uint32_t st = sbase + (uint32_t)(s * stage_bytes);
                     const uint32_t bar = smem_u32(&s_full[s]);
                     mbar_expect_tx(bar, a_bytes + b_bytes);
-                    asm volatile(
-                        "cp.async.bulk.tensor.4d.shared::cluster.global.tile.mbarrier::complete_tx::bytes "
-                        "[%0], [%1, {%2, %3, %4, %5}], [%6];" ::"r"(st),
-                        "l"(reinterpret_cast<uint64_t>(&tin)), "r"(kc * chunk), "r"(tx * kTcM + dx - 1),
-                        "r"(y - 1), "r"(img), "r"(bar)
-                        : "memory");
-                    const bf16 *wsrc =
-                        p.wtc + (((size_t)slice * p.nchunks + chunk) * 3 + dx) * (size_t)(3 * nt * kc);
+                    const bf16 *wsrc;
+                    if (sa) {
+                        // slabs 1..16: pixel groups k = 0..15 (x = x0 + 16 j + k), then
+                        // slab 0 (k = -1: the left neighbours) and slab 17 (k = 16)
+                        const int c0 = kc * k, j0 = tx * (kTcM / 16);
+                        asm volatile(
+                            "cp.async.bulk.tensor.5d.shared::cluster.global.tile.mbarrier::complete_tx::bytes "
+                            "[%0], [%1, {%2, %3, %4, %5, %6}], [%7];" ::"r"(st + slab),
+                            "l"(reinterpret_cast<uint64_t>(&tslab)), "r"(c0), "r"(j0), "r"(y - 1), "r"(0), "r"(img),
+                            "r"(bar)
+                            : "memory");
+                        asm volatile(
+                            "cp.async.bulk.tensor.5d.shared::cluster.global.tile.mbarrier::complete_tx::bytes "
+                            "[%0], [%1, {%2, %3, %4, %5, %6}], [%7];" ::"r"(st),
+                            "l"(reinterpret_cast<uint64_t>(&thalo)), "r"(c0), "r"(j0 - 1), "r"(y - 1), "r"(15),
+                            "r"(img), "r"(bar)
+                            : "memory");
+                        asm volatile(
+                            "cp.async.bulk.tensor.5d.shared::cluster.global.tile.mbarrier::complete_tx::bytes "
+                            "[%0], [%1, {%2, %3, %4, %5, %6}], [%7];" ::"r"(st + 17u * slab),
+                            "l"(reinterpret_cast<uint64_t>(&thalo)), "r"(c0), "r"(j0 + 1), "r"(y - 1), "r"(0),
+                            "r"(img), "r"(bar)
+                            : "memory");
+                        wsrc = p.wtc + ((size_t)slice * p.nchunks + k) * (size_t)(9 * nt * kc);
+                    } else {
+                        asm volatile(
+                            "cp.async.bulk.tensor.4d.shared::cluster.global.tile.mbarrier::complete_tx::bytes "
+                            "[%0], [%1, {%2, %3, %4, %5}], [%6];" ::"r"(st),
+                            "l"(reinterpret_cast<uint64_t>(&tin)), "r"(kc * chunk), "r"(tx * kTcM + dx - 1),
+                            "r"(y - 1), "r"(img), "r"(bar)
+                            : "memory");
+                        wsrc = p.wtc + (((size_t)slice * p.nchunks + chunk) * 3 + dx) * (size_t)(3 * nt * kc);
+                    }
                     asm volatile(
                         "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
                             st + a_bytes),
@@ -516,7 +563,10 @@ __global__ void __launch_bounds__(kTcThreads, 1) k_conv3x3_tc(const __grid_const
         const uint32_t idesc_pack = (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(96 >> 3) << 17) |
                                     ((uint32_t)(kTcM >> 4) << 24);
         const uint64_t desc0 = umma_desc_sw(sbase, kc);
-        const uint32_t a16 = (uint32_t)tc_a_bytes(kc, R) >> 4, row16 = (uint32_t)tc_row_bytes(kc) >> 4;
+        const uint32_t slab = (uint32_t)tc_slab_bytes(kc, R);
+        const uint64_t sdesc0 = umma_desc_sw64_sbo(sbase, slab);  // shared A: 8-row groups one slab apart
+        const uint32_t slab16 = slab >> 4;
+        const uint32_t a16 = (uint32_t)tc_a_bytes(kc, R, sa) >> 4, row16 = (uint32_t)tc_row_bytes(kc) >> 4;
         const uint32_t tap16 = (uint32_t)(nt * kc * 2) >> 4, stage16 = (uint32_t)stage_bytes >> 4;
         const uint32_t leader = lane == 0 ? 1u : 0u;
         int s = 0;
@@ -539,42 +589,51 @@ __global__ void __launch_bounds__(kTcThreads, 1) k_conv3x3_tc(const __grid_const
                 asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
                 const uint64_t ad0 = desc0 + (uint64_t)((uint32_t)s * stage16);
                 const uint64_t bd0 = ad0 + a16;
-                if (pack) {
-                    // box row i, all three row taps: N = 96 at columns 32 (R + 1 - i)
+                // shared A: the stage is a whole chunk; column tap dx reads the
+                // 16 slabs from slab dx on (one slab = one pixel column shift)
+                const int ndx = sa ? 3 : 1;
+                const uint32_t arow16 = sa ? (uint32_t)(8 * kc * 2) >> 4 : row16;  // next image row
 #pragma unroll 1
-                    for (int i = 0; i < R + 2; ++i)
+                for (int dxi = 0; dxi < ndx; ++dxi) {
+                    const uint64_t aB = sa ? sdesc0 + (uint32_t)s * stage16 + (uint32_t)dxi * slab16 : ad0;
+                    const uint64_t bB = bd0 + (uint32_t)dxi * 3u * tap16;
+                    if (pack) {
+                        // box row i, all three row taps: N = 96 at columns 32 (R + 1 - i)
+#pragma unroll 1
+                        for (int i = 0; i < R + 2; ++i)
 #pragma unroll
-                        for (int kk = 0; kk < 2; ++kk) {
-                            const uint64_t ad = ad0 + (uint32_t)i * row16 + (uint32_t)(2 * kk);
-                            const uint64_t bd = bd0 + (uint32_t)(2 * kk);
-                            asm volatile(
-                                "{\n\t.reg .pred p, e;\n\t"
-                                "setp.ne.b32 e, %9, 0;\n\t"
-                                "setp.ne.b32 p, %4, 0;\n\t"
-                                "@e tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, {%5, %6, %7, %8}, p;\n\t}"
-                                :
-                                : "r"(d + 32u * (uint32_t)(R + 1 - i)), "l"(ad), "l"(bd), "r"(idesc_pack), "r"(1u),
-                                  "r"(0u), "r"(0u), "r"(0u), "r"(0u), "r"(leader));
+                            for (int kk = 0; kk < 2; ++kk) {
+                                const uint64_t ad = aB + (uint32_t)i * arow16 + (uint32_t)(2 * kk);
+                                const uint64_t bd = bB + (uint32_t)(2 * kk);
+                                asm volatile(
+                                    "{\n\t.reg .pred p, e;\n\t"
+                                    "setp.ne.b32 e, %5, 0;\n\t"
+                                    "setp.ne.b32 p, %4, 0;\n\t"
+                                    "@e tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}"
+                                    :
+                                    : "r"(d + 32u * (uint32_t)(R + 1 - i)), "l"(ad), "l"(bd), "r"(idesc_pack),
+                                      "r"(1u), "r"(leader));
+                            }
+                    }
+#pragma unroll 1
+                    for (int dy = 0; dy < 3 && !pack; ++dy)
+#pragma unroll
+                        for (int kk = 0; kk < 2; ++kk) {  // kc = 32: two K16 steps
+                            const uint64_t bd = bB + (uint32_t)dy * tap16 + (uint32_t)(2 * kk);
+                            const uint32_t accum = (k > 0 || dxi > 0 || dy > 0 || kk > 0) ? 1u : 0u;
+                            for (int r = 0; r < R; ++r) {
+                                const uint64_t ad = aB + (uint32_t)(r + dy) * arow16 + (uint32_t)(2 * kk);
+                                asm volatile(
+                                    "{\n\t.reg .pred p, e;\n\t"
+                                    "setp.ne.b32 e, %5, 0;\n\t"
+                                    "setp.ne.b32 p, %4, 0;\n\t"
+                                    "@e tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}"
+                                    :
+                                    : "r"(d + (uint32_t)r * ncols), "l"(ad), "l"(bd), "r"(idesc), "r"(accum),
+                                      "r"(leader));
+                            }
                         }
                 }
-#pragma unroll 1
-                for (int dy = 0; dy < 3 && !pack; ++dy)
-#pragma unroll
-                    for (int kk = 0; kk < 2; ++kk) {  // kc = 32: two K16 steps
-                        const uint64_t bd = bd0 + (uint32_t)dy * tap16 + (uint32_t)(2 * kk);
-                        const uint32_t accum = (k > 0 || dy > 0 || kk > 0) ? 1u : 0u;
-                        for (int r = 0; r < R; ++r) {
-                            const uint64_t ad = ad0 + (uint32_t)(r + dy) * row16 + (uint32_t)(2 * kk);
-                            asm volatile(
-                                "{\n\t.reg .pred p, e;\n\t"
-                                "setp.ne.b32 e, %9, 0;\n\t"
-                                "setp.ne.b32 p, %4, 0;\n\t"
-                                "@e tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, {%5, %6, %7, %8}, p;\n\t}"
-                                :
-                                : "r"(d + (uint32_t)r * ncols), "l"(ad), "l"(bd), "r"(idesc), "r"(accum), "r"(0u),
-                                  "r"(0u), "r"(0u), "r"(0u), "r"(leader));
-                        }
-                    }
                 if (leader)
                     asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
                                      smem_u32(&s_empty[s]))
@@ -637,7 +696,9 @@ __global__ void __launch_bounds__(kTcThreads, 1) k_conv3x3_tc(const __grid_const
             asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
             const int tx = t % p.tiles_x, trow = t / p.tiles_x;
             const int img = trow / p.tiles_y, y0 = (trow - img * p.tiles_y) * R;
-            const int x = tx * kTcM + q * 32 + lane;
+            // shared A keeps the tile's pixels in slab order: accumulator lane
+            // m = 32 q + lane holds pixel 16 (m % 8) + m / 8 of the tile
+            const int x = sa ? tx * kTcM + 16 * (lane & 7) + 4 * q + (lane >> 3) : tx * kTcM + q * 32 + lane;
             const int cbase = slice * nt;
             const uint32_t tbase = tmem + (uint32_t)acc * acc_cols + ((uint32_t)(q * 32) << 16);
             // slice i: row i / per_row, columns 32 (i % per_row) ..
@@ -1262,21 +1323,55 @@ int conv_tc(const bf16 *in, int cin, int h, int w, int n, const bf16 *wtc, const
     // stages fit in shared memory
     const int kc = tc_kc(cin);
     const int pack = nt == 32 ? 1 : 0;
-    int R = 8;
-    while (R > 1 && (2u * tc_acc_cols(pack, R, nt) > 512u || tc_stages(nt, kc, R) < 3 ||
-                     (long long)n * ((h + R - 1) / R) * tiles_x * ny < num_sms()))
-        R >>= 1;
-    SDP_CHECK_ARG(tc_stages(nt, kc, R) >= 2, "tensor-core convolution: %d output channels do not fit", nt);
-    CUtensorMap tmap;
+    auto choose_rows = [&](int sa, int min_stages) {
+        int rr = 8;
+        while (rr > 1 && (2u * tc_acc_cols(pack, rr, nt) > 512u || tc_stages(nt, kc, rr, sa) < min_stages ||
+                          (long long)n * ((h + rr - 1) / rr) * tiles_x * ny < num_sms()))
+            rr >>= 1;
+        return rr;
+    };
     const cuuint64_t dims[4] = {(cuuint64_t)cin, (cuuint64_t)w, (cuuint64_t)h, (cuuint64_t)n};
     const cuuint64_t strides[3] = {(cuuint64_t)cin * 2, (cuuint64_t)w * cin * 2, (cuuint64_t)h * w * cin * 2};
-    const cuuint32_t box[4] = {(cuuint32_t)kc, (cuuint32_t)kTcM, (cuuint32_t)(R + 2), 1};
-    const cuuint32_t estr[4] = {1, 1, 1, 1};
-    const CUresult r = enc(&tmap, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 4, const_cast<bf16 *>(in), dims, strides, box,
-                           estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
-                           kc == 64 ? CU_TENSOR_MAP_SWIZZLE_128B : CU_TENSOR_MAP_SWIZZLE_64B,
-                           CU_TENSOR_MAP_L2_PROMOTION_L2_128B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
-    if (r != CUDA_SUCCESS) return set_error(SDP_ERR_CUDA, "cuTensorMapEncodeTiled failed (%d)", (int)r);
+    const cuuint32_t estr[5] = {1, 1, 1, 1, 1};
+    // Shared A (one load of each chunk serves the three column taps): the
+    // tile's 128 pixels x0 + 16 j + k (j < 8, k < 16) are staged as slabs
+    // k = -1 .. 16 of 8 pixels (rows of KC channels), slab-major, so a shift
+    // of one pixel is one slab (8 rows, one 512-byte swizzle atom) and the
+    // MMA of column tap dx starts at slab dx.  Two 5-D tensor maps view the
+    // image as {C, j (16 pixels apart), y, k (1 pixel apart), n}: slabs 0..15
+    // of one tile in one box, the two neighbour slabs (k = 15 of the group to
+    // the left, k = 0 of the group to the right) in boxes of one slab; reads
+    // outside the image (j or y out of range) return zero.  Needs W % 16 == 0
+    // and nt <= 64 (the chunk's nine weight blocks share the stage).
+    int sa = (w % 16 == 0 && nt <= 64) ? 1 : 0;
+    int R = sa ? choose_rows(1, 2) : choose_rows(0, 3);
+    CUtensorMap tmap, tslab, thalo;
+    if (sa) {
+        const cuuint64_t d5[5] = {(cuuint64_t)cin, (cuuint64_t)(w / 16), (cuuint64_t)h, 16, (cuuint64_t)n};
+        const cuuint64_t s5[4] = {(cuuint64_t)cin * 2 * 16, (cuuint64_t)w * cin * 2, (cuuint64_t)cin * 2,
+                                  (cuuint64_t)h * w * cin * 2};
+        const cuuint32_t bslab[5] = {(cuuint32_t)kc, 8, (cuuint32_t)(R + 2), 16, 1};
+        const cuuint32_t bhalo[5] = {(cuuint32_t)kc, 8, (cuuint32_t)(R + 2), 1, 1};
+        const CUresult r1 = enc(&tslab, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 5, const_cast<bf16 *>(in), d5, s5, bslab,
+                                estr, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_64B,
+                                CU_TENSOR_MAP_L2_PROMOTION_L2_128B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+        const CUresult r2 = enc(&thalo, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 5, const_cast<bf16 *>(in), d5, s5, bhalo,
+                                estr, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_64B,
+                                CU_TENSOR_MAP_L2_PROMOTION_L2_128B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+        if (r1 != CUDA_SUCCESS || r2 != CUDA_SUCCESS) {  // the driver refused the view: one box per column tap
+            sa = 0;
+            R = choose_rows(0, 3);
+        }
+    }
+    SDP_CHECK_ARG(tc_stages(nt, kc, R, sa) >= 2, "tensor-core convolution: %d output channels do not fit", nt);
+    {
+        const cuuint32_t box[4] = {(cuuint32_t)kc, (cuuint32_t)kTcM, (cuuint32_t)(R + 2), 1};
+        const CUresult r = enc(&tmap, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 4, const_cast<bf16 *>(in), dims, strides, box,
+                               estr, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_64B,
+                               CU_TENSOR_MAP_L2_PROMOTION_L2_128B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+        if (r != CUDA_SUCCESS) return set_error(SDP_ERR_CUDA, "cuTensorMapEncodeTiled failed (%d)", (int)r);
+    }
+    if (!sa) tslab = thalo = tmap;  // unused
     TcArgs a;
     a.n = n;
     a.h = h;
@@ -1290,7 +1385,7 @@ int conv_tc(const bf16 *in, int cin, int h, int w, int n, const bf16 *wtc, const
     a.tiles_x = tiles_x;
     a.tiles_y = (h + R - 1) / R;
     a.ntiles = n * a.tiles_y * tiles_x;
-    a.stages = tc_stages(nt, kc, R);
+    a.stages = tc_stages(nt, kc, R, sa);
     a.wtc = wtc;
     a.bias = bias;
     a.mask = mask;
@@ -1298,11 +1393,12 @@ int conv_tc(const bf16 *in, int cin, int h, int w, int n, const bf16 *wtc, const
     a.relu = relu;
     a.err = err;
     a.pack = pack;
+    a.sa = sa;
     int per_slice = num_sms() / ny;
     if (per_slice < 1) per_slice = 1;
     if (per_slice > a.ntiles) per_slice = a.ntiles;
-    const size_t smem = (size_t)a.stages * tc_stage_bytes(nt, kc, R) + 1024;
-    k_conv3x3_tc<<<dim3((unsigned)per_slice, ny), kTcThreads, smem, st>>>(tmap, a);
+    const size_t smem = (size_t)a.stages * tc_stage_bytes(nt, kc, R, sa) + 1024;
+    k_conv3x3_tc<<<dim3((unsigned)per_slice, ny), kTcThreads, smem, st>>>(tmap, tslab, thalo, a);
     SDP_LAUNCH_CHECK();
     return SDP_OK;
 }
