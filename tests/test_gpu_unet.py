@@ -16,7 +16,9 @@ The convolutions run on the tcgen05 path (the default); the mma.sync path
 is compared with it.  Sizes cover partial tiles at every level (24 x 40:
 the deepest level is 3 x 5) and, at 3 x 256 x 256, several tiles per row,
 64-channel chunks and the two output-channel slices of the 384-channel data
-gradient.
+gradient; widths divisible by 16 take the shared staged input of the
+32/64-channel layers (16 x 16: one partial tile; 40 x 384: three tiles per
+row at the top level, partial tile rows, tile edges inside the image).
 """
 from __future__ import annotations
 
@@ -47,7 +49,7 @@ def _setup(sdp, n, c, h, w, seed, training=True):
     return net, p, x, torch.from_numpy(x).cuda(), rng
 
 
-@pytest.mark.parametrize("n,c,h,w", [(2, 3, 24, 40), (1, 1, 16, 16)])
+@pytest.mark.parametrize("n,c,h,w", [(2, 3, 24, 40), (1, 1, 16, 16), (2, 3, 40, 384)])
 def test_forward_matches_oracle(sdp, device, n, c, h, w):
     import torch
     net, p, x, xd, rng = _setup(sdp, n, c, h, w, 11 + h)
@@ -180,7 +182,7 @@ def test_training_lowers_loss(sdp, device):
     net.close()
 
 
-@pytest.mark.parametrize("n,c,h,w", [(2, 3, 24, 40), (1, 3, 128, 256)])
+@pytest.mark.parametrize("n,c,h,w", [(2, 3, 24, 40), (1, 3, 128, 256), (2, 3, 40, 384)])
 def test_tensor_paths_agree(sdp, device, n, c, h, w):
     """tcgen05 (tensor memory, TMA) and mma.sync convolutions: the same network
     gives the same outputs and gradients up to BF16 rounding of
