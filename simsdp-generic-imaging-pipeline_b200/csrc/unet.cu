@@ -934,25 +934,26 @@ __global__ void __launch_bounds__(256) k_bias_grad(const bf16 *__restrict__ dz, 
 // ----------------------------------------------------------------------------
 // Element-wise kernels (8 channels = one 16-byte vector per thread)
 // ----------------------------------------------------------------------------
-// x[n][y][x][0..31] = in[n][c][y][x] / scale[n] (c < cin), 0 above.
+// x[n][y][x][0..31] = in[n][c][y][x] / scale[n] (c < cin), 0 above.  Only
+// the 8-channel groups that hold input channels are written: the groups
+// above are the zeros the arena was cleared to, and nothing else writes x.
 __global__ void k_pack_input(int n, int cin, int h, int w, const float *__restrict__ in,
                              const float *__restrict__ scale, bf16 *__restrict__ x)
 {
     const long long npix = (long long)n * h * w;
+    const int groups = (cin + 7) / 8;
     for (long long p = blockIdx.x * (long long)blockDim.x + threadIdx.x; p < npix;
          p += (long long)gridDim.x * blockDim.x) {
         const long long img = p / ((long long)h * w), yx = p - img * h * w;
         const float inv = scale ? 1.0f / scale[img] : 1.0f;
-        float f[kInPad];
-#pragma unroll
-        for (int c = 0; c < kInPad; ++c) f[c] = 0.f;
-        for (int c = 0; c < cin; ++c) f[c] = in[(img * cin + c) * h * w + yx] * inv;
         uint4 *dst = reinterpret_cast<uint4 *>(x + p * kInPad);
-#pragma unroll
-        for (int k = 0; k < kInPad / 8; ++k) {
+        for (int k = 0; k < groups; ++k) {
             float g[8];
 #pragma unroll
-            for (int e = 0; e < 8; ++e) g[e] = f[8 * k + e];
+            for (int e = 0; e < 8; ++e) {
+                const int c = 8 * k + e;
+                g[e] = c < cin ? in[(img * cin + c) * h * w + yx] * inv : 0.f;
+            }
             dst[k] = pack8(g);
         }
     }
