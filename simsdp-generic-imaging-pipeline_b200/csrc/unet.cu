@@ -350,6 +350,12 @@ struct TcArgs {
     int *err;            // set to 1 when a bounded wait gave up
     int pack;            // packed row taps (nt = 32)
     int sa;              // shared A: one stage per chunk, pixels in slab order
+    // 1x1 head fused into the epilogue (nt = cout = 32: a thread holds all of a pixel's channels):
+    // head_out[p] = (sum_c bf16(out[p][c]) bf16(head_w[c]) + head_b[0]) * head_scale[image];
+    // head_only: the BF16 output itself is not stored
+    const float *head_w, *head_b, *head_scale;
+    float *head_out;
+    int head_only;
 };
 
 __host__ __device__ constexpr uint32_t tc_acc_cols(int pack, int rows, int nt)
@@ -437,9 +443,12 @@ __global__ void __launch_bounds__(kTcThreads, 1) k_conv3x3_tc(const __grid_const
     __shared__ uint32_t s_tmem;
     __shared__ int s_fail;
     __shared__ float s_bias[256];
+    __shared__ float s_hw[32];
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
     const int nt = p.nt, S = p.stages, kc = p.kc, R = p.rows;
     for (int i = tid; i < nt; i += blockDim.x) s_bias[i] = p.bias ? p.bias[blockIdx.y * nt + i] : 0.f;
+    if (p.head_out)
+        for (int i = tid; i < nt; i += blockDim.x) s_hw[i] = __bfloat162float(__float2bfloat16_rn(p.head_w[i]));
     const int slice = blockIdx.y;
     const uint32_t ncols = tc_ncols(nt);
     const int pack = p.pack;
@@ -712,6 +721,7 @@ __global__ void __launch_bounds__(kTcThreads, 1) k_conv3x3_tc(const __grid_const
                 if (!(x < p.w && y < p.h)) return;
                 const size_t pix = ((size_t)img * p.h + y) * p.w + x;
                 const int cg = cbase + c;
+                float hs = 0.f;  // fused head: channels in order (one 32-channel slice per pixel)
 #pragma unroll
                 for (int gi = 0; gi < 4; ++gi) {
                     float v[8];
@@ -729,7 +739,19 @@ __global__ void __launch_bounds__(kTcThreads, 1) k_conv3x3_tc(const __grid_const
                         for (int e = 0; e < 8; ++e)
                             if (!(m[e] > 0.f)) v[e] = 0.f;
                     }
-                    *reinterpret_cast<uint4 *>(p.out + pix * p.cout + cg + 8 * gi) = pack8(v);
+                    const uint4 pk = pack8(v);
+                    if (!p.head_only) *reinterpret_cast<uint4 *>(p.out + pix * p.cout + cg + 8 * gi) = pk;
+                    if (p.head_out) {
+                        float vb[8];
+                        unpack8(pk, vb);  // the BF16 values the head reads
+#pragma unroll
+                        for (int e = 0; e < 8; ++e) hs = fmaf(vb[e], s_hw[c + 8 * gi + e], hs);
+                    }
+                }
+                if (p.head_out) {
+                    hs += p.head_b[0];
+                    if (p.head_scale) hs *= p.head_scale[img];
+                    p.head_out[pix] = hs;
                 }
             };
             // slices half, half + 2, ...; two register sets: the next slice's
@@ -1310,8 +1332,15 @@ PFN_cuTensorMapEncodeTiled_v12000 tensor_map_encoder()
     return fn;
 }
 
+// The 1x1 head fused into a convolution's epilogue (see TcArgs).
+struct HeadFuse {
+    const float *w = nullptr, *b = nullptr, *scale = nullptr;
+    float *out = nullptr;
+    int only = 0;
+};
+
 int conv_tc(const bf16 *in, int cin, int h, int w, int n, const bf16 *wtc, const float *bias, const bf16 *mask,
-            bf16 *out, int cout, int relu, int *err, cudaStream_t st)
+            bf16 *out, int cout, int relu, int *err, cudaStream_t st, const HeadFuse *head = nullptr)
 {
     SDP_CHECK_ARG(cin % 32 == 0 && cout % 32 == 0, "tensor-core convolution: channels %d -> %d", cin, cout);
     auto enc = tensor_map_encoder();
@@ -1395,6 +1424,12 @@ int conv_tc(const bf16 *in, int cin, int h, int w, int n, const bf16 *wtc, const
     a.err = err;
     a.pack = pack;
     a.sa = sa;
+    a.head_w = head ? head->w : nullptr;
+    a.head_b = head ? head->b : nullptr;
+    a.head_scale = head ? head->scale : nullptr;
+    a.head_out = head ? head->out : nullptr;
+    a.head_only = head ? head->only : 0;
+    SDP_CHECK_ARG(!head || (ny == 1 && nt == 32), "head fusion needs 32 output channels");
     int per_slice = num_sms() / ny;
     if (per_slice < 1) per_slice = 1;
     if (per_slice > a.ntiles) per_slice = a.ntiles;
@@ -1407,12 +1442,13 @@ int conv_tc(const bf16 *in, int cin, int h, int w, int n, const bf16 *wtc, const
 // wk: [9][cout][cin] for the mma.sync kernel; wtc: the same weights in the
 // tensor-core staging order (the tensor-core path reads a plain input, in.cb == 0).
 int conv(const sdp_unet *u, VIn in, const bf16 *wk, const bf16 *wtc, const float *bias, const bf16 *mask, bf16 *out,
-         int cout, int relu, int n, cudaStream_t st)
+         int cout, int relu, int n, cudaStream_t st, const HeadFuse *head = nullptr)
 {
     if (u->tensor_path) {
         SDP_CHECK_ARG(in.cb == 0, "tensor-core convolution reads a materialised input");
-        return conv_tc(in.a, in.ca, in.h, in.w, n, wtc, bias, mask, out, cout, relu, u->err, st);
+        return conv_tc(in.a, in.ca, in.h, in.w, n, wtc, bias, mask, out, cout, relu, u->err, st, head);
     }
+    SDP_CHECK_ARG(!head, "the head is fused on the tensor-core path only");
     ConvArgs a;
     a.in = in;
     a.wk = wk;
@@ -1748,13 +1784,26 @@ SDP_EXPORT int sdp_unet_forward(sdp_unet *u, int n, int h, int w, const float *i
             cat_in = vin(u->cat[l], c + c1, nullptr, 0, hl, wl);
         }
         SDP_TRY(conv(u, cat_in, La.w, La.wtc, P + La.boff, nullptr, u->d[l][0], c, 1, n, st));
+        // the top level's last convolution also computes the 1x1 head in its
+        // epilogue on the tensor-core path (and, without training buffers,
+        // does not store its activations: nothing reads them)
+        HeadFuse hf;
+        const bool fuse = u->tensor_path && l == 0 && ch(u, 0) == 32;
+        if (fuse) {
+            hf.w = P + u->head_off;
+            hf.b = P + u->head_off + ch(u, 0);
+            hf.scale = scale;
+            hf.out = output;
+            hf.only = u->training ? 0 : 1;
+        }
         SDP_TRY(conv(u, vin(u->d[l][0], c, nullptr, 0, hl, wl), Lb.w, Lb.wtc, P + Lb.boff, nullptr, u->d[l][1], c,
-                     1, n,
-                     st));
+                     1, n, st, fuse ? &hf : nullptr));
     }
-    k_head_fwd<<<grid_for(np), 256, 0, st>>>(np, (long long)h * w, ch(u, 0), u->d[0][1], P + u->head_off,
-                                             P + u->head_off + ch(u, 0), scale, output);
-    SDP_LAUNCH_CHECK();
+    if (!(u->tensor_path && ch(u, 0) == 32)) {
+        k_head_fwd<<<grid_for(np), 256, 0, st>>>(np, (long long)h * w, ch(u, 0), u->d[0][1], P + u->head_off,
+                                                 P + u->head_off + ch(u, 0), scale, output);
+        SDP_LAUNCH_CHECK();
+    }
     u->n = n;
     u->h = h;
     u->w = w;
