@@ -547,7 +547,10 @@ int sdp_hogbom(const sdp_clean_params *p, float *residual_inout, const float *ps
  * the process exits), so grid_size is limited to 4096 (larger sizes return
  * SDP_ERR_RANGE).  It calls no cudaMalloc/cudaFree.  The first call on a
  * device looks up the array's device address (cudaGetSymbolAddress); make
- * that first call before any stream capture.  Every call clears the state
+ * that first call before any stream capture.  The address is cached with
+ * the id of the context it was found in, so after cudaDeviceReset (or any
+ * re-creation of the device's context) the next call looks it up again:
+ * make that call, too, outside stream capture.  Every call clears the state
  * it needs; calls that overlap on the GPU share the array and race, so
  * serialise them (one stream, or events). */
 int sdp_hogbom_noalloc(const sdp_clean_params *p, float *residual_inout, const float *psf, float *model_inout,
@@ -646,6 +649,13 @@ int sdp_unet_set_tensor_path(sdp_unet *net, int tcgen05);
 /* Blocking: SDP_ERR_TIMEOUT when a tensor-core convolution gave up a bounded
  * wait since the last check (its outputs are then incomplete), else SDP_OK. */
 int sdp_unet_check(sdp_unet *net, void *stream);
+/* No counterpart in the reference: the failure path of the tensor-core
+ * convolution.  Sets how many times its epilogue polls for a finished
+ * accumulator before it gives up (0: the default, about a second).  A tiny
+ * limit makes the wait run out on purpose: the kernel then drains the copies
+ * and MMAs it had issued, returns, and sdp_unet_check reports
+ * SDP_ERR_TIMEOUT; the outputs of that pass are incomplete. */
+int sdp_unet_set_wait_limit(sdp_unet *net, long long epilogue_polls);
 /* One Adam step on the master weights (bias-corrected moments). */
 int sdp_unet_adam_step(sdp_unet *net, float lr, float beta1, float beta2, float eps, void *stream);
 /* loss = mean over pixels of (b * (pred - target))^2, b the 3x3 binomial

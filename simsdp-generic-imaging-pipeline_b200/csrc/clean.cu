@@ -797,6 +797,8 @@ SDP_EXPORT int sdp_selftest_bounded_wait(int nblocks, long long spin_limit, int 
 // minor-cycle state and the per-block partial results live in the fixed
 // array below, one per GPU, kept until the process exits.
 // ---------------------------------------------------------------------------
+#include <cuda.h>
+
 #include <mutex>
 
 namespace sdp {
@@ -810,24 +812,70 @@ static_assert(sizeof(CleanState) <= kNoAllocStateBytes, "CLEAN state must fit it
 
 static __device__ __align__(256) unsigned char g_clean_scratch[kNoAllocScratchBytes];
 
+// The array's device address belongs to the context the module was loaded
+// into.  It is cached per device together with that context's unique id
+// (cuCtxGetId), so a context made again after cudaDeviceReset (or after the
+// primary context was released) gets a fresh lookup instead of the old,
+// dangling address.
+struct ScratchSlot {
+    unsigned long long ctx_id = 0;
+    void *addr = nullptr;
+};
 static std::mutex g_clean_scratch_mutex;
-static void *g_clean_scratch_addr[128];
+static ScratchSlot g_clean_scratch_slot[128];
 
-// Device address of g_clean_scratch on the current device, looked up once per
-// device (the host-side name of the array is not a device address).
+typedef CUresult (*CtxGetCurrentFn)(CUcontext *);
+typedef CUresult (*CtxGetIdFn)(CUcontext, unsigned long long *);
+
+// Unique id of the current context; *id = 0 when no context is current yet
+// (a thread whose first runtime call this is).
+static int current_context_id(unsigned long long *id)
+{
+    *id = 0;
+    static CtxGetCurrentFn get_current = nullptr;
+    static CtxGetIdFn get_id = nullptr;
+    if (!get_current || !get_id) {
+        void *f1 = nullptr, *f2 = nullptr;
+        cudaDriverEntryPointQueryResult q1, q2;
+        if (cudaGetDriverEntryPoint("cuCtxGetCurrent", &f1, cudaEnableDefault, &q1) != cudaSuccess ||
+            q1 != cudaDriverEntryPointSuccess ||
+            cudaGetDriverEntryPoint("cuCtxGetId", &f2, cudaEnableDefault, &q2) != cudaSuccess ||
+            q2 != cudaDriverEntryPointSuccess)
+            return set_error(SDP_ERR_CUDA, "cuCtxGetCurrent / cuCtxGetId unavailable");
+        get_current = reinterpret_cast<CtxGetCurrentFn>(f1);
+        get_id = reinterpret_cast<CtxGetIdFn>(f2);
+    }
+    CUcontext ctx = nullptr;
+    if (get_current(&ctx) != CUDA_SUCCESS) return set_error(SDP_ERR_CUDA, "cuCtxGetCurrent failed");
+    if (ctx == nullptr) return SDP_OK;
+    if (get_id(ctx, id) != CUDA_SUCCESS) return set_error(SDP_ERR_CUDA, "cuCtxGetId failed");
+    return SDP_OK;
+}
+
+// Device address of g_clean_scratch in the current device's context, looked
+// up on the first call in each context (the host-side name of the array is
+// not a device address).
 static int clean_scratch_address(void **out)
 {
     int dev = 0;
     SDP_CUDA_TRY(cudaGetDevice(&dev));
     if (dev < 0 || dev >= 128) return set_error(SDP_ERR_RANGE, "device ordinal %d beyond 127", dev);
     std::lock_guard<std::mutex> lock(g_clean_scratch_mutex);
-    if (g_clean_scratch_addr[dev] == nullptr) {
+    unsigned long long id = 0;
+    SDP_TRY(current_context_id(&id));
+    ScratchSlot &s = g_clean_scratch_slot[dev];
+    if (id == 0 || s.addr == nullptr || s.ctx_id != id) {
+        // the lookup also makes the device's primary context current when
+        // this thread had none; the id is read again afterwards
         void *p = nullptr;
         cudaError_t e = cudaGetSymbolAddress(&p, g_clean_scratch);
         if (e != cudaSuccess) return cuda_error(e, "cudaGetSymbolAddress(g_clean_scratch)");
-        g_clean_scratch_addr[dev] = p;
+        SDP_TRY(current_context_id(&id));
+        if (id == 0) return set_error(SDP_ERR_CUDA, "no current CUDA context after the symbol lookup");
+        s.addr = p;
+        s.ctx_id = id;
     }
-    *out = g_clean_scratch_addr[dev];
+    *out = s.addr;
     return SDP_OK;
 }
 

@@ -306,7 +306,9 @@ __global__ void __launch_bounds__(128) k_conv3x3(ConvArgs p)
 //     accumulator.  Two accumulators in tensor memory let the
 //     epilogue of one tile overlap the MMAs of the next.
 // Every wait is bounded: on timeout the CTA records the error and each role
-// leaves its loop (its later waits are bounded too).
+// leaves its loop (its later waits are bounded too); before the tensor memory
+// is released the CTA waits, again bounded, for the copies and MMAs it had
+// already issued (the drain at the end of the kernel).
 // ----------------------------------------------------------------------------
 constexpr int kTcM = 128;                       // pixels per tile
 constexpr int kTcMaxStages = 16;
@@ -348,6 +350,8 @@ struct TcArgs {
     bf16 *out;           // [n][h][w][cout]
     int relu;
     int *err;            // set to 1 when a bounded wait gave up
+    long long spins;     // polls of a bounded mbarrier wait (loads, MMAs, the drain)
+    long long epi_spins; // polls of the epilogue's wait for an accumulator
     int pack;            // packed row taps (nt = 32)
     int sa;              // shared A: one stage per chunk, pixels in slab order
     // 1x1 head fused into the epilogue (nt = cout = 32: a thread holds all of a pixel's channels):
@@ -403,9 +407,9 @@ __device__ __forceinline__ void tmem_zero32(uint32_t taddr)
         : "memory");
 }
 
-__device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity)
+__device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity, long long limit = kTcSpins)
 {
-    for (long long i = 0; i < kTcSpins; ++i) {
+    for (long long i = 0; i < limit; ++i) {
         uint32_t done;
         asm volatile(
             "{\n\t.reg .pred P1;\n\t"
@@ -439,9 +443,9 @@ __global__ void __launch_bounds__(kTcThreads, 1) k_conv3x3_tc(const __grid_const
                                                            const __grid_constant__ CUtensorMap thalo, TcArgs p)
 {
     extern __shared__ __align__(128) unsigned char smem[];
-    __shared__ __align__(8) uint64_t s_full[kTcMaxStages], s_empty[kTcMaxStages], s_tfull[2], s_tempty[2];
+    __shared__ __align__(8) uint64_t s_full[kTcMaxStages], s_empty[kTcMaxStages], s_tfull[2], s_tempty[2], s_drain;
     __shared__ uint32_t s_tmem;
-    __shared__ int s_fail;
+    __shared__ int s_fail, s_issued, s_consumed;
     __shared__ float s_bias[256];
     __shared__ float s_hw[32];
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
@@ -474,8 +478,11 @@ __global__ void __launch_bounds__(kTcThreads, 1) k_conv3x3_tc(const __grid_const
             mbar_init(smem_u32(&s_tfull[i]), 1);
             mbar_init(smem_u32(&s_tempty[i]), kTcEpiWarps);
         }
+        mbar_init(smem_u32(&s_drain), 1);
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
         s_fail = 0;
+        s_issued = 0;
+        s_consumed = 0;
     }
     asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
     __syncthreads();
@@ -504,12 +511,13 @@ __global__ void __launch_bounds__(kTcThreads, 1) k_conv3x3_tc(const __grid_const
             int s = 0;
             uint32_t phase = 0;
             bool first_lap = true;
+            int issued = 0;  // stage loads issued (their sequence numbers are 0 .. issued - 1)
             for (int t = first; t < p.ntiles && !*fail; t += step) {
                 const int tx = t % p.tiles_x, trow = t / p.tiles_x;
                 const int img = trow / p.tiles_y, y = (trow - img * p.tiles_y) * R;
                 for (int k = 0; k < per_tile; ++k) {
                     const int chunk = k / 3, dx = k - 3 * chunk;
-                    if (!first_lap && !mbar_wait(smem_u32(&s_empty[s]), phase ^ 1u)) {
+                    if (!first_lap && !mbar_wait(smem_u32(&s_empty[s]), phase ^ 1u, p.spins)) {
                         *fail = 1;
                         break;
                     }
@@ -554,6 +562,7 @@ __global__ void __launch_bounds__(kTcThreads, 1) k_conv3x3_tc(const __grid_const
                             st + a_bytes),
                         "l"(wsrc), "r"(b_bytes), "r"(bar)
                         : "memory");
+                    ++issued;
                     if (++s == S) {
                         s = 0;
                         phase ^= 1u;
@@ -561,6 +570,7 @@ __global__ void __launch_bounds__(kTcThreads, 1) k_conv3x3_tc(const __grid_const
                     }
                 }
             }
+            s_issued = issued;
         }
     } else if (warp == 1) {
         // ---------------- MMAs ----------------
@@ -581,9 +591,11 @@ __global__ void __launch_bounds__(kTcThreads, 1) k_conv3x3_tc(const __grid_const
         int s = 0;
         uint32_t phase = 0;
         int j = 0;
+        int consumed = 0;  // stage loads waited for (their MMAs issued and committed)
         for (int t = first; t < p.ntiles && !*fail; t += step, ++j) {
             const int acc = j & 1, use = j >> 1;
-            if (use > 0 && !__all_sync(0xffffffffu, mbar_wait(smem_u32(&s_tempty[acc]), (uint32_t)((use - 1) & 1)))) {
+            if (use > 0 &&
+                !__all_sync(0xffffffffu, mbar_wait(smem_u32(&s_tempty[acc]), (uint32_t)((use - 1) & 1), p.spins))) {
                 if (leader) *fail = 1;
                 break;
             }
@@ -591,10 +603,11 @@ __global__ void __launch_bounds__(kTcThreads, 1) k_conv3x3_tc(const __grid_const
             const uint32_t d = tmem + (uint32_t)acc * acc_cols;
             bool ok = true;
             for (int k = 0; k < per_tile; ++k) {
-                if (!__all_sync(0xffffffffu, mbar_wait(smem_u32(&s_full[s]), phase))) {
+                if (!__all_sync(0xffffffffu, mbar_wait(smem_u32(&s_full[s]), phase, p.spins))) {
                     ok = false;
                     break;
                 }
+                ++consumed;
                 asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
                 const uint64_t ad0 = desc0 + (uint64_t)((uint32_t)s * stage16);
                 const uint64_t bd0 = ad0 + a16;
@@ -663,6 +676,7 @@ __global__ void __launch_bounds__(kTcThreads, 1) k_conv3x3_tc(const __grid_const
                              : "memory");
             __syncwarp();
         }
+        if (leader) s_consumed = consumed;
     } else {
         // ---------------- epilogue (warps 2..9) ----------------
         const int q = warp & 3;           // tensor-memory lane quarter this warp may read
@@ -696,7 +710,7 @@ __global__ void __launch_bounds__(kTcThreads, 1) k_conv3x3_tc(const __grid_const
         for (int t = first; t < p.ntiles; t += step, ++j) {
             const int acc = j & 1, use = j >> 1;
             if (__any_sync(0xffffffffu, *fail != 0)) break;
-            bool ok = mbar_wait(smem_u32(&s_tfull[acc]), (uint32_t)(use & 1));
+            bool ok = mbar_wait(smem_u32(&s_tfull[acc]), (uint32_t)(use & 1), p.epi_spins);
             ok = __all_sync(0xffffffffu, ok);
             if (!ok) {
                 if (lane == 0) *fail = 1;
@@ -777,7 +791,29 @@ __global__ void __launch_bounds__(kTcThreads, 1) k_conv3x3_tc(const __grid_const
         }
     }
     __syncthreads();
-    if (*fail && tid == 0 && p.err) atomicExch(p.err, 1);
+    if (*fail) {
+        // A wait gave up and the roles left their loops early: before the
+        // tensor memory and the stages are released, let every copy and MMA
+        // already issued finish.  Loads issued but never waited for have the
+        // sequence numbers consumed .. issued - 1 (at most S of them, each in
+        // its own stage, so the stage barrier's current phase is that load's);
+        // one more commit arrives when every MMA issued so far has completed.
+        // These waits are bounded too.
+        if (tid == 0)
+            for (int k = s_consumed; k < s_issued; ++k)
+                if (!mbar_wait(smem_u32(&s_full[k % S]), (uint32_t)((k / S) & 1), p.spins)) break;
+        if (warp == 1) {
+            if (lane == 0) {
+                asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
+                                 smem_u32(&s_drain))
+                             : "memory");
+                mbar_wait(smem_u32(&s_drain), 0u, p.spins);
+            }
+            __syncwarp();
+        }
+        __syncthreads();
+        if (tid == 0 && p.err) atomicExch(p.err, 1);
+    }
     if (warp == 0) {
         asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
         asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(tmem_cols));
@@ -1269,6 +1305,7 @@ struct sdp_unet {
     bool have_forward = false;
     int tensor_path = 1;    // 1: tcgen05 convolutions, 0: mma.sync
     int *err = nullptr;     // device flag: a bounded wait gave up
+    long long epi_spins = 0;  // epilogue wait limit of the tensor-core kernel (0: the default)
     void *arena = nullptr;
 };
 
@@ -1340,7 +1377,8 @@ struct HeadFuse {
 };
 
 int conv_tc(const bf16 *in, int cin, int h, int w, int n, const bf16 *wtc, const float *bias, const bf16 *mask,
-            bf16 *out, int cout, int relu, int *err, cudaStream_t st, const HeadFuse *head = nullptr)
+            bf16 *out, int cout, int relu, int *err, long long epi_spins, cudaStream_t st,
+            const HeadFuse *head = nullptr)
 {
     SDP_CHECK_ARG(cin % 32 == 0 && cout % 32 == 0, "tensor-core convolution: channels %d -> %d", cin, cout);
     auto enc = tensor_map_encoder();
@@ -1422,6 +1460,8 @@ int conv_tc(const bf16 *in, int cin, int h, int w, int n, const bf16 *wtc, const
     a.out = out;
     a.relu = relu;
     a.err = err;
+    a.spins = kTcSpins;
+    a.epi_spins = epi_spins > 0 ? epi_spins : kTcSpins;
     a.pack = pack;
     a.sa = sa;
     a.head_w = head ? head->w : nullptr;
@@ -1446,7 +1486,7 @@ int conv(const sdp_unet *u, VIn in, const bf16 *wk, const bf16 *wtc, const float
 {
     if (u->tensor_path) {
         SDP_CHECK_ARG(in.cb == 0, "tensor-core convolution reads a materialised input");
-        return conv_tc(in.a, in.ca, in.h, in.w, n, wtc, bias, mask, out, cout, relu, u->err, st, head);
+        return conv_tc(in.a, in.ca, in.h, in.w, n, wtc, bias, mask, out, cout, relu, u->err, u->epi_spins, st, head);
     }
     SDP_CHECK_ARG(!head, "the head is fused on the tensor-core path only");
     ConvArgs a;
@@ -1660,6 +1700,14 @@ SDP_EXPORT int sdp_unet_set_tensor_path(sdp_unet *u, int tcgen05)
 {
     SDP_CHECK_ARG(u, "NULL handle");
     u->tensor_path = tcgen05 ? 1 : 0;
+    return SDP_OK;
+}
+
+SDP_EXPORT int sdp_unet_set_wait_limit(sdp_unet *u, long long epilogue_polls)
+{
+    SDP_CHECK_ARG(u, "NULL handle");
+    SDP_CHECK_ARG(epilogue_polls >= 0, "epilogue_polls %lld is negative", epilogue_polls);
+    u->epi_spins = epilogue_polls;
     return SDP_OK;
 }
 

@@ -26,6 +26,13 @@ LIB_PATH = HERE / "libsdp_b200.so"
 HEADER = HERE.parent / "include" / "sdp_b200.h"
 
 SDP_OK = 0
+SDP_ERR_INVALID = 1
+SDP_ERR_RANGE = 2
+SDP_ERR_CUDA = 3
+SDP_ERR_NOMEM = 4
+SDP_ERR_TIMEOUT = 5
+SDP_ERR_DATA = 6
+SDP_ERR_IO = 7
 SDP_DEGRID_NEAREST = 0
 SDP_DEGRID_CONV = 1
 SDP_GRID_STD = 0
@@ -870,6 +877,11 @@ class UNet:
     def check(self, stream=None):
         """Raises when a tensor-core convolution gave up a bounded wait."""
         check(self.lib.sdp_unet_check(self.handle, _stream(stream)), self.lib)
+
+    def set_wait_limit(self, epilogue_polls: int):
+        """Polls of the tensor-core epilogue's bounded wait (0: the default);
+        a tiny value makes the wait run out (the failure path)."""
+        check(self.lib.sdp_unet_set_wait_limit(self.handle, C.c_longlong(epilogue_polls)), self.lib)
 
     def adam_step(self, lr, beta1=0.9, beta2=0.999, eps=1e-8, stream=None):
         check(self.lib.sdp_unet_adam_step(self.handle, C.c_float(lr), C.c_float(beta1), C.c_float(beta2),

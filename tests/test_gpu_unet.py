@@ -204,3 +204,30 @@ def test_tensor_paths_agree(sdp, device, n, c, h, w):
                 (np.linalg.norm(res[True][1]) * np.linalg.norm(res[False][1])))
     assert cos >= 0.99
     net.close()
+
+
+def test_tensor_core_wait_timeout_is_reported_and_recoverable(sdp, device):
+    """The failure path of the tcgen05 convolution: with an epilogue wait
+    limit of one poll the epilogue gives up before the first accumulator is
+    ready; the kernel drains the copies and MMAs it had issued, returns, and
+    sdp_unet_check reports SDP_ERR_TIMEOUT.  With the default limit restored
+    the same forward pass gives the earlier output bit for bit (the context
+    is still usable and the convolutions are deterministic)."""
+    import torch
+    n, c, h, w = 1, 3, 128, 256
+    net, p, x, xd, rng = _setup(sdp, n, c, h, w, 61, training=False)
+    ref = torch.empty((n, h, w), dtype=torch.float32, device="cuda")
+    net.forward(xd, ref)
+    net.check()
+    net.set_wait_limit(1)
+    out = torch.empty_like(ref)
+    net.forward(xd, out)
+    with pytest.raises(sdp.SdpError) as e:
+        net.check()
+    assert e.value.status == sdp.SDP_ERR_TIMEOUT
+    net.set_wait_limit(0)
+    out.zero_()
+    net.forward(xd, out)
+    net.check()
+    np.testing.assert_array_equal(out.cpu().numpy(), ref.cpu().numpy())
+    net.close()
