@@ -1,22 +1,33 @@
 """Benchmark: visibilities gridded + degridded per second on B200.
 
-One step = one major-cycle visibility pass of the FFT imaging pipeline over
-every visibility of the workload: W-projection degridding of the model grid
-(convolutional, the value degridgrid.c:147-191 computes), subtraction from
-the measured visibilities (gains_apply_run.c:273-297) and W-projection
-gridding of the residual visibilities (degridgrid.c:69-125).  Workload: the
-256-antenna, 10 km log-spiral array, 120 time steps -> 3,916,800
-visibilities, 2048^2 grid, 17 w-planes of half support 4, oversampling 16
-(seeded synthetic data; no public dataset is used).
+One step = one major-cycle visibility pass over every visibility of the
+largest configuration (the 8192^2 workload): 512 antennas on a seeded 40 km
+log spiral, 16 channels over 100-200 MHz x 200 time steps, 16 x 26,163,200 =
+418,611,200 visibilities, one 8192^2 grid per channel, 64 w-planes of half
+support 4 (kernels generated on the GPU), oversampling 16.  Per visibility:
+W-projection degridding of the model grid (convolutional,
+degridgrid.c:147-191), subtraction from the measured value
+(gains_apply_run.c:273-297) and gridding of the residual
+(degridgrid.c:69-125); all channels in one persistent batched launch
+(sdp_visbatch).  Measured visibilities: the exact DFT of a seeded sky of
+1000 points and 50 Gaussians plus noise (no public dataset is used).
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl b200|reference]
 
-value: device-resident throughput (inputs in HBM, L2 flushed between timed
-steps, CUDA events, max over ranks).  e2e: the same pass through the
-reference-facing C ABI (std_degridding, subtract_from_measurements_finegrid,
-std_gridding) with pinned host buffers and the host<->device copies inside
-the timed region.  --impl reference times the reference's own actor code
-compiled from its sources (oracle/_ref) on the host cores.
+value: device-resident throughput (inputs in HBM, several GB, larger than
+L2; L2 also flushed between timed steps; CUDA events; max over ranks).
+Under torchrun the 16 channels are dealt to the ranks by visibility count
+(strong scaling: the total work is fixed); N > 1 adds the continuum exchange
+step (each rank sums its channels' residual grids, then one NCCL
+all-reduce).  e2e: the same pass through the reference-facing C ABI
+(std_degridding, subtract_from_measurements_finegrid, std_gridding per
+channel) with pinned host buffers and the host<->device copies inside the
+timed region.  --impl reference times the reference's own actor code
+compiled from its sources (oracle/_ref) on the host cores, on the same
+workload, over a stated per-channel sample.  Other blocks of the line: the
+single 2048^2 channel (3.9 M visibilities), the graph-captured major cycle
+with Hogbom, the 64-channel batch, learned proposals, the FFTs and gain
+calibration.
 """
 from __future__ import annotations
 
@@ -50,26 +61,70 @@ PROFILES = ROOT / "profiles"
 def parse():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=50)
-    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
-    ap.add_argument("--e2e-steps", type=int, default=3)
+    ap.add_argument("--e2e-steps", type=int, default=2)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-major-cycle", action="store_true")
+    ap.add_argument("--no-c2", action="store_true", help="skip the single 2048^2 channel block")
     ap.add_argument("--no-c3", action="store_true", help="skip the batched 64-channel pass")
-    ap.add_argument("--no-c5", action="store_true", help="skip the 8192^2 single-channel measurement")
     ap.add_argument("--no-c4", action="store_true", help="skip the learned-proposal comparison")
-    ap.add_argument("--c4-skies", type=int, default=16, help="held-out skies of the learned-proposal comparison")
-    ap.add_argument("--cpu-sample", type=int, default=200_000, help="visibilities per CPU-baseline step")
+    ap.add_argument("--no-extras", action="store_true", help="headline only (no FFT / calibration blocks)")
+    ap.add_argument("--c4-skies", type=int, default=100, help="held-out skies of the learned-proposal comparison")
+    ap.add_argument("--cpu-sample", type=int, default=1_000_000,
+                    help="visibilities per channel per step of the reference arm / CPU baseline")
     return ap.parse_args()
 
 
-def workload(rank: int):
-    """C2-shaped workload; each rank images its own frequency channel (weak
-    scaling by channel, the reference's spectral parallelism)."""
-    freq = 140e6 * (1.0 + 0.05 * rank)
-    return synth.make_workload("c2_2048", 256, 5000.0, "spiral", 120, 2048, 200, 1e-3, 1.0, 1e-4, 17, 4,
-                               freq_hz=freq, seed=2 + rank, compute_vis=False)
+# The 8192^2 workload: 512 antennas, 40 km log spiral, 200 time steps per
+# channel, 16 channels evenly spaced over 100-200 MHz.
+C5_CHANNELS = 16
+C5_F_LO, C5_F_HI = 100e6, 200e6
+C5_GRID, C5_PLANES, C5_HS, C5_OS = 8192, 64, 4, 16
+
+
+def c5_frequencies():
+    return [C5_F_LO + (C5_F_HI - C5_F_LO) * c / (C5_CHANNELS - 1) for c in range(C5_CHANNELS)]
+
+
+def c5_base():
+    """uvw of the top channel (200 MHz; the others are scaled copies, uvw in
+    wavelengths is proportional to frequency), the imaging geometry (cell
+    chosen so the longest baseline at 200 MHz reaches 0.9 of the half grid)
+    and the host kernel tables the reference arm uses."""
+    return synth.make_workload("c5_8192", 512, 20000.0, "spiral", 200, C5_GRID, 1, 1e-3, 1.0, 1e-4, C5_PLANES,
+                               C5_HS, C5_OS, freq_hz=C5_F_HI, seed=5, compute_vis=False)
+
+
+def c5_sky(cell: float, G: int, seed: int = 55):
+    """1000 points (log-uniform 1e-3-1 Jy) and 50 circular Gaussians (FWHM
+    2-10 pixels, log-uniform 1e-2-1 Jy) in the central half of the field, as
+    (l, m, flux, sigma) rows for sdp_dft_gauss."""
+    rng = np.random.default_rng(seed)
+    fov = cell * G
+    half = 0.25 * fov
+    pts = np.zeros((1000, 4))
+    pts[:, :2] = rng.uniform(-half, half, (1000, 2))
+    pts[:, 2] = np.exp(rng.uniform(math.log(1e-3), 0.0, 1000))
+    gau = np.zeros((50, 4))
+    gau[:, :2] = rng.uniform(-half, half, (50, 2))
+    gau[:, 2] = np.exp(rng.uniform(math.log(1e-2), 0.0, 50))
+    gau[:, 3] = np.exp(rng.uniform(math.log(2.0), math.log(10.0), 50)) * cell / (2.0 * math.sqrt(2.0 * math.log(2.0)))
+    return np.concatenate([pts, gau]).astype(np.float32)
+
+
+def snap_uvw_host(uvw: np.ndarray, G: int, OS: int, us: float) -> np.ndarray:
+    """Fine-grid snap of the uvw (degridgrid.c:24-25, 52-54) in numpy with the
+    reference's rounding (the reference arm's inputs)."""
+    u = uvw.astype(np.float64)
+    fx = np.trunc((u[:, 0] * us + G // 2) * OS + 0.5)
+    fy = np.trunc((u[:, 1] * us + G // 2) * OS + 0.5)
+    out = np.empty_like(uvw)
+    out[:, 0] = ((fx / OS - G // 2) / us).astype(np.float32)
+    out[:, 1] = ((fy / OS - G // 2) / us).astype(np.float32)
+    out[:, 2] = uvw[:, 2]
+    return out
 
 
 def algorithmic_bytes(n_vis: int, G: int) -> int:
@@ -173,61 +228,8 @@ class ClockSampler:
 # ---------------------------------------------------------------------------
 # Reference arm / CPU baseline: the reference's actors on the host cores
 # ---------------------------------------------------------------------------
-def cpu_reference_pass(w, uvw_c, model_grid, sample: int, threads: int):
-    """Runs std_degridding + subtract_from_measurements_finegrid + std_gridding
-    of the reference (compiled from its sources, oracle/_ref; the oracle port
-    when that is absent) on `sample` visibilities split over `threads` slices,
-    as the reference's SLICES schedule does, and returns (seconds, kind)."""
-    sys.path.insert(0, str(ROOT / "oracle"))
-    import oracle as O
-    G, OS = w.cfg.grid_size, w.cfg.oversampling
-    cfg = O.make_config(G, w.cfg.uv_scale, w.cfg.w_scale, OS)
-    if O.RefLib.available("f32", "fast"):
-        lib, kind = O.RefLib("f32", "fast"), "reference"
-    elif O.RefLib.available("f32"):
-        lib, kind = O.RefLib("f32"), "reference"
-    else:
-        lib, kind = None, "port"
-    o = O.Oracle("f32") if lib is None else None
-    idx = np.linspace(0, uvw_c.shape[0] - 1, sample).astype(np.int64)
-    uvw = np.ascontiguousarray(uvw_c[idx])
-    vis = np.ascontiguousarray(w.vis[idx])
-    slices = np.array_split(np.arange(sample), threads)
-
-    def run(sl):
-        u = np.ascontiguousarray(uvw[sl])
-        v = np.ascontiguousarray(vis[sl])
-        if lib is not None:
-            pred = lib.std_degridding(cfg, G, OS, w.dkernels, w.supports, model_grid, u)
-            delta = lib.subtract_finegrid(v, pred)
-            return lib.std_gridding(cfg, G, OS, w.gkernels, w.supports, u, delta)
-        pred = o.std_degridding(G, OS, w.dkernels, w.supports, model_grid, u, w.cfg.uv_scale, w.cfg.w_scale, False)
-        delta = o.subtract_vis(v, pred)
-        return o.std_gridding(G, OS, w.gkernels, w.supports, u, delta, w.cfg.uv_scale, w.cfg.w_scale)
-
-    # silence the reference's progress printf
-    devnull = os.open(os.devnull, os.O_WRONLY)
-    saved = os.dup(1)
-    sys.stdout.flush()
-    os.dup2(devnull, 1)
-    try:
-        t0 = time.perf_counter()
-        with ThreadPoolExecutor(max_workers=threads) as ex:
-            grids = list(ex.map(run, slices))
-        if lib is not None and len(grids) > 1:
-            lib.merge_grids(G, np.concatenate(grids, axis=0))
-        t1 = time.perf_counter()
-    finally:
-        sys.stdout.flush()
-        os.dup2(saved, 1)
-        os.close(saved)
-        os.close(devnull)
-    return t1 - t0, kind
-
-
 def cpu_threads() -> int:
-    """Host threads for the CPU arm: every core, up to 64 (each slice owns a
-    full G^2 grid, as in the reference's SLICES schedule)."""
+    """Host threads for the reference arm: every core, up to 64."""
     try:
         n = len(os.sched_getaffinity(0))
     except AttributeError:
@@ -235,58 +237,124 @@ def cpu_threads() -> int:
     return max(1, min(64, n))
 
 
+class ReferencePass:
+    """The reference's own actors (compiled from its sources, oracle/_ref;
+    the oracle restatement when that build is absent) on the host cores over
+    a per-channel sample of the 8192^2 workload: per channel one
+    std_degridding (as shipped: the kernel sum is computed and then replaced
+    by the nearest cell, degridgrid.c:193-200), subtract_from_measurements
+    and std_gridding into the channel's own grid (cleared by the reference,
+    degridgrid.c:73) -- the calls one channel's PREESM firing makes.  The
+    channels run on parallel host threads (up to one per channel); the model
+    grid is padded once outside the timed region."""
+
+    def __init__(self, base, sample_per_channel: int, threads: int, seed: int = 77):
+        sys.path.insert(0, str(ROOT / "oracle"))
+        import oracle as O
+        self.O = O
+        G, OS, us, ws = base.cfg.grid_size, base.cfg.oversampling, base.cfg.uv_scale, base.cfg.w_scale
+        self.G, self.OS = G, OS
+        self.cfg = O.make_config(G, us, ws, OS)
+        if O.RefLib.available("f32", "fast"):
+            self.lib, self.kind = O.RefLib("f32", "fast"), "reference"
+        elif O.RefLib.available("f32"):
+            self.lib, self.kind = O.RefLib("f32"), "reference"
+        else:
+            self.lib, self.kind = None, "port"
+            self.o = O.Oracle("f32")
+        self.base = base
+        self.threads = max(1, min(threads, C5_CHANNELS))
+        rng = np.random.default_rng(seed)
+        self.sample = min(sample_per_channel, base.num_vis)
+        model = (rng.standard_normal((G * G, 2)) * 1e-3).astype(np.float32)
+        self.model = self.lib.padded_grid(G, model) if self.lib else model
+        self.uvw, self.vis = [], []
+        for c, f in enumerate(c5_frequencies()):
+            idx = np.sort(rng.choice(base.num_vis, self.sample, replace=False))
+            u = base.uvw[idx] * np.float32(f / C5_F_HI)
+            self.uvw.append(snap_uvw_host(u, G, OS, us))
+            self.vis.append((0.1 * rng.standard_normal((self.sample, 2))).astype(np.float32))
+        self.grids = [np.empty((G * G, 2), np.float32) for _ in range(self.threads)]
+
+    def _channel(self, c: int, t: int, n: int):
+        b, G, OS = self.base, self.G, self.OS
+        u = self.uvw[c][:n]
+        v = self.vis[c][:n]
+        if self.lib is not None:
+            p = self.lib.std_degridding(self.cfg, G, OS, b.dkernels, b.supports, self.model, u, padded=True)
+            d = self.lib.subtract_finegrid(v, p)
+            self.lib.std_gridding(self.cfg, G, OS, b.gkernels, b.supports, u, d, out=self.grids[t])
+        else:
+            o = self.o
+            p = o.std_degridding(G, OS, b.dkernels, b.supports, self.model, u, b.cfg.uv_scale, b.cfg.w_scale, False)
+            d = o.subtract_vis(v, p)
+            self.grids[t][:] = o.std_gridding(G, OS, b.gkernels, b.supports, u, d, b.cfg.uv_scale, b.cfg.w_scale)
+
+    def run(self, n: int | None = None) -> float:
+        """One step over all 16 channels (n visibilities each); seconds."""
+        n = self.sample if n is None else min(n, self.sample)
+
+        def worker(t):
+            for c in range(t, C5_CHANNELS, self.threads):
+                self._channel(c, t, n)
+
+        # silence the reference's progress printf
+        devnull = os.open(os.devnull, os.O_WRONLY)
+        saved = os.dup(1)
+        sys.stdout.flush()
+        os.dup2(devnull, 1)
+        try:
+            t0 = time.perf_counter()
+            with ThreadPoolExecutor(max_workers=self.threads) as ex:
+                list(ex.map(worker, range(self.threads)))
+            t1 = time.perf_counter()
+        finally:
+            sys.stdout.flush()
+            os.dup2(saved, 1)
+            os.close(saved)
+            os.close(devnull)
+        return t1 - t0
+
+    def describe(self) -> str:
+        return (f"{self.sample} visibilities of each of the 16 channels per step ({C5_CHANNELS * self.sample} in "
+                f"all, a {self.sample / self.base.num_vis:.3f} sample), one std_degridding + subtract + std_gridding "
+                f"call per channel, {self.threads} host threads")
+
+
+def c5_config_name(n_vis_total: int) -> str:
+    return (f"c5_8192: 512 antennas, 40 km log spiral, 16 channels 100-200 MHz x 200 time steps, "
+            f"{n_vis_total} vis, G=8192 per channel, 64 w-planes hs=4 OS=16")
+
+
 def reference_arm(args):
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return 0
-    w = workload(0)
-    G = w.cfg.grid_size
+    base = c5_base()
     threads = cpu_threads()
-    rng = np.random.default_rng(5)
-    model_grid = (rng.standard_normal((G * G, 2)) * 1e-3).astype(np.float32)
-    uvw_c = snap_host(w)
-    sample = max(threads * 2000, args.cpu_sample)
+    ref = ReferencePass(base, args.cpu_sample, threads)
     for _ in range(max(0, args.warmup)):
-        cpu_reference_pass(w, uvw_c, model_grid, min(sample, 20_000), threads)
-    times = []
-    kind = "port"
-    for _ in range(args.steps):
-        t, kind = cpu_reference_pass(w, uvw_c, model_grid, sample, threads)
-        times.append(t)
+        ref.run(20_000)
+    times = [ref.run() for _ in range(args.steps)]
     t = statistics.mean(times)
-    value = sample / t
+    nvis = C5_CHANNELS * ref.sample
+    value = nvis / t
     line = {
         "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": t * 1e3, "higher_is_better": True,
-        "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-        "config": {"workload": f"{w.name}: {w.num_vis} vis, G=2048, 17 w-planes hs=4 OS=16; "
-                               f"bounded sample of {sample} vis per step", "degrid": "convolutional"},
-        "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": kind,
-                         "sample": f"{sample} visibilities of the workload per step, {threads} slices"},
+        "scaling": "strong", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "config": {"workload": c5_config_name(C5_CHANNELS * base.num_vis),
+                   "degrid": "the reference's std_degridding as shipped: kernel sum computed, then replaced by "
+                             "the nearest cell (degridgrid.c:193-200)",
+                   "sample": ref.describe()},
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": ref.threads, "kind": ref.kind,
+                         "sample": ref.describe()},
         "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line), flush=True)
     return 0
 
 
-def snap_host(w):
-    """Fine-grid snap of the uvw (degridgrid.c:24-25, 52-54), on the host in
-    numpy with the reference's rounding; used only to feed the CPU arm the
-    same coordinates the GPU arm grids."""
-    G, OS, us = w.cfg.grid_size, w.cfg.oversampling, w.cfg.uv_scale
-    u = w.uvw.astype(np.float64)
-    fx = np.trunc((u[:, 0] * us + G // 2) * OS + 0.5)
-    fy = np.trunc((u[:, 1] * us + G // 2) * OS + 0.5)
-    out = np.empty_like(w.uvw)
-    out[:, 0] = ((fx / OS - G // 2) / us).astype(np.float32)
-    out[:, 1] = ((fy / OS - G // 2) / us).astype(np.float32)
-    out[:, 2] = w.uvw[:, 2]
-    return out
-
-
-# ---------------------------------------------------------------------------
-# B200 arm
-# ---------------------------------------------------------------------------
 def c3_block(S, D, dev, reps: int = 5):
     """The batched multi-channel workload: the 256-antenna layout at 64
     channels over 100-200 MHz, seeded per-channel flag fractions of 0-60 %
@@ -361,70 +429,126 @@ def c3_block(S, D, dev, reps: int = 5):
     return out
 
 
-def c5_block(S, D, dev, reps: int = 3):
-    """One channel of the large g2g-scale workload: 512 antennas on a seeded
-    40 km log spiral, 200 time steps (26,163,200 visibilities), 8192^2 grid,
-    64 w-planes of half support 4 (kernels generated on the GPU), OS 16.
-    Times the plan build, the fused visibility pass and a whole major cycle
-    (graph; 200 Hogbom minor cycles on 8192^2, the one-launch-per-cycle
-    path)."""
-    import torch
+class C5Device:
+    """The 8192^2 workload's channels owned by this rank on the device: the
+    W-projection kernels generated on the GPU, per channel the scaled and
+    snapped uvw, measured visibilities (exact DFT of the sky + 0.1 mJy noise)
+    and a visibility plan of the autotuned shape (tuned on the top channel,
+    the widest uv coverage), all channels in one sdp_visbatch; one shared
+    model grid (the model image is channel independent; its grid is too) and
+    one residual grid per channel."""
 
-    w = synth.make_workload("c5_8192", 512, 20000.0, "spiral", 200, 8192, 1, 1e-3, 1.0, 1e-4, 64, 4,
-                            freq_hz=140e6, seed=5, compute_vis=False)
-    G, OS, N = w.cfg.grid_size, w.cfg.oversampling, w.num_vis
-    fov = w.cfg.cell_size * G
-    gk, dk, sup = D.wkernels_generate([4] * 64, OS, w.cfg.max_w, fov)
-    sup_h = sup.cpu().numpy()
-    wk_g = S.Device.wkernels(gk, sup, sup_h)
-    wk_d = S.Device.wkernels(dk, sup, sup_h)
-    uvw_raw = torch.from_numpy(w.uvw).to(dev)
-    uvw = torch.empty_like(uvw_raw)
-    D.correct_to_finegrid(G, OS, w.cfg.uv_scale, uvw_raw, uvw)
-    del uvw_raw
-    gen = torch.Generator(device=dev).manual_seed(23)
-    meas = 0.1 * torch.randn((N, 2), device=dev, generator=gen)
-
-    def ev_time(fn, n):
-        fn()
+    def __init__(self, S, D, dev, base, owned, tune: bool = True, keep_host: bool = True):
+        import torch
+        self.S, self.D, self.dev = S, D, dev
+        G, OS = base.cfg.grid_size, base.cfg.oversampling
+        us, ws, cell = base.cfg.uv_scale, base.cfg.w_scale, base.cfg.cell_size
+        self.G, self.OS, self.owned, self.cell = G, OS, list(owned), cell
+        fov = cell * G
+        self.gk, self.dk, self.sup = D.wkernels_generate([C5_HS] * C5_PLANES, OS, base.cfg.max_w, fov)
+        self.sup_h = self.sup.cpu().numpy()
+        self.wk_g = S.Device.wkernels(self.gk, self.sup, self.sup_h)
+        self.wk_d = S.Device.wkernels(self.dk, self.sup, self.sup_h)
+        sky = torch.from_numpy(c5_sky(cell, G)).to(dev)
+        gen = torch.Generator(device=dev).manual_seed(23)
+        # model grid: half the flux of the 1000 points on their pixels, to a grid
+        img = torch.zeros(G * G, dtype=torch.float32, device=dev)
+        px = torch.round(sky[:1000, :2] / cell).long() + G // 2
+        img.index_put_((px[:, 1] * G + px[:, 0],), 0.5 * sky[:1000, 2], accumulate=True)
+        work = torch.empty((G * G, 2), dtype=torch.float32, device=dev)
+        self.model = torch.empty((G * G, 2), dtype=torch.float32, device=dev)
+        D.image_to_grid(G, img, work, self.model)
+        del img, work
+        uvw_top = torch.from_numpy(base.uvw).to(dev)
+        freqs = c5_frequencies()
+        self.resid = torch.empty((max(1, len(owned)), G * G, 2), dtype=torch.float32, device=dev)
+        self.shape = None
+        self.tune = None
+        self.plans, self.counts, self.host = [], [], []
+        order = sorted(owned, key=lambda c: -freqs[c])  # the top channel first (autotuned on)
+        built = {}
+        for c in order:
+            uvw_raw = (uvw_top * (freqs[c] / C5_F_HI)).contiguous()
+            uvw = torch.empty_like(uvw_raw)
+            D.correct_to_finegrid(G, OS, us, uvw_raw, uvw)
+            meas = torch.empty((uvw.shape[0], 2), dtype=torch.float32, device=dev)
+            D.dft_gauss(sky, uvw_raw, meas)
+            meas += 1e-4 * torch.randn(meas.shape, device=dev, generator=gen)
+            del uvw_raw
+            if tune and self.shape is None:
+                t0 = time.perf_counter()
+                shape, ms, n = D.autotune(G, OS, us, ws, uvw, self.wk_g, self.wk_d, meas, self.model, self.resid[0],
+                                          reps=3)
+                self.shape = shape
+                self.tune = {"tile": shape.tile, "chunk": shape.chunk, "lanes": shape.lanes, "warps": shape.warps,
+                             "ms_per_pass_one_channel": ms, "shapes_timed": n, "seconds": time.perf_counter() - t0,
+                             "tuned_on": f"channel {c} ({freqs[c] / 1e6:.1f} MHz)"}
+            pl = D.plan(G, OS, us, ws, uvw, self.wk_g, self.wk_d, keep=(self.gk, self.dk, self.sup),
+                        options=self.shape)
+            pl.set_measured(meas)
+            host = (uvw.cpu().numpy(), meas.cpu().numpy()) if keep_host else None
+            built[c] = (pl, int(uvw.shape[0]), host)
+            del uvw, meas
+        del uvw_top
+        for c in self.owned:
+            pl, n, host = built[c]
+            self.plans.append(pl)
+            self.counts.append(n)
+            self.host.append(host)
         torch.cuda.synchronize()
-        ts = []
-        for _ in range(n):
-            a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-            a.record()
-            fn()
-            b.record()
-            torch.cuda.synchronize()
-            ts.append(a.elapsed_time(b))
-        return statistics.median(ts)
+        for pl in self.plans:
+            pl.check_flags()
+        self.batch = D.batch(self.plans) if self.plans else None
+        if self.batch is not None:
+            self.batch.set_grids([self.model] * len(self.plans), [self.resid[k] for k in range(len(self.plans))])
+        self.num_vis = sum(self.counts)
 
-    plans = []
-    t_plan = ev_time(lambda: plans.append(D.plan(G, OS, w.cfg.uv_scale, w.cfg.w_scale, uvw, wk_g, wk_d,
-                                                 keep=(uvw, gk, dk, sup))), 2)
-    for pl in plans[:-1]:
-        pl.close()
-    plan = plans[-1]
-    plan.set_measured(meas)
-    model = (1e-3 * torch.randn((G * G, 2), device=dev, generator=gen)).contiguous()
-    res = torch.empty_like(model)
-    t_pass = ev_time(lambda: plan.cycle(model, res, S.SDP_DEGRID_CONV), reps)
+    def cycle(self):
+        if self.batch is not None:
+            self.batch.cycle(self.S.SDP_DEGRID_CONV)
+
+    def close(self):
+        if self.batch is not None:
+            self.batch.close()
+        for pl in self.plans:
+            pl.close()
+        self.plans = []
+
+
+def c5_major_cycle_block(S, D, dev, c5: "C5Device", reps: int = 2):
+    """One channel of the 8192^2 workload through the whole device major
+    cycle (image -> grid FFT, fused pass, grid -> image FFT + taper, 200
+    Hogbom minor cycles; CUDA graph): time per cycle."""
+    import torch
+    k = len(c5.owned) - 1
+    pl = c5.plans[k]
+    G, OS = c5.G, c5.OS
+    uvw_h, meas_h = c5.host[k]
+    uvw = torch.from_numpy(uvw_h).to(dev)
+    meas = torch.from_numpy(meas_h).to(dev)
     prol = torch.empty(G // 2 + 1, dtype=torch.float32, device=dev)
     D.prolate_table(G, prol)
     psf = torch.empty(G * G, dtype=torch.float32, device=dev)
-    psf_max = D.psf_generate(plan, prol, psf)
-    del model, res
-    torch.cuda.empty_cache()
-    pcfg = S.PipelineConfig(G, OS, w.cfg.uv_scale, w.cfg.w_scale, w.cfg.cell_size, 200, 200, 0.1, 1.5, 0.0002,
-                            psf_max, S.SDP_DEGRID_CONV, S.SDP_COORD_F32, 0, 1)
-    pipe = D.pipeline(pcfg, uvw, meas, psf, wk_g, wk_d, keep=(uvw, gk, dk, sup))
-    t_cyc = ev_time(pipe.major_cycle, 2)
-    out = {"workload": "512 antennas 40 km spiral, 200 time steps, 26163200 vis, G=8192, 64 w-planes hs=4 "
-                       "OS=16 (kernels generated on the GPU)",
-           "ms_plan_build": t_plan, "ms_fused_pass": t_pass, "vis_per_s_fused_pass": N / (t_pass * 1e-3),
-           "ms_major_cycle": t_cyc, "cuda_graph": pipe.graph_active(), "minor_cycles": 200}
+    psf_max = D.psf_generate(pl, prol, psf)
+    geom = pl.geom
+    pcfg = S.PipelineConfig(G, OS, geom.uv_scale, geom.w_scale, c5.cell, 200, 200, 0.1, 1.5, 0.0002, psf_max,
+                            S.SDP_DEGRID_CONV, S.SDP_COORD_F32, 0, 1)
+    pipe = D.pipeline(pcfg, uvw, meas, psf, c5.wk_g, c5.wk_d, keep=(uvw, c5.gk, c5.dk, c5.sup))
+    pipe.major_cycle()
+    torch.cuda.synchronize()
+    ts = []
+    for _ in range(reps):
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record()
+        pipe.major_cycle()
+        b.record()
+        torch.cuda.synchronize()
+        ts.append(a.elapsed_time(b))
+    out = {"channel": c5.owned[k], "vis": int(uvw.shape[0]), "ms_major_cycle": float(statistics.median(ts)),
+           "cuda_graph": pipe.graph_active(), "minor_cycles": 200,
+           "stages": "image->grid FFT, fused degrid/subtract/grid, grid->image FFT + taper, Hogbom x200"}
     pipe.close()
-    plan.close()
-    del psf, meas, uvw
+    del psf, uvw, meas
     torch.cuda.empty_cache()
     return out
 
@@ -674,6 +798,120 @@ def c4_learned_block(S, D, dev, skies: int):
     }
 
 
+def c2_block(S, D, dev, args, clocks_mhz=None):
+    """The single 2048^2 channel (256 antennas, 10 km log spiral, 120 time
+    steps: 3,916,800 visibilities; 17 w-planes hs=4, OS 16): the fused pass
+    with the autotuned plan shape (CUDA events, L2 flushed between passes),
+    its roofline figures, the graph-captured major cycle with 200 Hogbom
+    minor cycles, and the time to the plain pipeline's lowest residual RMS."""
+    import torch
+    stream = torch.cuda.current_stream()
+    w = synth.make_workload("c2_2048", 256, 5000.0, "spiral", 120, 2048, 200, 1e-3, 1.0, 1e-4, 17, 4,
+                            freq_hz=140e6, seed=2, compute_vis=False)
+    G, OS, N = w.cfg.grid_size, w.cfg.oversampling, w.num_vis
+    uvw_raw = torch.from_numpy(w.uvw).to(dev)
+    uvw = torch.empty_like(uvw_raw)
+    D.correct_to_finegrid(G, OS, w.cfg.uv_scale, uvw_raw, uvw)
+    gk = torch.from_numpy(w.gkernels).to(dev)
+    dk = torch.from_numpy(w.dkernels).to(dev)
+    sup = torch.from_numpy(w.supports).to(dev)
+    wk_g = S.Device.wkernels(gk, sup, w.supports)
+    wk_d = S.Device.wkernels(dk, sup, w.supports)
+    sky = torch.from_numpy(w.sky.astype(np.float32)).to(dev)
+    measured = torch.empty((N, 2), dtype=torch.float32, device=dev)
+    D.dft(sky, uvw, measured)
+    gen = torch.Generator(device=dev).manual_seed(17)
+    measured += 1e-4 * torch.randn(measured.shape, device=dev, generator=gen)
+    model_img = torch.zeros(G * G, dtype=torch.float32, device=dev)
+    pix = torch.randint(G // 4, 3 * G // 4, (200, 2), device=dev, generator=gen)
+    model_img[pix[:, 1] * G + pix[:, 0]] = torch.rand(200, device=dev, generator=gen)
+    work = torch.empty((G * G, 2), dtype=torch.float32, device=dev)
+    model_grid = torch.empty((G * G, 2), dtype=torch.float32, device=dev)
+    D.image_to_grid(G, model_img, work, model_grid)
+    residual = torch.empty((G * G, 2), dtype=torch.float32, device=dev)
+    t_tune = time.perf_counter()
+    shape, tuned_ms, n_shapes = D.autotune(G, OS, w.cfg.uv_scale, w.cfg.w_scale, uvw, wk_g, wk_d, measured,
+                                          model_grid, residual, reps=5)
+    tune = {"tile": shape.tile, "chunk": shape.chunk, "lanes": shape.lanes, "warps": shape.warps,
+            "ms_per_pass": tuned_ms, "shapes_timed": n_shapes, "seconds": time.perf_counter() - t_tune}
+    plan = D.plan(G, OS, w.cfg.uv_scale, w.cfg.w_scale, uvw, wk_g, wk_d, keep=(uvw, gk, dk, sup), options=shape)
+    plan.set_measured(measured)
+    flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device=dev)
+    for _ in range(3):
+        plan.cycle(model_grid, residual, S.SDP_DEGRID_CONV)
+    torch.cuda.synchronize()
+    plan.check_flags()
+    ts = []
+    for _ in range(max(5, args.steps)):
+        flush.zero_()
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record(stream)
+        plan.cycle(model_grid, residual, S.SDP_DEGRID_CONV)
+        b.record(stream)
+        torch.cuda.synchronize()
+        ts.append(a.elapsed_time(b))
+    t = statistics.mean(ts)
+    taps = (2 * w.half_support) ** 2
+    out = {"workload": f"{w.name}: 256 antennas, 10 km log spiral, 120 time steps, {N} vis, G=2048, "
+                       f"17 w-planes hs=4 OS=16", "ms_fused_pass": t, "vis_per_s": N / (t * 1e-3),
+           "plan_shape": tune, "algorithmic_bytes": algorithmic_bytes(N, G),
+           "achieved_gbs": algorithmic_bytes(N, G) / (t * 1e-3) / 1e9,
+           "fp32_tflops": algorithmic_flops(N, taps) / (t * 1e-3) / 1e12,
+           "traffic": read_traffic("k_vis_fast_cycle_c2_2048")}
+    del flush
+    if not args.no_major_cycle:
+        ones = torch.zeros((N, 2), dtype=torch.float32, device=dev)
+        ones[:, 0] = 1.0
+        pgrid = torch.empty((G * G, 2), dtype=torch.float32, device=dev)
+        plan.grid(ones, pgrid)
+        prol = torch.empty(G // 2 + 1, dtype=torch.float32, device=dev)
+        D.prolate_table(G, prol)
+        psf = torch.empty(G * G, dtype=torch.float32, device=dev)
+        D.grid_to_image(G, pgrid, prol, work, psf)
+        psf_max = float(psf.max().item())
+        psf /= psf_max
+        del ones, pgrid
+        pcfg = S.PipelineConfig(G, OS, w.cfg.uv_scale, w.cfg.w_scale, w.cfg.cell_size, 200, 200, 0.1, 1.5, 0.0002,
+                                psf_max, S.SDP_DEGRID_CONV, S.SDP_COORD_F32, 0, 1)
+        pl = D.pipeline(pcfg, uvw, measured, psf, wk_g, wk_d, keep=(uvw, gk, dk, sup))
+        for _ in range(2):
+            pl.major_cycle()
+        torch.cuda.synchronize()
+        n_cyc = 5
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(n_cyc):
+            pl.major_cycle()
+        e1.record(stream)
+        torch.cuda.synchronize()
+        t_cyc = e0.elapsed_time(e1) / n_cyc
+        major = {"ms_per_major_cycle": t_cyc, "vis_per_s": N / (t_cyc * 1e-3), "minor_cycles": 200,
+                 "cuda_graph": pl.graph_active(), "graph_error": pl.graph_error(),
+                 "stages": "image->grid FFT, fused degrid/subtract/grid, grid->image FFT + taper, Hogbom x200"}
+        pl.close()
+        pl = D.pipeline(pcfg, uvw, measured, psf, wk_g, wk_d, keep=(uvw, gk, dk, sup))
+        ms, rms = [], []
+        for _ in range(12):
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            pl.major_cycle()
+            e1.record(stream)
+            torch.cuda.synchronize()
+            ms.append(e0.elapsed_time(e1))
+            rms.append(pl.residual_rms())
+        target = 1.01 * min(rms)
+        k = next(i for i, r in enumerate(rms) if r <= target)
+        major["time_to_rms"] = {"target": "1.01 x the lowest FP64 residual RMS of 12 plain cycles",
+                                "cycles": k + 1, "ms": float(sum(ms[:k + 1])),
+                                "rms_per_cycle": [float(r) for r in rms]}
+        pl.close()
+        out["major_cycle"] = major
+    plan.close()
+    del work, residual, model_grid, measured, uvw
+    torch.cuda.empty_cache()
+    return out
+
+
 def b200_arm(args):
     import torch
     import torch.distributed as dist
@@ -693,56 +931,35 @@ def b200_arm(args):
     A = S.Actors(lib)
     stream = torch.cuda.current_stream()
 
-    w = workload(rank)
-    G, OS, NK = w.cfg.grid_size, w.cfg.oversampling, w.cfg.num_kernels
-    N = w.num_vis
-    taps = (2 * w.half_support) ** 2
-
-    # ---- device-resident inputs -------------------------------------------------------
-    uvw_raw = torch.from_numpy(w.uvw).to(dev)
-    uvw = torch.empty_like(uvw_raw)
-    D.correct_to_finegrid(G, OS, w.cfg.uv_scale, uvw_raw, uvw)
-    gk = torch.from_numpy(w.gkernels).to(dev)
-    dk = torch.from_numpy(w.dkernels).to(dev)
-    sup = torch.from_numpy(w.supports).to(dev)
-    wk_g = S.Device.wkernels(gk, sup, w.supports)
-    wk_d = S.Device.wkernels(dk, sup, w.supports)
-    # measured visibilities: DFT of the 200-point sky on the GPU plus noise
-    sky = torch.from_numpy(w.sky.astype(np.float32)).to(dev)
-    measured = torch.empty((N, 2), dtype=torch.float32, device=dev)
-    D.dft(sky, uvw, measured)
-    gen = torch.Generator(device=dev).manual_seed(17 + rank)
-    measured += 1e-4 * torch.randn(measured.shape, device=dev, generator=gen)
-    # model: 200 CLEAN-like components on the image, to a model grid
-    model_img = torch.zeros(G * G, dtype=torch.float32, device=dev)
-    pix = torch.randint(G // 4, 3 * G // 4, (200, 2), device=dev, generator=gen)
-    model_img[pix[:, 1] * G + pix[:, 0]] = torch.rand(200, device=dev, generator=gen)
-    work = torch.empty((G * G, 2), dtype=torch.float32, device=dev)
-    model_grid = torch.empty((G * G, 2), dtype=torch.float32, device=dev)
-    D.image_to_grid(G, model_img, work, model_grid)
-    residual = torch.empty((G * G, 2), dtype=torch.float32, device=dev)
-    # plan shape from the autotuner (tile side, visibilities per work item,
-    # lanes per visibility), timed on this workload's own fused pass
-    t_tune = time.perf_counter()
-    shape, tuned_ms, n_shapes = D.autotune(G, OS, w.cfg.uv_scale, w.cfg.w_scale, uvw, wk_g, wk_d, measured,
-                                          model_grid, residual, reps=5)
-    tune = {"tile": shape.tile, "chunk": shape.chunk, "lanes": shape.lanes or "from support",
-            "ms_per_pass": tuned_ms, "shapes_timed": n_shapes, "seconds": time.perf_counter() - t_tune,
-            "default": {"tile": 32, "chunk": 1024}}
-    plan = D.plan(G, OS, w.cfg.uv_scale, w.cfg.w_scale, uvw, wk_g, wk_d, keep=(uvw, gk, dk, sup), options=shape)
-    plan.set_measured(measured)
-    plan.check_flags()
-    n_items = plan.num_work_items()
-    flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device=dev)  # 256 MB > L2
+    # ---- the 8192^2 workload: this rank's channels on the device ---------------------
+    base = c5_base()
+    G, OS = base.cfg.grid_size, base.cfg.oversampling
+    counts_all = [base.num_vis] * C5_CHANNELS
+    owned = channels.assign_channels(counts_all, world)[rank]
+    total_vis = int(sum(counts_all))
+    t0 = time.perf_counter()
+    c5 = C5Device(S, D, dev, base, owned, tune=True, keep_host=True)
+    setup_s = time.perf_counter() - t0
+    n_items = c5.batch.num_work_items() if c5.batch is not None else 0
+    tune = c5.tune
+    cont = torch.empty((G * G, 2), dtype=torch.float32, device=dev) if world > 1 else None
 
     def step():
-        plan.cycle(model_grid, residual, S.SDP_DEGRID_CONV)
+        c5.cycle()
+        if world > 1:  # the continuum exchange: this rank's channel sum, all-reduced
+            if c5.plans:
+                D.merge_grids(G, len(c5.plans), c5.resid, cont)
+            else:
+                cont.zero_()
+            channels.continuum_sum_(cont)
 
+    flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device=dev)  # 256 MB > L2
     clocks = ClockSampler(local).__enter__()
     for _ in range(max(3, args.warmup)):
         step()
     torch.cuda.synchronize()
-    plan.check_flags()
+    for pl in c5.plans:
+        pl.check_flags()
 
     # ---- timed region (device) ---------------------------------------------------------
     starts = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
@@ -758,192 +975,159 @@ def b200_arm(args):
         ends[i].record(stream)
     torch.cuda.synchronize()
     clocks.mark(1)
-    clocks.__exit__(None, None, None)
     if world > 1:
         dist.barrier()
-    step_ms = [s.elapsed_time(e) for s, e in zip(starts, ends)]
-    t_step = sum(step_ms) / len(step_ms)
-    t_step = channels.max_over_ranks(t_step, device=dev)
-    value = world * N / (t_step * 1e-3)
+    step_ms = [a.elapsed_time(b) for a, b in zip(starts, ends)]
+    t_rank = sum(step_ms) / len(step_ms)
+    t_step = channels.max_over_ranks(t_rank, device=dev)
+    value = total_vis / (t_step * 1e-3)
 
-    # ---- roofline of the dominant kernel (the fused tile kernel) -----------------------
-    alg_bytes = algorithmic_bytes(N, G)
-    achieved = alg_bytes / (t_step * 1e-3) / 1e9
+    # ---- roofline of the dominant kernel: the batched fused pass of this rank --------
+    taps = (2 * C5_HS) ** 2
+    alg_bytes = sum(algorithmic_bytes(n, G) for n in c5.counts)
+    alg_flops = sum(algorithmic_flops(n, taps) for n in c5.counts)
+    t_pass = t_rank  # N = 1: the step is the pass (residual-grid clears + one k_vis_fast_batch launch)
+    if world > 1:
+        ts = []
+        for _ in range(3):
+            a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            a.record(stream)
+            c5.cycle()
+            b.record(stream)
+            torch.cuda.synchronize()
+            ts.append(a.elapsed_time(b))
+        t_pass = statistics.mean(ts)
+    achieved = alg_bytes / (t_pass * 1e-3) / 1e9
     peaks = {}
     pf = ROOT / "MEASURED_PEAKS.json"
     if pf.exists():
         peaks = json.loads(pf.read_text())
     peak = float(peaks.get("hbm_gbs", 6650.0))
     peak_src = "measured" if "hbm_gbs" in peaks else "fallback"
-    traffic = read_traffic("k_tiles_cycle_conv_c2_2048")
-    # the unit that binds this kernel: the shared-memory data pipe, one
-    # wavefront per SM per clock (wavefronts per launch from the committed
-    # ncu summary; clock: the median SM clock sampled in the timed region)
-    wf = read_profile_value("k_tiles_cycle_conv_c2_2048", "shared_wavefronts_per_launch")
-    binding = None
+    traffic = read_traffic("k_vis_fast_batch_c5_8192")
+    csum = clocks.summary()
+    clocks.__exit__(None, None, None)
+    sms = torch.cuda.get_device_properties(dev).multi_processor_count
+    sm_mhz = float(csum["sm_mhz"]) if csum.get("sm_mhz") else 1965.0
+    fp32_peak = sms * 128 * 2 * sm_mhz * 1e6 / 1e12
+    binding = {"fp32": {"achieved_tflops": alg_flops / (t_pass * 1e-3) / 1e12, "peak_tflops": fp32_peak,
+                        "frac": alg_flops / (t_pass * 1e-3) / 1e12 / fp32_peak,
+                        "peak_source": f"{sms} SMs x 128 FP32 lanes x 2 x the median SM clock in the timed region"}}
+    wf = read_profile_value("k_vis_fast_batch_c5_8192", "shared_wavefronts_per_launch")
+    if wf is not None:
+        peak_wf = sms * sm_mhz * 1e6
+        binding["shared_memory"] = {"achieved_wavefronts_per_s": wf / (t_pass * 1e-3), "peak": peak_wf,
+                                    "frac": wf / (t_pass * 1e-3) / peak_wf, "per_launch": wf,
+                                    "peak_source": f"{sms} SMs x 1 wavefront per clock x the median SM clock"}
 
-    # ---- whole major cycle (device pipeline, CUDA graph): image->grid, fused
-    #      vis pass, grid->image, 200 Hogbom minor cycles ---------------------------------
-    major = None
-    if not args.no_major_cycle:
-        ones = torch.zeros((N, 2), dtype=torch.float32, device=dev)
-        ones[:, 0] = 1.0
-        pgrid = torch.empty((G * G, 2), dtype=torch.float32, device=dev)
-        plan.grid(ones, pgrid)
-        prol = torch.empty(G // 2 + 1, dtype=torch.float32, device=dev)
-        D.prolate_table(G, prol)
-        psf = torch.empty(G * G, dtype=torch.float32, device=dev)
-        D.grid_to_image(G, pgrid, prol, work, psf)
-        psf_max = float(psf.max().item())
-        psf /= psf_max
-        del ones, pgrid
-        pcfg = S.PipelineConfig(G, OS, w.cfg.uv_scale, w.cfg.w_scale, w.cfg.cell_size, 200, 200, 0.1, 1.5, 0.0002,
-                                psf_max, S.SDP_DEGRID_CONV, S.SDP_COORD_F32, 0, 1)
-        pl = D.pipeline(pcfg, uvw, measured, psf, wk_g, wk_d, keep=(uvw, gk, dk, sup))
-        for _ in range(2):
-            pl.major_cycle()
-        torch.cuda.synchronize()
-        n_cyc = max(2, min(5, args.steps))
-        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        e0.record(stream)
-        for _ in range(n_cyc):
-            pl.major_cycle()
-        e1.record(stream)
-        torch.cuda.synchronize()
-        t_cyc = e0.elapsed_time(e1) / n_cyc
-        major = {"ms_per_major_cycle": t_cyc, "vis_per_s": N / (t_cyc * 1e-3), "minor_cycles": 200,
-                 "cuda_graph": pl.graph_active(), "graph_error": pl.graph_error(),
-                 "stages": "image->grid FFT, fused degrid/subtract/grid, grid->image FFT + taper, Hogbom x200"}
-        pl.close()
-        # time to the target residual RMS (plain Hogbom pipeline): from an empty
-        # model, cycles until the FP64 residual RMS is within 1 % of the lowest
-        # reached in 12 cycles
-        pl = D.pipeline(pcfg, uvw, measured, psf, wk_g, wk_d, keep=(uvw, gk, dk, sup))
-        ms, rms = [], []
-        for _ in range(12):
-            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-            e0.record(stream)
-            pl.major_cycle()
-            e1.record(stream)
-            torch.cuda.synchronize()
-            ms.append(e0.elapsed_time(e1))
-            rms.append(pl.residual_rms())
-        target = 1.01 * min(rms)
-        k = next(i for i, r in enumerate(rms) if r <= target)
-        major["time_to_rms"] = {"target": "1.01 x the lowest FP64 residual RMS of 12 plain cycles",
-                                "cycles": k + 1, "ms": float(sum(ms[:k + 1])),
-                                "rms_per_cycle": [float(r) for r in rms],
-                                "learned": "c4_learned (the reference's FFT-pipeline prediction does not converge; "
-                                           "the learned comparison runs on the DFT-predict major cycle)"}
-        pl.close()
+    # ---- e2e through the reference-facing C ABI with pinned host buffers -----------
+    e2e = None
+    if c5.plans:
+        gk_h, dk_h, sup_h = c5.gk.cpu().numpy(), c5.dk.cpu().numpy(), c5.sup_h
+        cfg = S.make_config(G, base.cfg.uv_scale, base.cfg.w_scale, OS)
 
-    # ---- the batched multi-channel pass (one GPU only) ---------------------------------
-    c3 = None
-    if world == 1 and not args.no_c3:
-        c3 = c3_block(S, D, dev)
+        def pinned(a):
+            t = torch.empty(a.shape, dtype=torch.float32).pin_memory()
+            t.numpy()[...] = a
+            return t
 
-    c5 = None
-    if world == 1 and not args.no_c5:
-        c5 = c5_block(S, D, dev)
+        uvw_p = [pinned(h[0]) for h in c5.host]
+        meas_p = [pinned(h[1]) for h in c5.host]
+        mgrid_p = pinned(c5.model.cpu().numpy())
+        nmax = max(c5.counts)
+        pred_p = torch.empty((nmax, 2), dtype=torch.float32).pin_memory()
+        delta_p = torch.empty((nmax, 2), dtype=torch.float32).pin_memory()
+        grid_p = torch.empty((G * G, 2), dtype=torch.float32).pin_memory()
+        A.set_degrid_mode(S.SDP_DEGRID_CONV)
 
-    c4 = None
-    if world == 1 and not args.no_c4:
-        c4 = c4_learned_block(S, D, dev, args.c4_skies)
-    fftc = fft_block(S, D, dev) if world == 1 and not args.no_c4 else None
-    calib = calibration_block(S, D, dev, not args.no_cpu_baseline) if world == 1 and not args.no_c4 else None
+        def e2e_step():
+            for k in range(len(c5.plans)):
+                n = c5.counts[k]
+                u, m = uvw_p[k].numpy(), meas_p[k].numpy()
+                p, d = pred_p.numpy()[:n], delta_p.numpy()[:n]
+                A.std_degridding(cfg, G, OS, dk_h, sup_h, mgrid_p.numpy(), u, out=p)
+                A.subtract_finegrid(m, p, out=d)
+                A.std_gridding(cfg, G, OS, gk_h, sup_h, u, d, out=grid_p.numpy())
 
-    # ---- e2e through the reference-facing C ABI with pinned host buffers ---------------
-    uvw_h = torch.empty((N, 3), dtype=torch.float32).pin_memory()
-    uvw_h.copy_(uvw.cpu())
-    meas_h = torch.empty((N, 2), dtype=torch.float32).pin_memory()
-    meas_h.copy_(measured.cpu())
-    mgrid_h = torch.empty((G * G, 2), dtype=torch.float32).pin_memory()
-    mgrid_h.copy_(model_grid.cpu())
-    pred_h = torch.empty((N, 2), dtype=torch.float32).pin_memory()
-    delta_h = torch.empty((N, 2), dtype=torch.float32).pin_memory()
-    grid_h = torch.empty((G * G, 2), dtype=torch.float32).pin_memory()
-    gk_h, dk_h, sup_h = w.gkernels, w.dkernels, w.supports
-    cfg = S.make_config(G, w.cfg.uv_scale, w.cfg.w_scale, OS)
-    uvw_n, meas_n, mgrid_n = uvw_h.numpy(), meas_h.numpy(), mgrid_h.numpy()
-    pred_n, delta_n, grid_n = pred_h.numpy(), delta_h.numpy(), grid_h.numpy()
-    A.set_degrid_mode(S.SDP_DEGRID_CONV)
-
-    def e2e_step():
-        A.std_degridding(cfg, G, OS, dk_h, sup_h, mgrid_n, uvw_n, out=pred_n)
-        A.subtract_finegrid(meas_n, pred_n, out=delta_n)
-        A.std_gridding(cfg, G, OS, gk_h, sup_h, uvw_n, delta_n, out=grid_n)
-
-    e2e_step()
-    torch.cuda.synchronize()
-    if world > 1:
-        dist.barrier()
-    t0 = time.perf_counter()
-    for _ in range(args.e2e_steps):
         e2e_step()
-    t_e2e = (time.perf_counter() - t0) / args.e2e_steps
-    t_e2e_t = torch.tensor([t_e2e], dtype=torch.float64, device=dev)
-    if world > 1:
-        dist.all_reduce(t_e2e_t, op=dist.ReduceOp.MAX)
-    t_e2e = float(t_e2e_t.item())
-    A.set_degrid_mode(S.SDP_DEGRID_NEAREST)
-    ksz = gk_h.nbytes + sup_h.nbytes
-    h2d = (N * 12 + G * G * 8 + ksz) + (2 * N * 8) + (ksz + N * 12 + N * 8)
-    d2h = N * 8 + N * 8 + G * G * 8
+        torch.cuda.synchronize()
+        if world > 1:
+            dist.barrier()
+        t0 = time.perf_counter()
+        for _ in range(args.e2e_steps):
+            e2e_step()
+        t_e2e = (time.perf_counter() - t0) / args.e2e_steps
+        A.set_degrid_mode(S.SDP_DEGRID_NEAREST)
+        ksz = gk_h.nbytes + sup_h.nbytes
+        h2d = sum((n * 12 + G * G * 8 + ksz) + 2 * n * 8 + (ksz + n * 12 + n * 8) for n in c5.counts)
+        d2h = sum(n * 8 + n * 8 + G * G * 8 for n in c5.counts)
+        e2e = (t_e2e, h2d, d2h)
+        del uvw_p, meas_p, mgrid_p, pred_p, delta_p, grid_p
+    else:
+        t_e2e, h2d, d2h = 0.0, 0, 0
+        if world > 1:
+            dist.barrier()
+    t_e2e = channels.max_over_ranks(e2e[0] if e2e else 0.0, device=dev)
+    h2d = e2e[1] if e2e else 0
+    d2h = e2e[2] if e2e else 0
 
-    # ---- CPU baseline (rank 0, N = 1) --------------------------------------------------
+    # ---- CPU baseline (rank 0, N = 1): the reference on a sample of the workload ----
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        threads = cpu_threads()
-        sample = max(threads * 2000, args.cpu_sample)
-        t_cpu, kind = cpu_reference_pass(w, uvw_h.numpy(), mgrid_n, sample, threads)
-        cpu = {"value": sample / t_cpu, "unit": UNIT, "cores": threads, "kind": kind,
-               "sample": f"{sample} visibilities of the workload, {threads} slices on {threads} threads"}
+        ref = ReferencePass(base, args.cpu_sample, cpu_threads())
+        ref.run(20_000)
+        t_cpu = ref.run()
+        cpu = {"value": C5_CHANNELS * ref.sample / t_cpu, "unit": UNIT, "cores": ref.threads, "kind": ref.kind,
+               "sample": ref.describe()}
+        del ref
 
-    csum = clocks.summary()
-    if wf is not None and csum.get("sm_mhz"):
-        sms = torch.cuda.get_device_properties(dev).multi_processor_count
-        peak_wf = sms * float(csum["sm_mhz"]) * 1e6
-        ach_wf = wf / (t_step * 1e-3)
-        binding = {"unit": "shared-memory wavefronts/s", "achieved": ach_wf, "peak": peak_wf,
-                   "frac": ach_wf / peak_wf, "per_launch": wf,
-                   "peak_source": f"{sms} SMs x 1 wavefront/clock x median SM clock in the timed region",
-                   "note": "the fused pass is bound by the L1/shared-memory pipe (emulated float atomics, "
-                           "bank conflicts), not HBM; see profiles/k_tiles_cycle_conv_c2_2048.txt"}
+    # ---- further blocks (one GPU only) ---------------------------------------------------
+    extras = {}
+    if world == 1:
+        if not args.no_major_cycle and not args.no_extras:
+            extras["c5_major_cycle_8192"] = c5_major_cycle_block(S, D, dev, c5)
+    c5.close()
+    del c5, flush
+    torch.cuda.empty_cache()
+    if world == 1:
+        if not args.no_c2:
+            extras["c2_2048"] = c2_block(S, D, dev, args)
+        if not args.no_c3:
+            extras["c3_batched"] = c3_block(S, D, dev)
+        if not args.no_c4:
+            extras["c4_learned"] = c4_learned_block(S, D, dev, args.c4_skies)
+        if not args.no_extras:
+            extras["fft_2048"] = fft_block(S, D, dev)
+            extras["gain_calibration"] = calibration_block(S, D, dev, not args.no_cpu_baseline)
+
     line = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
-        "warmup": max(3, args.warmup), "ms_per_step": t_step, "higher_is_better": True, "scaling": "weak",
+        "warmup": max(3, args.warmup), "ms_per_step": t_step, "higher_is_better": True, "scaling": "strong",
         "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-        "config": {"workload": f"{w.name}: 256 antennas, 10 km log spiral, 120 time steps, {N} vis per channel, "
-                               f"G=2048, 17 w-planes hs=4 OS=16, one channel per GPU",
+        "config": {"workload": c5_config_name(total_vis),
+                   "channels_per_rank": [len(o) for o in channels.assign_channels(counts_all, world)],
                    "degrid": "convolutional (normalised, degridgrid.c:147-191)",
-                   "l2": "flushed between timed steps (256 MB write)", "work_items": n_items,
-                   "plan_shape": tune},
-        "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
-                     "frac": achieved / peak, "traffic": traffic, "peak_source": peak_src,
-                     "kernel": "k_tiles<STD, OP_CYCLE_CONV>",
-                     "algorithmic_bytes_per_launch": alg_bytes,
-                     "fp32_flops_per_launch": algorithmic_flops(N, taps)},
+                   "measured": "exact DFT of 1000 points + 50 Gaussians (sdp_dft_gauss) + 0.1 mJy noise",
+                   "l2": "inputs of several GB (larger than L2); L2 also flushed between timed steps (256 MB write)",
+                   "exchange": "none at N = 1; N > 1: per-rank channel sum + NCCL all-reduce of the 8192^2 "
+                               "continuum residual grid each step" if world > 1 else "none (N = 1)",
+                   "work_items": n_items, "plan_shape": tune, "setup_s": setup_s},
+        "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                     "traffic": traffic, "peak_source": peak_src,
+                     "kernel": "sdp_visbatch_cycle: residual-grid clears + k_vis_fast_batch<float, 8>",
+                     "algorithmic_bytes_per_launch": alg_bytes, "fp32_flops_per_launch": alg_flops,
+                     "ms_per_launch": t_pass},
         "roofline_binding": binding,
-        "e2e": {"value": world * N / t_e2e, "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
-                "path": "std_degridding + subtract_from_measurements_finegrid + std_gridding (host buffers)"},
-        "gpu_launches": args.steps,
+        "e2e": {"value": total_vis / t_e2e if t_e2e > 0 else None, "unit": UNIT, "h2d_bytes_per_step": h2d,
+                "d2h_bytes_per_step": d2h,
+                "path": "per channel std_degridding + subtract_from_measurements_finegrid + std_gridding "
+                        "(host buffers, pinned), all 16 channels per step"},
+        "gpu_launches": args.steps * (2 if world > 1 else 1),
         "clocks": csum,
     }
-    if major is not None:
-        line["major_cycle"] = major
-    if c3 is not None:
-        line["c3_batched"] = c3
-    if c5 is not None:
-        line["c5_channel_8192"] = c5
-    if c4 is not None:
-        line["c4_learned"] = c4
-    if fftc is not None:
-        line["fft_2048"] = fftc
-    if calib is not None:
-        line["gain_calibration"] = calib
+    line.update(extras)
     if cpu is not None:
         line["cpu_baseline"] = cpu
-    plan.close()
     if world > 1:
         dist.barrier()
         dist.destroy_process_group()

@@ -350,23 +350,30 @@ int sdp_visplan_create(sdp_visplan **plan, const sdp_geometry *geom, const sdp_w
                        const sdp_wkernels *degrid_kernels, int num_vis, const sdp_float3 *uvw, int grid_mode,
                        void *stream);
 int sdp_visplan_destroy(sdp_visplan *plan);
-/* Plan shape (no counterpart in the reference): uv tile side (power of two,
- * 8..128, default 32), visibilities per work item (64..65536, default 1024),
- * lanes per visibility of the tile kernels (0: the fewest the support needs,
- * or 8 / 16 / 32).  Zero fields take the defaults.  Results are the same for
- * every shape up to the order of the floating-point sums. */
+/* Plan shape (no counterpart in the reference): uv tile side (a multiple of
+ * 8 in 8..128, default 32), visibilities per work item (64..65536, default
+ * 1024), lanes per visibility (0: std_gridding plans with half supports up
+ * to 4 take the warp-per-visibility kernel, one warp per visibility and a
+ * private subgrid per warp, other plans the fewest lanes their support needs;
+ * 8 / 16 / 32: the group kernels with that many lanes per visibility, several
+ * visibilities per warp on one shared subgrid), warps per CTA of the
+ * warp-per-visibility kernel (0: by occupancy, or 4 / 8).  Zero fields take
+ * the defaults.  Results are the same for every shape up to the order of the
+ * floating-point sums. */
 typedef struct sdp_plan_options {
     int tile;
     int chunk;
     int lanes;
+    int warps;
 } sdp_plan_options;
 int sdp_visplan_create_opt(sdp_visplan **plan, const sdp_geometry *geom, const sdp_wkernels *grid_kernels,
                            const sdp_wkernels *degrid_kernels, int num_vis, const sdp_float3 *uvw, int grid_mode,
                            const sdp_plan_options *options, void *stream);
 int sdp_visplan_options(const sdp_visplan *plan, sdp_plan_options *options);
-/* Autotuner: builds a plan for each candidate shape (tiles 16 / 32 / 64,
- * work items of 512 / 1024 / 2048 visibilities, lanes from the support or
- * 16), times reps fused major-cycle passes (sdp_visplan_cycle on model_grid,
+/* Autotuner: builds a plan for each candidate shape (warp-per-visibility
+ * kernel: tiles 8 / 16 / 24 / 32, work items of 256 / 512 / 1024
+ * visibilities, 4 or 8 warps per CTA; group kernels: tile 32 with 8 and 16
+ * lanes per visibility), times reps fused major-cycle passes (sdp_visplan_cycle on model_grid,
  * residual_grid as scratch) with CUDA events on the stream, and returns the
  * fastest shape, its time per pass (ms) and the number of shapes timed.
  * Blocking; allocates and frees one plan at a time. */
@@ -555,6 +562,37 @@ int sdp_hogbom(const sdp_clean_params *p, float *residual_inout, const float *ps
  * serialise them (one stream, or events). */
 int sdp_hogbom_noalloc(const sdp_clean_params *p, float *residual_inout, const float *psf, float *model_inout,
                        sdp_float3 *sources, int *num_sources_dev, void *stream);
+
+/* ---------------------------------------------------------------------------
+ * Binary input files (no counterpart in the reference, which reads text:
+ * top.c:139-222 visibilities, :224-380 kernel tables, :453-510 the PSF).
+ * A 64-byte header ("SDPBIN1", kind, count, aux, two payload sections on
+ * 4096-byte boundaries) followed by the raw little-endian arrays:
+ *   kind 1 visibilities: uvw float[n][3], vis float[n][2]; aux bit 0 = the
+ *          uvw are already snapped by correct_to_finegrid;
+ *   kind 2 kernel set: supports int[planes][2] (half support, offset), then
+ *          samples float[total][2]; count = total, aux = planes;
+ *   kind 3 image: float[rows][cols]; count = rows, aux = cols.
+ * The sdp_bin_load_* calls read the file with several host threads into a
+ * ring of pinned staging buffers and copy each filled buffer to the device
+ * asynchronously on `stream` while the next one is read; they return after
+ * the last copy has completed.  Errors: SDP_ERR_IO (open/read/write),
+ * SDP_ERR_DATA (not such a file, wrong kind, truncated), SDP_ERR_RANGE
+ * (larger than the caller's buffers).
+ * ------------------------------------------------------------------------- */
+int sdp_bin_info(const char *path, int *kind, long long *count, long long *aux);
+int sdp_bin_write_vis(const char *path, long long num_vis, const sdp_float3 *uvw, const sdp_float2 *vis, int snapped);
+int sdp_bin_write_kernels(const char *path, int num_planes, long long total_samples, const sdp_int2 *supports,
+                          const sdp_float2 *samples);
+int sdp_bin_write_image(const char *path, int rows, int cols, const float *image);
+int sdp_bin_read_vis_host(const char *path, long long max_vis, sdp_float3 *uvw, sdp_float2 *vis, long long *num_vis,
+                          int *snapped);
+int sdp_bin_load_vis(const char *path, long long max_vis, sdp_float3 *uvw_dev, sdp_float2 *vis_dev,
+                     long long *num_vis, int *snapped, void *stream);
+int sdp_bin_load_kernels(const char *path, int max_planes, long long max_samples, sdp_int2 *supports_dev,
+                         sdp_float2 *samples_dev, int *num_planes, long long *total_samples, void *stream);
+int sdp_bin_load_image(const char *path, int max_rows, int max_cols, float *image_dev, int *rows, int *cols,
+                       void *stream);
 
 /* ---------------------------------------------------------------------------
  * Device-resident major cycle of the FFT imaging pipeline

@@ -298,28 +298,44 @@ class RefLib:
             a = a.reshape(-1, cols)
         return a
 
-    def std_gridding(self, cfg: Config, grid_size, os_, kernels, supports, uvw, vis, num=None):
+    def std_gridding(self, cfg: Config, grid_size, os_, kernels, supports, uvw, vis, num=None, out=None):
+        """out: an optional preallocated (G^2, 2) grid of this precision (the
+        reference clears it itself, degridgrid.c:73)."""
         k = self._a(kernels, 2)
         s = np.ascontiguousarray(supports, dtype=np.int32)
         uvw = self._a(uvw, 3)
         vis = self._a(vis, 2)
         n = uvw.shape[0] if num is None else num
         nk = s.shape[0]
-        grid = np.zeros((grid_size * grid_size, 2), dtype=self.dtype)
+        if out is not None:
+            assert out.dtype == self.dtype and out.shape == (grid_size * grid_size, 2) and out.flags["C_CONTIGUOUS"]
+            grid = out
+        else:
+            grid = np.zeros((grid_size * grid_size, 2), dtype=self.dtype)
         maj = _i(0)
         nc = _i(n)
         self.lib.std_gridding(_i(grid_size), _i(n), _i(nk), _i(k.shape[0]), _i(os_), _i(0), C.byref(maj),
                               C.byref(nc), _ptr(k), _ptr(s), _ptr(uvw), _ptr(vis), C.byref(cfg), None, _ptr(grid))
         return grid
 
-    def std_degridding(self, cfg: Config, grid_size, os_, kernels, supports, grid, uvw, num=None):
-        k = self._a(kernels, 2)
-        s = np.ascontiguousarray(supports, dtype=np.int32)
-        # The nearest-cell read (degridgrid.c:194-199) has no bounds check; a
-        # point at the top edge reads past the grid.  Zero rows appended after
-        # the grid make that read defined (0), the value the oracle assigns.
+    def padded_grid(self, grid_size, grid):
+        """The grid with 2 G zero rows appended: the nearest-cell read
+        (degridgrid.c:194-199) has no bounds check, and a point at the top edge
+        reads past the grid; the zero rows make that read defined (0), the value
+        the oracle assigns."""
         g = np.zeros((grid_size * grid_size + 2 * grid_size, 2), dtype=self.dtype)
         g[: grid_size * grid_size] = self._a(grid, 2)
+        return g
+
+    def std_degridding(self, cfg: Config, grid_size, os_, kernels, supports, grid, uvw, num=None, padded=False):
+        """padded: grid already comes from padded_grid (no per-call copy)."""
+        k = self._a(kernels, 2)
+        s = np.ascontiguousarray(supports, dtype=np.int32)
+        if padded:
+            assert grid.dtype == self.dtype and grid.shape == (grid_size * grid_size + 2 * grid_size, 2)
+            g = grid
+        else:
+            g = self.padded_grid(grid_size, grid)
         uvw = self._a(uvw, 3)
         n = uvw.shape[0] if num is None else num
         out = np.zeros((uvw.shape[0], 2), dtype=self.dtype)

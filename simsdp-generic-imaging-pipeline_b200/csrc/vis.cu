@@ -63,6 +63,9 @@ struct PlanDev {
     int *item_counter;
     int *flags;
     const int *kdiff;  // bit 0: degridding set != gridding set; bit 1: != its conjugate
+    int pitch;          // row pitch (float2) of the shared tiles of the warp-per-visibility kernels
+    const uint2 *geo;   // packed tap-box geometry in plan order (see k_bin)
+    const int *perm;    // plan position -> original visibility index
 };
 
 // ----------------------------------------------------------------------------
@@ -187,11 +190,61 @@ __device__ __forceinline__ int floor_div(int a, int b) { return (a >= 0) ? a / b
 
 // Computes the record of each visibility and its bin key.  snap applies
 // correct_to_finegrid (degridgrid.c:24-25, 52-54) in precision T first.
+// Kernel index of tap i (0 .. 2 hs - 1) of a box whose first tap lies
+// hs - d below the visibility (0 < d <= 1): the taps below the visibility
+// (i < hs) read |round(OS (i - hs + d'))| = OS (hs - i) - ko + h, the others
+// OS (i - hs) + ko, with ko the index of tap hs and h in {0, 1} (h = 1 when
+// the sub-sample offset is exactly half a sample: round() goes away from zero
+// on both sides).  k_bin checks this form against the reference's expression
+// for every tap of a visibility before it marks the visibility for the fast
+// path.
+__host__ __device__ __forceinline__ int fast_kidx(int i, int hs, int os, int ko, int h)
+{
+    return i < hs ? os * (hs - i) - ko + h : os * (i - hs) + ko;
+}
+
+// Packed tap-box geometry of a visibility for the warp-per-visibility kernels:
+//   x: box origin in the tile (bits 0-7: column, 8-15: row), w-plane (16-31);
+//   y: ko of the columns (0-7) and rows (8-15), h of the columns (16) and
+//      rows (17), kernel conjugated (18: w < 0), fast path (19).
+// Fast path: std_gridding plan, both kernel sets with the same half support
+// 1 <= hs <= 4, a 2 hs x 2 hs box inside the grid, and every tap's kernel
+// index equal to fast_kidx (the reference's float subtraction (g - p) is
+// exact for all but the tiniest |p|; those, and every other visibility, take
+// the general path that evaluates degridgrid.c's expressions tap by tap).
+template <typename T>
+__device__ __forceinline__ uint2 fast_geometry(const Rec<T> &r, int plane, int hs, int hsd, int G, int OS, int tile,
+                                               int tx, int ty)
+{
+    uint2 g = make_uint2((uint32_t)plane << 16, (r.meta < 0) ? (1u << 18) : 0u);
+    if (hs != hsd || hs < 1 || hs > 4) return g;
+    const T fos = (T)OS;
+    const T lox = tceil(tsub(r.px, (T)hs)), loy = tceil(tsub(r.py, (T)hs));
+    const int ncols = (int)(tceil(tadd(r.px, (T)hs)) - lox);
+    const int nrows = (int)(tceil(tadd(r.py, (T)hs)) - loy);
+    const int n = 2 * hs;
+    const int ix0 = (int)lox + G / 2, iy0 = (int)loy + G / 2;
+    if (ncols != n || nrows != n || ix0 < 0 || iy0 < 0 || ix0 + n > G || iy0 + n > G) return g;
+    const int tx0 = ix0 - tx * tile, ty0 = iy0 - ty * tile;
+    if (tx0 < 0 || ty0 < 0 || tx0 >= tile || ty0 >= tile || tx0 > 255 || ty0 > 255) return g;
+    const int kox = ref_kidx((int)lox + hs, r.px, fos), koy = ref_kidx((int)loy + hs, r.py, fos);
+    const int hx = ref_kidx((int)lox, r.px, fos) + kox - OS * hs;
+    const int hy = ref_kidx((int)loy, r.py, fos) + koy - OS * hs;
+    if (kox < 0 || kox > 255 || koy < 0 || koy > 255 || (hx != 0 && hx != 1) || (hy != 0 && hy != 1)) return g;
+    for (int i = 0; i < n; ++i) {
+        if (ref_kidx((int)lox + i, r.px, fos) != fast_kidx(i, hs, OS, kox, hx)) return g;
+        if (ref_kidx((int)loy + i, r.py, fos) != fast_kidx(i, hs, OS, koy, hy)) return g;
+    }
+    g.x |= (uint32_t)tx0 | ((uint32_t)ty0 << 8);
+    g.y |= (uint32_t)kox | ((uint32_t)koy << 8) | ((uint32_t)hx << 16) | ((uint32_t)hy << 17) | (1u << 19);
+    return g;
+}
+
 template <typename T>
 __global__ void k_bin(const float3 *__restrict__ uvw, int n, int mode, int snap, int G, int OS, double uv_scale,
                       double w_scale, const int2 *__restrict__ sup, const int2 *__restrict__ dsup, int nk, int nkd,
                       long long ntot_g, long long ntot_d, int hs_max, int ntx, int nty, int tile,
-                      Rec<T> *__restrict__ rec_tmp,
+                      Rec<T> *__restrict__ rec_tmp, uint2 *__restrict__ geo_tmp,
                       int *__restrict__ keys, int *__restrict__ counts, int *__restrict__ flags)
 {
     int i = blockIdx.x * blockDim.x + threadIdx.x;
@@ -220,6 +273,7 @@ __global__ void k_bin(const float3 *__restrict__ uvw, int n, int mode, int snap,
     r.meta = plane | ((c.z < 0.0f) ? (int)0x80000000u : 0);
     r.idx = i;
     int key = -1;
+    uint2 geo = make_uint2(0u, 0u);
     if (plane < 0 || plane >= nk || plane >= nkd) {
         atomicOr(flags, FLAG_PLANE);
     } else {
@@ -238,16 +292,18 @@ __global__ void k_bin(const float3 *__restrict__ uvw, int n, int mode, int snap,
             int ty = min(max(floor_div(loy, tile), 0), nty - 1);
             key = (ty * ntx + tx) * nk + plane;
             atomicAdd(&counts[key], 1);
+            if (mode == SDP_GRID_STD) geo = fast_geometry<T>(r, plane, hs, hsd, G, OS, tile, tx, ty);
         }
     }
     rec_tmp[i] = r;
+    geo_tmp[i] = geo;
     keys[i] = key;
 }
 
 template <typename T>
-__global__ void k_scatter(const Rec<T> *__restrict__ rec_tmp, const int *__restrict__ keys, int n,
-                          const int *__restrict__ offsets, int *__restrict__ fill, Rec<T> *__restrict__ rec,
-                          int *__restrict__ perm)
+__global__ void k_scatter(const Rec<T> *__restrict__ rec_tmp, const uint2 *__restrict__ geo_tmp,
+                          const int *__restrict__ keys, int n, const int *__restrict__ offsets, int *__restrict__ fill,
+                          Rec<T> *__restrict__ rec, uint2 *__restrict__ geo, int *__restrict__ perm)
 {
     int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
@@ -255,6 +311,7 @@ __global__ void k_scatter(const Rec<T> *__restrict__ rec_tmp, const int *__restr
     if (key < 0) return;
     int pos = offsets[key] + atomicAdd(&fill[key], 1);
     rec[pos] = rec_tmp[i];
+    geo[pos] = geo_tmp[i];
     perm[pos] = i;
 }
 
@@ -685,6 +742,452 @@ __global__ void __launch_bounds__(kThreads, 4) k_tiles_batch(const PlanDev *__re
     }
 }
 
+// ----------------------------------------------------------------------------
+// Warp-per-visibility tile kernels (std_gridding plans, 1 <= hs <= 4)
+// ----------------------------------------------------------------------------
+// The group kernels above serve four visibilities per warp instruction and so
+// must update the CTA's subgrid with shared-memory atomics (on sm_100 a float
+// atomicAdd to shared memory is a compare-and-swap loop) and pay four-way
+// bank conflicts on every access.  Here a warp serves one visibility at a
+// time: lane (r, c) = (lane / 8, lane % 8) owns tap column c and tap rows r and
+// r + 4 of the 2 hs x 2 hs box, so one warp access covers four box rows of
+// eight cells (two conflict-free wavefronts with the row pitch = 8 mod 16),
+// and each warp accumulates into its own private subgrid with plain loads and
+// stores (the cells of one visibility are distinct; __syncwarp orders
+// consecutive visibilities).  The subgrids are summed and flushed with one
+// vector atomic per touched cell when the work item ends.  The tap geometry
+// comes precomputed from the plan (fast_geometry), so a visibility costs an
+// 8-byte load and a few integer operations per lane before its taps.
+// Degridding sums are reduced for four visibilities at once (a transposed
+// butterfly: 30 shuffles for 4 x 5 values).
+constexpr int kFastVB = 4;  // visibilities per warp batch
+
+// Lane's share of the five degridding sums of one general-path visibility
+// (degridgrid.c:147-186 tap by tap, edges mirrored; the whole warp strides
+// over the taps).
+struct Sums5 {
+    float v[5];
+};
+
+template <typename T>
+__device__ __forceinline__ Sums5 slow_degrid(const PlanDev &P, const Rec<T> rec, int hs_d, int doff,
+                                          const float2 *mtile, int ox, int oy, const float2 *__restrict__ in_grid)
+{
+    Sums5 acc = {{0.f, 0.f, 0.f, 0.f, 0.f}};
+    const int lane = threadIdx.x & 31;
+    const T fos = (T)P.OS;
+    const int A = hs_d + 1, stride = A * P.OS;
+    const T dlox = tceil(tsub(rec.px, (T)hs_d));
+    const T dloy = tceil(tsub(rec.py, (T)hs_d));
+    const int dnc = (int)(tceil(tadd(rec.px, (T)hs_d)) - dlox);
+    const int dnr = (int)(tceil(tadd(rec.py, (T)hs_d)) - dloy);
+    const int S = P.S;
+    for (int t = lane; t < dnc * dnr; t += 32) {
+        const int cc = t % dnc, rr = t / dnc;
+        const int cu = mirror((int)dlox + cc, P.gc);
+        const int kx = ref_kidx(cu, rec.px, fos);
+        const int cv = mirror((int)dloy + rr, P.gc);
+        const int ky = ref_kidx(cv, rec.py, fos);
+        float2 ks = make_float2(0.f, 0.f);
+        if (kx < stride && ky < stride) ks = __ldg(&P.dk[doff + kcol(P, A, kx) + krow(P, A, ky)]);
+        const int gx = cu + P.gc, gy = cv + P.gc;
+        const int tx = gx - ox, ty = gy - oy;
+        float2 gv;
+        if ((unsigned)tx < (unsigned)S && (unsigned)ty < (unsigned)S) {
+            gv = mtile[ty * P.pitch + tx];
+        } else if (gx >= 0 && gy >= 0 && gx < P.G && gy < P.G) {
+            gv = __ldg(&in_grid[(size_t)gy * P.G + gx]);
+        } else {
+            gv = make_float2(0.f, 0.f);
+        }
+        acc.v[0] = fmaf(gv.x, ks.x, acc.v[0]);
+        acc.v[1] = fmaf(gv.y, ks.x, acc.v[1]);
+        acc.v[2] = fmaf(gv.x, ks.y, acc.v[2]);
+        acc.v[3] = fmaf(gv.y, ks.y, acc.v[3]);
+        acc.v[4] = fmaf(ks.x, ks.x, fmaf(ks.y, ks.y, acc.v[4]));
+    }
+    return acc;
+}
+
+// General-path gridding of one visibility into the warp's private subgrid
+// (degridgrid.c:93-122 tap by tap; taps outside the grid skipped).  The taps
+// of one visibility are distinct cells, so plain read-modify-writes suffice.
+template <typename T>
+__device__ __forceinline__ void slow_grid(const PlanDev &P, const Rec<T> rec, int hs_g, int goff, float2 *sub, int ox,
+                                       int oy, float2 gval, float conj)
+{
+    const int lane = threadIdx.x & 31;
+    const T fos = (T)P.OS;
+    const int A = hs_g + 1, stride = A * P.OS;
+    const T lox = tceil(tsub(rec.px, (T)hs_g));
+    const T loy = tceil(tsub(rec.py, (T)hs_g));
+    const int ncols = (int)(tceil(tadd(rec.px, (T)hs_g)) - lox);
+    const int nrows = (int)(tceil(tadd(rec.py, (T)hs_g)) - loy);
+    const float ca = conj * gval.y, cb = conj * gval.x;
+    const int S = P.S;
+    for (int t = lane; t < ncols * nrows; t += 32) {
+        const int c = t % ncols, rr = t / ncols;
+        const int u = (int)lox + c, v = (int)loy + rr;
+        const int gx = u + P.gc, gy = v + P.gc;
+        if (gx < 0 || gx >= P.G || gy < 0 || gy >= P.G) continue;
+        const int tx = gx - ox, ty = gy - oy;
+        const int kx = ref_kidx(u, rec.px, fos), ky = ref_kidx(v, rec.py, fos);
+        if (kx >= stride || ky >= stride || (unsigned)tx >= (unsigned)S || (unsigned)ty >= (unsigned)S) {
+            atomicOr(P.flags, FLAG_BOX);  // cannot happen for a valid plan
+            continue;
+        }
+        const float2 ks = __ldg(&P.gk[goff + kcol(P, A, kx) + krow(P, A, ky)]);
+        float2 *cell = sub + ty * P.pitch + tx;
+        float2 a = *cell;
+        a.x += fmaf(-ca, ks.y, gval.x * ks.x);
+        a.y += fmaf(cb, ks.y, gval.y * ks.x);
+        *cell = a;
+    }
+}
+
+// g[j] for a runtime j < 4 without indexing the register array (which would
+// move it to local memory).
+__device__ __forceinline__ uint2 pick4(const uint2 (&g)[kFastVB], int j)
+{
+    return j == 0 ? g[0] : j == 1 ? g[1] : j == 2 ? g[2] : g[3];
+}
+
+// Reduces v[j][q] (j < 4 visibilities, q < 5 sums) over the warp; lanes
+// 8 j .. 8 j + 7 end with visibility j's five totals in out[0..4].
+__device__ __forceinline__ void reduce4x5(const float (&v)[kFastVB][5], float (&out)[5])
+{
+    const int lane = threadIdx.x & 31;
+    const bool b4 = (lane & 16) != 0, b3 = (lane & 8) != 0;
+    float w[2][5];
+#pragma unroll
+    for (int jj = 0; jj < 2; ++jj)
+#pragma unroll
+        for (int q = 0; q < 5; ++q) {
+            const float keep = b4 ? v[2 + jj][q] : v[jj][q];
+            const float send = b4 ? v[jj][q] : v[2 + jj][q];
+            w[jj][q] = keep + __shfl_xor_sync(0xffffffffu, send, 16);
+        }
+#pragma unroll
+    for (int q = 0; q < 5; ++q) {
+        const float keep = b3 ? w[1][q] : w[0][q];
+        const float send = b3 ? w[0][q] : w[1][q];
+        out[q] = keep + __shfl_xor_sync(0xffffffffu, send, 8);
+    }
+#pragma unroll
+    for (int o = 4; o > 0; o >>= 1)
+#pragma unroll
+        for (int q = 0; q < 5; ++q) out[q] += __shfl_xor_sync(0xffffffffu, out[q], o);
+}
+
+// One work item of the warp-per-visibility kernels (the whole CTA).
+// OP is OP_GRID, OP_DEGRID or OP_CYCLE_CONV.  smem: the model tile (OP !=
+// OP_GRID) and NW private subgrids (OP != OP_DEGRID), S rows of P.pitch cells.
+template <typename T, int OP, int NW>
+__device__ __forceinline__ void fast_item(const PlanDev &P, const int4 it, float2 *mtile, float2 *subs,
+                                          float *wscr_all, const int4 *planes, bool share, float share_sign,
+                                          const float2 *__restrict__ vis_in, const float2 *__restrict__ in_grid,
+                                          float2 *__restrict__ out_grid, float2 *__restrict__ pred_out,
+                                          float2 *__restrict__ delta_out, const float2 *__restrict__ measured)
+{
+    constexpr bool kGrids = (OP != OP_DEGRID);
+    constexpr bool kConv = (OP != OP_GRID);
+    const int S = P.S, pitch = P.pitch, OS = P.OS;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int c = lane & 7, r = lane >> 3;
+    const int ox = (it.x % P.ntx) * P.tile, oy = (it.x / P.ntx) * P.tile;
+    float2 *sub = subs + (size_t)warp * S * pitch;
+    float *wscr = wscr_all + warp * (kFastVB * 5);  // general-path sums of this warp's batch
+    const Rec<T> *__restrict__ recs = static_cast<const Rec<T> *>(P.rec);
+    if (kConv) {
+        for (int k = threadIdx.x; k < S * S; k += 32 * NW) {
+            const int y = k / S, x = k - y * S;
+            const int gy = oy + y, gx = ox + x;
+            mtile[y * pitch + x] =
+                (gx < P.G && gy < P.G) ? __ldg(&in_grid[(size_t)gy * P.G + gx]) : make_float2(0.f, 0.f);
+        }
+        __syncthreads();
+    }
+
+    for (int b = it.y + warp * kFastVB; b < it.z; b += NW * kFastVB) {
+        const int nv = min(kFastVB, it.z - b);  // visibilities in this batch (warp-uniform)
+        uint2 g[kFastVB];
+#pragma unroll
+        for (int j = 0; j < kFastVB; ++j) g[j] = (j < nv) ? P.geo[b + j] : make_uint2(0u, 0u);
+        // per visibility: this lane's two taps (kernel samples and cell)
+        float2 k0[kFastVB], k1[kFastVB];
+        int cell[kFastVB];
+        unsigned act = 0;  // bit 2j: tap (r, c) active, bit 2j+1: tap (r + 4, c) active
+        unsigned slow = 0;  // bit j: visibility j takes the general path (warp-uniform)
+#pragma unroll
+        for (int j = 0; j < kFastVB; ++j)
+            if (j < nv && !(g[j].y & (1u << 19))) slow |= 1u << j;
+        float2 gval = make_float2(0.f, 0.f);  // lanes 8 j ..: visibility j's residual (CONV) / value (GRID)
+        if (kConv) {
+            if (slow) {
+                // general-path visibilities of the batch: their sums, reduced
+                // over the warp, go to shared memory (lane 0 adds them below)
+                for (int j = 0; j < nv; ++j) {
+                    if (!((slow >> j) & 1u)) continue;
+                    const int4 pl = planes[pick4(g, j).x >> 16];
+                    Sums5 t = slow_degrid<T>(P, recs[b + j], pl.x, pl.y, mtile, ox, oy, in_grid);
+#pragma unroll
+                    for (int o = 16; o > 0; o >>= 1)
+#pragma unroll
+                        for (int q = 0; q < 5; ++q) t.v[q] += __shfl_xor_sync(0xffffffffu, t.v[q], o);
+                    if (lane == 0)
+#pragma unroll
+                        for (int q = 0; q < 5; ++q) wscr[j * 5 + q] = t.v[q];
+                }
+                __syncwarp();
+            }
+            float acc[kFastVB][5];
+#pragma unroll
+            for (int j = 0; j < kFastVB; ++j) {
+#pragma unroll
+                for (int q = 0; q < 5; ++q) acc[j][q] = 0.f;
+                k0[j] = k1[j] = make_float2(0.f, 0.f);
+                cell[j] = 0;
+                if (j >= nv) continue;
+                const int4 pl = planes[g[j].x >> 16];
+                if (g[j].y & (1u << 19)) {
+                    const int hs = pl.x, A = hs + 1, n = 2 * hs;
+                    const int kx = fast_kidx(c, hs, OS, g[j].y & 255, (g[j].y >> 16) & 1);
+                    const int ky0 = fast_kidx(r, hs, OS, (g[j].y >> 8) & 255, (g[j].y >> 17) & 1);
+                    const int ky1 = fast_kidx(r + 4, hs, OS, (g[j].y >> 8) & 255, (g[j].y >> 17) & 1);
+                    const int colp = pl.y + kcol(P, A, kx);
+                    const bool a0 = c < n && r < n, a1 = c < n && r + 4 < n;
+                    const int ce = (int)((g[j].x >> 8) & 255) * pitch + (int)(g[j].x & 255) + r * pitch + c;
+                    cell[j] = ce;
+                    act |= (a0 ? 1u : 0u) << (2 * j);
+                    act |= (a1 ? 2u : 0u) << (2 * j);
+                    float2 m0 = make_float2(0.f, 0.f), m1 = make_float2(0.f, 0.f);
+                    if (a0) {
+                        k0[j] = __ldg(&P.dk[colp + krow(P, A, ky0)]);
+                        m0 = mtile[ce];
+                    }
+                    if (a1) {
+                        k1[j] = __ldg(&P.dk[colp + krow(P, A, ky1)]);
+                        m1 = mtile[ce + 4 * pitch];
+                    }
+                    acc[j][0] = fmaf(m0.x, k0[j].x, m1.x * k1[j].x);
+                    acc[j][1] = fmaf(m0.y, k0[j].x, m1.y * k1[j].x);
+                    acc[j][2] = fmaf(m0.x, k0[j].y, m1.x * k1[j].y);
+                    acc[j][3] = fmaf(m0.y, k0[j].y, m1.y * k1[j].y);
+                    acc[j][4] = fmaf(k0[j].x, k0[j].x, fmaf(k0[j].y, k0[j].y, fmaf(k1[j].x, k1[j].x, k1[j].y * k1[j].y)));
+                } else if (lane == 0) {
+#pragma unroll
+                    for (int q = 0; q < 5; ++q) acc[j][q] = wscr[j * 5 + q];
+                }
+            }
+            float tot[5];
+            reduce4x5(acc, tot);
+            // lanes 8 j .. 8 j + 7: visibility j (degridgrid.c:188-191; the
+            // conjugation of k for w < 0 applied after the sum)
+            const int j = r;
+            const uint32_t gy_ = pick4(g, j).y;
+            const float conj = (gy_ & (1u << 18)) ? -1.f : 1.f;
+            const float sx = fmaf(-conj, tot[3], tot[0]);
+            const float sy = fmaf(conj, tot[2], tot[1]);
+            const float cn = __fsqrt_rn(tot[4]);
+            const bool tiny = cn < 1e-5f;
+            const float inv = tiny ? 1e5f : __frcp_rn(cn);
+            const float nx = sx * inv;
+            const float ny = tiny ? nx * inv : sy * inv;
+            const float2 value = make_float2(nx, ny);
+            if (j < nv) {
+                const int i = b + j;
+                if (OP == OP_CYCLE_CONV) {
+                    const float2 m = measured[i];
+                    gval = make_float2(__fsub_rn(m.x, value.x), __fsub_rn(m.y, value.y));
+                    if (c == 0 && (pred_out || delta_out)) {
+                        const int o = P.perm[i];
+                        if (pred_out) pred_out[o] = value;
+                        if (delta_out) delta_out[o] = gval;
+                    }
+                } else if (c == 0) {
+                    pred_out[P.perm[i]] = value;
+                }
+            }
+        }
+
+        if (kGrids) {
+#pragma unroll
+            for (int j = 0; j < kFastVB; ++j) {
+                if (j >= nv) break;
+                float2 gv;
+                if (kConv) {
+                    gv.x = __shfl_sync(0xffffffffu, gval.x, 8 * j);
+                    gv.y = __shfl_sync(0xffffffffu, gval.y, 8 * j);
+                } else {
+                    gv = __ldg(&vis_in[P.perm[b + j]]);
+                }
+                if (!(g[j].y & (1u << 19))) continue;  // general path below
+                const float conj = (g[j].y & (1u << 18)) ? -1.f : 1.f;
+                const int4 pl = planes[g[j].x >> 16];
+                {
+                    float2 q0, q1;
+                    int ce;
+                    unsigned aj;
+                    if (kConv && share) {
+                        q0 = make_float2(k0[j].x, share_sign * k0[j].y);
+                        q1 = make_float2(k1[j].x, share_sign * k1[j].y);
+                        ce = cell[j];
+                        aj = (act >> (2 * j)) & 3u;
+                    } else {
+                        const int hs = pl.z, A = hs + 1, n = 2 * hs;
+                        const int kx = fast_kidx(c, hs, OS, g[j].y & 255, (g[j].y >> 16) & 1);
+                        const int ky0 = fast_kidx(r, hs, OS, (g[j].y >> 8) & 255, (g[j].y >> 17) & 1);
+                        const int ky1 = fast_kidx(r + 4, hs, OS, (g[j].y >> 8) & 255, (g[j].y >> 17) & 1);
+                        const int colp = pl.w + kcol(P, A, kx);
+                        aj = ((c < n && r < n) ? 1u : 0u) | ((c < n && r + 4 < n) ? 2u : 0u);
+                        ce = (int)((g[j].x >> 8) & 255) * pitch + (int)(g[j].x & 255) + r * pitch + c;
+                        q0 = (aj & 1u) ? __ldg(&P.gk[colp + krow(P, A, ky0)]) : make_float2(0.f, 0.f);
+                        q1 = (aj & 2u) ? __ldg(&P.gk[colp + krow(P, A, ky1)]) : make_float2(0.f, 0.f);
+                    }
+                    // vis * (kr + i conj ki): re = vr kr - (conj vi) ki, im = vi kr + (conj vr) ki
+                    const float ca = conj * gv.y, cb = conj * gv.x;
+                    if (aj & 1u) {
+                        float2 a = sub[ce];
+                        a.x += fmaf(-ca, q0.y, gv.x * q0.x);
+                        a.y += fmaf(cb, q0.y, gv.y * q0.x);
+                        sub[ce] = a;
+                    }
+                    if (aj & 2u) {
+                        float2 a = sub[ce + 4 * pitch];
+                        a.x += fmaf(-ca, q1.y, gv.x * q1.x);
+                        a.y += fmaf(cb, q1.y, gv.y * q1.x);
+                        sub[ce + 4 * pitch] = a;
+                    }
+                }
+                __syncwarp();
+            }
+            if (slow) {
+                for (int j = 0; j < nv; ++j) {
+                    if (!((slow >> j) & 1u)) continue;
+                    float2 gv;
+                    if (kConv) {
+                        gv.x = __shfl_sync(0xffffffffu, gval.x, 8 * j);
+                        gv.y = __shfl_sync(0xffffffffu, gval.y, 8 * j);
+                    } else {
+                        gv = __ldg(&vis_in[P.perm[b + j]]);
+                    }
+                    const uint2 gj = pick4(g, j);
+                    const int4 pl = planes[gj.x >> 16];
+                    slow_grid<T>(P, recs[b + j], pl.z, pl.w, sub, ox, oy, gv, (gj.y & (1u << 18)) ? -1.f : 1.f);
+                    __syncwarp();
+                }
+            }
+        }
+    }
+    if (kGrids) {
+        __syncthreads();
+        // flush: the warps' subgrids summed, one vector atomic per touched cell
+        for (int k = threadIdx.x; k < S * S; k += 32 * NW) {
+            const int y = k / S, x = k - y * S;
+            const int o = y * pitch + x;
+            float2 v = make_float2(0.f, 0.f);
+#pragma unroll
+            for (int w = 0; w < NW; ++w) {
+                const float2 t = subs[(size_t)w * S * pitch + o];
+                v.x += t.x;
+                v.y += t.y;
+                subs[(size_t)w * S * pitch + o] = make_float2(0.f, 0.f);
+            }
+            if (v.x != 0.f || v.y != 0.f) {
+                const int gy = oy + y, gx = ox + x;
+                if (gx < P.G && gy < P.G) atomicAdd(&out_grid[(size_t)gy * P.G + gx], v);
+            }
+        }
+    }
+    __syncthreads();
+}
+
+// Shared-memory layout of the warp-per-visibility kernels: per-plane
+// constants (nk int4), then the model tile and the NW subgrids.
+__host__ __device__ __forceinline__ size_t fast_smem_bytes(int op, int nw, int S, int pitch, int nk)
+{
+    const size_t tilef2 = (size_t)S * pitch;
+    return 16 * (size_t)nk + 8 * tilef2 * ((op != OP_GRID ? 1 : 0) + (op != OP_DEGRID ? nw : 0));
+}
+
+template <typename T, int OP, int NW>
+__global__ void __launch_bounds__(32 * NW) k_vis_fast(PlanDev P, const float2 *__restrict__ vis_in,
+                                                      const float2 *__restrict__ in_grid,
+                                                      float2 *__restrict__ out_grid, float2 *__restrict__ pred_out,
+                                                      float2 *__restrict__ delta_out,
+                                                      const float2 *__restrict__ measured)
+{
+    extern __shared__ __align__(16) unsigned char smem_fast[];
+    int4 *planes = reinterpret_cast<int4 *>(smem_fast);
+    float2 *mtile = reinterpret_cast<float2 *>(smem_fast + 16 * (size_t)P.nk_g);
+    float2 *subs = mtile + (OP != OP_GRID ? (size_t)P.S * P.pitch : 0);
+    __shared__ float s_wscr[NW * kFastVB * 5];
+    __shared__ int s_item;
+    for (int k = threadIdx.x; k < P.nk_g; k += 32 * NW)
+        planes[k] = make_int4(OP != OP_GRID && k < P.nk_d ? P.ds[k].x : 0,
+                              OP != OP_GRID && k < P.nk_d ? P.dpoff[k] : 0, OP != OP_DEGRID ? P.gs[k].x : 0,
+                              OP != OP_DEGRID ? P.gpoff[k] : 0);
+    if (OP != OP_DEGRID)
+        for (size_t k = threadIdx.x; k < (size_t)NW * P.S * P.pitch; k += 32 * NW) subs[k] = make_float2(0.f, 0.f);
+    const int kdiff = (OP == OP_CYCLE_CONV) ? *P.kdiff : 3;
+    const bool share = (kdiff & 1) == 0 || (kdiff & 2) == 0;
+    const float share_sign = (kdiff & 1) == 0 ? 1.f : -1.f;
+    __syncthreads();
+    for (;;) {
+        if (threadIdx.x == 0) s_item = atomicAdd(P.item_counter, 1);
+        __syncthreads();
+        const int item = s_item;
+        if (item >= *P.n_items) break;
+        fast_item<T, OP, NW>(P, P.items[item], mtile, subs, s_wscr, planes, share, share_sign, vis_in, in_grid,
+                             out_grid, pred_out, delta_out, measured);
+    }
+}
+
+// The fused pass of several plans (one per frequency channel) in one
+// persistent launch over the (channel, tile) queue; smem sized for the
+// largest channel (S_max rows of pitch_max, nk_max planes).
+template <typename T, int NW>
+__global__ void __launch_bounds__(32 * NW) k_vis_fast_batch(const PlanDev *__restrict__ plans,
+                                                            const BatchIO *__restrict__ io,
+                                                            const int4 *__restrict__ items, int n_items,
+                                                            int *item_counter, int nk_max, int tile_f2)
+{
+    extern __shared__ __align__(16) unsigned char smem_fast[];
+    int4 *planes = reinterpret_cast<int4 *>(smem_fast);
+    float2 *mtile = reinterpret_cast<float2 *>(smem_fast + 16 * (size_t)nk_max);
+    float2 *subs = mtile + tile_f2;
+    __shared__ PlanDev sP;
+    __shared__ BatchIO sIO;
+    __shared__ int s_item, s_share;
+    __shared__ float s_wscr[NW * kFastVB * 5];
+    for (size_t k = threadIdx.x; k < (size_t)NW * tile_f2; k += 32 * NW) subs[k] = make_float2(0.f, 0.f);
+    int cur = -1;
+    for (;;) {
+        if (threadIdx.x == 0) s_item = atomicAdd(item_counter, 1);
+        __syncthreads();
+        const int item = s_item;
+        if (item >= n_items) break;
+        const int4 it = items[item];
+        if (it.w != cur) {
+            if (threadIdx.x == 0) {
+                sP = plans[it.w];
+                sIO = io[it.w];
+                s_share = *sP.kdiff;
+            }
+            __syncthreads();
+            for (int k = threadIdx.x; k < sP.nk_g; k += 32 * NW)
+                planes[k] = make_int4(k < sP.nk_d ? sP.ds[k].x : 0, k < sP.nk_d ? sP.dpoff[k] : 0, sP.gs[k].x,
+                                      sP.gpoff[k]);
+            __syncthreads();
+            cur = it.w;
+        }
+        const int kdiff = s_share;
+        fast_item<T, OP_CYCLE_CONV, NW>(sP, it, mtile, subs, s_wscr, planes, (kdiff & 1) == 0 || (kdiff & 2) == 0,
+                                        (kdiff & 1) == 0 ? 1.f : -1.f, nullptr, sIO.in_grid, sIO.out_grid,
+                                        sIO.pred_out, sIO.delta_out, sIO.measured);
+    }
+}
+
 // Phase-major copy of a kernel set (see kcol / krow).  One thread per output
 // sample; plane p of the source starts at supports[p].y, of the copy at
 // poff[p] (planes packed back to back).
@@ -814,6 +1317,9 @@ static PlanDev plan_dev(const sdp_visplan *p)
     d.n_items = p->n_items;
     d.item_counter = p->item_counter;
     d.flags = p->flags;
+    d.pitch = p->pitch;
+    d.geo = p->geo;
+    d.perm = p->perm;
     return d;
 }
 
@@ -860,6 +1366,8 @@ static void plan_layout(const sdp_visplan *p, size_t *off, size_t *total)
     const size_t per = (size_t)(p->hs_max + 1) * p->geom.oversampling * (p->hs_max + 1) * p->geom.oversampling;
     off[14] = o; o = align_up(o + (p->phase_major ? sizeof(float2) * per * p->gk.num_kernels : 0), 256);  // gk2
     off[15] = o; o = align_up(o + (p->phase_major ? sizeof(float2) * per * p->dk.num_kernels : 0), 256);  // dk2
+    off[16] = o; o = align_up(o + sizeof(uint2) * (size_t)std::max(n, 1), 256);          // geo
+    off[17] = o; o = align_up(o + sizeof(uint2) * (size_t)std::max(n, 1), 256);          // geo_tmp
     *total = o;
 }
 
@@ -896,6 +1404,9 @@ int visplan_setup(sdp_visplan *p, const sdp_geometry *geom, const sdp_wkernels *
     p->hs_max = std::max(gk->max_half_support, dk->max_half_support);
     p->W = 2 * p->hs_max + 1;
     p->S = p->tile + 2 * p->hs_max;
+    // rows of 8-byte cells whose starts are 16 banks apart: the four rows a
+    // warp touches in one access fall into two conflict-free bank halves
+    p->pitch = p->S + ((8 - p->S % 16) + 16) % 16;
     const int os = geom->oversampling;
     p->phase_major = (os & (os - 1)) == 0 ? 1 : 0;
     return SDP_OK;
@@ -903,7 +1414,7 @@ int visplan_setup(sdp_visplan *p, const sdp_geometry *geom, const sdp_wkernels *
 
 size_t visplan_arena_bytes(const sdp_visplan *p)
 {
-    size_t off[16], total;
+    size_t off[18], total;
     plan_layout(p, off, &total);
     return total;
 }
@@ -952,7 +1463,7 @@ int visplan_kernels(sdp_visplan *p, cudaStream_t st)
 
 int visplan_build(sdp_visplan *p, void *arena, const float3 *uvw, cudaStream_t st)
 {
-    size_t off[16], total;
+    size_t off[18], total;
     plan_layout(p, off, &total);
     char *a = static_cast<char *>(arena);
     p->arena = arena;
@@ -976,6 +1487,8 @@ int visplan_build(sdp_visplan *p, void *arena, const float3 *uvw, cudaStream_t s
     p->dpoff = reinterpret_cast<int *>(a + off[13]);
     p->gk2 = reinterpret_cast<float2 *>(a + off[14]);
     p->dk2 = reinterpret_cast<float2 *>(a + off[15]);
+    p->geo = reinterpret_cast<uint2 *>(a + off[16]);
+    uint2 *geo_tmp = reinterpret_cast<uint2 *>(a + off[17]);
     const int n = p->n;
 
     SDP_CUDA_TRY(cudaMemsetAsync(scalars, 0, sizeof(int) * 4, st));
@@ -988,14 +1501,14 @@ int visplan_build(sdp_visplan *p, void *arena, const float3 *uvw, cudaStream_t s
             k_bin<double><<<(n + 255) / 256, 256, 0, st>>>(
                 uvw, n, p->mode, p->snap, p->geom.grid_size, p->geom.oversampling, p->geom.uv_scale, p->geom.w_scale,
                 gs, ds, p->gk.num_kernels, p->dk.num_kernels, (long long)p->gk.total_samples,
-                (long long)p->dk.total_samples, p->hs_max, p->ntx, p->nty, p->tile, static_cast<Rec<double> *>(rec_tmp), keys,
-                counts, p->flags);
+                (long long)p->dk.total_samples, p->hs_max, p->ntx, p->nty, p->tile, static_cast<Rec<double> *>(rec_tmp),
+                geo_tmp, keys, counts, p->flags);
         } else {
             k_bin<float><<<(n + 255) / 256, 256, 0, st>>>(
                 uvw, n, p->mode, p->snap, p->geom.grid_size, p->geom.oversampling, p->geom.uv_scale, p->geom.w_scale,
                 gs, ds, p->gk.num_kernels, p->dk.num_kernels, (long long)p->gk.total_samples,
-                (long long)p->dk.total_samples, p->hs_max, p->ntx, p->nty, p->tile, static_cast<Rec<float> *>(rec_tmp), keys,
-                counts, p->flags);
+                (long long)p->dk.total_samples, p->hs_max, p->ntx, p->nty, p->tile, static_cast<Rec<float> *>(rec_tmp),
+                geo_tmp, keys, counts, p->flags);
         }
         SDP_LAUNCH_CHECK();
     }
@@ -1004,13 +1517,13 @@ int visplan_build(sdp_visplan *p, void *arena, const float3 *uvw, cudaStream_t s
     if (n > 0) SDP_CUDA_TRY(cudaMemsetAsync(p->perm, 0xff, sizeof(int) * (size_t)n, st));  // unbinned slots: -1
     if (n > 0) {
         if (p->coord_f64)
-            k_scatter<double><<<(n + 255) / 256, 256, 0, st>>>(static_cast<const Rec<double> *>(rec_tmp), keys, n,
-                                                               offsets, counts, static_cast<Rec<double> *>(p->rec),
-                                                               p->perm);
+            k_scatter<double><<<(n + 255) / 256, 256, 0, st>>>(static_cast<const Rec<double> *>(rec_tmp), geo_tmp,
+                                                               keys, n, offsets, counts,
+                                                               static_cast<Rec<double> *>(p->rec), p->geo, p->perm);
         else
-            k_scatter<float><<<(n + 255) / 256, 256, 0, st>>>(static_cast<const Rec<float> *>(rec_tmp), keys, n,
-                                                              offsets, counts, static_cast<Rec<float> *>(p->rec),
-                                                              p->perm);
+            k_scatter<float><<<(n + 255) / 256, 256, 0, st>>>(static_cast<const Rec<float> *>(rec_tmp), geo_tmp, keys,
+                                                              n, offsets, counts, static_cast<Rec<float> *>(p->rec),
+                                                              p->geo, p->perm);
         SDP_LAUNCH_CHECK();
     }
     k_item_counts<<<(p->ntiles + 255) / 256, 256, 0, st>>>(offsets, p->ntiles, p->nk, p->chunk, item_counts);
@@ -1082,13 +1595,16 @@ SDP_EXPORT int sdp_visplan_create_opt(sdp_visplan **out, const sdp_geometry *geo
     const int tile = (opt && opt->tile) ? opt->tile : kTile;
     const int chunk = (opt && opt->chunk) ? opt->chunk : kChunk;
     const int lanes = opt ? opt->lanes : 0;
-    SDP_CHECK_ARG(tile >= 8 && tile <= 128 && (tile & (tile - 1)) == 0, "tile %d: a power of two in 8..128", tile);
+    const int warps = opt ? opt->warps : 0;
+    SDP_CHECK_ARG(tile >= 8 && tile <= 128 && tile % 8 == 0, "tile %d: a multiple of 8 in 8..128", tile);
     SDP_CHECK_ARG(chunk >= 64 && chunk <= (1 << 16), "chunk %d: 64..65536 visibilities", chunk);
     SDP_CHECK_ARG(lanes == 0 || lanes == 8 || lanes == 16 || lanes == 32, "lanes %d: 0, 8, 16 or 32", lanes);
+    SDP_CHECK_ARG(warps == 0 || warps == 4 || warps == 8, "warps %d: 0, 4 or 8", warps);
     sdp_visplan *p = new sdp_visplan();
     p->tile = tile;
     p->chunk = chunk;
     p->lanes = lanes;
+    p->warps = warps;
     int status = visplan_setup(p, geom, gk, dk, num_vis, grid_mode);
     if (status == SDP_OK && lanes != 0 && 2 * p->hs_max > lanes)
         status = set_error(SDP_ERR_INVALID, "lanes %d below the %d tap columns of the support", lanes,
@@ -1120,6 +1636,7 @@ SDP_EXPORT int sdp_visplan_options(const sdp_visplan *p, sdp_plan_options *opt)
     opt->tile = p->tile;
     opt->chunk = p->chunk;
     opt->lanes = p->lanes;
+    opt->warps = p->warps;
     return SDP_OK;
 }
 
@@ -1132,9 +1649,17 @@ SDP_EXPORT int sdp_visplan_autotune(const sdp_geometry *geom, const sdp_wkernels
     SDP_CHECK_ARG(best && best_ms && measured && model_grid && residual_grid, "NULL argument");
     SDP_CHECK_ARG(reps >= 1 && reps <= 100, "reps %d: 1..100", reps);
     cudaStream_t st = as_stream(stream);
-    static const int tiles[] = {16, 32, 64};
-    static const int chunks[] = {512, 1024, 2048};
-    static const int lanes_c[] = {0, 16};
+    // candidates: the warp-per-visibility kernel (lanes 0) over tile sides,
+    // work-item sizes and warps per CTA, and two shapes of the group kernels
+    struct Cand {
+        int tile, chunk, lanes, warps;
+    };
+    std::vector<Cand> cands;
+    for (int ti : {8, 16, 24, 32})
+        for (int ch : {256, 512, 1024})
+            for (int nw : {4, 8}) cands.push_back({ti, ch, 0, nw});
+    cands.push_back({32, 512, 8, 0});
+    cands.push_back({32, 1024, 16, 0});
     cudaEvent_t e0 = nullptr, e1 = nullptr;
     SDP_CUDA_TRY(cudaEventCreate(&e0));
     cudaError_t ce = cudaEventCreate(&e1);
@@ -1146,11 +1671,9 @@ SDP_EXPORT int sdp_visplan_autotune(const sdp_geometry *geom, const sdp_wkernels
     int tried = 0;
     bool have = false;
     int status = SDP_OK;
-    for (int ti : tiles)
-        for (int ch : chunks)
-            for (int ln : lanes_c) {
+    for (const Cand &cd : cands) {
                 if (status != SDP_OK) break;
-                sdp_plan_options o{ti, ch, ln};
+                sdp_plan_options o{cd.tile, cd.chunk, cd.lanes, cd.warps};
                 sdp_visplan *p = nullptr;
                 // candidates the device cannot hold (shared memory, lanes) are skipped
                 if (sdp_visplan_create_opt(&p, geom, gk, dk, num_vis, uvw, grid_mode, &o, stream) != SDP_OK) continue;
@@ -1253,9 +1776,77 @@ static int launch_tiles_lg(sdp_visplan *p, int op, const float2 *vis_in, const f
     return SDP_OK;
 }
 
+// The warp-per-visibility kernels serve std_gridding plans with half
+// supports 1..4 (boxes of at most 8 x 8 taps) unless the plan asks for the
+// group kernels (lanes != 0).
+static bool fast_eligible(const sdp_visplan *p)
+{
+    return p->mode == SDP_GRID_STD && p->lanes == 0 && p->hs_max >= 1 && p->hs_max <= 4;
+}
+
+template <typename T, int OP, int NW>
+static int launch_fast_nw(sdp_visplan *p, const float2 *vis_in, const float2 *in_grid, float2 *out_grid,
+                          float2 *pred, float2 *delta, cudaStream_t st, int *resident_warps)
+{
+    const size_t smem = fast_smem_bytes(OP, NW, p->S, p->pitch, p->gk.num_kernels);
+    void (*fn)(PlanDev, const float2 *, const float2 *, float2 *, float2 *, float2 *, const float2 *) =
+        k_vis_fast<T, OP, NW>;
+    if (smem > 227 * 1024) {
+        if (resident_warps) {
+            *resident_warps = 0;
+            return SDP_OK;
+        }
+        return set_error(SDP_ERR_RANGE, "tile kernel does not fit (%zu B shared memory)", smem);
+    }
+    if (smem > 48 * 1024) SDP_CUDA_TRY(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    int per_sm = 0;
+    SDP_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, 32 * NW, smem));
+    if (resident_warps) {  // query only
+        *resident_warps = per_sm * NW;
+        return SDP_OK;
+    }
+    if (per_sm < 1) return set_error(SDP_ERR_RANGE, "tile kernel does not fit (%zu B shared memory)", smem);
+    PlanDev d = plan_dev(p);
+    SDP_CUDA_TRY(cudaMemsetAsync(p->item_counter, 0, sizeof(int), st));
+    fn<<<per_sm * num_sms(), 32 * NW, smem, st>>>(d, vis_in, in_grid, out_grid, pred, delta, p->measured);
+    SDP_LAUNCH_CHECK();
+    return SDP_OK;
+}
+
+template <typename T, int OP>
+static int launch_fast_op(sdp_visplan *p, const float2 *vis_in, const float2 *in_grid, float2 *out_grid,
+                          float2 *pred, float2 *delta, cudaStream_t st)
+{
+    int nw = p->warps;
+    if (nw == 0) {  // the shape that keeps more warps resident (8 on a tie)
+        int w4 = 0, w8 = 0;
+        SDP_TRY((launch_fast_nw<T, OP, 4>(p, vis_in, in_grid, out_grid, pred, delta, st, &w4)));
+        SDP_TRY((launch_fast_nw<T, OP, 8>(p, vis_in, in_grid, out_grid, pred, delta, st, &w8)));
+        nw = (w4 > w8) ? 4 : 8;
+    }
+    if (nw == 4) return launch_fast_nw<T, OP, 4>(p, vis_in, in_grid, out_grid, pred, delta, st, nullptr);
+    return launch_fast_nw<T, OP, 8>(p, vis_in, in_grid, out_grid, pred, delta, st, nullptr);
+}
+
+template <typename T>
+static int launch_fast(sdp_visplan *p, int op, const float2 *vis_in, const float2 *in_grid, float2 *out_grid,
+                       float2 *pred, float2 *delta, cudaStream_t st)
+{
+    switch (op) {
+    case OP_GRID: return launch_fast_op<T, OP_GRID>(p, vis_in, in_grid, out_grid, pred, delta, st);
+    case OP_DEGRID: return launch_fast_op<T, OP_DEGRID>(p, vis_in, in_grid, out_grid, pred, delta, st);
+    case OP_CYCLE_CONV: return launch_fast_op<T, OP_CYCLE_CONV>(p, vis_in, in_grid, out_grid, pred, delta, st);
+    default: return set_error(SDP_ERR_INVALID, "internal: op %d", op);
+    }
+}
+
 static int launch_tiles(sdp_visplan *p, int op, const float2 *vis_in, const float2 *in_grid, float2 *out_grid,
                         float2 *pred, float2 *delta, cudaStream_t st)
 {
+    if (fast_eligible(p) && (op == OP_GRID || op == OP_DEGRID || op == OP_CYCLE_CONV)) {
+        if (p->coord_f64) return launch_fast<double>(p, op, vis_in, in_grid, out_grid, pred, delta, st);
+        return launch_fast<float>(p, op, vis_in, in_grid, out_grid, pred, delta, st);
+    }
     // lanes per visibility: the tap columns (2 hs + 1 at most) in at most two
     // passes; a plan may ask for more lanes than its support needs
     if (p->lanes == 16 && 2 * p->hs_max <= 16) {
@@ -1340,7 +1931,10 @@ SDP_EXPORT int sdp_visplan_g2g(sdp_visplan *p, const sdp_float2 *in_grid, sdp_fl
 struct sdp_visbatch {
     int n = 0;
     bool f64 = false;
+    bool fast = true;  // every plan takes the warp-per-visibility kernel
+    int warps = 0;
     int hs_max = 0, S_max = 0, nk_max = 0, n_items = 0;
+    size_t tile_f2 = 0;  // largest S x pitch of the plans
     std::vector<sdp_visplan *> plans;
     std::vector<sdp::BatchIO> io;
     sdp::PlanDev *d_plans = nullptr;
@@ -1370,6 +1964,47 @@ static int launch_batch_lg(sdp_visbatch *b, int op, cudaStream_t st)
                                                    stride);
     SDP_LAUNCH_CHECK();
     return SDP_OK;
+}
+
+template <typename T, int NW>
+static int launch_batch_fast_nw(sdp_visbatch *b, cudaStream_t st, int *resident_warps)
+{
+    const size_t smem = 16 * (size_t)b->nk_max + 8 * b->tile_f2 * (1 + NW);
+    void (*fn)(const PlanDev *, const BatchIO *, const int4 *, int, int *, int, int) = k_vis_fast_batch<T, NW>;
+    if (smem > 227 * 1024) {
+        if (resident_warps) {
+            *resident_warps = 0;
+            return SDP_OK;
+        }
+        return set_error(SDP_ERR_RANGE, "batched tile kernel does not fit (%zu B shared memory)", smem);
+    }
+    if (smem > 48 * 1024) SDP_CUDA_TRY(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    int per_sm = 0;
+    SDP_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, 32 * NW, smem));
+    if (resident_warps) {
+        *resident_warps = per_sm * NW;
+        return SDP_OK;
+    }
+    if (per_sm < 1) return set_error(SDP_ERR_RANGE, "batched tile kernel does not fit (%zu B shared memory)", smem);
+    SDP_CUDA_TRY(cudaMemsetAsync(b->d_counter, 0, sizeof(int), st));
+    fn<<<per_sm * num_sms(), 32 * NW, smem, st>>>(b->d_plans, b->d_io, b->d_items, b->n_items, b->d_counter,
+                                                  b->nk_max, (int)b->tile_f2);
+    SDP_LAUNCH_CHECK();
+    return SDP_OK;
+}
+
+template <typename T>
+static int launch_batch_fast(sdp_visbatch *b, cudaStream_t st)
+{
+    int nw = b->warps;
+    if (nw == 0) {
+        int w4 = 0, w8 = 0;
+        SDP_TRY((launch_batch_fast_nw<T, 4>(b, st, &w4)));
+        SDP_TRY((launch_batch_fast_nw<T, 8>(b, st, &w8)));
+        nw = (w4 > w8) ? 4 : 8;
+    }
+    if (nw == 4) return launch_batch_fast_nw<T, 4>(b, st, nullptr);
+    return launch_batch_fast_nw<T, 8>(b, st, nullptr);
 }
 
 }  // namespace sdp
@@ -1404,6 +2039,9 @@ SDP_EXPORT int sdp_visbatch_create(sdp_visbatch **out, sdp_visplan *const *plans
         devs.push_back(plan_dev(p));
         b->hs_max = std::max(b->hs_max, p->hs_max);
         b->S_max = std::max(b->S_max, p->S);
+        b->tile_f2 = std::max(b->tile_f2, (size_t)p->S * p->pitch);
+        b->fast = b->fast && fast_eligible(p);
+        if (c == 0) b->warps = p->warps;
         b->nk_max = std::max(b->nk_max, p->gk.num_kernels);
         int ni = 0;
         cudaError_t e = cudaMemcpyAsync(&ni, p->n_items, sizeof(int), cudaMemcpyDeviceToHost, st);
@@ -1469,6 +2107,7 @@ SDP_EXPORT int sdp_visbatch_cycle(sdp_visbatch *b, int degrid_mode, void *stream
     }
     if (b->n_items == 0) return SDP_OK;
     const int op = degrid_mode == SDP_DEGRID_CONV ? OP_CYCLE_CONV : OP_CYCLE_NEAR;
+    if (op == OP_CYCLE_CONV && b->fast) return b->f64 ? launch_batch_fast<double>(b, st) : launch_batch_fast<float>(b, st);
     const int taps = 2 * b->hs_max;
     if (b->f64) {
         if (taps <= 8) return launch_batch_lg<double, 8>(b, op, st);

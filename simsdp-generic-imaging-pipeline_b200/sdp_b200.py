@@ -168,6 +168,52 @@ def _f32(x, cols=None):
 
 
 # ---------------------------------------------------------------------------
+# Binary input files (sdp_bin_*)
+# ---------------------------------------------------------------------------
+_ll = C.c_longlong
+
+
+def bin_info(path, lib: C.CDLL | None = None):
+    """(kind, count, aux) of an sdp binary file."""
+    lib = lib or load()
+    k, n, a = _i(0), _ll(0), _ll(0)
+    check(lib.sdp_bin_info(str(path).encode(), C.byref(k), C.byref(n), C.byref(a)), lib)
+    return k.value, n.value, a.value
+
+
+def bin_write_vis(path, uvw, vis, snapped=False, lib: C.CDLL | None = None):
+    lib = lib or load()
+    u, v = _f32(uvw, 3), _f32(vis, 2)
+    assert u.shape[0] == v.shape[0]
+    check(lib.sdp_bin_write_vis(str(path).encode(), _ll(u.shape[0]), _ptr(u), _ptr(v), _i(1 if snapped else 0)), lib)
+
+
+def bin_write_kernels(path, supports, samples, lib: C.CDLL | None = None):
+    lib = lib or load()
+    s = np.ascontiguousarray(supports, dtype=np.int32).reshape(-1, 2)
+    k = _f32(samples, 2)
+    check(lib.sdp_bin_write_kernels(str(path).encode(), _i(s.shape[0]), _ll(k.shape[0]), _ptr(s), _ptr(k)), lib)
+
+
+def bin_write_image(path, image, lib: C.CDLL | None = None):
+    lib = lib or load()
+    a = _f32(image)
+    assert a.ndim == 2
+    check(lib.sdp_bin_write_image(str(path).encode(), _i(a.shape[0]), _i(a.shape[1]), _ptr(a)), lib)
+
+
+def bin_read_vis_host(path, lib: C.CDLL | None = None):
+    """(uvw, vis, snapped) read into host arrays."""
+    lib = lib or load()
+    _, n, _ = bin_info(path, lib)
+    u = np.empty((n, 3), np.float32)
+    v = np.empty((n, 2), np.float32)
+    got, sn = _ll(0), _i(0)
+    check(lib.sdp_bin_read_vis_host(str(path).encode(), _ll(n), _ptr(u), _ptr(v), C.byref(got), C.byref(sn)), lib)
+    return u, v, bool(sn.value)
+
+
+# ---------------------------------------------------------------------------
 # Actor layer (host arrays)
 # ---------------------------------------------------------------------------
 class Actors:
@@ -409,8 +455,9 @@ def _stream(s=None):
 
 class PlanOptions(C.Structure):
     """Plan shape: uv tile side, visibilities per work item, lanes per
-    visibility (0 = default)."""
-    _fields_ = [("tile", _i), ("chunk", _i), ("lanes", _i)]
+    visibility (0: the warp-per-visibility kernel where it applies), warps per
+    CTA of that kernel (0 = by occupancy)."""
+    _fields_ = [("tile", _i), ("chunk", _i), ("lanes", _i), ("warps", _i)]
 
 
 class VisPlan:
@@ -647,6 +694,33 @@ class Device:
     def grid_to_image(self, grid_size, grid, prolate_ext, work, image, stream=None):
         check(self.lib.sdp_grid_to_image(_i(grid_size), _dp(grid), _dp(prolate_ext), _dp(work), _dp(image),
                                          _stream(stream)), self.lib)
+
+    def bin_load_vis(self, path, uvw, vis, stream=None):
+        """Loads a visibility file into device tensors uvw [n][3], vis [n][2]
+        (pinned staging, asynchronous copies); returns (n, snapped)."""
+        n, sn = _ll(0), _i(0)
+        check(self.lib.sdp_bin_load_vis(str(path).encode(), _ll(min(uvw.shape[0], vis.shape[0])), _dp(uvw), _dp(vis),
+                                        C.byref(n), C.byref(sn), _stream(stream)), self.lib)
+        return n.value, bool(sn.value)
+
+    def bin_load_kernels(self, path, supports, samples, stream=None):
+        """Loads a kernel-set file into device tensors supports [planes][2]
+        (int32) and samples [total][2]; returns (planes, total)."""
+        npl, tot = _i(0), _ll(0)
+        check(self.lib.sdp_bin_load_kernels(str(path).encode(), _i(supports.shape[0]), _ll(samples.shape[0]),
+                                            _dp(supports), _dp(samples), C.byref(npl), C.byref(tot),
+                                            _stream(stream)), self.lib)
+        return npl.value, tot.value
+
+    def bin_load_image(self, path, image, rows, cols, stream=None):
+        r, c = _i(0), _i(0)
+        check(self.lib.sdp_bin_load_image(str(path).encode(), _i(rows), _i(cols), _dp(image), C.byref(r), C.byref(c),
+                                          _stream(stream)), self.lib)
+        return r.value, c.value
+
+    def merge_grids(self, grid_size, slices, grids, out, stream=None):
+        """out = sum of `slices` contiguous G^2 grids (merge_gridded_visibilities)."""
+        check(self.lib.sdp_merge_grids(_i(grid_size), _i(slices), _dp(grids), _dp(out), _stream(stream)), self.lib)
 
     def image_to_grid(self, grid_size, image, work, grid, stream=None):
         check(self.lib.sdp_image_to_grid(_i(grid_size), _dp(image), _dp(work), _dp(grid), _stream(stream)),

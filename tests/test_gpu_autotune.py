@@ -61,12 +61,15 @@ def _run(sdp, device, st, options):
     return res.cpu().numpy(), pred.cpu().numpy(), grid.cpu().numpy(), deg.cpu().numpy(), opts
 
 
-@pytest.mark.parametrize("tile,chunk,lanes", [(16, 512, 0), (64, 2048, 0), (32, 1024, 16), (64, 64, 32),
-                                              (8, 4096, 0)])
-def test_plan_shapes_agree(sdp, device, setup, tile, chunk, lanes):
+@pytest.mark.parametrize("tile,chunk,lanes,warps", [(16, 512, 0, 0), (64, 2048, 0, 0), (32, 1024, 16, 0),
+                                                    (64, 64, 32, 0), (8, 4096, 0, 0), (24, 256, 0, 4),
+                                                    (32, 1024, 8, 0), (16, 300, 0, 8)])
+def test_plan_shapes_agree(sdp, device, setup, tile, chunk, lanes, warps):
+    """Warp-per-visibility kernel (lanes 0) and the group kernels (8 / 16 /
+    32 lanes) over tile sides and work-item sizes against the default plan."""
     ref = _run(sdp, device, setup, None)
-    got = _run(sdp, device, setup, sdp.PlanOptions(tile, chunk, lanes))
-    assert (got[4].tile, got[4].chunk, got[4].lanes) == (tile, chunk, lanes)
+    got = _run(sdp, device, setup, sdp.PlanOptions(tile, chunk, lanes, warps))
+    assert (got[4].tile, got[4].chunk, got[4].lanes, got[4].warps) == (tile, chunk, lanes, warps)
     assert (ref[4].tile, ref[4].chunk) == (32, 1024)
     for a, b in zip(got[:4], ref[:4]):
         assert rel_rms(a, b) <= 1e-6
@@ -75,8 +78,8 @@ def test_plan_shapes_agree(sdp, device, setup, tile, chunk, lanes):
 def test_bad_options_rejected(sdp, device, setup):
     import torch
     w, G = setup["w"], setup["G"]
-    for o in (sdp.PlanOptions(24, 0, 0), sdp.PlanOptions(0, 10, 0), sdp.PlanOptions(0, 0, 12),
-              sdp.PlanOptions(0, 0, 8 if setup["w"].half_support > 4 else 4)):
+    for o in (sdp.PlanOptions(20, 0, 0), sdp.PlanOptions(0, 10, 0), sdp.PlanOptions(0, 0, 12),
+              sdp.PlanOptions(0, 0, 8 if setup["w"].half_support > 4 else 4), sdp.PlanOptions(0, 0, 0, 6)):
         with pytest.raises(sdp.SdpError):
             device.plan(G, setup["OS"], w.cfg.uv_scale, w.cfg.w_scale, setup["uvw"], setup["wg"], setup["wd"],
                         keep=setup["keep"], options=o)
@@ -88,8 +91,9 @@ def test_autotune_picks_a_valid_shape(sdp, device, setup):
     scratch = torch.empty((G * G, 2), dtype=torch.float32, device="cuda")
     best, ms, cand = device.autotune(G, setup["OS"], w.cfg.uv_scale, w.cfg.w_scale, setup["uvw"], setup["wg"],
                                      setup["wd"], setup["meas"], setup["model"], scratch)
-    assert cand >= 9 and ms > 0
-    assert best.tile in (16, 32, 64) and best.chunk in (512, 1024, 2048) and best.lanes in (0, 16)
+    assert cand >= 20 and ms > 0
+    assert best.tile in (8, 16, 24, 32) and best.chunk in (256, 512, 1024) and best.lanes in (0, 8, 16)
+    assert best.warps in (0, 4, 8)
     ref = _run(sdp, device, setup, None)
     got = _run(sdp, device, setup, best)
     for a, b in zip(got[:4], ref[:4]):
