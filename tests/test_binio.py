@@ -70,7 +70,7 @@ def test_csv_to_binary_is_exact(sdp, lib, tmp_path):
     np.testing.assert_array_equal(v, vis)
 
 
-def test_bad_files_refused(sdp, tmp_path):
+def test_bad_files_refused(sdp, lib, tmp_path):
     with pytest.raises(sdp.SdpError) as e:
         sdp.bin_info(tmp_path / "missing.bin")
     assert e.value.status == sdp.SDP_ERR_IO
@@ -91,6 +91,7 @@ def test_bad_files_refused(sdp, tmp_path):
     with pytest.raises(sdp.SdpError) as e:
         sdp.bin_read_vis_host(tmp_path / "i.bin")
     assert e.value.status == sdp.SDP_ERR_DATA
+    lib.sdp_clear_error()  # the status is thread-local and outlives the call
 
 
 @pytest.mark.gpu

@@ -98,6 +98,7 @@ def test_visibility_host_set_up(lib, tmp_path, ra, w1, n_rec, declared, partial)
                      force_weight_to_one=w1, max_w=1500.0)
     uvw = np.zeros((declared, 3), np.float32)
     vis = np.zeros((declared, 2), np.float32)
+    lib.sdp_clear_error()
     lib.visibility_host_set_up(_i(declared), C.byref(cfg), uvw.ctypes.data_as(_p), vis.ctypes.data_as(_p))
     assert lib.sdp_last_status() == 0
     toks = path.read_text().split()[1:]
