@@ -72,6 +72,9 @@ def parse():
     ap.add_argument("--no-c4", action="store_true", help="skip the learned-proposal comparison")
     ap.add_argument("--no-extras", action="store_true", help="headline only (no FFT / calibration blocks)")
     ap.add_argument("--c4-skies", type=int, default=100, help="held-out skies of the learned-proposal comparison")
+    ap.add_argument("--c5-skies", type=int, default=2, help="held-out skies of the 8192^2 learned comparison")
+    ap.add_argument("--channels", type=int, default=C5_CHANNELS,
+                    help="headline on the first K of the 16 channels (profiling captures of a few GB)")
     ap.add_argument("--cpu-sample", type=int, default=1_000_000,
                     help="visibilities per channel per step of the reference arm / CPU baseline")
     return ap.parse_args()
@@ -553,6 +556,40 @@ def c5_major_cycle_block(S, D, dev, c5: "C5Device", reps: int = 2):
     return out
 
 
+def c5_learned_block(S, D, dev, base, shape, skies: int = 2):
+    """Learned proposals against plain Hogbom on the 8192^2 workload: all 16
+    channels imaged into one continuum image (learned.ContinuumImaging), sky
+    of 1000 points + 50 Gaussians (FWHM 2-10 px) per held-out seed, DFT
+    predict, 200 Hogbom minor cycles per plain major cycle (10 cycles); the
+    learned pipeline (the network trained at 1024^2 on the 10 km array,
+    proposals verified by an exact predict/grid cycle, Hogbom fallback) runs
+    until the plain final FP64 residual RMS x 1.01."""
+    import torch
+    import learned as L
+    G, cell = base.cfg.grid_size, base.cfg.cell_size
+    chans = [np.ascontiguousarray(base.uvw * np.float32(f / C5_F_HI)) for f in c5_frequencies()]
+    opts = S.PlanOptions(shape["tile"], shape["chunk"], shape["lanes"], shape["warps"]) if shape else None
+    t0 = time.perf_counter()
+    img = L.ContinuumImaging(D, chans, G, cell, base.cfg.max_w, num_planes=C5_PLANES, half_support=C5_HS,
+                             oversampling=C5_OS, options=opts)
+    setup_s = time.perf_counter() - t0
+    del chans
+    sampler = L.SkySampler(G, cell, seed=991, points=(1000, 1000), gaussians=(50, 50))
+    rows = L.evaluate(img, L.load_weights(), skies, seed=991, sampler=sampler, max_components=512)
+    img.close()
+    torch.cuda.empty_cache()
+    sp = [r["plain_s"] / r["learned_s"] for r in rows if r["learned_s"]]
+    return {"workload": "16 channels 100-200 MHz continuum, 418611200 vis, G=8192, 64 w-planes hs=4; held-out skies "
+                        "of 1000 points + 50 Gaussians (FWHM 2-10 px)",
+            "skies": len(rows), "reached": len(sp), "setup_s": setup_s,
+            "plain": "10 major cycles x 200 Hogbom minor cycles (gain 0.1), DFT predict over all channels",
+            "target": "plain final FP64 residual RMS x 1.01",
+            "speedup": sp, "speedup_median": float(statistics.median(sp)) if sp else None,
+            "rows": [{k: r[k] for k in ("plain_s", "learned_s", "learned_cycles", "learned_kinds", "rms0",
+                                        "plain_final", "learned_final", "plain_rms", "learned_rms")}
+                     for r in rows]}
+
+
 def unet_flops(n: int, h: int, w: int, base: int = 32, backward: bool = False) -> int:
     """Tensor FLOPs (2 per multiply-add) of the U-Net's 3x3 convolutions and
     head for n images of h x w; backward: the data gradients (all but the
@@ -934,7 +971,8 @@ def b200_arm(args):
     # ---- the 8192^2 workload: this rank's channels on the device ---------------------
     base = c5_base()
     G, OS = base.cfg.grid_size, base.cfg.oversampling
-    counts_all = [base.num_vis] * C5_CHANNELS
+    nch = max(1, min(C5_CHANNELS, args.channels))
+    counts_all = [base.num_vis] * nch
     owned = channels.assign_channels(counts_all, world)[rank]
     total_vis = int(sum(counts_all))
     t0 = time.perf_counter()
@@ -1087,8 +1125,11 @@ def b200_arm(args):
         if not args.no_major_cycle and not args.no_extras:
             extras["c5_major_cycle_8192"] = c5_major_cycle_block(S, D, dev, c5)
     c5.close()
-    del c5, flush
+    c5 = None
+    del flush
     torch.cuda.empty_cache()
+    if world == 1 and not args.no_c4:
+        extras["c5_learned"] = c5_learned_block(S, D, dev, base, tune, skies=args.c5_skies)
     if world == 1:
         if not args.no_c2:
             extras["c2_2048"] = c2_block(S, D, dev, args)
@@ -1104,7 +1145,8 @@ def b200_arm(args):
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
         "warmup": max(3, args.warmup), "ms_per_step": t_step, "higher_is_better": True, "scaling": "strong",
         "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-        "config": {"workload": c5_config_name(total_vis),
+        "config": {"workload": c5_config_name(total_vis) + ("" if nch == C5_CHANNELS else
+                                                            f" (first {nch} of the 16 channels)"),
                    "channels_per_rank": [len(o) for o in channels.assign_channels(counts_all, world)],
                    "degrid": "convolutional (normalised, degridgrid.c:147-191)",
                    "measured": "exact DFT of 1000 points + 50 Gaussians (sdp_dft_gauss) + 0.1 mJy noise",

@@ -145,8 +145,15 @@ struct Lines {
     int G, first, L;
     __device__ __forceinline__ int row(int l, int i) const { return ROWS ? first + l : i; }
     __device__ __forceinline__ int col(int l, int i) const { return ROWS ? i : first + l; }
-    // shared memory: rows line-major, columns element-major (lines interleaved)
-    __device__ __forceinline__ int sidx(int l, int i, int N) const { return ROWS ? l * N + i : i * L + l; }
+    // shared memory: rows line-major, columns element-major (lines
+    // interleaved), with one padding element after every 16: the first
+    // radix-16 stage writes at a stride of 16 elements (128 bytes), which
+    // without the padding puts a warp's stores on one bank pair
+    __device__ __forceinline__ int sidx(int l, int i, int N) const
+    {
+        const int k = ROWS ? l * N + i : i * L + l;
+        return k + (k >> 4);
+    }
 };
 
 template <bool ROWS>
@@ -353,7 +360,7 @@ static int launch_pass(int G, const void *in, void *out, const float2 *tw, bool 
     A.load_op = load_op;
     A.store_op = store_op;
     const int threads = std::max(32, (A.L * G) / kElemsPerThread);
-    const size_t smem = sizeof(float2) * (size_t)A.L * G;
+    const size_t smem = sizeof(float2) * ((size_t)A.L * G + (size_t)A.L * G / 16);  // + the padding (sidx)
     switch (G) {
     case 16: return launch_pass_n<ROWS, 4>(A, G, smem, threads, st);
     case 32: return launch_pass_n<ROWS, 5>(A, G, smem, threads, st);

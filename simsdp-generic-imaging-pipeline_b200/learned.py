@@ -107,6 +107,72 @@ class Imaging:
         self.plan.close()
 
 
+class ContinuumImaging:
+    """Several channels imaged into one continuum (multi-frequency) image,
+    with the interface Deconvolver uses: the visibilities of all channels
+    are one array (channel-major), so a DFT predict or a sky's visibilities
+    is one launch over every channel (uvw in wavelengths carry the
+    frequency); image() grids each channel with its own plan into one
+    continuum grid (accumulating), then FFT + taper, in flux units of the
+    continuum PSF's peak.  channel_uvw: raw uvw (wavelengths) per channel;
+    the geometry (cell, max_w) is shared.  Kernels are generated on the GPU."""
+
+    def __init__(self, D: S.Device, channel_uvw, grid_size: int, cell: float, max_w: float, num_planes: int = 64,
+                 half_support: int = 4, oversampling: int = 16, options: "S.PlanOptions | None" = None):
+        torch = _torch()
+        self.D = D
+        G = self.G = grid_size
+        dev = self.dev = torch.device("cuda", torch.cuda.current_device())
+        self.layout = ArrayLayout(np.zeros((0, 3), np.float32), G, cell, max_w)
+        fov = cell * G
+        us, ws = cell * G, (num_planes - 1) ** 2 / max_w
+        self.gk, self.dk, self.sup = D.wkernels_generate([half_support] * num_planes, oversampling, max_w, fov)
+        sup_h = self.sup.cpu().numpy()
+        self.wk = S.Device.wkernels(self.gk, self.sup, sup_h)
+        counts = [int(u.shape[0]) for u in channel_uvw]
+        self.offsets = np.concatenate([[0], np.cumsum(counts)]).astype(np.int64)
+        self.n = int(self.offsets[-1])
+        self.uvw_raw = torch.empty((self.n, 3), dtype=torch.float32, device=dev)
+        self.plans = []
+        snapped = torch.empty((max(counts), 3), dtype=torch.float32, device=dev)
+        for c, u in enumerate(channel_uvw):
+            a, b = int(self.offsets[c]), int(self.offsets[c + 1])
+            raw = self.uvw_raw[a:b]
+            raw.copy_(torch.as_tensor(u, device=dev))
+            sn = snapped[: b - a]
+            D.correct_to_finegrid(G, oversampling, us, raw, sn)
+            self.plans.append(D.plan(G, oversampling, us, ws, sn, self.wk, self.wk,
+                                     keep=(self.gk, self.dk, self.sup), options=options))
+        torch.cuda.synchronize()
+        del snapped
+        self.prol = torch.empty(G // 2 + 1, dtype=torch.float32, device=dev)
+        D.prolate_table(G, self.prol)
+        self.grid = torch.empty((G * G, 2), dtype=torch.float32, device=dev)
+        self.work = torch.empty_like(self.grid)
+        # continuum PSF: unit visibilities of every channel, imaged; peak 1
+        ones = torch.zeros((max(counts), 2), dtype=torch.float32, device=dev)
+        ones[:, 0] = 1.0
+        for c, pl in enumerate(self.plans):
+            pl.grid(ones[: int(self.offsets[c + 1] - self.offsets[c])], self.grid, accumulate=c > 0)
+        del ones
+        self.psf = torch.empty(G * G, dtype=torch.float32, device=dev)
+        D.grid_to_image(G, self.grid, self.prol, self.work, self.psf)
+        self.psf_max = float(self.psf.max().item())
+        self.psf /= self.psf_max
+
+    def image(self, vis, out):
+        """out (G^2) = continuum image of vis (all channels) in flux units."""
+        for c, pl in enumerate(self.plans):
+            pl.grid(vis[int(self.offsets[c]):int(self.offsets[c + 1])], self.grid, accumulate=c > 0)
+        self.D.grid_to_image(self.G, self.grid, self.prol, self.work, out)
+        self.D.scale(out, 1.0 / self.psf_max)
+
+    def close(self):
+        for pl in self.plans:
+            pl.close()
+        self.plans = []
+
+
 class SkySampler:
     """Seeded skies: 10-500 points (log-uniform 1e-3-1 Jy) and 0-20 circular
     Gaussians (FWHM 2-10 px, log-uniform 1e-2-1 Jy), centred on pixels in
@@ -513,14 +579,15 @@ def time_to_target(recs, target: float):
     return None, None
 
 
-def evaluate(img: Imaging, params: np.ndarray, skies: int, seed: int = 777, plain_cycles: int = 10,
-             max_learned_cycles: int = 10, noise_sigma: float = 1e-4, verbose: bool = False, **kw):
+def evaluate(img, params: np.ndarray, skies: int, seed: int = 777, plain_cycles: int = 10,
+             max_learned_cycles: int = 10, noise_sigma: float = 1e-4, verbose: bool = False, sampler=None, **kw):
     """Held-out skies: the plain pipeline runs plain_cycles Hogbom cycles; its
-    final RMS x 1.01 is the target the learned pipeline must reach.  Returns
-    one dict per sky."""
+    final RMS x 1.01 is the target the learned pipeline must reach.  img is
+    an Imaging (one channel) or a ContinuumImaging (several channels).
+    Returns one dict per sky."""
     torch = _torch()
     dec = Deconvolver(img, params, **kw)
-    sampler = SkySampler(img.G, img.layout.cell, seed)
+    sampler = sampler or SkySampler(img.G, img.layout.cell, seed)
     gen = torch.Generator(device=img.dev).manual_seed(seed + 1)
     meas = torch.empty((img.n, 2), dtype=torch.float32, device=img.dev)
     rows = []
@@ -534,7 +601,9 @@ def evaluate(img: Imaging, params: np.ndarray, skies: int, seed: int = 777, plai
         tl, cl = time_to_target(lrn, target)
         row = dict(sky=k, components=int(comps.shape[0]), rms0=rms0, plain_final=plain[-1].rms, target=target,
                    plain_s=tp, plain_cycles=cp, learned_s=tl, learned_cycles=cl,
-                   learned_kinds="".join(r.kind[0] for r in lrn), learned_final=lrn[-1].rms)
+                   learned_kinds="".join(r.kind[0] for r in lrn), learned_final=lrn[-1].rms,
+                   plain_rms=[r.rms for r in plain], learned_rms=[r.rms for r in lrn],
+                   learned_seconds=[r.seconds for r in lrn], plain_seconds=[r.seconds for r in plain])
         rows.append(row)
         if verbose:
             print(row, flush=True)
