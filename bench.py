@@ -820,6 +820,10 @@ def c4_learned_block(S, D, dev, skies: int):
         "plain_ms_median": med([r["plain_s"] * 1e3 for r in rows]),
         "learned_ms_median": med([r["learned_s"] * 1e3 for r in rows if r["learned_s"]]),
         "learned_cycles": [r["learned_cycles"] for r in rows], "learned_kinds": [r["learned_kinds"] for r in rows],
+        "learned_rms_ratio": [[round(b / a, 3) for a, b in zip([r["rms0"]] + r["learned_rms"][:-1], r["learned_rms"])]
+                              for r in rows],
+        "plain_rms_ratio": [[round(b / a, 3) for a, b in zip([r["rms0"]] + r["plain_rms"][:-1], r["plain_rms"])]
+                            for r in rows[:8]],
         "at_2048": {"skies": len(rows2), "reached": sum(1 for r in rows2 if r["learned_s"]),
                     "speedup_median": med(sp2),
                     "speedup_geomean": float(np.exp(np.mean(np.log(sp2)))) if sp2 else None,

@@ -46,6 +46,16 @@ def weighted_rel_rms(a, b, G):
     return rel_rms(np.asarray(a, np.float64) * t, np.asarray(b, np.float64) * t)
 
 
+def inner_rel_rms(a, b, G):
+    """Unweighted rel-RMS over the inner half of the image (|x|, |y| < G/4
+    from the centre), where the taper correction divides by at least
+    prolate(1/2)^2 ~ 0.13."""
+    sl = slice(G // 4, 3 * G // 4)
+    a = np.asarray(a, np.float64).reshape(G, G)[sl, sl]
+    b = np.asarray(b, np.float64).reshape(G, G)[sl, sl]
+    return rel_rms(a, b)
+
+
 def _setup(seed=17, G=256, minor=60):
     w = synth.small_workload(seed=seed, grid_size=G, n_ant=24, n_time=20, num_planes=5, half_support=3,
                              oversampling=16, n_src=6)
@@ -99,7 +109,11 @@ def test_pipeline_float_build_matches_oracle(sdp, device, oracle32, nearest):
         assert rel_rms(model_g, model_r) <= 1e-4
 
 
-def test_pipeline_fp64_coordinates_within_1e4_of_fp64_oracle(sdp, device, oracle64):
+def test_pipeline_fp64_coordinates_within_1e4_of_fp64_oracle(sdp, device, oracle64, record_property):
+    """Every image within 1e-4 rel-RMS of the FP64 oracle, taper-weighted
+    (the domain the FFT and gridding produce); the unweighted figures over
+    the inner half and over the whole image (dominated by the edge pixels,
+    where the taper correction divides by ~1e-8) are recorded beside it."""
     w, uvw, vis, minor = _setup(seed=23)
     G = w.cfg.grid_size
     psf, psf_max = O.dirty_psf(oracle64, G, 16, uvw, w.gkernels, w.supports, w.cfg.uv_scale, w.cfg.w_scale)
@@ -108,7 +122,10 @@ def test_pipeline_fp64_coordinates_within_1e4_of_fp64_oracle(sdp, device, oracle
     got, _ = _gpu_pipeline(sdp, device, w, uvw, vis, psf.astype(np.float32), psf_max, 3, minor,
                            sdp.SDP_COORD_F64, False, False)
     for k, ((img_r, model_r, n_r, src_r), (img_g, model_g, src_g, n_g)) in enumerate(zip(ref, got)):
-        assert weighted_rel_rms(img_g, img_r, G) <= FP64_IMAGE_TOL, (k, weighted_rel_rms(img_g, img_r, G))
+        wr, ir, ur = weighted_rel_rms(img_g, img_r, G), inner_rel_rms(img_g, img_r, G), rel_rms(img_g, img_r)
+        record_property(f"cycle{k}_rel_rms", {"taper_weighted": wr, "unweighted_inner_half": ir,
+                                               "unweighted_whole_image": ur})
+        assert wr <= FP64_IMAGE_TOL, (k, wr)
         assert n_g == n_r
         np.testing.assert_array_equal(src_g[:, :2], src_r[:, :2].astype(np.float32))
 
