@@ -73,6 +73,8 @@ def parse():
     ap.add_argument("--no-extras", action="store_true", help="headline only (no FFT / calibration blocks)")
     ap.add_argument("--c4-skies", type=int, default=100, help="held-out skies of the learned-proposal comparison")
     ap.add_argument("--c5-skies", type=int, default=2, help="held-out skies of the 8192^2 learned comparison")
+    ap.add_argument("--c2-only", action="store_true", help="only the single 2048^2 channel block (profiling)")
+    ap.add_argument("--c2-shape", default="", help="tile,chunk,lanes,warps for the 2048^2 block (no autotune)")
     ap.add_argument("--channels", type=int, default=C5_CHANNELS,
                     help="headline on the first K of the 16 channels (profiling captures of a few GB)")
     ap.add_argument("--cpu-sample", type=int, default=1_000_000,
@@ -441,7 +443,7 @@ class C5Device:
     model grid (the model image is channel independent; its grid is too) and
     one residual grid per channel."""
 
-    def __init__(self, S, D, dev, base, owned, tune: bool = True, keep_host: bool = True):
+    def __init__(self, S, D, dev, base, owned, tune: bool = True, keep_host: bool = True, shape=None):
         import torch
         self.S, self.D, self.dev = S, D, dev
         G, OS = base.cfg.grid_size, base.cfg.oversampling
@@ -465,7 +467,7 @@ class C5Device:
         uvw_top = torch.from_numpy(base.uvw).to(dev)
         freqs = c5_frequencies()
         self.resid = torch.empty((max(1, len(owned)), G * G, 2), dtype=torch.float32, device=dev)
-        self.shape = None
+        self.shape = shape
         self.tune = None
         self.plans, self.counts, self.host = [], [], []
         order = sorted(owned, key=lambda c: -freqs[c])  # the top channel first (autotuned on)
@@ -871,8 +873,11 @@ def c2_block(S, D, dev, args, clocks_mhz=None):
     D.image_to_grid(G, model_img, work, model_grid)
     residual = torch.empty((G * G, 2), dtype=torch.float32, device=dev)
     t_tune = time.perf_counter()
-    shape, tuned_ms, n_shapes = D.autotune(G, OS, w.cfg.uv_scale, w.cfg.w_scale, uvw, wk_g, wk_d, measured,
-                                          model_grid, residual, reps=5)
+    if args.c2_shape:
+        shape, tuned_ms, n_shapes = S.PlanOptions(*[int(x) for x in args.c2_shape.split(",")]), None, 0
+    else:
+        shape, tuned_ms, n_shapes = D.autotune(G, OS, w.cfg.uv_scale, w.cfg.w_scale, uvw, wk_g, wk_d, measured,
+                                              model_grid, residual, reps=5)
     tune = {"tile": shape.tile, "chunk": shape.chunk, "lanes": shape.lanes, "warps": shape.warps,
             "ms_per_pass": tuned_ms, "shapes_timed": n_shapes, "seconds": time.perf_counter() - t_tune}
     plan = D.plan(G, OS, w.cfg.uv_scale, w.cfg.w_scale, uvw, wk_g, wk_d, keep=(uvw, gk, dk, sup), options=shape)
@@ -971,6 +976,9 @@ def b200_arm(args):
     D = S.Device(lib)
     A = S.Actors(lib)
     stream = torch.cuda.current_stream()
+    if args.c2_only:
+        print(json.dumps({"c2_2048": c2_block(S, D, dev, args)}), flush=True)
+        return 0
 
     # ---- the 8192^2 workload: this rank's channels on the device ---------------------
     base = c5_base()

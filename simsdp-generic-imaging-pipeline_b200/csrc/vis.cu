@@ -32,7 +32,7 @@
 
 namespace sdp {
 
-constexpr int kTile = 32;    // default uv tile side
+constexpr int kTile = 16;    // default uv tile side
 constexpr int kChunk = 1024;  // default visibilities per work item
 constexpr int kMaxHalfSupport = 15;
 
@@ -883,7 +883,7 @@ __device__ __forceinline__ void reduce4x5(const float (&v)[kFastVB][5], float (&
 // OP is OP_GRID, OP_DEGRID or OP_CYCLE_CONV.  smem: the model tile (OP !=
 // OP_GRID) and NW private subgrids (OP != OP_DEGRID), S rows of P.pitch cells.
 template <typename T, int OP, int NW>
-__device__ __forceinline__ void fast_item(const PlanDev &P, const int4 it, float2 *mtile, float2 *subs,
+__device__ __forceinline__ void fast_item(const PlanDev &Pin, const int4 it, float2 *mtile, float2 *subs,
                                           float *wscr_all, const int4 *planes, bool share, float share_sign,
                                           const float2 *__restrict__ vis_in, const float2 *__restrict__ in_grid,
                                           float2 *__restrict__ out_grid, float2 *__restrict__ pred_out,
@@ -891,6 +891,9 @@ __device__ __forceinline__ void fast_item(const PlanDev &P, const int4 it, float
 {
     constexpr bool kGrids = (OP != OP_DEGRID);
     constexpr bool kConv = (OP != OP_GRID);
+    // a private copy: the batch kernel's description lives in shared memory,
+    // where every read would be repeated after each subgrid store
+    const PlanDev P = Pin;
     const int S = P.S, pitch = P.pitch, OS = P.OS;
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const int c = lane & 7, r = lane >> 3;
@@ -908,11 +911,27 @@ __device__ __forceinline__ void fast_item(const PlanDev &P, const int4 it, float
         __syncthreads();
     }
 
+    // the loads of a batch's geometry are issued one batch ahead, and its
+    // measured values at the start of the batch, so their latency overlaps
+    // the previous batch's work
+    uint2 gn[kFastVB];
+    {
+        const int b0 = it.y + warp * kFastVB;
+#pragma unroll
+        for (int j = 0; j < kFastVB; ++j) gn[j] = (b0 + j < it.z) ? P.geo[b0 + j] : make_uint2(0u, 0u);
+    }
     for (int b = it.y + warp * kFastVB; b < it.z; b += NW * kFastVB) {
         const int nv = min(kFastVB, it.z - b);  // visibilities in this batch (warp-uniform)
         uint2 g[kFastVB];
 #pragma unroll
-        for (int j = 0; j < kFastVB; ++j) g[j] = (j < nv) ? P.geo[b + j] : make_uint2(0u, 0u);
+        for (int j = 0; j < kFastVB; ++j) g[j] = gn[j];
+        {
+            const int bn = b + NW * kFastVB;
+#pragma unroll
+            for (int j = 0; j < kFastVB; ++j) gn[j] = (bn + j < it.z) ? P.geo[bn + j] : make_uint2(0u, 0u);
+        }
+        float2 meas_r = make_float2(0.f, 0.f);  // lanes 8 j ..: visibility j's measured value
+        if (OP == OP_CYCLE_CONV && r < nv) meas_r = measured[b + r];
         // per visibility: this lane's two taps (kernel samples and cell)
         float2 k0[kFastVB], k1[kFastVB];
         int cell[kFastVB];
@@ -997,7 +1016,7 @@ __device__ __forceinline__ void fast_item(const PlanDev &P, const int4 it, float
             if (j < nv) {
                 const int i = b + j;
                 if (OP == OP_CYCLE_CONV) {
-                    const float2 m = measured[i];
+                    const float2 m = meas_r;
                     gval = make_float2(__fsub_rn(m.x, value.x), __fsub_rn(m.y, value.y));
                     if (c == 0 && (pred_out || delta_out)) {
                         const int o = P.perm[i];
