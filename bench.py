@@ -577,13 +577,17 @@ def c5_learned_block(S, D, dev, base, shape, skies: int = 2):
     setup_s = time.perf_counter() - t0
     del chans
     sampler = L.SkySampler(G, cell, seed=991, points=(1000, 1000), gaussians=(50, 50))
-    rows = L.evaluate(img, L.load_weights(), skies, seed=991, sampler=sampler, max_components=512)
+    c5w = L.WEIGHTS_C5.exists()
+    rows = L.evaluate(img, L.load_weights(L.WEIGHTS_C5 if c5w else L.WEIGHTS), skies, seed=991, sampler=sampler,
+                      max_components=512)
     img.close()
     torch.cuda.empty_cache()
     sp = [r["plain_s"] / r["learned_s"] for r in rows if r["learned_s"]]
     return {"workload": "16 channels 100-200 MHz continuum, 418611200 vis, G=8192, 64 w-planes hs=4; held-out skies "
                         "of 1000 points + 50 Gaussians (FWHM 2-10 px)",
             "skies": len(rows), "reached": len(sp), "setup_s": setup_s,
+            "network": ("weights/unet_c5.npz: trained on the 40 km array's 16-channel continuum (2048^2 images with "
+                        "this cell, every 8th time step)") if c5w else "weights/unet_c4.npz (10 km array, 1024^2)",
             "plain": "10 major cycles x 200 Hogbom minor cycles (gain 0.1), DFT predict over all channels",
             "target": "plain final FP64 residual RMS x 1.01",
             "speedup": sp, "speedup_median": float(statistics.median(sp)) if sp else None,

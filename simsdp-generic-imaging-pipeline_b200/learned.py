@@ -36,6 +36,8 @@ import sdp_b200 as S
 import synth
 
 WEIGHTS = Path(__file__).resolve().parent / "weights" / "unet_c4.npz"
+# network trained for the 512-antenna 40 km array's 16-channel continuum PSF
+WEIGHTS_C5 = Path(__file__).resolve().parent / "weights" / "unet_c5.npz"
 
 
 def _torch():
@@ -66,6 +68,25 @@ def spiral_layout(grid_size: int = 1024, n_ant: int = 256, radius_m: float = 500
     uvw = synth.uvw_tracks(enu, -27.0, -30.0, np.linspace(-1.0, 1.0, n_time), freq_hz)
     uv_max = float(np.max(np.abs(uvw[:, :2])))
     return ArrayLayout(uvw.astype(np.float32), grid_size, 0.45 / uv_max, float(np.max(np.abs(uvw[:, 2]))) * 1.0001)
+
+
+def c5_channels(time_stride: int = 1, n_channels: int = 16, f_lo: float = 100e6, f_hi: float = 200e6,
+                seed: int = 5):
+    """The 512-antenna, 40 km log spiral (seed 5), 200 time steps over +-1 h,
+    n_channels evenly spaced over f_lo-f_hi: (per-channel uvw in wavelengths,
+    cell, max_w), the cell chosen so the longest baseline at f_hi reaches 0.9
+    of the half grid (uv_max * cell * G = 0.45 G, for any G), max_w the
+    largest |w| at f_hi.  Every time_stride-th time step is kept (1: all)."""
+    rng = np.random.default_rng(seed)
+    enu = synth.layout_log_spiral(512, 20000.0, rng)
+    top = synth.uvw_tracks(enu, -27.0, -30.0, np.linspace(-1.0, 1.0, 200), f_hi)
+    uv_max = float(np.max(np.abs(top[:, :2])))
+    cell = 0.45 / uv_max
+    max_w = float(np.max(np.abs(top[:, 2]))) * 1.0001
+    nbl = top.shape[0] // 200
+    sub = top.reshape(200, nbl, 3)[::time_stride].reshape(-1, 3)
+    freqs = [f_lo + (f_hi - f_lo) * c / (n_channels - 1) for c in range(n_channels)]
+    return [np.ascontiguousarray((sub * (f / f_hi)).astype(np.float32)) for f in freqs], cell, max_w
 
 
 class Imaging:
@@ -627,6 +648,9 @@ def main(argv=None) -> int:
     ap.add_argument("--weights", type=Path, default=WEIGHTS)
     ap.add_argument("--eval-skies", type=int, default=8)
     ap.add_argument("--log", type=Path, default=None)
+    ap.add_argument("--config", choices=["c4", "c5"], default="c4",
+                    help="c4: one channel of the 10 km array; c5: the 40 km array's 16-channel continuum "
+                         "(every 8th time step, imaged at --grid with the 8192^2 image's cell)")
     a = ap.parse_args(argv)
     torch.cuda.init()
     D = S.Device()
@@ -645,7 +669,13 @@ def main(argv=None) -> int:
         print(f"forward {a.grid}^2: {e0.elapsed_time(e1):.3f} ms")
         net.close()
         return 0
-    img = Imaging(D, spiral_layout(a.grid))
+    if a.config == "c5":
+        chans, cell, max_w = c5_channels(time_stride=8)
+        img = ContinuumImaging(D, chans, a.grid, cell, max_w)
+        if a.out == WEIGHTS:
+            a.out = WEIGHTS_C5
+    else:
+        img = Imaging(D, spiral_layout(a.grid))
     if a.cmd == "train":
         params, log = train(img, TrainConfig(skies=a.skies))
         save_weights(params, a.out)
