@@ -34,7 +34,7 @@ struct sdp_visplan {
     int lanes = 0;                // lanes per visibility of the group kernels (0: warp-per-visibility kernel)
     int warps = 0;                // warps per CTA of the warp-per-visibility kernel (0: by occupancy)
     int pitch = 0;                // row pitch (float2) of the shared tiles: >= S, = 8 mod 16
-    uint2 *geo = nullptr;         // plan order: packed tap-box geometry (fast path), see k_bin
+    uint4 *geo = nullptr;         // plan order: packed tap-box geometry (fast path), see fast_geometry
     void *rec = nullptr;          // Rec<float> or Rec<double>
     int coord_f64 = 0;            // index arithmetic of the double build
     int snap = 0;                 // correct_to_finegrid applied to the uvw at plan build

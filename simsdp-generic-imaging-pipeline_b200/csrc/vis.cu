@@ -64,7 +64,7 @@ struct PlanDev {
     int *flags;
     const int *kdiff;  // bit 0: degridding set != gridding set; bit 1: != its conjugate
     int pitch;          // row pitch (float2) of the shared tiles of the warp-per-visibility kernels
-    const uint2 *geo;   // packed tap-box geometry in plan order (see k_bin)
+    const uint4 *geo;   // packed tap-box geometry in plan order (see fast_geometry)
     const int *perm;    // plan position -> original visibility index
 };
 
@@ -203,20 +203,38 @@ __host__ __device__ __forceinline__ int fast_kidx(int i, int hs, int os, int ko,
     return i < hs ? os * (hs - i) - ko + h : os * (i - hs) + ko;
 }
 
-// Packed tap-box geometry of a visibility for the warp-per-visibility kernels:
+// Offsets of kernel sample (ky, kx) within a plane of half support A - 1, in
+// the plan's table layout (phase-major for power-of-two OS, see kcol / krow
+// below: pm = 1), as the plan build computes them.
+__device__ __forceinline__ int geo_kcol(int kx, int A, int pm, int OS, int shift)
+{
+    return pm ? ((kx & (OS - 1)) * A * A + (kx >> shift)) : kx;
+}
+__device__ __forceinline__ int geo_krow(int ky, int A, int pm, int OS, int shift)
+{
+    return pm ? ((ky & (OS - 1)) * OS * A * A + (ky >> shift) * A) : ky * A * OS;
+}
+
+// Packed tap-box geometry of a visibility for the warp-per-visibility kernels
+// (16 bytes):
 //   x: box origin in the tile (bits 0-7: column, 8-15: row), w-plane (16-31);
-//   y: ko of the columns (0-7) and rows (8-15), h of the columns (16) and
-//      rows (17), kernel conjugated (18: w < 0), fast path (19).
+//   y: CN (0-15), CP (16-31): table offsets of the columns; tap column i < hs
+//      sits at CN - i * SC, column i >= hs at CP + (i - hs) * SC;
+//   z: RN (0-15), RP (16-31): the same for the rows with step RS;
+//   w: hs (0-3), kernel conjugated (4: w < 0), fast path (5).
+// SC = 1, RS = hs + 1 in the phase-major layout (SC = OS, RS = (hs + 1) OS
+// otherwise): below the visibility the kernel index falls by OS per tap
+// (the phase stays, the block index falls by one), above it rises by OS.
 // Fast path: std_gridding plan, both kernel sets with the same half support
 // 1 <= hs <= 4, a 2 hs x 2 hs box inside the grid, and every tap's kernel
 // index equal to fast_kidx (the reference's float subtraction (g - p) is
 // exact for all but the tiniest |p|; those, and every other visibility, take
 // the general path that evaluates degridgrid.c's expressions tap by tap).
 template <typename T>
-__device__ __forceinline__ uint2 fast_geometry(const Rec<T> &r, int plane, int hs, int hsd, int G, int OS, int tile,
-                                               int tx, int ty)
+__device__ __forceinline__ uint4 fast_geometry(const Rec<T> &r, int plane, int hs, int hsd, int G, int OS, int tile,
+                                               int tx, int ty, int pm, int shift)
 {
-    uint2 g = make_uint2((uint32_t)plane << 16, (r.meta < 0) ? (1u << 18) : 0u);
+    uint4 g = make_uint4((uint32_t)plane << 16, 0u, 0u, (r.meta < 0) ? (1u << 4) : 0u);
     if (hs != hsd || hs < 1 || hs > 4) return g;
     const T fos = (T)OS;
     const T lox = tceil(tsub(r.px, (T)hs)), loy = tceil(tsub(r.py, (T)hs));
@@ -228,15 +246,21 @@ __device__ __forceinline__ uint2 fast_geometry(const Rec<T> &r, int plane, int h
     const int tx0 = ix0 - tx * tile, ty0 = iy0 - ty * tile;
     if (tx0 < 0 || ty0 < 0 || tx0 >= tile || ty0 >= tile || tx0 > 255 || ty0 > 255) return g;
     const int kox = ref_kidx((int)lox + hs, r.px, fos), koy = ref_kidx((int)loy + hs, r.py, fos);
-    const int hx = ref_kidx((int)lox, r.px, fos) + kox - OS * hs;
-    const int hy = ref_kidx((int)loy, r.py, fos) + koy - OS * hs;
-    if (kox < 0 || kox > 255 || koy < 0 || koy > 255 || (hx != 0 && hx != 1) || (hy != 0 && hy != 1)) return g;
+    const int kx0 = ref_kidx((int)lox, r.px, fos), ky0 = ref_kidx((int)loy, r.py, fos);
+    const int hx = kx0 + kox - OS * hs, hy = ky0 + koy - OS * hs;
+    if ((hx != 0 && hx != 1) || (hy != 0 && hy != 1)) return g;
     for (int i = 0; i < n; ++i) {
         if (ref_kidx((int)lox + i, r.px, fos) != fast_kidx(i, hs, OS, kox, hx)) return g;
         if (ref_kidx((int)loy + i, r.py, fos) != fast_kidx(i, hs, OS, koy, hy)) return g;
     }
+    const int A = hs + 1;
+    const int cn = geo_kcol(kx0, A, pm, OS, shift), cp = geo_kcol(kox, A, pm, OS, shift);
+    const int rn = geo_krow(ky0, A, pm, OS, shift), rp = geo_krow(koy, A, pm, OS, shift);
+    if (cn > 65535 || cp > 65535 || rn > 65535 || rp > 65535) return g;
     g.x |= (uint32_t)tx0 | ((uint32_t)ty0 << 8);
-    g.y |= (uint32_t)kox | ((uint32_t)koy << 8) | ((uint32_t)hx << 16) | ((uint32_t)hy << 17) | (1u << 19);
+    g.y = (uint32_t)cn | ((uint32_t)cp << 16);
+    g.z = (uint32_t)rn | ((uint32_t)rp << 16);
+    g.w |= (uint32_t)hs | (1u << 5);
     return g;
 }
 
@@ -244,7 +268,7 @@ template <typename T>
 __global__ void k_bin(const float3 *__restrict__ uvw, int n, int mode, int snap, int G, int OS, double uv_scale,
                       double w_scale, const int2 *__restrict__ sup, const int2 *__restrict__ dsup, int nk, int nkd,
                       long long ntot_g, long long ntot_d, int hs_max, int ntx, int nty, int tile,
-                      Rec<T> *__restrict__ rec_tmp, uint2 *__restrict__ geo_tmp,
+                      Rec<T> *__restrict__ rec_tmp, uint4 *__restrict__ geo_tmp, int pm, int os_shift,
                       int *__restrict__ keys, int *__restrict__ counts, int *__restrict__ flags)
 {
     int i = blockIdx.x * blockDim.x + threadIdx.x;
@@ -273,7 +297,7 @@ __global__ void k_bin(const float3 *__restrict__ uvw, int n, int mode, int snap,
     r.meta = plane | ((c.z < 0.0f) ? (int)0x80000000u : 0);
     r.idx = i;
     int key = -1;
-    uint2 geo = make_uint2(0u, 0u);
+    uint4 geo = make_uint4(0u, 0u, 0u, 0u);
     if (plane < 0 || plane >= nk || plane >= nkd) {
         atomicOr(flags, FLAG_PLANE);
     } else {
@@ -292,7 +316,7 @@ __global__ void k_bin(const float3 *__restrict__ uvw, int n, int mode, int snap,
             int ty = min(max(floor_div(loy, tile), 0), nty - 1);
             key = (ty * ntx + tx) * nk + plane;
             atomicAdd(&counts[key], 1);
-            if (mode == SDP_GRID_STD) geo = fast_geometry<T>(r, plane, hs, hsd, G, OS, tile, tx, ty);
+            if (mode == SDP_GRID_STD) geo = fast_geometry<T>(r, plane, hs, hsd, G, OS, tile, tx, ty, pm, os_shift);
         }
     }
     rec_tmp[i] = r;
@@ -301,9 +325,9 @@ __global__ void k_bin(const float3 *__restrict__ uvw, int n, int mode, int snap,
 }
 
 template <typename T>
-__global__ void k_scatter(const Rec<T> *__restrict__ rec_tmp, const uint2 *__restrict__ geo_tmp,
+__global__ void k_scatter(const Rec<T> *__restrict__ rec_tmp, const uint4 *__restrict__ geo_tmp,
                           const int *__restrict__ keys, int n, const int *__restrict__ offsets, int *__restrict__ fill,
-                          Rec<T> *__restrict__ rec, uint2 *__restrict__ geo, int *__restrict__ perm)
+                          Rec<T> *__restrict__ rec, uint4 *__restrict__ geo, int *__restrict__ perm)
 {
     int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
@@ -847,9 +871,27 @@ __device__ __forceinline__ void slow_grid(const PlanDev &P, const Rec<T> rec, in
 
 // g[j] for a runtime j < 4 without indexing the register array (which would
 // move it to local memory).
-__device__ __forceinline__ uint2 pick4(const uint2 (&g)[kFastVB], int j)
+__device__ __forceinline__ uint4 pick4(const uint4 (&g)[kFastVB], int j)
 {
     return j == 0 ? g[0] : j == 1 ? g[1] : j == 2 ? g[2] : g[3];
+}
+
+// This lane's two taps (column c, rows r and r + 4) of a fast-path
+// visibility: table offsets relative to the plane, the subgrid cell of tap
+// (r, c), and which of the two taps lie in the 2 hs x 2 hs box (bits 0, 1).
+__device__ __forceinline__ void fast_taps(const uint4 g, int c, int r, int lanecell, int pitch, int pm, int OS,
+                                          int &off0, int &off1, int &ce, unsigned &aj)
+{
+    const int hs = (int)(g.w & 15u), A = hs + 1, n = 2 * hs;
+    const int sc = pm ? 1 : OS, rs = pm ? A : A * OS;
+    const int cn = (int)(g.y & 0xffffu), cp = (int)(g.y >> 16);
+    const int rn = (int)(g.z & 0xffffu), rp = (int)(g.z >> 16);
+    const int colp = (c < hs) ? cn - c * sc : cp + (c - hs) * sc;
+    const int r1 = r + 4;
+    off0 = colp + ((r < hs) ? rn - r * rs : rp + (r - hs) * rs);
+    off1 = colp + ((r1 < hs) ? rn - r1 * rs : rp + (r1 - hs) * rs);
+    ce = (int)((g.x >> 8) & 255u) * pitch + (int)(g.x & 255u) + lanecell;
+    aj = ((c < n && r < n) ? 1u : 0u) | ((c < n && r1 < n) ? 2u : 0u);
 }
 
 // Reduces v[j][q] (j < 4 visibilities, q < 5 sums) over the warp; lanes
@@ -911,25 +953,13 @@ __device__ __forceinline__ void fast_item(const PlanDev &Pin, const int4 it, flo
         __syncthreads();
     }
 
-    // the loads of a batch's geometry are issued one batch ahead, and its
-    // measured values at the start of the batch, so their latency overlaps
-    // the previous batch's work
-    uint2 gn[kFastVB];
-    {
-        const int b0 = it.y + warp * kFastVB;
-#pragma unroll
-        for (int j = 0; j < kFastVB; ++j) gn[j] = (b0 + j < it.z) ? P.geo[b0 + j] : make_uint2(0u, 0u);
-    }
+    const int lanecell = r * pitch + c;
+    const int pm = P.phase_major;
     for (int b = it.y + warp * kFastVB; b < it.z; b += NW * kFastVB) {
         const int nv = min(kFastVB, it.z - b);  // visibilities in this batch (warp-uniform)
-        uint2 g[kFastVB];
+        uint4 g[kFastVB];
 #pragma unroll
-        for (int j = 0; j < kFastVB; ++j) g[j] = gn[j];
-        {
-            const int bn = b + NW * kFastVB;
-#pragma unroll
-            for (int j = 0; j < kFastVB; ++j) gn[j] = (bn + j < it.z) ? P.geo[bn + j] : make_uint2(0u, 0u);
-        }
+        for (int j = 0; j < kFastVB; ++j) g[j] = (j < nv) ? P.geo[b + j] : make_uint4(0u, 0u, 0u, 0u);
         float2 meas_r = make_float2(0.f, 0.f);  // lanes 8 j ..: visibility j's measured value
         if (OP == OP_CYCLE_CONV && r < nv) meas_r = measured[b + r];
         // per visibility: this lane's two taps (kernel samples and cell)
@@ -939,7 +969,7 @@ __device__ __forceinline__ void fast_item(const PlanDev &Pin, const int4 it, flo
         unsigned slow = 0;  // bit j: visibility j takes the general path (warp-uniform)
 #pragma unroll
         for (int j = 0; j < kFastVB; ++j)
-            if (j < nv && !(g[j].y & (1u << 19))) slow |= 1u << j;
+            if (j < nv && !(g[j].w & (1u << 5))) slow |= 1u << j;
         float2 gval = make_float2(0.f, 0.f);  // lanes 8 j ..: visibility j's residual (CONV) / value (GRID)
         if (kConv) {
             if (slow) {
@@ -967,25 +997,20 @@ __device__ __forceinline__ void fast_item(const PlanDev &Pin, const int4 it, flo
                 k0[j] = k1[j] = make_float2(0.f, 0.f);
                 cell[j] = 0;
                 if (j >= nv) continue;
-                const int4 pl = planes[g[j].x >> 16];
-                if (g[j].y & (1u << 19)) {
-                    const int hs = pl.x, A = hs + 1, n = 2 * hs;
-                    const int kx = fast_kidx(c, hs, OS, g[j].y & 255, (g[j].y >> 16) & 1);
-                    const int ky0 = fast_kidx(r, hs, OS, (g[j].y >> 8) & 255, (g[j].y >> 17) & 1);
-                    const int ky1 = fast_kidx(r + 4, hs, OS, (g[j].y >> 8) & 255, (g[j].y >> 17) & 1);
-                    const int colp = pl.y + kcol(P, A, kx);
-                    const bool a0 = c < n && r < n, a1 = c < n && r + 4 < n;
-                    const int ce = (int)((g[j].x >> 8) & 255) * pitch + (int)(g[j].x & 255) + r * pitch + c;
+                if (g[j].w & (1u << 5)) {
+                    const int doff = planes[g[j].x >> 16].y;
+                    int off0, off1, ce;
+                    unsigned aj;
+                    fast_taps(g[j], c, r, lanecell, pitch, pm, OS, off0, off1, ce, aj);
                     cell[j] = ce;
-                    act |= (a0 ? 1u : 0u) << (2 * j);
-                    act |= (a1 ? 2u : 0u) << (2 * j);
+                    act |= aj << (2 * j);
                     float2 m0 = make_float2(0.f, 0.f), m1 = make_float2(0.f, 0.f);
-                    if (a0) {
-                        k0[j] = __ldg(&P.dk[colp + krow(P, A, ky0)]);
+                    if (aj & 1u) {
+                        k0[j] = __ldg(&P.dk[doff + off0]);
                         m0 = mtile[ce];
                     }
-                    if (a1) {
-                        k1[j] = __ldg(&P.dk[colp + krow(P, A, ky1)]);
+                    if (aj & 2u) {
+                        k1[j] = __ldg(&P.dk[doff + off1]);
                         m1 = mtile[ce + 4 * pitch];
                     }
                     acc[j][0] = fmaf(m0.x, k0[j].x, m1.x * k1[j].x);
@@ -1003,8 +1028,7 @@ __device__ __forceinline__ void fast_item(const PlanDev &Pin, const int4 it, flo
             // lanes 8 j .. 8 j + 7: visibility j (degridgrid.c:188-191; the
             // conjugation of k for w < 0 applied after the sum)
             const int j = r;
-            const uint32_t gy_ = pick4(g, j).y;
-            const float conj = (gy_ & (1u << 18)) ? -1.f : 1.f;
+            const float conj = (pick4(g, j).w & (1u << 4)) ? -1.f : 1.f;
             const float sx = fmaf(-conj, tot[3], tot[0]);
             const float sy = fmaf(conj, tot[2], tot[1]);
             const float cn = __fsqrt_rn(tot[4]);
@@ -1033,6 +1057,7 @@ __device__ __forceinline__ void fast_item(const PlanDev &Pin, const int4 it, flo
 #pragma unroll
             for (int j = 0; j < kFastVB; ++j) {
                 if (j >= nv) break;
+                if (!(g[j].w & (1u << 5))) continue;  // general path below
                 float2 gv;
                 if (kConv) {
                     gv.x = __shfl_sync(0xffffffffu, gval.x, 8 * j);
@@ -1040,43 +1065,39 @@ __device__ __forceinline__ void fast_item(const PlanDev &Pin, const int4 it, flo
                 } else {
                     gv = __ldg(&vis_in[P.perm[b + j]]);
                 }
-                if (!(g[j].y & (1u << 19))) continue;  // general path below
-                const float conj = (g[j].y & (1u << 18)) ? -1.f : 1.f;
-                const int4 pl = planes[g[j].x >> 16];
-                {
-                    float2 q0, q1;
-                    int ce;
-                    unsigned aj;
-                    if (kConv && share) {
-                        q0 = make_float2(k0[j].x, share_sign * k0[j].y);
-                        q1 = make_float2(k1[j].x, share_sign * k1[j].y);
-                        ce = cell[j];
-                        aj = (act >> (2 * j)) & 3u;
-                    } else {
-                        const int hs = pl.z, A = hs + 1, n = 2 * hs;
-                        const int kx = fast_kidx(c, hs, OS, g[j].y & 255, (g[j].y >> 16) & 1);
-                        const int ky0 = fast_kidx(r, hs, OS, (g[j].y >> 8) & 255, (g[j].y >> 17) & 1);
-                        const int ky1 = fast_kidx(r + 4, hs, OS, (g[j].y >> 8) & 255, (g[j].y >> 17) & 1);
-                        const int colp = pl.w + kcol(P, A, kx);
-                        aj = ((c < n && r < n) ? 1u : 0u) | ((c < n && r + 4 < n) ? 2u : 0u);
-                        ce = (int)((g[j].x >> 8) & 255) * pitch + (int)(g[j].x & 255) + r * pitch + c;
-                        q0 = (aj & 1u) ? __ldg(&P.gk[colp + krow(P, A, ky0)]) : make_float2(0.f, 0.f);
-                        q1 = (aj & 2u) ? __ldg(&P.gk[colp + krow(P, A, ky1)]) : make_float2(0.f, 0.f);
-                    }
-                    // vis * (kr + i conj ki): re = vr kr - (conj vi) ki, im = vi kr + (conj vr) ki
-                    const float ca = conj * gv.y, cb = conj * gv.x;
-                    if (aj & 1u) {
-                        float2 a = sub[ce];
-                        a.x += fmaf(-ca, q0.y, gv.x * q0.x);
-                        a.y += fmaf(cb, q0.y, gv.y * q0.x);
-                        sub[ce] = a;
-                    }
-                    if (aj & 2u) {
-                        float2 a = sub[ce + 4 * pitch];
-                        a.x += fmaf(-ca, q1.y, gv.x * q1.x);
-                        a.y += fmaf(cb, q1.y, gv.y * q1.x);
-                        sub[ce + 4 * pitch] = a;
-                    }
+                const float conj = (g[j].w & (1u << 4)) ? -1.f : 1.f;
+                float2 q0, q1;
+                int ce;
+                unsigned aj;
+                float ksign;  // sign of the imaginary part of the gridding sample
+                if (kConv && share) {
+                    q0 = k0[j];
+                    q1 = k1[j];
+                    ce = cell[j];
+                    aj = (act >> (2 * j)) & 3u;
+                    ksign = share_sign;
+                } else {
+                    const int goff = planes[g[j].x >> 16].w;
+                    int off0, off1;
+                    fast_taps(g[j], c, r, lanecell, pitch, pm, OS, off0, off1, ce, aj);
+                    q0 = (aj & 1u) ? __ldg(&P.gk[goff + off0]) : make_float2(0.f, 0.f);
+                    q1 = (aj & 2u) ? __ldg(&P.gk[goff + off1]) : make_float2(0.f, 0.f);
+                    ksign = 1.f;
+                }
+                // vis * (kr + i conj ki): re = vr kr - (conj vi) ki, im = vi kr + (conj vr) ki,
+                // with ki = ksign * (the stored imaginary part)
+                const float nca = -conj * ksign * gv.y, ncb = conj * ksign * gv.x;
+                if (aj & 1u) {
+                    float2 a = sub[ce];
+                    a.x = fmaf(nca, q0.y, fmaf(gv.x, q0.x, a.x));
+                    a.y = fmaf(ncb, q0.y, fmaf(gv.y, q0.x, a.y));
+                    sub[ce] = a;
+                }
+                if (aj & 2u) {
+                    float2 a = sub[ce + 4 * pitch];
+                    a.x = fmaf(nca, q1.y, fmaf(gv.x, q1.x, a.x));
+                    a.y = fmaf(ncb, q1.y, fmaf(gv.y, q1.x, a.y));
+                    sub[ce + 4 * pitch] = a;
                 }
                 __syncwarp();
             }
@@ -1090,9 +1111,9 @@ __device__ __forceinline__ void fast_item(const PlanDev &Pin, const int4 it, flo
                     } else {
                         gv = __ldg(&vis_in[P.perm[b + j]]);
                     }
-                    const uint2 gj = pick4(g, j);
+                    const uint4 gj = pick4(g, j);
                     const int4 pl = planes[gj.x >> 16];
-                    slow_grid<T>(P, recs[b + j], pl.z, pl.w, sub, ox, oy, gv, (gj.y & (1u << 18)) ? -1.f : 1.f);
+                    slow_grid<T>(P, recs[b + j], pl.z, pl.w, sub, ox, oy, gv, (gj.w & (1u << 4)) ? -1.f : 1.f);
                     __syncwarp();
                 }
             }
@@ -1385,8 +1406,8 @@ static void plan_layout(const sdp_visplan *p, size_t *off, size_t *total)
     const size_t per = (size_t)(p->hs_max + 1) * p->geom.oversampling * (p->hs_max + 1) * p->geom.oversampling;
     off[14] = o; o = align_up(o + (p->phase_major ? sizeof(float2) * per * p->gk.num_kernels : 0), 256);  // gk2
     off[15] = o; o = align_up(o + (p->phase_major ? sizeof(float2) * per * p->dk.num_kernels : 0), 256);  // dk2
-    off[16] = o; o = align_up(o + sizeof(uint2) * (size_t)std::max(n, 1), 256);          // geo
-    off[17] = o; o = align_up(o + sizeof(uint2) * (size_t)std::max(n, 1), 256);          // geo_tmp
+    off[16] = o; o = align_up(o + sizeof(uint4) * (size_t)std::max(n, 1), 256);          // geo
+    off[17] = o; o = align_up(o + sizeof(uint4) * (size_t)std::max(n, 1), 256);          // geo_tmp
     *total = o;
 }
 
@@ -1506,8 +1527,10 @@ int visplan_build(sdp_visplan *p, void *arena, const float3 *uvw, cudaStream_t s
     p->dpoff = reinterpret_cast<int *>(a + off[13]);
     p->gk2 = reinterpret_cast<float2 *>(a + off[14]);
     p->dk2 = reinterpret_cast<float2 *>(a + off[15]);
-    p->geo = reinterpret_cast<uint2 *>(a + off[16]);
-    uint2 *geo_tmp = reinterpret_cast<uint2 *>(a + off[17]);
+    p->geo = reinterpret_cast<uint4 *>(a + off[16]);
+    uint4 *geo_tmp = reinterpret_cast<uint4 *>(a + off[17]);
+    int os_shift = 0;
+    while ((1 << os_shift) < p->geom.oversampling) ++os_shift;
     const int n = p->n;
 
     SDP_CUDA_TRY(cudaMemsetAsync(scalars, 0, sizeof(int) * 4, st));
@@ -1521,13 +1544,13 @@ int visplan_build(sdp_visplan *p, void *arena, const float3 *uvw, cudaStream_t s
                 uvw, n, p->mode, p->snap, p->geom.grid_size, p->geom.oversampling, p->geom.uv_scale, p->geom.w_scale,
                 gs, ds, p->gk.num_kernels, p->dk.num_kernels, (long long)p->gk.total_samples,
                 (long long)p->dk.total_samples, p->hs_max, p->ntx, p->nty, p->tile, static_cast<Rec<double> *>(rec_tmp),
-                geo_tmp, keys, counts, p->flags);
+                geo_tmp, p->phase_major, os_shift, keys, counts, p->flags);
         } else {
             k_bin<float><<<(n + 255) / 256, 256, 0, st>>>(
                 uvw, n, p->mode, p->snap, p->geom.grid_size, p->geom.oversampling, p->geom.uv_scale, p->geom.w_scale,
                 gs, ds, p->gk.num_kernels, p->dk.num_kernels, (long long)p->gk.total_samples,
                 (long long)p->dk.total_samples, p->hs_max, p->ntx, p->nty, p->tile, static_cast<Rec<float> *>(rec_tmp),
-                geo_tmp, keys, counts, p->flags);
+                geo_tmp, p->phase_major, os_shift, keys, counts, p->flags);
         }
         SDP_LAUNCH_CHECK();
     }
