@@ -883,14 +883,23 @@ __device__ __forceinline__ void fast_taps(const uint4 g, int c, int r, int lanec
                                           int &off0, int &off1, int &ce, unsigned &aj)
 {
     const int hs = (int)(g.w & 15u), A = hs + 1, n = 2 * hs;
-    const int sc = pm ? 1 : OS, rs = pm ? A : A * OS;
     const int cn = (int)(g.y & 0xffffu), cp = (int)(g.y >> 16);
     const int rn = (int)(g.z & 0xffffu), rp = (int)(g.z >> 16);
+    ce = (int)((g.x >> 8) & 255u) * pitch + (int)(g.x & 255u) + lanecell;
+    if (hs == 4 && pm) {
+        // the common case: every tap of the 8 x 8 box is active, rows r are
+        // below the visibility and rows r + 4 above it (steps 1 and A = 5)
+        const int colp = (c < 4) ? cn - c : cp + c - 4;
+        off0 = colp + rn - 5 * r;
+        off1 = colp + rp + 5 * r;
+        aj = 3u;
+        return;
+    }
+    const int sc = pm ? 1 : OS, rs = pm ? A : A * OS;
     const int colp = (c < hs) ? cn - c * sc : cp + (c - hs) * sc;
     const int r1 = r + 4;
     off0 = colp + ((r < hs) ? rn - r * rs : rp + (r - hs) * rs);
     off1 = colp + ((r1 < hs) ? rn - r1 * rs : rp + (r1 - hs) * rs);
-    ce = (int)((g.x >> 8) & 255u) * pitch + (int)(g.x & 255u) + lanecell;
     aj = ((c < n && r < n) ? 1u : 0u) | ((c < n && r1 < n) ? 2u : 0u);
 }
 
@@ -933,9 +942,7 @@ __device__ __forceinline__ void fast_item(const PlanDev &Pin, const int4 it, flo
 {
     constexpr bool kGrids = (OP != OP_DEGRID);
     constexpr bool kConv = (OP != OP_GRID);
-    // a private copy: the batch kernel's description lives in shared memory,
-    // where every read would be repeated after each subgrid store
-    const PlanDev P = Pin;
+    const PlanDev &P = Pin;
     const int S = P.S, pitch = P.pitch, OS = P.OS;
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const int c = lane & 7, r = lane >> 3;
