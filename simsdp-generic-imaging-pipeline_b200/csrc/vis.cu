@@ -886,15 +886,6 @@ __device__ __forceinline__ void fast_taps(const uint4 g, int c, int r, int lanec
     const int cn = (int)(g.y & 0xffffu), cp = (int)(g.y >> 16);
     const int rn = (int)(g.z & 0xffffu), rp = (int)(g.z >> 16);
     ce = (int)((g.x >> 8) & 255u) * pitch + (int)(g.x & 255u) + lanecell;
-    if (hs == 4 && pm) {
-        // the common case: every tap of the 8 x 8 box is active, rows r are
-        // below the visibility and rows r + 4 above it (steps 1 and A = 5)
-        const int colp = (c < 4) ? cn - c : cp + c - 4;
-        off0 = colp + rn - 5 * r;
-        off1 = colp + rp + 5 * r;
-        aj = 3u;
-        return;
-    }
     const int sc = pm ? 1 : OS, rs = pm ? A : A * OS;
     const int colp = (c < hs) ? cn - c * sc : cp + (c - hs) * sc;
     const int r1 = r + 4;
@@ -969,6 +960,105 @@ __device__ __forceinline__ void fast_item(const PlanDev &Pin, const int4 it, flo
         for (int j = 0; j < kFastVB; ++j) g[j] = (j < nv) ? P.geo[b + j] : make_uint4(0u, 0u, 0u, 0u);
         float2 meas_r = make_float2(0.f, 0.f);  // lanes 8 j ..: visibility j's measured value
         if (OP == OP_CYCLE_CONV && r < nv) meas_r = measured[b + r];
+        // A batch of four fast-path visibilities of half support 4 in the
+        // phase-major layout (nearly every batch): straight-line code, every
+        // tap of the 8 x 8 box active (rows r below the visibility at RN - 5 r,
+        // rows r + 4 above it at RP + 5 r; columns c < 4 at CN - c, the others
+        // at CP + c - 4), packed FP32x2 arithmetic.
+        bool all4 = (nv == kFastVB) && pm;
+#pragma unroll
+        for (int j = 0; j < kFastVB; ++j) all4 = all4 && (g[j].w & 0x2fu) == 0x24u;  // fast, hs = 4
+        if (all4) {
+            float2 q0[kFastVB], q1[kFastVB];
+            int ce4[kFastVB];
+            float2 gv4 = make_float2(0.f, 0.f);
+            if (kConv) {
+                float acc[kFastVB][5];
+#pragma unroll
+                for (int j = 0; j < kFastVB; ++j) {
+                    const uint4 gj = g[j];
+                    const int colp = (c < 4) ? (int)(gj.y & 0xffffu) - c : (int)(gj.y >> 16) + c - 4;
+                    const float2 *kp = P.dk + planes[gj.x >> 16].y + colp;
+                    q0[j] = __ldg(kp + (int)(gj.z & 0xffffu) - 5 * r);
+                    q1[j] = __ldg(kp + (int)(gj.z >> 16) + 5 * r);
+                    const int ce = (int)((gj.x >> 8) & 255u) * pitch + (int)(gj.x & 255u) + lanecell;
+                    ce4[j] = ce;
+                    const float2 m0 = mtile[ce], m1 = mtile[ce + 4 * pitch];
+                    const float2 a1 = __ffma2_rn(m1, make_float2(q1[j].x, q1[j].x),
+                                                 __fmul2_rn(m0, make_float2(q0[j].x, q0[j].x)));
+                    const float2 a2 = __ffma2_rn(m1, make_float2(q1[j].y, q1[j].y),
+                                                 __fmul2_rn(m0, make_float2(q0[j].y, q0[j].y)));
+                    const float2 nn = __ffma2_rn(q1[j], q1[j], __fmul2_rn(q0[j], q0[j]));
+                    acc[j][0] = a1.x;
+                    acc[j][1] = a1.y;
+                    acc[j][2] = a2.x;
+                    acc[j][3] = a2.y;
+                    acc[j][4] = nn.x + nn.y;
+                }
+                float tot[5];
+                reduce4x5(acc, tot);
+                const float conj = (pick4(g, r).w & (1u << 4)) ? -1.f : 1.f;  // lanes 8 j ..: visibility j
+                const float sx = fmaf(-conj, tot[3], tot[0]);
+                const float sy = fmaf(conj, tot[2], tot[1]);
+                const float cn = __fsqrt_rn(tot[4]);
+                const bool tiny = cn < 1e-5f;
+                const float inv = tiny ? 1e5f : __frcp_rn(cn);
+                const float nx = sx * inv;
+                const float ny = tiny ? nx * inv : sy * inv;
+                const float2 value = make_float2(nx, ny);
+                const int i = b + r;
+                if (OP == OP_CYCLE_CONV) {
+                    gv4 = make_float2(__fsub_rn(meas_r.x, value.x), __fsub_rn(meas_r.y, value.y));
+                    if (c == 0 && (pred_out || delta_out)) {
+                        const int o = P.perm[i];
+                        if (pred_out) pred_out[o] = value;
+                        if (delta_out) delta_out[o] = gv4;
+                    }
+                } else if (c == 0) {
+                    pred_out[P.perm[i]] = value;
+                }
+            }
+            if (kGrids) {
+#pragma unroll
+                for (int j = 0; j < kFastVB; ++j) {
+                    const uint4 gj = g[j];
+                    float2 gv;
+                    if (kConv) {
+                        gv.x = __shfl_sync(0xffffffffu, gv4.x, 8 * j);
+                        gv.y = __shfl_sync(0xffffffffu, gv4.y, 8 * j);
+                    } else {
+                        gv = __ldg(&vis_in[P.perm[b + j]]);
+                    }
+                    float2 t0, t1;
+                    int ce;
+                    float ks;
+                    if (kConv && share) {
+                        t0 = q0[j];
+                        t1 = q1[j];
+                        ce = ce4[j];
+                        ks = share_sign;
+                    } else {
+                        const int colp = (c < 4) ? (int)(gj.y & 0xffffu) - c : (int)(gj.y >> 16) + c - 4;
+                        const float2 *kp = P.gk + planes[gj.x >> 16].w + colp;
+                        t0 = __ldg(kp + (int)(gj.z & 0xffffu) - 5 * r);
+                        t1 = __ldg(kp + (int)(gj.z >> 16) + 5 * r);
+                        ce = (int)((gj.x >> 8) & 255u) * pitch + (int)(gj.x & 255u) + lanecell;
+                        ks = 1.f;
+                    }
+                    // vis * (kr + i conj ki): re = vr kr - (conj vi) ki, im = vi kr + (conj vr) ki
+                    const float conj = (gj.w & (1u << 4)) ? -1.f : 1.f;
+                    const float2 nc = make_float2(-conj * ks * gv.y, conj * ks * gv.x);
+                    float2 s0 = sub[ce];
+                    s0 = __ffma2_rn(nc, make_float2(t0.y, t0.y), __ffma2_rn(gv, make_float2(t0.x, t0.x), s0));
+                    sub[ce] = s0;
+                    float2 s1 = sub[ce + 4 * pitch];
+                    s1 = __ffma2_rn(nc, make_float2(t1.y, t1.y), __ffma2_rn(gv, make_float2(t1.x, t1.x), s1));
+                    sub[ce + 4 * pitch] = s1;
+                    __syncwarp();
+                }
+            }
+            continue;
+        }
         // per visibility: this lane's two taps (kernel samples and cell)
         float2 k0[kFastVB], k1[kFastVB];
         int cell[kFastVB];
