@@ -1172,7 +1172,8 @@ def b200_arm(args):
                    "work_items": n_items, "plan_shape": tune, "setup_s": setup_s},
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
                      "traffic": traffic, "peak_source": peak_src,
-                     "kernel": "sdp_visbatch_cycle: residual-grid clears + k_vis_fast_batch<float, 8>",
+                     "kernel": "sdp_visbatch_cycle: residual-grid clears + k_vis_fast_batch<float, %s warps>"
+                               % ((tune or {}).get("warps") or "auto"),
                      "algorithmic_bytes_per_launch": alg_bytes, "fp32_flops_per_launch": alg_flops,
                      "ms_per_launch": t_pass},
         "roofline_binding": binding,
