@@ -464,7 +464,8 @@ class Deconvolver:
     gridding and imaging is the image of measured - (model + alpha x
     proposal) visibilities.  The proposal is kept when the residual RMS
     (FP64) falls by more than min_gain (relative); otherwise the cycle runs
-    Hogbom, and after give_up rejections the network is not asked again.
+    Hogbom, the network is asked again in the next cycle, and after give_up
+    rejections it is not asked again.
     Proposals come from the central window (fraction `window` of each axis):
     the outer band of the image holds the taper correction's amplified
     imaging errors (w-term truncation, aliasing), which the network, trained
@@ -472,7 +473,7 @@ class Deconvolver:
 
     def __init__(self, img: Imaging, params: np.ndarray | None, num_minor: int = 200, loop_gain: float = 0.1,
                  max_components: int = 1024, rel_threshold: float = 0.05, alpha_max: float = 2.0,
-                 min_gain: float = 0.05, give_up: int = 1, noise_factor: float = 1.5,
+                 min_gain: float = 0.05, give_up: int = 3, noise_factor: float = 1.5,
                  weak_source_percent: float = 0.0002, signed: bool = True, window: float = 0.75):
         torch = _torch()
         self.img, self.D = img, img.D
