@@ -45,7 +45,7 @@ enum : int {
 };
 
 // Device-side error flags (OR-ed together).
-enum : int { FLAG_PLANE = 1, FLAG_SUPPORT = 2, FLAG_BOX = 4 };
+enum : int { FLAG_PLANE = 1, FLAG_SUPPORT = 2, FLAG_BOX = 4, FLAG_STAGE = 8 };
 
 struct PlanDev {
     int G, gc, OS, nk_g, nk_d, ntx, nty, W, S, tile;
@@ -64,6 +64,7 @@ struct PlanDev {
     int *flags;
     const int *kdiff;  // bit 0: degridding set != gridding set; bit 1: != its conjugate
     int pitch;          // row pitch (float2) of the shared tiles of the warp-per-visibility kernels
+    int chunk;          // visibilities per work item (at most)
     const uint4 *geo;   // packed tap-box geometry in plan order (see fast_geometry)
     const int *perm;    // plan position -> original visibility index
 };
@@ -921,11 +922,60 @@ __device__ __forceinline__ void reduce4x5(const float (&v)[kFastVB][5], float (&
         for (int q = 0; q < 5; ++q) out[q] += __shfl_xor_sync(0xffffffffu, out[q], o);
 }
 
+// Bulk (TMA) staging of a work item's records: one thread arms an mbarrier
+// with the byte count and issues cp.async.bulk copies of the item's 16-byte
+// geometry records and measured values into shared memory; the wait is
+// bounded.  Addresses are 16-byte aligned: the geometry records are 16 bytes
+// each, and the measured values (8 bytes) are copied from the even index at
+// or below the item's first to the even index at or above its end (the
+// plan's measured array is padded to 256 bytes, so the one value past the
+// last item stays inside it).
+constexpr long long kStageSpins = 1LL << 22;  // bounded mbarrier polls (well over a second)
+
+__device__ __forceinline__ void stage_arm(uint32_t bar, uint32_t bytes)
+{
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar), "r"(bytes) : "memory");
+}
+
+__device__ __forceinline__ void stage_copy(uint32_t dst, const void *src, uint32_t bytes, uint32_t bar)
+{
+    asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(dst),
+                 "l"(src), "r"(bytes), "r"(bar)
+                 : "memory");
+}
+
+__device__ __forceinline__ bool stage_wait(uint32_t bar, uint32_t parity)
+{
+    for (long long i = 0; i < kStageSpins; ++i) {
+        uint32_t done;
+        asm volatile(
+            "{\n\t.reg .pred P1;\n\t"
+            "mbarrier.try_wait.parity.shared::cta.b64 P1, [%1], %2;\n\t"
+            "selp.b32 %0, 1, 0, P1;\n\t}"
+            : "=r"(done)
+            : "r"(bar), "r"(parity)
+            : "memory");
+        if (done) return true;
+    }
+    return false;
+}
+
+// Per-CTA staging state: the item's records in shared memory and the
+// mbarrier's phase.
+struct ItemStage {
+    uint4 *geo;         // chunk records
+    float2 *meas;       // chunk + 2 values (from the even index at or below the item's first)
+    uint64_t *bar;
+    uint32_t phase;     // parity of the next completion
+    int *fail;          // shared flag: a staging wait gave up
+};
+
 // One work item of the warp-per-visibility kernels (the whole CTA).
 // OP is OP_GRID, OP_DEGRID or OP_CYCLE_CONV.  smem: the model tile (OP !=
 // OP_GRID) and NW private subgrids (OP != OP_DEGRID), S rows of P.pitch cells.
 template <typename T, int OP, int NW>
-__device__ __forceinline__ void fast_item(const PlanDev &Pin, const int4 it, float2 *mtile, float2 *subs,
+__device__ __forceinline__ bool fast_item(const PlanDev &Pin, const int4 it, ItemStage &stg, float2 *mtile,
+                                          float2 *subs,
                                           float *wscr_all, const int4 *planes, bool share, float share_sign,
                                           const float2 *__restrict__ vis_in, const float2 *__restrict__ in_grid,
                                           float2 *__restrict__ out_grid, float2 *__restrict__ pred_out,
@@ -941,6 +991,21 @@ __device__ __forceinline__ void fast_item(const PlanDev &Pin, const int4 it, flo
     float2 *sub = subs + (size_t)warp * S * pitch;
     float *wscr = wscr_all + warp * (kFastVB * 5);  // general-path sums of this warp's batch
     const Rec<T> *__restrict__ recs = static_cast<const Rec<T> *>(P.rec);
+    // the item's records and measured values, copied into shared memory while
+    // the model tile is staged
+    const int m0 = it.y & ~1;
+    const uint32_t bar = (uint32_t)__cvta_generic_to_shared(stg.bar);
+    if (threadIdx.x == 0) {
+        // the previous item's records were read through the generic proxy
+        // (the CTA synchronised since): order those reads before the bulk
+        // copies overwrite them
+        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+        const uint32_t gbytes = (uint32_t)(it.z - it.y) * 16u;
+        const uint32_t mbytes = (OP == OP_CYCLE_CONV) ? (uint32_t)(((it.z + 1) & ~1) - m0) * 8u : 0u;
+        stage_arm(bar, gbytes + mbytes);
+        stage_copy((uint32_t)__cvta_generic_to_shared(stg.geo), P.geo + it.y, gbytes, bar);
+        if (OP == OP_CYCLE_CONV) stage_copy((uint32_t)__cvta_generic_to_shared(stg.meas), measured + m0, mbytes, bar);
+    }
     if (kConv) {
         for (int k = threadIdx.x; k < S * S; k += 32 * NW) {
             const int y = k / S, x = k - y * S;
@@ -948,8 +1013,21 @@ __device__ __forceinline__ void fast_item(const PlanDev &Pin, const int4 it, flo
             mtile[y * pitch + x] =
                 (gx < P.G && gy < P.G) ? __ldg(&in_grid[(size_t)gy * P.G + gx]) : make_float2(0.f, 0.f);
         }
-        __syncthreads();
     }
+    if (threadIdx.x == 0) {
+        if (!stage_wait(bar, stg.phase)) {
+            // record the failure, then give the copies in flight one more
+            // bounded wait before the CTA stops
+            atomicOr(P.flags, FLAG_STAGE);
+            stage_wait(bar, stg.phase);
+            *stg.fail = 1;
+        }
+    }
+    stg.phase ^= 1u;
+    __syncthreads();
+    if (*stg.fail) return false;
+    const uint4 *sgeo = stg.geo - it.y;   // indexed by plan position
+    const float2 *smeas = stg.meas - m0;
 
     const int lanecell = r * pitch + c;
     const int pm = P.phase_major;
@@ -957,9 +1035,9 @@ __device__ __forceinline__ void fast_item(const PlanDev &Pin, const int4 it, flo
         const int nv = min(kFastVB, it.z - b);  // visibilities in this batch (warp-uniform)
         uint4 g[kFastVB];
 #pragma unroll
-        for (int j = 0; j < kFastVB; ++j) g[j] = (j < nv) ? P.geo[b + j] : make_uint4(0u, 0u, 0u, 0u);
+        for (int j = 0; j < kFastVB; ++j) g[j] = (j < nv) ? sgeo[b + j] : make_uint4(0u, 0u, 0u, 0u);
         float2 meas_r = make_float2(0.f, 0.f);  // lanes 8 j ..: visibility j's measured value
-        if (OP == OP_CYCLE_CONV && r < nv) meas_r = measured[b + r];
+        if (OP == OP_CYCLE_CONV && r < nv) meas_r = smeas[b + r];
         // A batch of four fast-path visibilities of half support 4 in the
         // phase-major layout (nearly every batch): straight-line code, every
         // tap of the 8 x 8 box active (rows r below the visibility at RN - 5 r,
@@ -1237,14 +1315,22 @@ __device__ __forceinline__ void fast_item(const PlanDev &Pin, const int4 it, flo
         }
     }
     __syncthreads();
+    return true;
 }
 
-// Shared-memory layout of the warp-per-visibility kernels: per-plane
-// constants (nk int4), then the model tile and the NW subgrids.
-__host__ __device__ __forceinline__ size_t fast_smem_bytes(int op, int nw, int S, int pitch, int nk)
+// Shared-memory layout of the warp-per-visibility kernels: the staged
+// records of one work item (chunk 16-byte records, chunk + 2 measured
+// values), per-plane constants (nk int4), then the model tile and the NW
+// subgrids.
+__host__ __device__ __forceinline__ size_t fast_stage_bytes(int chunk)
+{
+    return (16 * (size_t)chunk + 8 * ((size_t)chunk + 2) + 15) / 16 * 16;  // the plane table after it is int4
+}
+__host__ __device__ __forceinline__ size_t fast_smem_bytes(int op, int nw, int S, int pitch, int nk, int chunk)
 {
     const size_t tilef2 = (size_t)S * pitch;
-    return 16 * (size_t)nk + 8 * tilef2 * ((op != OP_GRID ? 1 : 0) + (op != OP_DEGRID ? nw : 0));
+    return fast_stage_bytes(chunk) + 16 * (size_t)nk +
+           8 * tilef2 * ((op != OP_GRID ? 1 : 0) + (op != OP_DEGRID ? nw : 0));
 }
 
 template <typename T, int OP, int NW>
@@ -1255,11 +1341,20 @@ __global__ void __launch_bounds__(32 * NW) k_vis_fast(PlanDev P, const float2 *_
                                                       const float2 *__restrict__ measured)
 {
     extern __shared__ __align__(16) unsigned char smem_fast[];
-    int4 *planes = reinterpret_cast<int4 *>(smem_fast);
-    float2 *mtile = reinterpret_cast<float2 *>(smem_fast + 16 * (size_t)P.nk_g);
+    const size_t stage_b = fast_stage_bytes(P.chunk);
+    int4 *planes = reinterpret_cast<int4 *>(smem_fast + stage_b);
+    float2 *mtile = reinterpret_cast<float2 *>(smem_fast + stage_b + 16 * (size_t)P.nk_g);
     float2 *subs = mtile + (OP != OP_GRID ? (size_t)P.S * P.pitch : 0);
     __shared__ float s_wscr[NW * kFastVB * 5];
-    __shared__ int s_item;
+    __shared__ int s_item, s_fail;
+    __shared__ __align__(8) uint64_t s_bar;
+    ItemStage stg{reinterpret_cast<uint4 *>(smem_fast), reinterpret_cast<float2 *>(smem_fast + 16 * (size_t)P.chunk),
+                  &s_bar, 0u, &s_fail};
+    if (threadIdx.x == 0) {
+        s_fail = 0;
+        asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"((uint32_t)__cvta_generic_to_shared(&s_bar)));
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
     for (int k = threadIdx.x; k < P.nk_g; k += 32 * NW)
         planes[k] = make_int4(OP != OP_GRID && k < P.nk_d ? P.ds[k].x : 0,
                               OP != OP_GRID && k < P.nk_d ? P.dpoff[k] : 0, OP != OP_DEGRID ? P.gs[k].x : 0,
@@ -1275,8 +1370,9 @@ __global__ void __launch_bounds__(32 * NW) k_vis_fast(PlanDev P, const float2 *_
         __syncthreads();
         const int item = s_item;
         if (item >= *P.n_items) break;
-        fast_item<T, OP, NW>(P, P.items[item], mtile, subs, s_wscr, planes, share, share_sign, vis_in, in_grid,
-                             out_grid, pred_out, delta_out, measured);
+        if (!fast_item<T, OP, NW>(P, P.items[item], stg, mtile, subs, s_wscr, planes, share, share_sign, vis_in,
+                                  in_grid, out_grid, pred_out, delta_out, measured))
+            break;
     }
 }
 
@@ -1287,16 +1383,26 @@ template <typename T, int NW>
 __global__ void __launch_bounds__(32 * NW) k_vis_fast_batch(const PlanDev *__restrict__ plans,
                                                             const BatchIO *__restrict__ io,
                                                             const int4 *__restrict__ items, int n_items,
-                                                            int *item_counter, int nk_max, int tile_f2)
+                                                            int *item_counter, int nk_max, int tile_f2,
+                                                            int chunk_max)
 {
     extern __shared__ __align__(16) unsigned char smem_fast[];
-    int4 *planes = reinterpret_cast<int4 *>(smem_fast);
-    float2 *mtile = reinterpret_cast<float2 *>(smem_fast + 16 * (size_t)nk_max);
+    const size_t stage_b = fast_stage_bytes(chunk_max);
+    int4 *planes = reinterpret_cast<int4 *>(smem_fast + stage_b);
+    float2 *mtile = reinterpret_cast<float2 *>(smem_fast + stage_b + 16 * (size_t)nk_max);
     float2 *subs = mtile + tile_f2;
     __shared__ PlanDev sP;
     __shared__ BatchIO sIO;
-    __shared__ int s_item, s_share;
+    __shared__ int s_item, s_share, s_fail;
     __shared__ float s_wscr[NW * kFastVB * 5];
+    __shared__ __align__(8) uint64_t s_bar;
+    ItemStage stg{reinterpret_cast<uint4 *>(smem_fast), reinterpret_cast<float2 *>(smem_fast + 16 * (size_t)chunk_max),
+                  &s_bar, 0u, &s_fail};
+    if (threadIdx.x == 0) {
+        s_fail = 0;
+        asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"((uint32_t)__cvta_generic_to_shared(&s_bar)));
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
     for (size_t k = threadIdx.x; k < (size_t)NW * tile_f2; k += 32 * NW) subs[k] = make_float2(0.f, 0.f);
     int cur = -1;
     for (;;) {
@@ -1319,9 +1425,11 @@ __global__ void __launch_bounds__(32 * NW) k_vis_fast_batch(const PlanDev *__res
             cur = it.w;
         }
         const int kdiff = s_share;
-        fast_item<T, OP_CYCLE_CONV, NW>(sP, it, mtile, subs, s_wscr, planes, (kdiff & 1) == 0 || (kdiff & 2) == 0,
-                                        (kdiff & 1) == 0 ? 1.f : -1.f, nullptr, sIO.in_grid, sIO.out_grid,
-                                        sIO.pred_out, sIO.delta_out, sIO.measured);
+        if (!fast_item<T, OP_CYCLE_CONV, NW>(sP, it, stg, mtile, subs, s_wscr, planes,
+                                             (kdiff & 1) == 0 || (kdiff & 2) == 0, (kdiff & 1) == 0 ? 1.f : -1.f,
+                                             nullptr, sIO.in_grid, sIO.out_grid, sIO.pred_out, sIO.delta_out,
+                                             sIO.measured))
+            break;
     }
 }
 
@@ -1455,6 +1563,7 @@ static PlanDev plan_dev(const sdp_visplan *p)
     d.item_counter = p->item_counter;
     d.flags = p->flags;
     d.pitch = p->pitch;
+    d.chunk = p->chunk;
     d.geo = p->geo;
     d.perm = p->perm;
     return d;
@@ -1682,10 +1791,11 @@ int visplan_check_flags(sdp_visplan *p, cudaStream_t st)
     SDP_CUDA_TRY(cudaStreamSynchronize(st));
     if (flags) {
         SDP_CUDA_TRY(cudaMemsetAsync(p->flags, 0, sizeof(int), st));
-        return set_error(SDP_ERR_DATA, "visibility data outside the kernel tables (flags 0x%x:%s%s%s)", flags,
+        return set_error(SDP_ERR_DATA, "visibility data outside the kernel tables (flags 0x%x:%s%s%s%s)", flags,
                          (flags & FLAG_PLANE) ? " w-plane index beyond NUM_KERNELS;" : "",
                          (flags & FLAG_SUPPORT) ? " support beyond the declared maximum or table;" : "",
-                         (flags & FLAG_BOX) ? " tap box wider than 2*hs+1;" : "");
+                         (flags & FLAG_BOX) ? " tap box wider than 2*hs+1;" : "",
+                         (flags & FLAG_STAGE) ? " a work item's records did not arrive in shared memory;" : "");
     }
     return SDP_OK;
 }
@@ -1927,7 +2037,7 @@ template <typename T, int OP, int NW>
 static int launch_fast_nw(sdp_visplan *p, const float2 *vis_in, const float2 *in_grid, float2 *out_grid,
                           float2 *pred, float2 *delta, cudaStream_t st, int *resident_warps)
 {
-    const size_t smem = fast_smem_bytes(OP, NW, p->S, p->pitch, p->gk.num_kernels);
+    const size_t smem = fast_smem_bytes(OP, NW, p->S, p->pitch, p->gk.num_kernels, p->chunk);
     void (*fn)(PlanDev, const float2 *, const float2 *, float2 *, float2 *, float2 *, const float2 *) =
         k_vis_fast<T, OP, NW>;
     if (smem > 227 * 1024) {
@@ -2074,6 +2184,7 @@ struct sdp_visbatch {
     int warps = 0;
     int hs_max = 0, S_max = 0, nk_max = 0, n_items = 0;
     size_t tile_f2 = 0;  // largest S x pitch of the plans
+    int chunk_max = 0;   // largest work item of the plans
     std::vector<sdp_visplan *> plans;
     std::vector<sdp::BatchIO> io;
     sdp::PlanDev *d_plans = nullptr;
@@ -2108,8 +2219,8 @@ static int launch_batch_lg(sdp_visbatch *b, int op, cudaStream_t st)
 template <typename T, int NW>
 static int launch_batch_fast_nw(sdp_visbatch *b, cudaStream_t st, int *resident_warps)
 {
-    const size_t smem = 16 * (size_t)b->nk_max + 8 * b->tile_f2 * (1 + NW);
-    void (*fn)(const PlanDev *, const BatchIO *, const int4 *, int, int *, int, int) = k_vis_fast_batch<T, NW>;
+    const size_t smem = fast_stage_bytes(b->chunk_max) + 16 * (size_t)b->nk_max + 8 * b->tile_f2 * (1 + NW);
+    void (*fn)(const PlanDev *, const BatchIO *, const int4 *, int, int *, int, int, int) = k_vis_fast_batch<T, NW>;
     if (smem > 227 * 1024) {
         if (resident_warps) {
             *resident_warps = 0;
@@ -2127,7 +2238,7 @@ static int launch_batch_fast_nw(sdp_visbatch *b, cudaStream_t st, int *resident_
     if (per_sm < 1) return set_error(SDP_ERR_RANGE, "batched tile kernel does not fit (%zu B shared memory)", smem);
     SDP_CUDA_TRY(cudaMemsetAsync(b->d_counter, 0, sizeof(int), st));
     fn<<<per_sm * num_sms(), 32 * NW, smem, st>>>(b->d_plans, b->d_io, b->d_items, b->n_items, b->d_counter,
-                                                  b->nk_max, (int)b->tile_f2);
+                                                  b->nk_max, (int)b->tile_f2, b->chunk_max);
     SDP_LAUNCH_CHECK();
     return SDP_OK;
 }
@@ -2179,6 +2290,7 @@ SDP_EXPORT int sdp_visbatch_create(sdp_visbatch **out, sdp_visplan *const *plans
         b->hs_max = std::max(b->hs_max, p->hs_max);
         b->S_max = std::max(b->S_max, p->S);
         b->tile_f2 = std::max(b->tile_f2, (size_t)p->S * p->pitch);
+        b->chunk_max = std::max(b->chunk_max, p->chunk);
         b->fast = b->fast && fast_eligible(p);
         if (c == 0) b->warps = p->warps;
         b->nk_max = std::max(b->nk_max, p->gk.num_kernels);
