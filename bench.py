@@ -845,6 +845,62 @@ def c4_learned_block(S, D, dev, skies: int):
     }
 
 
+def peaks_block(D, dev) -> dict:
+    """On-chip ceilings measured on this GPU (sdp_peak_measure): L2 reads of a
+    32 MB buffer, conflict-free shared-memory reads, scalar and packed FP32
+    FMA, and the rate of the Hogbom residual update in the reference's types."""
+    import torch
+    scratch = torch.zeros(32 << 20, dtype=torch.uint8, device=dev)
+    r = {k: D.peak(k, scratch, reps=10) for k in D.PEAK_KINDS}
+    del scratch
+    return {"l2_read_gbs": r["l2_read"] / 1e9, "smem_read_gbs": r["smem_read"] / 1e9,
+            "fp32_fma_tflops": r["fp32_fma"] / 1e12, "fp32x2_fma_tflops": r["fp32x2_fma"] / 1e12,
+            "hogbom_update_gpix_s": r["hogbom_update"] / 1e9,
+            "method": "csrc/peaks.cu: one kernel per ceiling, 4 x 512 threads per SM, 10 launches after one "
+                      "warm-up, CUDA events"}
+
+
+def hogbom_block(S, D, dev, G, dirty, psf, psf_max, cell, peaks, reps=5):
+    """Hogbom alone (sdp_hogbom, 200 minor cycles, gain 0.1) on a dirty image:
+    time per minor cycle, and the PSF pass against the measured L2 read and
+    residual-update ceilings.  The pass reads, per minor cycle, the PSF window
+    the component's position selects (deconvolution_run.c:264-272): 4 bytes of
+    PSF and one update per pixel of the window."""
+    import torch
+    prm = S.CleanParams(G, 200, 200, 0.1, 1.5, 0.0002, psf_max, cell)
+    ws = torch.empty(max(1, D.hogbom_workspace_bytes(G)), dtype=torch.uint8, device=dev)
+    res = torch.empty_like(dirty)
+    model = torch.zeros_like(dirty)
+    src = torch.zeros((200, 3), dtype=torch.float32, device=dev)
+    cnt = torch.zeros(1, dtype=torch.int32, device=dev)
+    ts = []
+    for i in range(reps + 2):
+        res.copy_(dirty)
+        model.zero_()
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record()
+        D.hogbom(prm, res, psf, model, src, cnt, ws)
+        b.record()
+        torch.cuda.synchronize()
+        if i >= 2:
+            ts.append(a.elapsed_time(b))
+    n = int(cnt.item())
+    t = float(statistics.median(ts))
+    h = G // 2
+    pix = 0
+    for x, y, _ in src[:n].cpu().numpy().astype(np.float64):
+        mx, my = int(round(x / cell)) + h, int(round(y / cell)) + h
+        pix += (min(mx, h) + min(G - mx, h)) * (min(my, h) + min(G - my, h))
+    out = {"grid": G, "minor_cycles": n, "ms": t, "us_per_minor_cycle": t * 1e3 / max(n, 1),
+           "window_pixels_per_minor_cycle": pix / max(n, 1),
+           "psf_l2_gbs": 4.0 * pix / (t * 1e-3) / 1e9,
+           "updates_gpix_s": pix / (t * 1e-3) / 1e9}
+    if peaks:
+        out["psf_l2_frac_of_measured"] = out["psf_l2_gbs"] / peaks["l2_read_gbs"]
+        out["update_frac_of_measured"] = out["updates_gpix_s"] / peaks["hogbom_update_gpix_s"]
+    return out
+
+
 def c2_block(S, D, dev, args, clocks_mhz=None):
     """The single 2048^2 channel (256 antennas, 10 km log spiral, 120 time
     steps: 3,916,800 visibilities; 17 w-planes hs=4, OS 16): the fused pass
@@ -921,6 +977,18 @@ def c2_block(S, D, dev, args, clocks_mhz=None):
         psf_max = float(psf.max().item())
         psf /= psf_max
         del ones, pgrid
+        # Hogbom alone on the dirty image
+        dgrid = torch.zeros((G * G, 2), dtype=torch.float32, device=dev)
+        plan.grid(measured, dgrid)
+        dirty = torch.empty(G * G, dtype=torch.float32, device=dev)
+        D.grid_to_image(G, dgrid, prol, work, dirty)
+        dirty /= psf_max
+        del dgrid
+        peaks = getattr(args, "peaks", None)
+        out["hogbom"] = hogbom_block(S, D, dev, G, dirty, psf, psf_max, w.cfg.cell_size, peaks)
+        del dirty
+        if peaks:
+            out["fp32_frac_of_measured_fp32x2"] = out["fp32_tflops"] / peaks["fp32x2_fma_tflops"]
         pcfg = S.PipelineConfig(G, OS, w.cfg.uv_scale, w.cfg.w_scale, w.cfg.cell_size, 200, 200, 0.1, 1.5, 0.0002,
                                 psf_max, S.SDP_DEGRID_CONV, S.SDP_COORD_F32, 0, 1)
         pl = D.pipeline(pcfg, uvw, measured, psf, wk_g, wk_d, keep=(uvw, gk, dk, sup))
@@ -980,8 +1048,9 @@ def b200_arm(args):
     D = S.Device(lib)
     A = S.Actors(lib)
     stream = torch.cuda.current_stream()
+    args.peaks = peaks_block(D, dev) if world == 1 else None
     if args.c2_only:
-        print(json.dumps({"c2_2048": c2_block(S, D, dev, args)}), flush=True)
+        print(json.dumps({"c2_2048": c2_block(S, D, dev, args), "peaks_measured": args.peaks}), flush=True)
         return 0
 
     # ---- the 8192^2 workload: this rank's channels on the device ---------------------
@@ -1137,6 +1206,8 @@ def b200_arm(args):
 
     # ---- further blocks (one GPU only) ---------------------------------------------------
     extras = {}
+    if args.peaks:
+        extras["peaks_measured"] = args.peaks
     if world == 1:
         if not args.no_major_cycle and not args.no_extras:
             extras["c5_major_cycle_8192"] = c5_major_cycle_block(S, D, dev, c5)

@@ -757,6 +757,26 @@ int sdp_selftest_bounded_wait(int nblocks, long long spin_limit, int *status);
  * more than launched; *status = SDP_ERR_TIMEOUT when its waits ran out. */
 int sdp_selftest_svd_barrier(int nblocks, long long spin_limit, int *status);
 
+/* Measured on-chip ceilings (no counterpart in the reference): the
+ * denominators of the roofline fractions of kernels that HBM does not bound.
+ *   SDP_PEAK_L2_READ        bytes/s of 16-byte L1-bypassing loads from the
+ *                           L2-resident part of scratch (pass 32 MB or so)
+ *   SDP_PEAK_SMEM_READ      bytes/s of conflict-free 16-byte shared loads
+ *   SDP_PEAK_FP32_FMA       FLOP/s of scalar FP32 fused multiply-adds
+ *   SDP_PEAK_FP32X2_FMA     FLOP/s of packed two-lane FP32 multiply-adds
+ *   SDP_PEAK_HOGBOM_UPDATE  pixel updates/s of the Hogbom residual update
+ *                           float(double(r) - (scale * double(psf)) * psf_max)
+ * scratch: a 16-byte aligned device buffer of at least 4096 bytes; reps
+ * timed launches after one warm-up launch on `stream` (blocking). */
+enum {
+    SDP_PEAK_L2_READ = 0,
+    SDP_PEAK_SMEM_READ = 1,
+    SDP_PEAK_FP32_FMA = 2,
+    SDP_PEAK_FP32X2_FMA = 3,
+    SDP_PEAK_HOGBOM_UPDATE = 4
+};
+int sdp_peak_measure(int kind, void *scratch, size_t scratch_bytes, int reps, double *rate, void *stream);
+
 #ifdef __cplusplus
 }
 #endif

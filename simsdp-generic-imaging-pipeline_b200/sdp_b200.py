@@ -839,6 +839,18 @@ class Device:
         check(self.lib.sdp_svd_check(_dp(workspace), C.byref(sw), _stream(stream)), self.lib)
         return sw.value
 
+    PEAK_KINDS = {"l2_read": 0, "smem_read": 1, "fp32_fma": 2, "fp32x2_fma": 3, "hogbom_update": 4}
+
+    def peak(self, kind: str, scratch, reps: int = 10, stream=None) -> float:
+        """Measured on-chip ceiling (sdp_peak_measure): bytes/s for l2_read and
+        smem_read, FLOP/s for the FMA kinds, pixel updates/s for hogbom_update.
+        scratch: a device tensor (its size is the L2 read buffer)."""
+        r = C.c_double(0.0)
+        check(self.lib.sdp_peak_measure(_i(self.PEAK_KINDS[kind]), _dp(scratch),
+                                        _sz(scratch.numel() * scratch.element_size()), _i(reps), C.byref(r),
+                                        _stream(stream)), self.lib)
+        return r.value
+
     def gaincal_suq(self, n, S, U, Q, SUQ, stream=None):
         check(self.lib.sdp_gaincal_suq(_i(n), _dp(S), _dp(U), _dp(Q), _dp(SUQ), _stream(stream)), self.lib)
 
