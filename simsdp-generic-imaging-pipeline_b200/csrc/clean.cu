@@ -294,15 +294,33 @@ __global__ void k_clean_finish(int G, double cell, int max_records, float3 *__re
 // block sets an error flag, every block stops at its next wait, and the host
 // reads SDP_ERR_TIMEOUT.
 // ---------------------------------------------------------------------------
+// One block's result of a minor cycle: two 64-bit words that each carry the
+// minor cycle's tag ((minor cycle + 1) mod 512), so a reader that sees the
+// tag in both has both values from one round of loads (no flag, no second
+// round trip).  Each word is written and read whole (8-byte relaxed atomics).
+//   a: bits 0-22 the first pixel of the slice's max |r| (kNoPixel: empty
+//      slice), bits 23-31 the tag, bits 32-63 r there (float bits)
+//   b: the sum of |r| over the slice (double; block 0 leaves out pixel 0,
+//      which the reference's running mean skips) with its 9 low mantissa
+//      bits replaced by the tag
 struct PPart {
-    float amax;  // max |r| of the block's slice
-    int idx;     // its first pixel index
-    float val;   // r there (signed)
-    int flag;    // minor cycle + 1 once the fields above are written
-    double sum;  // sum of |r| over the slice
-    float a0;    // |r[0]| (block 0): the running mean skips index 0
-    int pad;
+    unsigned long long a;
+    unsigned long long b;
 };
+constexpr unsigned kTagMask = 511u;
+constexpr int kPixelBits = 23;                       // G <= 2752 for the on-chip path: G^2 < 2^23
+constexpr unsigned kNoPixel = (1u << kPixelBits) - 1u;
+
+__device__ __forceinline__ unsigned part_tag(int minor) { return (unsigned)(minor + 1) & kTagMask; }
+
+__device__ __forceinline__ void part_store(PPart *p, unsigned tag, float val, int idx, double sum)
+{
+    const unsigned lo = ((unsigned)idx & kNoPixel) | (tag << kPixelBits);
+    const unsigned long long a = ((unsigned long long)__float_as_uint(val) << 32) | lo;
+    const unsigned long long b = ((unsigned long long)__double_as_longlong(sum) & ~(unsigned long long)kTagMask) | tag;
+    cuda::atomic_ref<unsigned long long, cuda::thread_scope_device>(p->a).store(a, cuda::memory_order_relaxed);
+    cuda::atomic_ref<unsigned long long, cuda::thread_scope_device>(p->b).store(b, cuda::memory_order_relaxed);
+}
 
 struct CleanBar {
     int err;
@@ -323,28 +341,44 @@ __device__ __forceinline__ void better3(float &v, int &i, float &sv, float v2, i
     }
 }
 
-// Waits (one warp) until the results of blocks 0..nb-1 in buf carry flag
-// `target`.  Lane l watches blocks l, l + 32, ...: each polling round issues
-// all of its flag loads at once (relaxed, so they are in flight together and
-// a round costs one L2 round trip, not one per block), and one acquire fence
-// after the last round orders the result reads behind the flags.  Bounded:
-// after spin_limit rounds, or once another block has timed out, it sets
-// bar->err and returns false.  nb <= 32 * kWaitPerLane.
-constexpr int kWaitPerLane = 8;
+// Waits (one warp) until the results of blocks 0..nb-1 in buf carry `tag`,
+// then folds lane l's blocks l, l + 32, ... into (bv, bi, bs, sum) in block
+// order.  Each polling round issues all of a lane's loads at once (a round
+// costs one L2 round trip).  Bounded: after spin_limit rounds, or once
+// another block has timed out, it sets bar->err and returns false.
+// nb <= 32 * kWaitPerLane.  Not inlined: its registers stay out of the
+// pixel pass of the kernel that calls it.
+constexpr int kWaitPerLane = 5;  // 160 blocks: one per SM of a 148-SM part
 
-__device__ bool wait_results(PPart *buf, int nb, int target, CleanBar *bar, long long spin_limit)
+struct PBest {
+    float bv;    // max |r| (-1: none)
+    int bi;      // its first pixel
+    float bs;    // r there
+    int ok;      // 0: the wait gave up
+    double sum;  // sum of |r|
+};
+
+__device__ __noinline__ PBest wait_results(PPart *buf, int nb, unsigned tag, CleanBar *bar, long long spin_limit)
 {
+    float bv = -1.f, bs = 0.f;
+    int bi = 0x7fffffff;
+    double sum = 0.0;
     cuda::atomic_ref<int, cuda::thread_scope_device> err(bar->err);
     const int lane = (int)(threadIdx.x & 31);
+    unsigned long long a[kWaitPerLane], b[kWaitPerLane];
     int fail = 0;
     for (long long spins = 0;;) {
         bool ready = true;
 #pragma unroll
         for (int j = 0; j < kWaitPerLane; ++j) {
-            const int b = lane + 32 * j;
-            if (b < nb)
-                ready &= cuda::atomic_ref<int, cuda::thread_scope_device>(buf[b].flag).load(
-                             cuda::memory_order_relaxed) == target;
+            const int k = lane + 32 * j;
+            if (k < nb) {
+                a[j] = cuda::atomic_ref<unsigned long long, cuda::thread_scope_device>(buf[k].a).load(
+                    cuda::memory_order_relaxed);
+                b[j] = cuda::atomic_ref<unsigned long long, cuda::thread_scope_device>(buf[k].b).load(
+                    cuda::memory_order_relaxed);
+                ready &= (((unsigned)a[j] >> kPixelBits) & kTagMask) == tag && ((unsigned)b[j] & kTagMask) == tag;
+            }
         }
         if (ready) break;
         if (err.load(cuda::memory_order_relaxed) != 0 || ++spins > spin_limit) {
@@ -354,8 +388,27 @@ __device__ bool wait_results(PPart *buf, int nb, int target, CleanBar *bar, long
         }
         __nanosleep(32);
     }
-    cuda::atomic_thread_fence(cuda::memory_order_acquire, cuda::thread_scope_device);
-    return !__any_sync(0xffffffffu, fail);
+    if (!fail) {
+#pragma unroll
+        for (int j = 0; j < kWaitPerLane; ++j)
+            if (lane + 32 * j < nb) {
+                const unsigned pix = (unsigned)a[j] & kNoPixel;
+                const float val = __uint_as_float((unsigned)(a[j] >> 32));
+                if (pix != kNoPixel && (fabsf(val) > bv || (fabsf(val) == bv && (int)pix < bi))) {
+                    bv = fabsf(val);
+                    bi = (int)pix;
+                    bs = val;
+                }
+                sum += __longlong_as_double((long long)(b[j] & ~(unsigned long long)kTagMask));
+            }
+    }
+    PBest r;
+    r.bv = bv;
+    r.bi = bi;
+    r.bs = bs;
+    r.sum = sum;
+    r.ok = !__any_sync(0xffffffffu, fail);
+    return r;
 }
 
 __device__ __forceinline__ void block_reduce3(float &bv, int &bi, float &bs, double &sum)
@@ -394,7 +447,8 @@ __device__ __forceinline__ void block_reduce3(float &bv, int &bi, float &bs, dou
             sum += __shfl_xor_sync(0xffffffffu, sum, o);
         }
     }
-    __syncthreads();
+    // no barrier here: only warp 0 goes on with the result, and the next
+    // call's writes to the arrays above come after the caller's next barrier
 }
 
 __device__ __forceinline__ void cp_async4(float *dst_smem, const float *src)
@@ -415,7 +469,7 @@ __global__ void __launch_bounds__(kPersistThreads, 1) k_clean_persistent(
     double noise, double weak, double psf_max, double cell, PPart *__restrict__ parts, CleanBar *bar, int P,
     long long spin_limit)
 {
-    extern __shared__ float sr[];
+    extern __shared__ __align__(16) float sr[];
     __shared__ int s_pending, s_mx, s_my, s_stop, s_fail;
     __shared__ float s_val;
     const int tid = threadIdx.x;
@@ -439,6 +493,10 @@ __global__ void __launch_bounds__(kPersistThreads, 1) k_clean_persistent(
     double model_add = 0.0;
     const int half = G / 2;
     const int step_y = kPersistThreads / G, step_x = kPersistThreads - (kPersistThreads / G) * G;
+    // quads: G and the slice start are multiples of 4, so a quad never
+    // crosses a row
+    const bool quad = (G & 3) == 0 && (P & 3) == 0;
+    const int step_y4 = 4 * kPersistThreads / G, step_x4 = 4 * kPersistThreads - step_y4 * G;
     for (int it = 0; it <= num_minor; ++it) {
         const bool apply_only = (it == num_minor);
         const int pending = s_pending, mx = s_mx, my = s_my;
@@ -498,7 +556,64 @@ __global__ void __launch_bounds__(kPersistThreads, 1) k_clean_persistent(
                 }
             }
         }
-        for (int kb = tid; !STAGE && kb < n; kb += kBatch * kPersistThreads) {
+        if (!STAGE && quad) {
+            // four adjacent pixels of one row per thread and step (one
+            // 16-byte shared access; window rows and PSF offsets once per
+            // quad): quad q = tid + m * 1024 is pixels p0 + 4 q .. + 3, two
+            // quads' PSF loads in flight together
+            float4 *sr4 = reinterpret_cast<float4 *>(sr);
+            const int nq = n >> 2;
+            int qy = (p0 + 4 * tid) / G, qx = (p0 + 4 * tid) - qy * G;
+            for (int qb = tid; qb < nq; qb += 2 * kPersistThreads) {
+                float4 w4[2];
+                float pv[2][4];
+                bool in[2][4];
+                int qi[2];
+#pragma unroll
+                for (int u = 0; u < 2; ++u) {
+                    const int q = qb + u * kPersistThreads;
+                    const bool live = q < nq;
+                    qi[u] = qy * G + qx;
+                    w4[u] = live ? sr4[q] : make_float4(0.f, 0.f, 0.f, 0.f);
+                    const bool iny = live && pending && (unsigned)(qy - y0) < (unsigned)wy;
+                    const int ux = qx - x0;
+                    const int pi = qi[u] - 2 * qx + pofs;  // PSF index of the quad's pixel 0; pixel j: pi - j
+#pragma unroll
+                    for (int j = 0; j < 4; ++j) {
+                        in[u][j] = iny && (unsigned)(ux + j) < (unsigned)wx && pi - j < g2;
+                        pv[u][j] = in[u][j] ? __ldg(&psf[pi - j]) : 0.f;
+                    }
+                    qx += step_x4;
+                    qy += step_y4;
+                    if (qx >= G) {
+                        qx -= G;
+                        qy += 1;
+                    }
+                }
+#pragma unroll
+                for (int u = 0; u < 2; ++u) {
+                    float wv[4] = {w4[u].x, w4[u].y, w4[u].z, w4[u].w};
+#pragma unroll
+                    for (int j = 0; j < 4; ++j)
+                        if (in[u][j])
+                            wv[j] = __double2float_rn(
+                                __dsub_rn((double)wv[j], __dmul_rn(__dmul_rn(scale, (double)pv[u][j]), psf_max)));
+                    if (in[u][0] || in[u][1] || in[u][2] || in[u][3])
+                        sr4[qb + u * kPersistThreads] = make_float4(wv[0], wv[1], wv[2], wv[3]);
+#pragma unroll
+                    for (int j = 0; j < 4; ++j) {
+                        const float a = fabsf(wv[j]);
+                        if (a > bv) {  // pixels visited in increasing index: the first maximum wins
+                            bv = a;
+                            bi = qi[u] + j;
+                            bs = wv[j];
+                        }
+                        rsum += a;  // 0 for the padding past the slice
+                    }
+                }
+            }
+        }
+        for (int kb = tid; !STAGE && !quad && kb < n; kb += kBatch * kPersistThreads) {
             float w[kBatch], pv[kBatch];
             int ii[kBatch];
             bool in[kBatch];
@@ -538,14 +653,11 @@ __global__ void __launch_bounds__(kPersistThreads, 1) k_clean_persistent(
         double sum = (double)rsum;
         block_reduce3(bv, bi, bs, sum);
         PPart *buf = parts + (size_t)(it & 1) * nb;
+        const unsigned tag = part_tag(it);
         if (tid == 0) {
-            PPart *mine = buf + blockIdx.x;
-            mine->amax = bv;
-            mine->idx = bi;
-            mine->val = bs;
-            mine->sum = sum;
-            mine->a0 = (blockIdx.x == 0 && n > 0) ? fabsf(sr[0]) : 0.f;
-            cuda::atomic_ref<int, cuda::thread_scope_device>(mine->flag).store(it + 1, cuda::memory_order_release);
+            // block 0 leaves out pixel 0 (the reference's running mean skips it)
+            if (blockIdx.x == 0 && n > 0) sum = __dsub_rn(sum, (double)fabsf(sr[0]));
+            part_store(buf + blockIdx.x, tag, bs, bv < 0.f ? (int)kNoPixel : bi, sum);
             // block 0 adds the previous component to the model here, off the
             // critical path (model updates keep the reference's order)
             if (model_idx >= 0) {
@@ -557,19 +669,12 @@ __global__ void __launch_bounds__(kPersistThreads, 1) k_clean_persistent(
         // minor cycle, reduces them in the same order and takes the same
         // decision
         if (tid < 32) {
-            bv = -1.f;
-            bi = 0x7fffffff;
-            bs = 0.f;
-            sum = 0.0;
-            float a0 = 0.f;
-            const int fail = wait_results(buf, nb, it + 1, bar, spin_limit) ? 0 : 1;
-            if (!fail)
-                for (int b = tid; b < nb; b += 32) {
-                    const PPart *pq = buf + b;
-                    better3(bv, bi, bs, __ldcg(&pq->amax), __ldcg(&pq->idx), __ldcg(&pq->val));
-                    sum += __ldcg(&pq->sum);
-                    if (b == 0) a0 = __ldcg(&pq->a0);
-                }
+            const PBest w = wait_results(buf, nb, tag, bar, spin_limit);
+            const int fail = w.ok ? 0 : 1;
+            bv = w.bv;
+            bi = w.bi;
+            bs = w.bs;
+            sum = w.sum;
 #pragma unroll
             for (int o = 16; o > 0; o >>= 1) {
                 const float v2 = __shfl_xor_sync(0xffffffffu, bv, o);
@@ -578,7 +683,6 @@ __global__ void __launch_bounds__(kPersistThreads, 1) k_clean_persistent(
                 better3(bv, bi, bs, v2, i2, s2);
                 sum += __shfl_xor_sync(0xffffffffu, sum, o);
             }
-            a0 = __shfl_sync(0xffffffffu, a0, 0);
             if (tid == 0) {
                 if (fail) {
                     s_fail = 1;
@@ -593,7 +697,7 @@ __global__ void __launch_bounds__(kPersistThreads, 1) k_clean_persistent(
                         idx = 0;
                         sval = 0.f;
                     }
-                    const float avg = (g2 > 1) ? (float)(__dsub_rn(sum, (double)a0) / (double)(g2 - 1)) : 0.f;
+                    const float avg = (g2 > 1) ? (float)(sum / (double)(g2 - 1)) : 0.f;
                     const bool extracting_noise = (double)fabsf(curr_max) < noise * (double)avg * gain;  // :238
                     const bool weak_source =
                         count > 0 && (double)fabsf(curr_max) < (double)fabsf(first_z) * weak;  // :239
@@ -641,9 +745,8 @@ __global__ void __launch_bounds__(kPersistThreads, 1) k_clean_persistent(
 // the kernel ends with the error flag set (the host reads SDP_ERR_TIMEOUT).
 __global__ void k_wait_timeout_probe(PPart *parts, CleanBar *bar, long long spin_limit)
 {
-    if (threadIdx.x == 0)
-        cuda::atomic_ref<int, cuda::thread_scope_device>(parts[blockIdx.x].flag).store(1, cuda::memory_order_release);
-    if (threadIdx.x < 32) wait_results(parts, (int)gridDim.x + 1, 1, bar, spin_limit);
+    if (threadIdx.x == 0) part_store(parts + blockIdx.x, part_tag(0), 1.f, (int)blockIdx.x, 1.0);
+    if (threadIdx.x < 32) wait_results(parts, (int)gridDim.x + 1, part_tag(0), bar, spin_limit);
 }
 
 static void persist_layout(int nb, size_t base, size_t *bar_off, size_t *parts_off, size_t *total)

@@ -1322,6 +1322,13 @@ __device__ __forceinline__ bool fast_item(const PlanDev &Pin, const int4 it, Ite
 // records of one work item (chunk 16-byte records, chunk + 2 measured
 // values), per-plane constants (nk int4), then the model tile and the NW
 // subgrids.
+// Shared memory of a block on sm_100 (opt-in limit) and an upper bound on
+// the static arrays of the tile kernels (at most 896 B): the dynamic part
+// must fit in what is left, and needs the opt-in attribute once the two
+// together pass 48 KB.
+constexpr size_t kSmemOptin = 227 * 1024;
+constexpr size_t kStaticSmem = 1024;
+
 __host__ __device__ __forceinline__ size_t fast_stage_bytes(int chunk)
 {
     return (16 * (size_t)chunk + 8 * ((size_t)chunk + 2) + 15) / 16 * 16;  // the plane table after it is int4
@@ -2015,7 +2022,7 @@ static int launch_tiles_lg(sdp_visplan *p, int op, const float2 *vis_in, const f
     case OP_G2G: fn = k_tiles<T, SDP_GRID_STD, OP_G2G, LG>; break;
     default: return set_error(SDP_ERR_INVALID, "internal: op %d", op);
     }
-    if (smem > 48 * 1024) SDP_CUDA_TRY(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    if (smem + kStaticSmem > 48 * 1024) SDP_CUDA_TRY(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     int per_sm = 0;
     SDP_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, kThreads, smem));
     if (per_sm < 1) return set_error(SDP_ERR_RANGE, "tile kernel does not fit (%zu B shared memory)", smem);
@@ -2030,7 +2037,8 @@ static int launch_tiles_lg(sdp_visplan *p, int op, const float2 *vis_in, const f
 // group kernels (lanes != 0).
 static bool fast_eligible(const sdp_visplan *p)
 {
-    return p->mode == SDP_GRID_STD && p->lanes == 0 && p->hs_max >= 1 && p->hs_max <= 4;
+    return p->mode == SDP_GRID_STD && p->lanes == 0 && p->hs_max >= 1 && p->hs_max <= 4 &&
+           fast_smem_bytes(OP_CYCLE_CONV, 4, p->S, p->pitch, p->gk.num_kernels, p->chunk) + kStaticSmem <= kSmemOptin;
 }
 
 template <typename T, int OP, int NW>
@@ -2040,14 +2048,14 @@ static int launch_fast_nw(sdp_visplan *p, const float2 *vis_in, const float2 *in
     const size_t smem = fast_smem_bytes(OP, NW, p->S, p->pitch, p->gk.num_kernels, p->chunk);
     void (*fn)(PlanDev, const float2 *, const float2 *, float2 *, float2 *, float2 *, const float2 *) =
         k_vis_fast<T, OP, NW>;
-    if (smem > 227 * 1024) {
+    if (smem + kStaticSmem > kSmemOptin) {
         if (resident_warps) {
             *resident_warps = 0;
             return SDP_OK;
         }
         return set_error(SDP_ERR_RANGE, "tile kernel does not fit (%zu B shared memory)", smem);
     }
-    if (smem > 48 * 1024) SDP_CUDA_TRY(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    if (smem + kStaticSmem > 48 * 1024) SDP_CUDA_TRY(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     int per_sm = 0;
     SDP_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, 32 * NW, smem));
     if (resident_warps) {  // query only
@@ -2205,7 +2213,7 @@ static int launch_batch_lg(sdp_visbatch *b, int op, cudaStream_t st)
     void (*fn)(const PlanDev *, const BatchIO *, const int4 *, int, int *, int) =
         op == OP_CYCLE_CONV ? k_tiles_batch<T, SDP_GRID_STD, OP_CYCLE_CONV, LG>
                             : k_tiles_batch<T, SDP_GRID_STD, OP_CYCLE_NEAR, LG>;
-    if (smem > 48 * 1024) SDP_CUDA_TRY(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    if (smem + kStaticSmem > 48 * 1024) SDP_CUDA_TRY(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     int per_sm = 0;
     SDP_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, kThreads, smem));
     if (per_sm < 1) return set_error(SDP_ERR_RANGE, "batched tile kernel does not fit (%zu B shared memory)", smem);
@@ -2221,14 +2229,14 @@ static int launch_batch_fast_nw(sdp_visbatch *b, cudaStream_t st, int *resident_
 {
     const size_t smem = fast_stage_bytes(b->chunk_max) + 16 * (size_t)b->nk_max + 8 * b->tile_f2 * (1 + NW);
     void (*fn)(const PlanDev *, const BatchIO *, const int4 *, int, int *, int, int, int) = k_vis_fast_batch<T, NW>;
-    if (smem > 227 * 1024) {
+    if (smem + kStaticSmem > kSmemOptin) {
         if (resident_warps) {
             *resident_warps = 0;
             return SDP_OK;
         }
         return set_error(SDP_ERR_RANGE, "batched tile kernel does not fit (%zu B shared memory)", smem);
     }
-    if (smem > 48 * 1024) SDP_CUDA_TRY(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    if (smem + kStaticSmem > 48 * 1024) SDP_CUDA_TRY(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     int per_sm = 0;
     SDP_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, 32 * NW, smem));
     if (resident_warps) {
@@ -2311,6 +2319,10 @@ SDP_EXPORT int sdp_visbatch_create(sdp_visbatch **out, sdp_visplan *const *plans
         }
         for (int4 it : pi) items.push_back(make_int4(it.x, it.y, it.z, c));
     }
+    // the batched kernel holds the largest channel's tiles and work item
+    if (b->fast && fast_stage_bytes(b->chunk_max) + 16 * (size_t)b->nk_max + 8 * b->tile_f2 * (1 + 4) + kStaticSmem >
+                       kSmemOptin)
+        b->fast = false;
     b->n_items = (int)items.size();
     b->io.resize((size_t)num_plans);
     cudaError_t e = cudaMalloc(&b->d_plans, sizeof(PlanDev) * devs.size());
