@@ -1132,16 +1132,24 @@ def b200_arm(args):
     clocks.__exit__(None, None, None)
     sms = torch.cuda.get_device_properties(dev).multi_processor_count
     sm_mhz = float(csum["sm_mhz"]) if csum.get("sm_mhz") else 1965.0
-    fp32_peak = sms * 128 * 2 * sm_mhz * 1e6 / 1e12
+    pk = getattr(args, "peaks", None)
+    if pk:
+        fp32_peak = pk["fp32x2_fma_tflops"]
+        fp32_src = "measured: packed FP32 FMA (csrc/peaks.cu)"
+        peak_wf = pk["smem_read_gbs"] * 1e9 / 128.0
+        wf_src = "measured: conflict-free 16-byte shared loads (csrc/peaks.cu), 128 B per wavefront"
+    else:
+        fp32_peak = sms * 128 * 2 * sm_mhz * 1e6 / 1e12
+        fp32_src = f"{sms} SMs x 128 FP32 lanes x 2 x the median SM clock in the timed region"
+        peak_wf = sms * sm_mhz * 1e6
+        wf_src = f"{sms} SMs x 1 wavefront per clock x the median SM clock"
     binding = {"fp32": {"achieved_tflops": alg_flops / (t_pass * 1e-3) / 1e12, "peak_tflops": fp32_peak,
-                        "frac": alg_flops / (t_pass * 1e-3) / 1e12 / fp32_peak,
-                        "peak_source": f"{sms} SMs x 128 FP32 lanes x 2 x the median SM clock in the timed region"}}
+                        "frac": alg_flops / (t_pass * 1e-3) / 1e12 / fp32_peak, "peak_source": fp32_src}}
     wf = read_profile_value("k_vis_fast_batch_c5_8192", "shared_wavefronts_per_launch")
     if wf is not None:
-        peak_wf = sms * sm_mhz * 1e6
         binding["shared_memory"] = {"achieved_wavefronts_per_s": wf / (t_pass * 1e-3), "peak": peak_wf,
                                     "frac": wf / (t_pass * 1e-3) / peak_wf, "per_launch": wf,
-                                    "peak_source": f"{sms} SMs x 1 wavefront per clock x the median SM clock"}
+                                    "peak_source": wf_src}
 
     # ---- e2e through the reference-facing C ABI with pinned host buffers -----------
     e2e = None

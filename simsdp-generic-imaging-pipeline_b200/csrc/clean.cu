@@ -140,6 +140,14 @@ __device__ void select_component(int G, int max_records, float curr_max, int idx
     st->val = max_val;
 }
 
+// The reference's residual update of one pixel (deconvolution_run.c:271 in
+// its types: float residual, double gain x max_val, float PSF, double
+// psf_max_value).
+__device__ __forceinline__ float hogbom_update(float w, float p, double scale, double psf_max)
+{
+    return __double2float_rn(__dsub_rn((double)w, __dmul_rn(__dmul_rn(scale, (double)p), psf_max)));
+}
+
 // Subtraction of the pending component at pixel (y, x) (:266-272).
 __device__ __forceinline__ float clean_pixel(float v, int x, bool row_in, int x0, int x1, long long pbase,
                                              long long g2, const float *__restrict__ psf, double scale,
@@ -148,7 +156,7 @@ __device__ __forceinline__ float clean_pixel(float v, int x, bool row_in, int x0
     if (row_in && x >= x0 && x < x1) {
         const long long pi = pbase - x;  // mirrored in x; index G*G reads 0
         const float pv = (pi < g2) ? __ldg(&psf[pi]) : 0.f;
-        v = __double2float_rn(__dsub_rn((double)v, __dmul_rn(__dmul_rn(scale, (double)pv), psf_max)));
+        v = hogbom_update(v, pv, scale, psf_max);
     }
     return v;
 }
@@ -313,13 +321,33 @@ constexpr unsigned kNoPixel = (1u << kPixelBits) - 1u;
 
 __device__ __forceinline__ unsigned part_tag(int minor) { return (unsigned)(minor + 1) & kTagMask; }
 
+// SUM = false: only word a is written and read (the noise test cannot stop
+// the loop, see k_clean_persistent).
+template <bool SUM>
 __device__ __forceinline__ void part_store(PPart *p, unsigned tag, float val, int idx, double sum)
 {
     const unsigned lo = ((unsigned)idx & kNoPixel) | (tag << kPixelBits);
     const unsigned long long a = ((unsigned long long)__float_as_uint(val) << 32) | lo;
-    const unsigned long long b = ((unsigned long long)__double_as_longlong(sum) & ~(unsigned long long)kTagMask) | tag;
     cuda::atomic_ref<unsigned long long, cuda::thread_scope_device>(p->a).store(a, cuda::memory_order_relaxed);
-    cuda::atomic_ref<unsigned long long, cuda::thread_scope_device>(p->b).store(b, cuda::memory_order_relaxed);
+    if constexpr (SUM) {
+        const unsigned long long b =
+            ((unsigned long long)__double_as_longlong(sum) & ~(unsigned long long)kTagMask) | tag;
+        cuda::atomic_ref<unsigned long long, cuda::thread_scope_device>(p->b).store(b, cuda::memory_order_relaxed);
+    }
+}
+
+// Order key of a candidate (max |r| v >= 0, or v < 0 for none): larger v,
+// larger key; none is 0.  Non-negative floats order as their bit patterns.
+__device__ __forceinline__ unsigned cand_key(float v) { return v < 0.f ? 0u : __float_as_uint(v) + 1u; }
+__device__ __forceinline__ float key_value(unsigned k) { return k == 0u ? -1.f : __uint_as_float(k - 1u); }
+
+// Warp-wide best candidate: the largest key, on ties the smallest pixel
+// index (every lane gets the result).
+__device__ __forceinline__ void warp_best(unsigned &key, unsigned &idx)
+{
+    const unsigned kmax = __reduce_max_sync(0xffffffffu, key);
+    idx = __reduce_min_sync(0xffffffffu, key == kmax ? idx : 0xffffffffu);
+    key = kmax;
 }
 
 struct CleanBar {
@@ -332,14 +360,6 @@ constexpr int kPersistSlice = 51200;           // floats of residual per block (
 constexpr int kBatch = 8;                      // pixels per thread whose PSF loads are in flight together
 constexpr long long kBarrierSpins = 4000000;   // polling rounds of ~32 ns sleep + an L2 read: one to two seconds
 
-__device__ __forceinline__ void better3(float &v, int &i, float &sv, float v2, int i2, float sv2)
-{
-    if (v2 > v || (v2 == v && i2 < i)) {
-        v = v2;
-        i = i2;
-        sv = sv2;
-    }
-}
 
 // Waits (one warp) until the results of blocks 0..nb-1 in buf carry `tag`,
 // then folds lane l's blocks l, l + 32, ... into (bv, bi, bs, sum) in block
@@ -355,14 +375,12 @@ struct PBest {
     int bi;      // its first pixel
     float bs;    // r there
     int ok;      // 0: the wait gave up
-    double sum;  // sum of |r|
+    double sum;  // sum of |r| (SUM)
 };
 
+template <bool SUM>
 __device__ __noinline__ PBest wait_results(PPart *buf, int nb, unsigned tag, CleanBar *bar, long long spin_limit)
 {
-    float bv = -1.f, bs = 0.f;
-    int bi = 0x7fffffff;
-    double sum = 0.0;
     cuda::atomic_ref<int, cuda::thread_scope_device> err(bar->err);
     const int lane = (int)(threadIdx.x & 31);
     unsigned long long a[kWaitPerLane], b[kWaitPerLane];
@@ -375,9 +393,12 @@ __device__ __noinline__ PBest wait_results(PPart *buf, int nb, unsigned tag, Cle
             if (k < nb) {
                 a[j] = cuda::atomic_ref<unsigned long long, cuda::thread_scope_device>(buf[k].a).load(
                     cuda::memory_order_relaxed);
-                b[j] = cuda::atomic_ref<unsigned long long, cuda::thread_scope_device>(buf[k].b).load(
-                    cuda::memory_order_relaxed);
-                ready &= (((unsigned)a[j] >> kPixelBits) & kTagMask) == tag && ((unsigned)b[j] & kTagMask) == tag;
+                ready &= (((unsigned)a[j] >> kPixelBits) & kTagMask) == tag;
+                if constexpr (SUM) {
+                    b[j] = cuda::atomic_ref<unsigned long long, cuda::thread_scope_device>(buf[k].b).load(
+                        cuda::memory_order_relaxed);
+                    ready &= ((unsigned)b[j] & kTagMask) == tag;
+                }
             }
         }
         if (ready) break;
@@ -388,63 +409,73 @@ __device__ __noinline__ PBest wait_results(PPart *buf, int nb, unsigned tag, Cle
         }
         __nanosleep(32);
     }
+    // this lane's blocks in block order, then the warp
+    unsigned key = 0u, idx = 0xffffffffu;
+    float val = 0.f;
+    double sum = 0.0;
     if (!fail) {
 #pragma unroll
         for (int j = 0; j < kWaitPerLane; ++j)
             if (lane + 32 * j < nb) {
                 const unsigned pix = (unsigned)a[j] & kNoPixel;
-                const float val = __uint_as_float((unsigned)(a[j] >> 32));
-                if (pix != kNoPixel && (fabsf(val) > bv || (fabsf(val) == bv && (int)pix < bi))) {
-                    bv = fabsf(val);
-                    bi = (int)pix;
-                    bs = val;
+                const float v = __uint_as_float((unsigned)(a[j] >> 32));
+                const unsigned k = pix == kNoPixel ? 0u : cand_key(fabsf(v));
+                if (k > key || (k == key && k != 0u && pix < idx)) {
+                    key = k;
+                    idx = pix;
+                    val = v;
                 }
-                sum += __longlong_as_double((long long)(b[j] & ~(unsigned long long)kTagMask));
+                if constexpr (SUM) sum += __longlong_as_double((long long)(b[j] & ~(unsigned long long)kTagMask));
             }
     }
+    const unsigned key0 = key, idx0 = idx;
+    warp_best(key, idx);
+    const unsigned win = __ballot_sync(0xffffffffu, key0 == key && idx0 == idx);
+    val = __shfl_sync(0xffffffffu, val, win ? __ffs(win) - 1 : 0);
+    if constexpr (SUM) {
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) sum += __shfl_xor_sync(0xffffffffu, sum, o);
+    }
     PBest r;
-    r.bv = bv;
-    r.bi = bi;
-    r.bs = bs;
+    r.bv = key_value(key);
+    r.bi = (int)idx;
+    r.bs = val;
     r.sum = sum;
     r.ok = !__any_sync(0xffffffffu, fail);
     return r;
 }
 
-__device__ __forceinline__ void block_reduce3(float &bv, int &bi, float &bs, double &sum)
+// Block-wide best candidate (bv, bi) and, with SUM, the sum; the result is
+// in warp 0 (all lanes).
+template <bool SUM>
+__device__ __forceinline__ void block_best(float &bv, int &bi, double &sum)
 {
-    __shared__ float sv[32], sval[32];
-    __shared__ int si[32];
-    __shared__ double ss[32];
+    __shared__ unsigned s_key[32], s_idx[32];
+    __shared__ double s_sum[32];
     const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    unsigned key = cand_key(bv), idx = (unsigned)bi;
+    warp_best(key, idx);
+    if constexpr (SUM) {
 #pragma unroll
-    for (int o = 16; o > 0; o >>= 1) {
-        const float v2 = __shfl_xor_sync(0xffffffffu, bv, o);
-        const int i2 = __shfl_xor_sync(0xffffffffu, bi, o);
-        const float s2 = __shfl_xor_sync(0xffffffffu, bs, o);
-        better3(bv, bi, bs, v2, i2, s2);
-        sum += __shfl_xor_sync(0xffffffffu, sum, o);
+        for (int o = 16; o > 0; o >>= 1) sum += __shfl_xor_sync(0xffffffffu, sum, o);
     }
     if (lane == 0) {
-        sv[wid] = bv;
-        si[wid] = bi;
-        sval[wid] = bs;
-        ss[wid] = sum;
+        s_key[wid] = key;
+        s_idx[wid] = idx;
+        if constexpr (SUM) s_sum[wid] = sum;
     }
     __syncthreads();
     if (wid == 0) {
         const int nw = blockDim.x / 32;
-        bv = (lane < nw) ? sv[lane] : -1.f;
-        bi = (lane < nw) ? si[lane] : 0x7fffffff;
-        bs = (lane < nw) ? sval[lane] : 0.f;
-        sum = (lane < nw) ? ss[lane] : 0.0;
+        key = lane < nw ? s_key[lane] : 0u;
+        idx = lane < nw ? s_idx[lane] : 0xffffffffu;
+        warp_best(key, idx);
+        bv = key_value(key);
+        bi = (int)idx;
+        if constexpr (SUM) {
+            sum = lane < nw ? s_sum[lane] : 0.0;
 #pragma unroll
-        for (int o = 16; o > 0; o >>= 1) {
-            const float v2 = __shfl_xor_sync(0xffffffffu, bv, o);
-            const int i2 = __shfl_xor_sync(0xffffffffu, bi, o);
-            const float s2 = __shfl_xor_sync(0xffffffffu, bs, o);
-            better3(bv, bi, bs, v2, i2, s2);
-            sum += __shfl_xor_sync(0xffffffffu, sum, o);
+            for (int o = 16; o > 0; o >>= 1) sum += __shfl_xor_sync(0xffffffffu, sum, o);
         }
     }
     // no barrier here: only warp 0 goes on with the result, and the next
@@ -457,12 +488,19 @@ __device__ __forceinline__ void cp_async4(float *dst_smem, const float *src)
     asm volatile("cp.async.ca.shared.global [%0], [%1], 4;" ::"r"(d), "l"(src) : "memory");
 }
 
-// STAGE: the PSF samples of a minor cycle are first copied into a second
-// shared-memory slice with asynchronous copies (all of a thread's copies in
-// flight at once, one wait), then the pass reads them from shared memory.
-// Used for small slices (at most two pixels per thread, G <= ~550 on 148
-// SMs); larger slices keep the batched direct loads.
-template <bool STAGE>
+// Pass variants of the persistent kernel (one per instantiation, chosen by
+// the host):
+//   kPassStage  the PSF samples of a minor cycle are first copied into a
+//               second shared-memory slice with asynchronous copies (all of
+//               a thread's copies in flight at once, one wait), then read
+//               from there; small slices (at most two pixels per thread,
+//               G <= ~550 on 148 SMs)
+//   kPassScalar one pixel per thread and step, eight PSF loads in flight
+//   kPassQuad   four adjacent pixels per thread and step (G and the slice
+//               length multiples of 4)
+enum : int { kPassStage = 0, kPassScalar = 1, kPassQuad = 2 };
+
+template <int MODE, bool SUM>
 __global__ void __launch_bounds__(kPersistThreads, 1) k_clean_persistent(
     int G, float *__restrict__ r, const float *__restrict__ psf, float *__restrict__ model,
     float3 *__restrict__ src, int *__restrict__ count_out, int max_records, int num_minor, double gain,
@@ -495,7 +533,7 @@ __global__ void __launch_bounds__(kPersistThreads, 1) k_clean_persistent(
     const int step_y = kPersistThreads / G, step_x = kPersistThreads - (kPersistThreads / G) * G;
     // quads: G and the slice start are multiples of 4, so a quad never
     // crosses a row
-    const bool quad = (G & 3) == 0 && (P & 3) == 0;
+    constexpr bool STAGE = MODE == kPassStage;
     const int step_y4 = 4 * kPersistThreads / G, step_x4 = 4 * kPersistThreads - step_y4 * G;
     for (int it = 0; it <= num_minor; ++it) {
         const bool apply_only = (it == num_minor);
@@ -538,7 +576,7 @@ __global__ void __launch_bounds__(kPersistThreads, 1) k_clean_persistent(
             for (int k = tid; k < n; k += kPersistThreads) {
                 float wv = sr[k];
                 if (pending && (unsigned)(y - y0) < (unsigned)wy && (unsigned)(x - x0) < (unsigned)wx) {
-                    wv = __double2float_rn(__dsub_rn((double)wv, __dmul_rn(__dmul_rn(scale, (double)ps[k]), psf_max)));
+                    wv = hogbom_update(wv, ps[k], scale, psf_max);
                     sr[k] = wv;
                 }
                 const float a = fabsf(wv);
@@ -547,7 +585,7 @@ __global__ void __launch_bounds__(kPersistThreads, 1) k_clean_persistent(
                     bi = y * G + x;
                     bs = wv;
                 }
-                rsum += a;
+                if constexpr (SUM) rsum += a;
                 x += step_x;
                 y += step_y;
                 if (x >= G) {
@@ -556,7 +594,7 @@ __global__ void __launch_bounds__(kPersistThreads, 1) k_clean_persistent(
                 }
             }
         }
-        if (!STAGE && quad) {
+        if constexpr (MODE == kPassQuad) {
             // four adjacent pixels of one row per thread and step (one
             // 16-byte shared access; window rows and PSF offsets once per
             // quad): quad q = tid + m * 1024 is pixels p0 + 4 q .. + 3, two
@@ -596,8 +634,7 @@ __global__ void __launch_bounds__(kPersistThreads, 1) k_clean_persistent(
 #pragma unroll
                     for (int j = 0; j < 4; ++j)
                         if (in[u][j])
-                            wv[j] = __double2float_rn(
-                                __dsub_rn((double)wv[j], __dmul_rn(__dmul_rn(scale, (double)pv[u][j]), psf_max)));
+                            wv[j] = hogbom_update(wv[j], pv[u][j], scale, psf_max);
                     if (in[u][0] || in[u][1] || in[u][2] || in[u][3])
                         sr4[qb + u * kPersistThreads] = make_float4(wv[0], wv[1], wv[2], wv[3]);
 #pragma unroll
@@ -608,12 +645,12 @@ __global__ void __launch_bounds__(kPersistThreads, 1) k_clean_persistent(
                             bi = qi[u] + j;
                             bs = wv[j];
                         }
-                        rsum += a;  // 0 for the padding past the slice
+                        if constexpr (SUM) rsum += a;  // 0 for the padding past the slice
                     }
                 }
             }
         }
-        for (int kb = tid; !STAGE && !quad && kb < n; kb += kBatch * kPersistThreads) {
+        for (int kb = tid; MODE == kPassScalar && kb < n; kb += kBatch * kPersistThreads) {
             float w[kBatch], pv[kBatch];
             int ii[kBatch];
             bool in[kBatch];
@@ -637,7 +674,7 @@ __global__ void __launch_bounds__(kPersistThreads, 1) k_clean_persistent(
             for (int u = 0; u < kBatch; ++u) {
                 float wv = w[u];
                 if (in[u]) {
-                    wv = __double2float_rn(__dsub_rn((double)wv, __dmul_rn(__dmul_rn(scale, (double)pv[u]), psf_max)));
+                    wv = hogbom_update(wv, pv[u], scale, psf_max);
                     sr[kb + u * kPersistThreads] = wv;
                 }
                 const float a = fabsf(wv);
@@ -646,18 +683,18 @@ __global__ void __launch_bounds__(kPersistThreads, 1) k_clean_persistent(
                     bi = ii[u];
                     bs = wv;
                 }
-                rsum += a;  // 0 for the padding past the slice
+                if constexpr (SUM) rsum += a;  // 0 for the padding past the slice
             }
         }
         if (apply_only) break;
         double sum = (double)rsum;
-        block_reduce3(bv, bi, bs, sum);
+        block_best<SUM>(bv, bi, sum);
         PPart *buf = parts + (size_t)(it & 1) * nb;
         const unsigned tag = part_tag(it);
         if (tid == 0) {
             // block 0 leaves out pixel 0 (the reference's running mean skips it)
-            if (blockIdx.x == 0 && n > 0) sum = __dsub_rn(sum, (double)fabsf(sr[0]));
-            part_store(buf + blockIdx.x, tag, bs, bv < 0.f ? (int)kNoPixel : bi, sum);
+            if (SUM && blockIdx.x == 0 && n > 0) sum = __dsub_rn(sum, (double)fabsf(sr[0]));
+            part_store<SUM>(buf + blockIdx.x, tag, bv < 0.f ? 0.f : sr[bi - p0], bv < 0.f ? (int)kNoPixel : bi, sum);
             // block 0 adds the previous component to the model here, off the
             // critical path (model updates keep the reference's order)
             if (model_idx >= 0) {
@@ -669,20 +706,12 @@ __global__ void __launch_bounds__(kPersistThreads, 1) k_clean_persistent(
         // minor cycle, reduces them in the same order and takes the same
         // decision
         if (tid < 32) {
-            const PBest w = wait_results(buf, nb, tag, bar, spin_limit);
+            const PBest w = wait_results<SUM>(buf, nb, tag, bar, spin_limit);
             const int fail = w.ok ? 0 : 1;
             bv = w.bv;
             bi = w.bi;
             bs = w.bs;
             sum = w.sum;
-#pragma unroll
-            for (int o = 16; o > 0; o >>= 1) {
-                const float v2 = __shfl_xor_sync(0xffffffffu, bv, o);
-                const int i2 = __shfl_xor_sync(0xffffffffu, bi, o);
-                const float s2 = __shfl_xor_sync(0xffffffffu, bs, o);
-                better3(bv, bi, bs, v2, i2, s2);
-                sum += __shfl_xor_sync(0xffffffffu, sum, o);
-            }
             if (tid == 0) {
                 if (fail) {
                     s_fail = 1;
@@ -697,8 +726,10 @@ __global__ void __launch_bounds__(kPersistThreads, 1) k_clean_persistent(
                         idx = 0;
                         sval = 0.f;
                     }
-                    const float avg = (g2 > 1) ? (float)(sum / (double)(g2 - 1)) : 0.f;
-                    const bool extracting_noise = (double)fabsf(curr_max) < noise * (double)avg * gain;  // :238
+                    // :238; without SUM (noise x gain < 0.5) it cannot hold: the mean of
+                    // |r| is at most the max
+                    const float avg = (SUM && g2 > 1) ? (float)(sum / (double)(g2 - 1)) : 0.f;
+                    const bool extracting_noise = SUM && (double)fabsf(curr_max) < noise * (double)avg * gain;
                     const bool weak_source =
                         count > 0 && (double)fabsf(curr_max) < (double)fabsf(first_z) * weak;  // :239
                     if (extracting_noise || weak_source) {
@@ -745,8 +776,8 @@ __global__ void __launch_bounds__(kPersistThreads, 1) k_clean_persistent(
 // the kernel ends with the error flag set (the host reads SDP_ERR_TIMEOUT).
 __global__ void k_wait_timeout_probe(PPart *parts, CleanBar *bar, long long spin_limit)
 {
-    if (threadIdx.x == 0) part_store(parts + blockIdx.x, part_tag(0), 1.f, (int)blockIdx.x, 1.0);
-    if (threadIdx.x < 32) wait_results(parts, (int)gridDim.x + 1, part_tag(0), bar, spin_limit);
+    if (threadIdx.x == 0) part_store<true>(parts + blockIdx.x, part_tag(0), 1.f, (int)blockIdx.x, 1.0);
+    if (threadIdx.x < 32) wait_results<true>(parts, (int)gridDim.x + 1, part_tag(0), bar, spin_limit);
 }
 
 static void persist_layout(int nb, size_t base, size_t *bar_off, size_t *parts_off, size_t *total)
@@ -819,7 +850,14 @@ int sdp::hogbom_launch(const sdp_clean_params *p, float *residual, const float *
         const bool stage = P <= 2 * kPersistThreads &&
                            2 * sizeof(float) * (size_t)P + 2048 <= (size_t)optin;  // 2 KB: the static arrays
         const size_t smem = sizeof(float) * (size_t)P * (stage ? 2 : 1);
-        auto fn = stage ? k_clean_persistent<true> : k_clean_persistent<false>;
+        const bool quad = (G & 3) == 0 && (P & 3) == 0;
+        // the noise test (|max| < noise x mean |r| x gain) cannot stop the
+        // loop when noise x gain < 0.5, since the mean of |r| is at most its
+        // max: the kernel then skips the sum of |r|
+        const bool sum = !(p->noise_factor * p->loop_gain < 0.5);
+        auto fn = stage  ? (sum ? k_clean_persistent<kPassStage, true> : k_clean_persistent<kPassStage, false>)
+                  : quad ? (sum ? k_clean_persistent<kPassQuad, true> : k_clean_persistent<kPassQuad, false>)
+                         : (sum ? k_clean_persistent<kPassScalar, true> : k_clean_persistent<kPassScalar, false>);
         SDP_CUDA_TRY(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
         int per_sm = 0;
         SDP_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, kPersistThreads, smem));

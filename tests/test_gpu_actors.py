@@ -291,14 +291,16 @@ def test_hogbom_large_bit_exact_vs_oracle(sdp, actors, oracle32, G):
     np.testing.assert_array_equal(m2, m1)
 
 
-@pytest.mark.parametrize("G,psf_offset", [(1024, 0), (2048, 1)])
+@pytest.mark.parametrize("G,psf_offset", [(1024, 0), (2048, 0), (2048, 1), (1500, 0), (1001, 0)])
 def test_hogbom_persistent_sidelobes_vs_oracle(sdp, device, oracle32, G, psf_offset):
     """Persistent CLEAN through the device entry point against the oracle,
     with a PSF whose sidelobes are nonzero everywhere (so every PSF sample of
     the window, the x-mirrored rows, the wrap into the next PSF row and the
     reads past the PSF's end all enter the residual), peaks up to the image
     edges: components, model and the final residual bit for bit.
-    psf_offset = 1 passes a PSF that starts 4 bytes into its allocation."""
+    psf_offset = 1 passes a PSF that starts 4 bytes into its allocation.
+    Pass variants: four pixels per thread and step (1024, 2048, 2048 with
+    the offset PSF, 1500), one pixel per step (1001)."""
     import torch
     dev = torch.device("cuda", 0)
     rng = np.random.default_rng(G + 7 * psf_offset)
@@ -325,6 +327,43 @@ def test_hogbom_persistent_sidelobes_vs_oracle(sdp, device, oracle32, G, psf_off
     torch.cuda.synchronize()
     n2 = int(c.item())
     assert n1 == n2 > 20
+    np.testing.assert_array_equal(s[:n2].cpu().numpy(), s1)
+    np.testing.assert_array_equal(m.cpu().numpy(), m1)
+    np.testing.assert_array_equal(r.cpu().numpy(), r1)
+
+
+@pytest.mark.parametrize("G", [1024, 1500])
+def test_hogbom_noise_stop_vs_oracle(sdp, device, oracle32, G):
+    """noise_factor x gain above 1, so the noise test (|max| < noise x mean
+    |r| x gain, deconvolution_run.c:238) can end the loop: a few sources on
+    noise, cleaned until only noise is left.  The persistent kernel then
+    carries the sum of |r| through every minor cycle; the stop, components,
+    model and residual must match the oracle."""
+    import torch
+    dev = torch.device("cuda", 0)
+    rng = np.random.default_rng(G + 3)
+    yy, xx = np.mgrid[0:G, 0:G]
+    psf = np.exp(-((xx - G // 2) ** 2 + (yy - G // 2) ** 2) / 8.0)
+    psf = (psf / psf.max()).astype(np.float32)
+    res = 0.01 * rng.standard_normal((G, G))
+    for _ in range(6):
+        x0, y0 = rng.integers(G // 4, 3 * G // 4, 2)
+        res += rng.uniform(0.5, 1.0) * np.roll(np.roll(psf, y0 - G // 2, 0), x0 - G // 2, 1)
+    res, psf = res.astype(np.float32).reshape(-1), psf.reshape(-1)
+    minor, gain, noise = 400, 0.1, 80.0
+    n1, s1, m1, r1 = oracle32.hogbom(G, minor, minor, res, psf, 1.0, 1e-5, loop_gain=gain, noise_factor=noise)
+    params = sdp.CleanParams(G, minor, minor, gain, noise, 0.0002, 1.0, 1e-5)
+    r = torch.from_numpy(res.copy()).to(dev)
+    psf_d = torch.from_numpy(psf).to(dev)
+    m = torch.zeros(G * G, dtype=torch.float32, device=dev)
+    s = torch.zeros((minor, 3), dtype=torch.float32, device=dev)
+    c = torch.zeros(1, dtype=torch.int32, device=dev)
+    ws = torch.empty(device.hogbom_workspace_bytes(G), dtype=torch.uint8, device=dev)
+    device.hogbom(params, r, psf_d, m, s, c, ws)
+    torch.cuda.synchronize()
+    n2 = int(c.item())
+    assert 10 < n1 < minor, n1  # the noise test ended the loop
+    assert n2 == n1
     np.testing.assert_array_equal(s[:n2].cpu().numpy(), s1)
     np.testing.assert_array_equal(m.cpu().numpy(), m1)
     np.testing.assert_array_equal(r.cpu().numpy(), r1)
