@@ -705,6 +705,13 @@ int sdp_blur_mse(int batch, int height, int width, const float *pred, const floa
  * r / s, sign(r) sqrt(|r| / s), psf, with s = max |r| written to scale_dev. */
 int sdp_unet_input_planes(int grid_size, const float *residual, const float *psf, float *planes, float *scale_dev,
                           void *stream);
+/* The same planes for the centred window x 0 .. window-1 of the image,
+ * offset (grid_size - window) / 2 in both axes (planes are window^2 each; s
+ * is the whole image's max |r|).  A network run on the window gives the
+ * full-image run's output wherever its receptive field stays inside the
+ * window; with the offset a multiple of 16 its pooling levels line up. */
+int sdp_unet_input_planes_window(int grid_size, int window, const float *residual, const float *psf, float *planes,
+                                 float *scale_dev, void *stream);
 /* Components from a proposal image: the largest values (signed_values = 0:
  * positive values; 1: largest |value|, either sign) at or above
  * rel_threshold x the maximum, at most max_count of them (whole histogram

@@ -599,23 +599,24 @@ __global__ void __launch_bounds__(kPersistThreads, 1) k_clean_persistent(
             // 16-byte shared access; window rows and PSF offsets once per
             // quad): quad q = tid + m * 1024 is pixels p0 + 4 q .. + 3, two
             // quads' PSF loads in flight together
+            // the argmax keeps the first quad holding the thread's max |r|
+            // (bq); its first pixel with that |r| is read back afterwards
             float4 *sr4 = reinterpret_cast<float4 *>(sr);
             const int nq = n >> 2;
             int qy = (p0 + 4 * tid) / G, qx = (p0 + 4 * tid) - qy * G;
+            int bq = 0;
             for (int qb = tid; qb < nq; qb += 2 * kPersistThreads) {
                 float4 w4[2];
                 float pv[2][4];
                 bool in[2][4];
-                int qi[2];
 #pragma unroll
                 for (int u = 0; u < 2; ++u) {
                     const int q = qb + u * kPersistThreads;
                     const bool live = q < nq;
-                    qi[u] = qy * G + qx;
                     w4[u] = live ? sr4[q] : make_float4(0.f, 0.f, 0.f, 0.f);
                     const bool iny = live && pending && (unsigned)(qy - y0) < (unsigned)wy;
                     const int ux = qx - x0;
-                    const int pi = qi[u] - 2 * qx + pofs;  // PSF index of the quad's pixel 0; pixel j: pi - j
+                    const int pi = qy * G - qx + pofs;  // PSF index of the quad's pixel 0; pixel j: pi - j
 #pragma unroll
                     for (int j = 0; j < 4; ++j) {
                         in[u][j] = iny && (unsigned)(ux + j) < (unsigned)wx && pi - j < g2;
@@ -630,24 +631,35 @@ __global__ void __launch_bounds__(kPersistThreads, 1) k_clean_persistent(
                 }
 #pragma unroll
                 for (int u = 0; u < 2; ++u) {
+                    const int q = qb + u * kPersistThreads;
                     float wv[4] = {w4[u].x, w4[u].y, w4[u].z, w4[u].w};
 #pragma unroll
                     for (int j = 0; j < 4; ++j)
                         if (in[u][j])
                             wv[j] = hogbom_update(wv[j], pv[u][j], scale, psf_max);
                     if (in[u][0] || in[u][1] || in[u][2] || in[u][3])
-                        sr4[qb + u * kPersistThreads] = make_float4(wv[0], wv[1], wv[2], wv[3]);
-#pragma unroll
-                    for (int j = 0; j < 4; ++j) {
-                        const float a = fabsf(wv[j]);
-                        if (a > bv) {  // pixels visited in increasing index: the first maximum wins
-                            bv = a;
-                            bi = qi[u] + j;
-                            bs = wv[j];
-                        }
-                        if constexpr (SUM) rsum += a;  // 0 for the padding past the slice
+                        sr4[q] = make_float4(wv[0], wv[1], wv[2], wv[3]);
+                    const float a0 = fabsf(wv[0]), a1 = fabsf(wv[1]), a2 = fabsf(wv[2]), a3 = fabsf(wv[3]);
+                    const float qm = fmaxf(fmaxf(a0, a1), fmaxf(a2, a3));
+                    if (q < nq && qm > bv) {  // quads visited in increasing index: the first maximum wins
+                        bv = qm;
+                        bq = q;
+                    }
+                    if constexpr (SUM) {
+                        rsum += a0;  // 0 for the padding past the slice
+                        rsum += a1;
+                        rsum += a2;
+                        rsum += a3;
                     }
                 }
+            }
+            if (bv >= 0.f) {  // the first pixel of the best quad with |r| = bv
+                const float4 wq = sr4[bq];
+                int j = 3;
+                if (fabsf(wq.z) == bv) j = 2;
+                if (fabsf(wq.y) == bv) j = 1;
+                if (fabsf(wq.x) == bv) j = 0;
+                bi = p0 + 4 * bq + j;
             }
         }
         for (int kb = tid; MODE == kPassScalar && kb < n; kb += kBatch * kPersistThreads) {

@@ -57,6 +57,27 @@ __global__ void k_planes(long long n, const float *__restrict__ r, const float *
     }
 }
 
+// The same planes for the centred window of side W of a G x G residual and
+// PSF (offset o = (G - W) / 2 in both axes); s is still the whole image's
+// max |r|.
+__global__ void k_planes_window(int G, int W, const float *__restrict__ r, const float *__restrict__ psf,
+                                const float *__restrict__ smax, float *__restrict__ planes)
+{
+    const float s = smax[0] > 0.f ? smax[0] : 1.f;
+    const float inv = 1.f / s;
+    const long long n = (long long)W * W;
+    const int o = (G - W) / 2;
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
+         i += (long long)gridDim.x * blockDim.x) {
+        const int y = (int)(i / W), x = (int)(i - (long long)y * W);
+        const long long src = (long long)(y + o) * G + (x + o);
+        const float v = r[src] * inv;
+        planes[i] = v;
+        planes[n + i] = copysignf(sqrtf(fabsf(v)), v);
+        planes[2 * n + i] = psf[src];
+    }
+}
+
 // Largest value (signed = 0: of the positive values; 1: of |x|).
 __device__ __forceinline__ float sel_key(float v, int signed_values) { return signed_values ? fabsf(v) : v; }
 
@@ -279,6 +300,22 @@ SDP_EXPORT int sdp_unet_input_planes(int grid_size, const float *residual, const
     k_absmax<<<blocks_for(n), kThreads, 0, st>>>(n, residual, scale_dev);
     SDP_LAUNCH_CHECK();
     k_planes<<<blocks_for(n), kThreads, 0, st>>>(n, residual, psf, scale_dev, planes);
+    SDP_LAUNCH_CHECK();
+    return SDP_OK;
+}
+
+SDP_EXPORT int sdp_unet_input_planes_window(int grid_size, int window, const float *residual, const float *psf,
+                                            float *planes, float *scale_dev, void *stream)
+{
+    SDP_CHECK_ARG(grid_size > 0 && window > 0 && window <= grid_size && (grid_size - window) % 2 == 0,
+                  "window %d must be positive, at most grid_size %d and of the same parity", window, grid_size);
+    SDP_CHECK_ARG(residual && psf && planes && scale_dev, "NULL argument");
+    cudaStream_t st = as_stream(stream);
+    const long long n = (long long)grid_size * grid_size, nw = (long long)window * window;
+    SDP_CUDA_TRY(cudaMemsetAsync(scale_dev, 0, sizeof(float), st));
+    k_absmax<<<blocks_for(n), kThreads, 0, st>>>(n, residual, scale_dev);
+    SDP_LAUNCH_CHECK();
+    k_planes_window<<<blocks_for(nw), kThreads, 0, st>>>(grid_size, window, residual, psf, scale_dev, planes);
     SDP_LAUNCH_CHECK();
     return SDP_OK;
 }

@@ -38,6 +38,7 @@ import synth
 WEIGHTS = Path(__file__).resolve().parent / "weights" / "unet_c4.npz"
 # network trained for the 512-antenna 40 km array's 16-channel continuum PSF
 WEIGHTS_C5 = Path(__file__).resolve().parent / "weights" / "unet_c5.npz"
+CROP_MARGIN = 64  # pixels of image kept around the proposal window for the network
 
 
 def _torch():
@@ -474,7 +475,8 @@ class Deconvolver:
     def __init__(self, img: Imaging, params: np.ndarray | None, num_minor: int = 200, loop_gain: float = 0.1,
                  max_components: int = 1024, rel_threshold: float = 0.05, alpha_max: float = 2.0,
                  min_gain: float = 0.05, give_up: int = 3, noise_factor: float = 1.5,
-                 weak_source_percent: float = 0.0002, signed: bool = True, window: float = 0.75):
+                 weak_source_percent: float = 0.0002, signed: bool = True, window: float = 0.75,
+                 crop: bool = True):
         torch = _torch()
         self.img, self.D = img, img.D
         G, dev, n = img.G, img.dev, img.n
@@ -482,11 +484,18 @@ class Deconvolver:
         self.rel_threshold, self.alpha_max, self.min_gain, self.give_up = rel_threshold, alpha_max, min_gain, give_up
         self.signed = signed
         self.border = int(round(G * (1.0 - window) / 2.0))
+        # the network runs on the centred crop that holds the proposal window
+        # plus a margin wider than its receptive field (radius < 64 pixels:
+        # 2 convolutions per level, 2 x 2 pooling, 4 levels), offset a
+        # multiple of 16 so the pooling levels line up with the full image's;
+        # its output inside the window is then the full image's
+        off = max(0, (self.border - CROP_MARGIN) // 16 * 16) if crop else 0
+        self.crop_off, self.W = off, G - 2 * off
         self.params = S.CleanParams(G, num_minor, num_minor, loop_gain, noise_factor, weak_source_percent, 1.0,
                                     img.layout.cell)
         self.net = None
         if params is not None:
-            self.net = S.UNet(img.D.lib, IN_CHANNELS, 1, G, G, training=False)
+            self.net = S.UNet(img.D.lib, IN_CHANNELS, 1, self.W, self.W, training=False)
             self.net.set_params(params)
         f32 = dict(dtype=torch.float32, device=dev)
         self.model_vis = torch.zeros((n, 2), **f32)
@@ -497,8 +506,8 @@ class Deconvolver:
         self.prop_img = torch.empty(G * G, **f32)
         self.clean_img = torch.empty(G * G, **f32)
         self.model_img = torch.zeros(G * G, **f32)
-        self.planes = torch.empty((1, IN_CHANNELS, G, G), **f32)
-        self.out = torch.empty((1, G, G), **f32)
+        self.planes = torch.empty((1, IN_CHANNELS, self.W, self.W), **f32)
+        self.out = torch.empty((1, self.W, self.W), **f32)
         self.scale = torch.empty(1, **f32)
         self.comps = torch.empty((max_components, 4), **f32)
         self.count = torch.zeros(1, dtype=torch.int32, device=dev)
@@ -528,14 +537,21 @@ class Deconvolver:
             D.dft_pixels(self.sources[:n], self.img.layout.cell, self.img.uvw_raw, self.model_vis, accumulate=True)
         return self._residual(measured), n
 
+    def _select(self) -> int:
+        """The network's proposal for the current residual: components in
+        self.comps, returns their number."""
+        D, G, W = self.D, self.img.G, self.W
+        D.unet_input_planes_window(G, W, self.residual, self.img.psf, self.planes, self.scale)
+        self.net.forward(self.planes, self.out)
+        D.zero_border(W, self.border - self.crop_off, self.out)
+        # a centred crop keeps (x - W/2) cell = (x + off - G/2) cell
+        D.select_components(W, self.img.layout.cell, self.out, self.scale, self.rel_threshold,
+                            self.max_components, self.comps, self.count, None, self.sel_ws, signed=self.signed)
+        return int(self.count.item())
+
     def _propose(self, rms) -> tuple[bool, float, float, int]:
         D, G = self.D, self.img.G
-        D.unet_input_planes(G, self.residual, self.img.psf, self.planes, self.scale)
-        self.net.forward(self.planes, self.out)
-        D.zero_border(G, self.border, self.out)
-        D.select_components(G, self.img.layout.cell, self.out, self.scale, self.rel_threshold,
-                            self.max_components, self.comps, self.count, None, self.sel_ws, signed=self.signed)
-        n = int(self.count.item())
+        n = self._select()
         if n == 0:
             return False, rms, 0.0, 0
         D.dft_pixels(self.comps[:n], self.img.layout.cell, self.img.uvw_raw, self.prop_vis)

@@ -794,6 +794,12 @@ class Device:
         check(self.lib.sdp_unet_input_planes(_i(grid_size), _dp(residual), _dp(psf), _dp(planes), _dp(scale),
                                              _stream(stream)), self.lib)
 
+    def unet_input_planes_window(self, grid_size, window, residual, psf, planes, scale, stream=None):
+        """The planes of the centred window^2 part of the image (offset
+        (grid_size - window) / 2); scale[0] = max |r| over the whole image."""
+        check(self.lib.sdp_unet_input_planes_window(_i(grid_size), _i(window), _dp(residual), _dp(psf), _dp(planes),
+                                                    _dp(scale), _stream(stream)), self.lib)
+
     def select_workspace(self):
         import torch
         b = _sz(0)

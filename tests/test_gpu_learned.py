@@ -114,3 +114,40 @@ def test_no_proposal_falls_back_to_hogbom(imaging, sdp):
         # gridder's float-atomic order magnified at the image edges
         assert abs(a.rms - b.rms) <= 1e-3 * a.rms and a.components == b.components
     dec.close()
+
+
+@pytest.mark.parametrize("grid", [1024, 2048])
+def test_network_on_window_crop_matches_full_image(device, grid):
+    """The network runs on the centred crop that holds the proposal window
+    plus 64 pixels (offset a multiple of 16): on the same residual image its
+    output inside the window, and so the components it proposes, are the
+    full-image run's bit for bit.  (The residual is imaged once: imaging
+    twice differs in the last bits, the gridder's float atomics.)"""
+    import torch
+    import learned as L
+    img = L.Imaging(device, L.spiral_layout(grid))
+    try:
+        comps = torch.from_numpy(L.SkySampler(img.G, img.layout.cell, 77).sample()).to(img.dev)
+        meas = torch.empty((img.n, 2), dtype=torch.float32, device=img.dev)
+        L.measured_vis(img, comps, meas, 1e-4, torch.Generator(device=img.dev).manual_seed(6))
+        full = L.Deconvolver(img, L.load_weights(), crop=False)
+        crop = L.Deconvolver(img, L.load_weights(), crop=True)
+        full._residual(meas)
+        crop.residual.copy_(full.residual)
+        G, W, off = img.G, crop.W, crop.crop_off
+        assert full.W == G and W < G and off % 16 == 0
+        got = []
+        for dec in (full, crop):
+            n = dec._select()
+            c = dec.comps[:n].cpu().numpy().copy()
+            got.append(c[np.lexsort((c[:, 2], c[:, 1], c[:, 0]))])
+        b = full.border
+        out_full = full.out.reshape(G, G)[b:G - b, b:G - b]
+        out_crop = crop.out.reshape(W, W)[b - off:W - (b - off), b - off:W - (b - off)]
+        assert torch.equal(out_full, out_crop)
+        assert len(got[0]) == len(got[1]) > 0
+        np.testing.assert_array_equal(got[1], got[0])
+        full.close()
+        crop.close()
+    finally:
+        img.close()
