@@ -50,6 +50,8 @@ struct sdp_visplan {
     int *dpoff = nullptr;         // plane offsets into the degridding table in use
     float2 *gk2 = nullptr;        // phase-major gridding kernels
     float2 *dk2 = nullptr;        // phase-major degridding kernels
+    float *dinv = nullptr;        // 1 / sqrt(sum |k|^2) of each fast-path tap box of the degridding set (nullptr: none)
+    int dinv_nc = 0;              // tap-box configurations per axis of dinv, 2 (OS + 1)
     void *arena = nullptr;
     bool owns_arena = true;
 };

@@ -28,9 +28,18 @@
 #include <algorithm>
 #include <vector>
 
+#include <cub/device/device_radix_sort.cuh>
+
 #include "internal.cuh"
 
 namespace sdp {
+
+// Order of the visibilities inside a uv tile: by w-plane, then by tap-box
+// origin (0), or by origin, then by plane (1, the default: longer runs of
+// one origin, which the warp-per-visibility kernels exploit).
+#ifndef SDP_SORT_CELL_MAJOR
+#define SDP_SORT_CELL_MAJOR 1
+#endif
 
 constexpr int kTile = 16;    // default uv tile side
 constexpr int kChunk = 1024;  // default visibilities per work item
@@ -67,6 +76,7 @@ struct PlanDev {
     int chunk;          // visibilities per work item (at most)
     const uint4 *geo;   // packed tap-box geometry in plan order (see fast_geometry)
     const int *perm;    // plan position -> original visibility index
+    const float *dinv;  // degridding normalisation of each fast-path tap box (nullptr: none), see k_dinv
 };
 
 // ----------------------------------------------------------------------------
@@ -218,11 +228,15 @@ __device__ __forceinline__ int geo_krow(int ky, int A, int pm, int OS, int shift
 
 // Packed tap-box geometry of a visibility for the warp-per-visibility kernels
 // (16 bytes):
-//   x: box origin in the tile (bits 0-7: column, 8-15: row), w-plane (16-31);
+//   x: box origin in the tile as a cell of the kernels' shared tiles
+//      (row * pitch + column, bits 0-15), w-plane (16-31);
 //   y: CN (0-15), CP (16-31): table offsets of the columns; tap column i < hs
 //      sits at CN - i * SC, column i >= hs at CP + (i - hs) * SC;
 //   z: RN (0-15), RP (16-31): the same for the rows with step RS;
-//   w: hs (0-3), kernel conjugated (4: w < 0), fast path (5).
+//   w: hs (0-3), kernel conjugated (4: w < 0), fast path (5), index of the
+//      tap box's degridding normalisation in the plan's dinv table (6-31:
+//      (plane NC + row configuration) NC + column configuration, NC =
+//      2 (OS + 1); a configuration is 2 ko + h of fast_kidx).
 // SC = 1, RS = hs + 1 in the phase-major layout (SC = OS, RS = (hs + 1) OS
 // otherwise): below the visibility the kernel index falls by OS per tap
 // (the phase stays, the block index falls by one), above it rises by OS.
@@ -233,7 +247,7 @@ __device__ __forceinline__ int geo_krow(int ky, int A, int pm, int OS, int shift
 // the general path that evaluates degridgrid.c's expressions tap by tap).
 template <typename T>
 __device__ __forceinline__ uint4 fast_geometry(const Rec<T> &r, int plane, int hs, int hsd, int G, int OS, int tile,
-                                               int tx, int ty, int pm, int shift)
+                                               int tx, int ty, int pm, int shift, int nc, int pitch)
 {
     uint4 g = make_uint4((uint32_t)plane << 16, 0u, 0u, (r.meta < 0) ? (1u << 4) : 0u);
     if (hs != hsd || hs < 1 || hs > 4) return g;
@@ -258,10 +272,12 @@ __device__ __forceinline__ uint4 fast_geometry(const Rec<T> &r, int plane, int h
     const int cn = geo_kcol(kx0, A, pm, OS, shift), cp = geo_kcol(kox, A, pm, OS, shift);
     const int rn = geo_krow(ky0, A, pm, OS, shift), rp = geo_krow(koy, A, pm, OS, shift);
     if (cn > 65535 || cp > 65535 || rn > 65535 || rp > 65535) return g;
-    g.x |= (uint32_t)tx0 | ((uint32_t)ty0 << 8);
+    if (ty0 * pitch + tx0 > 65535) return g;
+    g.x |= (uint32_t)(ty0 * pitch + tx0);
     g.y = (uint32_t)cn | ((uint32_t)cp << 16);
     g.z = (uint32_t)rn | ((uint32_t)rp << 16);
     g.w |= (uint32_t)hs | (1u << 5);
+    if (nc) g.w |= (uint32_t)((plane * nc + 2 * koy + hy) * nc + 2 * kox + hx) << 6;
     return g;
 }
 
@@ -270,7 +286,9 @@ __global__ void k_bin(const float3 *__restrict__ uvw, int n, int mode, int snap,
                       double w_scale, const int2 *__restrict__ sup, const int2 *__restrict__ dsup, int nk, int nkd,
                       long long ntot_g, long long ntot_d, int hs_max, int ntx, int nty, int tile,
                       Rec<T> *__restrict__ rec_tmp, uint4 *__restrict__ geo_tmp, int pm, int os_shift,
-                      int *__restrict__ keys, int *__restrict__ counts, int *__restrict__ flags)
+                      int nc, int pitch, int cbits, int pbits, unsigned long long *__restrict__ skeys,
+                      int *__restrict__ svals,
+                      int *__restrict__ counts, int *__restrict__ flags)
 {
     int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
@@ -297,7 +315,7 @@ __global__ void k_bin(const float3 *__restrict__ uvw, int n, int mode, int snap,
     }
     r.meta = plane | ((c.z < 0.0f) ? (int)0x80000000u : 0);
     r.idx = i;
-    int key = -1;
+    unsigned long long skey = ~0ull;  // unbinned: sorts after every binned visibility
     uint4 geo = make_uint4(0u, 0u, 0u, 0u);
     if (plane < 0 || plane >= nk || plane >= nkd) {
         atomicOr(flags, FLAG_PLANE);
@@ -315,29 +333,42 @@ __global__ void k_bin(const float3 *__restrict__ uvw, int n, int mode, int snap,
             int loy = (int)tceil(tsub(r.py, (T)hs)) + G / 2;
             int tx = min(max(floor_div(lox, tile), 0), ntx - 1);
             int ty = min(max(floor_div(loy, tile), 0), nty - 1);
-            key = (ty * ntx + tx) * nk + plane;
+            const int key = (ty * ntx + tx) * nk + plane;
             atomicAdd(&counts[key], 1);
-            if (mode == SDP_GRID_STD) geo = fast_geometry<T>(r, plane, hs, hsd, G, OS, tile, tx, ty, pm, os_shift);
+            // sort key: the (tile, plane) bin, then the tap-box origin in the
+            // tile, so that visibilities of one origin are adjacent
+            const int cx = min(max(lox - tx * tile, 0), tile - 1), cy = min(max(loy - ty * tile, 0), tile - 1);
+            const unsigned long long cell = (unsigned long long)(cy * tile + cx);
+#if SDP_SORT_CELL_MAJOR
+            skey = ((((unsigned long long)(ty * ntx + tx) << cbits) | cell) << pbits) | (unsigned long long)plane;
+#else
+            skey = ((unsigned long long)key << cbits) | cell;
+#endif
+            if (mode == SDP_GRID_STD) geo = fast_geometry<T>(r, plane, hs, hsd, G, OS, tile, tx, ty, pm, os_shift, nc, pitch);
         }
     }
     rec_tmp[i] = r;
     geo_tmp[i] = geo;
-    keys[i] = key;
+    skeys[i] = skey;
+    svals[i] = i;
 }
 
+// Plan order from the sorted visibility indices (perm): binned visibilities
+// occupy positions [0, offsets[nbins]), the rest are marked -1.
 template <typename T>
-__global__ void k_scatter(const Rec<T> *__restrict__ rec_tmp, const uint4 *__restrict__ geo_tmp,
-                          const int *__restrict__ keys, int n, const int *__restrict__ offsets, int *__restrict__ fill,
-                          Rec<T> *__restrict__ rec, uint4 *__restrict__ geo, int *__restrict__ perm)
+__global__ void k_gather_plan(const Rec<T> *__restrict__ rec_tmp, const uint4 *__restrict__ geo_tmp, int n,
+                              const int *__restrict__ n_binned, int *__restrict__ perm, Rec<T> *__restrict__ rec,
+                              uint4 *__restrict__ geo)
 {
-    int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= n) return;
-    int key = keys[i];
-    if (key < 0) return;
-    int pos = offsets[key] + atomicAdd(&fill[key], 1);
+    int pos = blockIdx.x * blockDim.x + threadIdx.x;
+    if (pos >= n) return;
+    if (pos >= *n_binned) {
+        perm[pos] = -1;
+        return;
+    }
+    const int i = perm[pos];
     rec[pos] = rec_tmp[i];
     geo[pos] = geo_tmp[i];
-    perm[pos] = i;
 }
 
 __global__ void k_item_counts(const int *__restrict__ offsets, int ntiles, int nk, int chunk,
@@ -886,7 +917,7 @@ __device__ __forceinline__ void fast_taps(const uint4 g, int c, int r, int lanec
     const int hs = (int)(g.w & 15u), A = hs + 1, n = 2 * hs;
     const int cn = (int)(g.y & 0xffffu), cp = (int)(g.y >> 16);
     const int rn = (int)(g.z & 0xffffu), rp = (int)(g.z >> 16);
-    ce = (int)((g.x >> 8) & 255u) * pitch + (int)(g.x & 255u) + lanecell;
+    ce = (int)(g.x & 0xffffu) + lanecell;
     const int sc = pm ? 1 : OS, rs = pm ? A : A * OS;
     const int colp = (c < hs) ? cn - c * sc : cp + (c - hs) * sc;
     const int r1 = r + 4;
@@ -920,6 +951,37 @@ __device__ __forceinline__ void reduce4x5(const float (&v)[kFastVB][5], float (&
     for (int o = 4; o > 0; o >>= 1)
 #pragma unroll
         for (int q = 0; q < 5; ++q) out[q] += __shfl_xor_sync(0xffffffffu, out[q], o);
+}
+
+// Reduces v[j][q] (j < 4 visibilities, q < 2 sums) over the warp; lanes
+// 8 j .. 8 j + 7 end with visibility j's two totals in s0, s1.
+__device__ __forceinline__ void reduce4x2(const float (&v)[kFastVB][2], float &s0, float &s1)
+{
+    const int lane = threadIdx.x & 31;
+    const bool b4 = (lane & 16) != 0, b3 = (lane & 8) != 0, b2 = (lane & 4) != 0;
+    float w[2][2];
+#pragma unroll
+    for (int jj = 0; jj < 2; ++jj)
+#pragma unroll
+        for (int q = 0; q < 2; ++q) {
+            const float keep = b4 ? v[2 + jj][q] : v[jj][q];
+            const float send = b4 ? v[jj][q] : v[2 + jj][q];
+            w[jj][q] = keep + __shfl_xor_sync(0xffffffffu, send, 16);
+        }
+    float u[2];
+#pragma unroll
+    for (int q = 0; q < 2; ++q) {
+        const float keep = b3 ? w[1][q] : w[0][q];
+        const float send = b3 ? w[0][q] : w[1][q];
+        u[q] = keep + __shfl_xor_sync(0xffffffffu, send, 8);
+    }
+    // lanes 8 j + 4 q .. 8 j + 4 q + 3: sum q of visibility j
+    float t = (b2 ? u[1] : u[0]) + __shfl_xor_sync(0xffffffffu, b2 ? u[0] : u[1], 4);
+    t += __shfl_xor_sync(0xffffffffu, t, 2);
+    t += __shfl_xor_sync(0xffffffffu, t, 1);
+    const float o = __shfl_xor_sync(0xffffffffu, t, 4);
+    s0 = b2 ? o : t;
+    s1 = b2 ? t : o;
 }
 
 // Bulk (TMA) staging of a work item's records: one thread arms an mbarrier
@@ -1031,6 +1093,10 @@ __device__ __forceinline__ bool fast_item(const PlanDev &Pin, const int4 it, Ite
 
     const int lanecell = r * pitch + c;
     const int pm = P.phase_major;
+    // half support 4: column c < 4 of a box reads CN - c, the others CP + c - 4
+    // (byte_perm picks the 16-bit field of the geometry word)
+    const unsigned csel = (c < 4) ? 0x4410u : 0x4432u;
+    const int cofs = (c < 4) ? -c : c - 4;
     for (int b = it.y + warp * kFastVB; b < it.z; b += NW * kFastVB) {
         const int nv = min(kFastVB, it.z - b);  // visibilities in this batch (warp-uniform)
         uint4 g[kFastVB];
@@ -1043,44 +1109,56 @@ __device__ __forceinline__ bool fast_item(const PlanDev &Pin, const int4 it, Ite
         // tap of the 8 x 8 box active (rows r below the visibility at RN - 5 r,
         // rows r + 4 above it at RP + 5 r; columns c < 4 at CN - c, the others
         // at CP + c - 4), packed FP32x2 arithmetic.
-        bool all4 = (nv == kFastVB) && pm;
+        bool all4 = (nv == kFastVB) && pm && P.dinv != nullptr;
 #pragma unroll
         for (int j = 0; j < kFastVB; ++j) all4 = all4 && (g[j].w & 0x2fu) == 0x24u;  // fast, hs = 4
         if (all4) {
             float2 q0[kFastVB], q1[kFastVB];
             int ce4[kFastVB];
             float2 gv4 = make_float2(0.f, 0.f);
+            float ie = 0.f;  // lanes 8 j ..: visibility j's normalisation entry, loaded ahead of its use
             if (kConv) {
-                float acc[kFastVB][5];
+                const unsigned wr = r == 0 ? g[0].w : r == 1 ? g[1].w : r == 2 ? g[2].w : g[3].w;
+                ie = __ldg(&P.dinv[wr >> 6]);
+            }
+            if (kConv) {
+                // per visibility the lane's share of the real and imaginary
+                // parts of sum m k (the kernel's imaginary part conjugated for
+                // w < 0, degridgrid.c:176-183); the normalisation comes from
+                // the plan's table
+                float acc[kFastVB][2];
+                float2 m0 = make_float2(0.f, 0.f), m1 = m0;
 #pragma unroll
                 for (int j = 0; j < kFastVB; ++j) {
                     const uint4 gj = g[j];
-                    const int colp = (c < 4) ? (int)(gj.y & 0xffffu) - c : (int)(gj.y >> 16) + c - 4;
+                    const int colp = (int)__byte_perm(gj.y, 0u, csel) + cofs;
                     const float2 *kp = P.dk + planes[gj.x >> 16].y + colp;
                     q0[j] = __ldg(kp + (int)(gj.z & 0xffffu) - 5 * r);
                     q1[j] = __ldg(kp + (int)(gj.z >> 16) + 5 * r);
-                    const int ce = (int)((gj.x >> 8) & 255u) * pitch + (int)(gj.x & 255u) + lanecell;
+                    const int ce = (int)(gj.x & 0xffffu) + lanecell;
                     ce4[j] = ce;
-                    const float2 m0 = mtile[ce], m1 = mtile[ce + 4 * pitch];
+                    // the plan orders a tile's visibilities by tap-box origin:
+                    // a visibility with its predecessor's origin reads the same
+                    // model cells
+                    if (j == 0 || ((gj.x ^ g[j - 1].x) & 0xffffu) != 0u) {
+                        m0 = mtile[ce];
+                        m1 = mtile[ce + 4 * pitch];
+                    }
+                    // a1 = (sum m.x kr, sum m.y kr), a2 = (sum m.x ki, sum m.y ki)
                     const float2 a1 = __ffma2_rn(m1, make_float2(q1[j].x, q1[j].x),
                                                  __fmul2_rn(m0, make_float2(q0[j].x, q0[j].x)));
                     const float2 a2 = __ffma2_rn(m1, make_float2(q1[j].y, q1[j].y),
                                                  __fmul2_rn(m0, make_float2(q0[j].y, q0[j].y)));
-                    const float2 nn = __ffma2_rn(q1[j], q1[j], __fmul2_rn(q0[j], q0[j]));
-                    acc[j][0] = a1.x;
-                    acc[j][1] = a1.y;
-                    acc[j][2] = a2.x;
-                    acc[j][3] = a2.y;
-                    acc[j][4] = nn.x + nn.y;
+                    const float cj = (gj.w & (1u << 4)) ? -1.f : 1.f;
+                    acc[j][0] = fmaf(-cj, a2.y, a1.x);
+                    acc[j][1] = fmaf(cj, a2.x, a1.y);
                 }
-                float tot[5];
-                reduce4x5(acc, tot);
-                const float conj = (pick4(g, r).w & (1u << 4)) ? -1.f : 1.f;  // lanes 8 j ..: visibility j
-                const float sx = fmaf(-conj, tot[3], tot[0]);
-                const float sy = fmaf(conj, tot[2], tot[1]);
-                const float cn = __fsqrt_rn(tot[4]);
-                const bool tiny = cn < 1e-5f;
-                const float inv = tiny ? 1e5f : __frcp_rn(cn);
+                float sx, sy;
+                reduce4x2(acc, sx, sy);
+                // normalisation (degridgrid.c:188-191; a negative entry marks
+                // sqrt(sum |k|^2) < 1e-5)
+                const bool tiny = ie < 0.f;
+                const float inv = fabsf(ie);
                 const float nx = sx * inv;
                 const float ny = tiny ? nx * inv : sy * inv;
                 const float2 value = make_float2(nx, ny);
@@ -1097,6 +1175,11 @@ __device__ __forceinline__ bool fast_item(const PlanDev &Pin, const int4 it, Ite
                 }
             }
             if (kGrids) {
+                // a run of visibilities with one tap-box origin accumulates in
+                // registers: one read and one write of the lane's two cells per
+                // run, in the same order of operations as cell by cell
+                float2 s0 = make_float2(0.f, 0.f), s1 = s0;
+                int run_ce = 0;
 #pragma unroll
                 for (int j = 0; j < kFastVB; ++j) {
                     const uint4 gj = g[j];
@@ -1116,24 +1199,32 @@ __device__ __forceinline__ bool fast_item(const PlanDev &Pin, const int4 it, Ite
                         ce = ce4[j];
                         ks = share_sign;
                     } else {
-                        const int colp = (c < 4) ? (int)(gj.y & 0xffffu) - c : (int)(gj.y >> 16) + c - 4;
+                        const int colp = (int)__byte_perm(gj.y, 0u, csel) + cofs;
                         const float2 *kp = P.gk + planes[gj.x >> 16].w + colp;
                         t0 = __ldg(kp + (int)(gj.z & 0xffffu) - 5 * r);
                         t1 = __ldg(kp + (int)(gj.z >> 16) + 5 * r);
-                        ce = (int)((gj.x >> 8) & 255u) * pitch + (int)(gj.x & 255u) + lanecell;
+                        ce = (int)(gj.x & 0xffffu) + lanecell;
                         ks = 1.f;
                     }
                     // vis * (kr + i conj ki): re = vr kr - (conj vi) ki, im = vi kr + (conj vr) ki
                     const float conj = (gj.w & (1u << 4)) ? -1.f : 1.f;
                     const float2 nc = make_float2(-conj * ks * gv.y, conj * ks * gv.x);
-                    float2 s0 = sub[ce];
+                    if (j == 0 || ((gj.x ^ g[j - 1].x) & 0xffffu) != 0u) {
+                        if (j > 0) {
+                            sub[run_ce] = s0;
+                            sub[run_ce + 4 * pitch] = s1;
+                            __syncwarp();
+                        }
+                        run_ce = ce;
+                        s0 = sub[ce];
+                        s1 = sub[ce + 4 * pitch];
+                    }
                     s0 = __ffma2_rn(nc, make_float2(t0.y, t0.y), __ffma2_rn(gv, make_float2(t0.x, t0.x), s0));
-                    sub[ce] = s0;
-                    float2 s1 = sub[ce + 4 * pitch];
                     s1 = __ffma2_rn(nc, make_float2(t1.y, t1.y), __ffma2_rn(gv, make_float2(t1.x, t1.x), s1));
-                    sub[ce + 4 * pitch] = s1;
-                    __syncwarp();
                 }
+                sub[run_ce] = s0;
+                sub[run_ce + 4 * pitch] = s1;
+                __syncwarp();
             }
             continue;
         }
@@ -1341,7 +1432,7 @@ __host__ __device__ __forceinline__ size_t fast_smem_bytes(int op, int nw, int S
 }
 
 template <typename T, int OP, int NW>
-__global__ void __launch_bounds__(32 * NW) k_vis_fast(PlanDev P, const float2 *__restrict__ vis_in,
+__global__ void __launch_bounds__(32 * NW, 20 / NW) k_vis_fast(PlanDev P, const float2 *__restrict__ vis_in,
                                                       const float2 *__restrict__ in_grid,
                                                       float2 *__restrict__ out_grid, float2 *__restrict__ pred_out,
                                                       float2 *__restrict__ delta_out,
@@ -1387,7 +1478,7 @@ __global__ void __launch_bounds__(32 * NW) k_vis_fast(PlanDev P, const float2 *_
 // persistent launch over the (channel, tile) queue; smem sized for the
 // largest channel (S_max rows of pitch_max, nk_max planes).
 template <typename T, int NW>
-__global__ void __launch_bounds__(32 * NW) k_vis_fast_batch(const PlanDev *__restrict__ plans,
+__global__ void __launch_bounds__(32 * NW, 20 / NW) k_vis_fast_batch(const PlanDev *__restrict__ plans,
                                                             const BatchIO *__restrict__ io,
                                                             const int4 *__restrict__ items, int n_items,
                                                             int *item_counter, int nk_max, int tile_f2,
@@ -1438,6 +1529,40 @@ __global__ void __launch_bounds__(32 * NW) k_vis_fast_batch(const PlanDev *__res
                                              sIO.measured))
             break;
     }
+}
+
+// Degridding normalisation of every fast-path tap box (degridgrid.c:145-191)
+// of a phase-major degridding set: entry (plane NC + cy) NC + cx, with
+// c = 2 ko + h per axis (fast_kidx), holds 1 / sqrt(sum of |k|^2 over the
+// 2 hs x 2 hs taps), summed row by row and column by column as the reference
+// does; -1e5 when sqrt(sum) < 1e-5 (the reference then divides by 1e-5 and
+// takes the imaginary part from the real one).  Planes outside the fast
+// path's half supports (1..4) get 0.
+__global__ void k_dinv(const float2 *__restrict__ dk2, const int *__restrict__ dpoff, const int2 *__restrict__ ds,
+                       int nk, int OS, int shift, int nc, float *__restrict__ dinv)
+{
+    const int e = blockIdx.x * blockDim.x + threadIdx.x;
+    if (e >= nk * nc * nc) return;
+    const int plane = e / (nc * nc), cy = (e / nc) % nc, cx = e % nc;
+    const int hs = ds[plane].x;
+    float v = 0.f;
+    if (hs >= 1 && hs <= 4) {
+        const int A = hs + 1;
+        const int kox = cx >> 1, hx = cx & 1, koy = cy >> 1, hy = cy & 1;
+        const float2 *k = dk2 + dpoff[plane];
+        float norm = 0.f;
+        for (int i = 0; i < 2 * hs; ++i) {
+            const int ky = fast_kidx(i, hs, OS, koy, hy);
+            for (int j = 0; j < 2 * hs; ++j) {
+                const int kx = fast_kidx(j, hs, OS, kox, hx);
+                const float2 t = k[geo_kcol(kx, A, 1, OS, shift) + geo_krow(ky, A, 1, OS, shift)];
+                norm = __fadd_rn(norm, __fadd_rn(__fmul_rn(t.x, t.x), __fmul_rn(t.y, t.y)));
+            }
+        }
+        const float cn = __fsqrt_rn(norm);
+        v = cn < 1e-5f ? -1e5f : __frcp_rn(cn);
+    }
+    dinv[e] = v;
 }
 
 // Phase-major copy of a kernel set (see kcol / krow).  One thread per output
@@ -1573,6 +1698,7 @@ static PlanDev plan_dev(const sdp_visplan *p)
     d.chunk = p->chunk;
     d.geo = p->geo;
     d.perm = p->perm;
+    d.dinv = p->dinv;
     return d;
 }
 
@@ -1595,6 +1721,57 @@ static int check_kernels(const sdp_wkernels *k, const char *what)
     return SDP_OK;
 }
 
+// Bits of the plan's sort key (k_bin): cbits for the tap-box origin in the
+// tile, pbits for the plane (cell-major order only), end_bit in all.  The
+// bin field is one bit wider than the largest bin needs, so the all-ones key
+// of an unbinned visibility sorts after every binned one.
+static int bit_length(unsigned long long x)
+{
+    int b = 0;
+    while (b < 64 && (x >> b) != 0ull) ++b;
+    return b;
+}
+
+static void plan_sort_bits(const sdp_visplan *p, int *cbits, int *pbits, int *end_bit)
+{
+    *cbits = bit_length((unsigned long long)p->tile * p->tile - 1);
+#if SDP_SORT_CELL_MAJOR
+    *pbits = bit_length((unsigned long long)p->nk - 1);
+    *end_bit = bit_length((unsigned long long)p->ntiles) + *cbits + *pbits;
+#else
+    *pbits = 0;
+    *end_bit = bit_length((unsigned long long)p->nbins) + *cbits;
+#endif
+}
+
+// Temporary storage of the radix sort of the plan build (the keys and
+// values ping-pong between arena regions that are free at that point).
+static size_t plan_sort_temp_bytes(const sdp_visplan *p)
+{
+    if (p->n <= 0) return 0;
+    int cbits, pbits, end_bit;
+    plan_sort_bits(p, &cbits, &pbits, &end_bit);
+    cub::DoubleBuffer<unsigned long long> k(nullptr, nullptr);
+    cub::DoubleBuffer<int> v(nullptr, nullptr);
+    size_t bytes = 0;
+    if (cub::DeviceRadixSort::SortPairs(nullptr, bytes, k, v, p->n, 0, end_bit) != cudaSuccess) {
+        (void)cudaGetLastError();
+        // no device to ask: a bound well above what the sort needs (its
+        // per-tile histograms and look-back state)
+        bytes = ((size_t)64 << 20) + (size_t)p->n;
+    }
+    return bytes;
+}
+
+// Entries of the degridding normalisation table (0: not built).  The fast
+// path's packed geometry has 26 bits for the entry index.
+static size_t plan_dinv_entries(const sdp_visplan *p)
+{
+    if (!p->phase_major || p->dinv_nc <= 0) return 0;
+    const size_t e = (size_t)p->dk.num_kernels * p->dinv_nc * p->dinv_nc;
+    return e < ((size_t)1 << 26) ? e : 0;
+}
+
 // Arena layout of a plan (offsets in bytes).
 static void plan_layout(const sdp_visplan *p, size_t *off, size_t *total)
 {
@@ -1605,7 +1782,7 @@ static void plan_layout(const sdp_visplan *p, size_t *off, size_t *total)
     off[0] = o; o = align_up(o + rb * (size_t)std::max(n, 1), 256);                       // rec
     off[1] = o; o = align_up(o + rb * (size_t)std::max(n, 1), 256);                       // rec_tmp
     off[2] = o; o = align_up(o + sizeof(int) * (size_t)std::max(n, 1), 256);              // perm
-    off[3] = o; o = align_up(o + sizeof(int) * (size_t)std::max(n, 1), 256);              // keys
+    off[3] = o; o = align_up(o + sizeof(int) * (size_t)std::max(n, 1), 256);              // sort values
     off[4] = o; o = align_up(o + sizeof(int) * ((size_t)p->nbins + 1), 256);              // counts / fill
     off[5] = o; o = align_up(o + sizeof(int) * ((size_t)p->nbins + 1), 256);              // offsets
     off[6] = o; o = align_up(o + sizeof(int) * ((size_t)p->ntiles + 1), 256);             // item counts
@@ -1621,6 +1798,8 @@ static void plan_layout(const sdp_visplan *p, size_t *off, size_t *total)
     off[15] = o; o = align_up(o + (p->phase_major ? sizeof(float2) * per * p->dk.num_kernels : 0), 256);  // dk2
     off[16] = o; o = align_up(o + sizeof(uint4) * (size_t)std::max(n, 1), 256);          // geo
     off[17] = o; o = align_up(o + sizeof(uint4) * (size_t)std::max(n, 1), 256);          // geo_tmp
+    off[18] = o; o = align_up(o + plan_sort_temp_bytes(p), 256);                           // sort temp
+    off[19] = o; o = align_up(o + sizeof(float) * plan_dinv_entries(p), 256);              // dinv
     *total = o;
 }
 
@@ -1662,12 +1841,13 @@ int visplan_setup(sdp_visplan *p, const sdp_geometry *geom, const sdp_wkernels *
     p->pitch = p->S + ((8 - p->S % 16) + 16) % 16;
     const int os = geom->oversampling;
     p->phase_major = (os & (os - 1)) == 0 ? 1 : 0;
+    p->dinv_nc = 2 * (os + 1);
     return SDP_OK;
 }
 
 size_t visplan_arena_bytes(const sdp_visplan *p)
 {
-    size_t off[18], total;
+    size_t off[20], total;
     plan_layout(p, off, &total);
     return total;
 }
@@ -1709,6 +1889,12 @@ int visplan_kernels(sdp_visplan *p, cudaStream_t st)
             reinterpret_cast<const int2 *>(p->gk.supports), reinterpret_cast<const int2 *>(p->dk.supports), p->gpoff,
             p->dpoff, p->gk2, p->dk2, related, nk, os, per, p->kshare);
         SDP_LAUNCH_CHECK();
+        if (p->dinv) {
+            const int ne = (int)plan_dinv_entries(p);
+            k_dinv<<<(ne + 255) / 256, 256, 0, st>>>(p->dk2, p->dpoff, reinterpret_cast<const int2 *>(p->dk.supports),
+                                                     p->dk.num_kernels, os, os_shift, p->dinv_nc, p->dinv);
+            SDP_LAUNCH_CHECK();
+        }
     }
 
     return SDP_OK;
@@ -1716,14 +1902,14 @@ int visplan_kernels(sdp_visplan *p, cudaStream_t st)
 
 int visplan_build(sdp_visplan *p, void *arena, const float3 *uvw, cudaStream_t st)
 {
-    size_t off[18], total;
+    size_t off[20], total;
     plan_layout(p, off, &total);
     char *a = static_cast<char *>(arena);
     p->arena = arena;
     p->rec = a + off[0];
     void *rec_tmp = a + off[1];
     p->perm = reinterpret_cast<int *>(a + off[2]);
-    int *keys = reinterpret_cast<int *>(a + off[3]);
+    int *svals = reinterpret_cast<int *>(a + off[3]);
     int *counts = reinterpret_cast<int *>(a + off[4]);
     int *offsets = reinterpret_cast<int *>(a + off[5]);
     int *item_counts = reinterpret_cast<int *>(a + off[6]);
@@ -1742,6 +1928,14 @@ int visplan_build(sdp_visplan *p, void *arena, const float3 *uvw, cudaStream_t s
     p->dk2 = reinterpret_cast<float2 *>(a + off[15]);
     p->geo = reinterpret_cast<uint4 *>(a + off[16]);
     uint4 *geo_tmp = reinterpret_cast<uint4 *>(a + off[17]);
+    void *sort_temp = a + off[18];
+    p->dinv = plan_dinv_entries(p) ? reinterpret_cast<float *>(a + off[19]) : nullptr;
+    // sort keys: both buffers in the geo region (16 bytes per visibility),
+    // written by the gather only after the sort
+    unsigned long long *skeys0 = reinterpret_cast<unsigned long long *>(p->geo);
+    unsigned long long *skeys1 = skeys0 + std::max(p->n, 1);
+    int cbits, pbits, end_bit;
+    plan_sort_bits(p, &cbits, &pbits, &end_bit);
     int os_shift = 0;
     while ((1 << os_shift) < p->geom.oversampling) ++os_shift;
     const int n = p->n;
@@ -1757,28 +1951,38 @@ int visplan_build(sdp_visplan *p, void *arena, const float3 *uvw, cudaStream_t s
                 uvw, n, p->mode, p->snap, p->geom.grid_size, p->geom.oversampling, p->geom.uv_scale, p->geom.w_scale,
                 gs, ds, p->gk.num_kernels, p->dk.num_kernels, (long long)p->gk.total_samples,
                 (long long)p->dk.total_samples, p->hs_max, p->ntx, p->nty, p->tile, static_cast<Rec<double> *>(rec_tmp),
-                geo_tmp, p->phase_major, os_shift, keys, counts, p->flags);
+                geo_tmp, p->phase_major, os_shift, p->dinv ? p->dinv_nc : 0, p->pitch, cbits, pbits, skeys0, svals, counts,
+                p->flags);
         } else {
             k_bin<float><<<(n + 255) / 256, 256, 0, st>>>(
                 uvw, n, p->mode, p->snap, p->geom.grid_size, p->geom.oversampling, p->geom.uv_scale, p->geom.w_scale,
                 gs, ds, p->gk.num_kernels, p->dk.num_kernels, (long long)p->gk.total_samples,
                 (long long)p->dk.total_samples, p->hs_max, p->ntx, p->nty, p->tile, static_cast<Rec<float> *>(rec_tmp),
-                geo_tmp, p->phase_major, os_shift, keys, counts, p->flags);
+                geo_tmp, p->phase_major, os_shift, p->dinv ? p->dinv_nc : 0, p->pitch, cbits, pbits, skeys0, svals, counts,
+                p->flags);
         }
         SDP_LAUNCH_CHECK();
     }
     SDP_TRY(exclusive_scan(counts, offsets, p->nbins, scan_scratch, st));
-    SDP_CUDA_TRY(cudaMemsetAsync(counts, 0, sizeof(int) * ((size_t)p->nbins + 1), st));
-    if (n > 0) SDP_CUDA_TRY(cudaMemsetAsync(p->perm, 0xff, sizeof(int) * (size_t)n, st));  // unbinned slots: -1
     if (n > 0) {
+        // visibilities in (tile, plane, tap-box origin) order: a stable radix
+        // sort of the keys with the original indices (the result lands in
+        // perm); then records and geometry gathered into plan order
+        cub::DoubleBuffer<unsigned long long> dk(skeys0, skeys1);
+        cub::DoubleBuffer<int> dv(svals, p->perm);
+        size_t temp_bytes = total - off[18];
+        SDP_CUDA_TRY(cub::DeviceRadixSort::SortPairs(sort_temp, temp_bytes, dk, dv, n, 0, end_bit, st));
+        if (dv.Current() != p->perm)
+            SDP_CUDA_TRY(cudaMemcpyAsync(p->perm, dv.Current(), sizeof(int) * (size_t)n, cudaMemcpyDeviceToDevice, st));
+        const int *n_binned = offsets + p->nbins;
         if (p->coord_f64)
-            k_scatter<double><<<(n + 255) / 256, 256, 0, st>>>(static_cast<const Rec<double> *>(rec_tmp), geo_tmp,
-                                                               keys, n, offsets, counts,
-                                                               static_cast<Rec<double> *>(p->rec), p->geo, p->perm);
+            k_gather_plan<double><<<(n + 255) / 256, 256, 0, st>>>(static_cast<const Rec<double> *>(rec_tmp), geo_tmp,
+                                                                   n, n_binned, p->perm,
+                                                                   static_cast<Rec<double> *>(p->rec), p->geo);
         else
-            k_scatter<float><<<(n + 255) / 256, 256, 0, st>>>(static_cast<const Rec<float> *>(rec_tmp), geo_tmp, keys,
-                                                              n, offsets, counts, static_cast<Rec<float> *>(p->rec),
-                                                              p->geo, p->perm);
+            k_gather_plan<float><<<(n + 255) / 256, 256, 0, st>>>(static_cast<const Rec<float> *>(rec_tmp), geo_tmp,
+                                                                  n, n_binned, p->perm,
+                                                                  static_cast<Rec<float> *>(p->rec), p->geo);
         SDP_LAUNCH_CHECK();
     }
     k_item_counts<<<(p->ntiles + 255) / 256, 256, 0, st>>>(offsets, p->ntiles, p->nk, p->chunk, item_counts);
