@@ -77,6 +77,7 @@ struct PlanDev {
     const uint4 *geo;   // packed tap-box geometry in plan order (see fast_geometry)
     const int *perm;    // plan position -> original visibility index
     const float *dinv;  // degridding normalisation of each fast-path tap box (nullptr: none), see k_dinv
+    const uint4 *gbase; // four-quadrant table bases of each fast visibility in plan order (nullptr: none)
 };
 
 // ----------------------------------------------------------------------------
@@ -234,7 +235,7 @@ __device__ __forceinline__ int geo_krow(int ky, int A, int pm, int OS, int shift
 //      sits at CN - i * SC, column i >= hs at CP + (i - hs) * SC;
 //   z: RN (0-15), RP (16-31): the same for the rows with step RS;
 //   w: hs (0-3), kernel conjugated (4: w < 0), fast path (5), index of the
-//      tap box's degridding normalisation in the plan's dinv table (6-31:
+//      tap box's degridding normalisation in the plan's dinv table (7-31:
 //      (plane NC + row configuration) NC + column configuration, NC =
 //      2 (OS + 1); a configuration is 2 ko + h of fast_kidx).
 // SC = 1, RS = hs + 1 in the phase-major layout (SC = OS, RS = (hs + 1) OS
@@ -277,7 +278,7 @@ __device__ __forceinline__ uint4 fast_geometry(const Rec<T> &r, int plane, int h
     g.y = (uint32_t)cn | ((uint32_t)cp << 16);
     g.z = (uint32_t)rn | ((uint32_t)rp << 16);
     g.w |= (uint32_t)hs | (1u << 5);
-    if (nc) g.w |= (uint32_t)((plane * nc + 2 * koy + hy) * nc + 2 * kox + hx) << 6;
+    if (nc) g.w |= (uint32_t)((plane * nc + 2 * koy + hy) * nc + 2 * kox + hx) << 7;
     return g;
 }
 
@@ -355,10 +356,14 @@ __global__ void k_bin(const float3 *__restrict__ uvw, int n, int mode, int snap,
 
 // Plan order from the sorted visibility indices (perm): binned visibilities
 // occupy positions [0, offsets[nbins]), the rest are marked -1.
+// With gbase, also each fast visibility's four tap-quadrant bases in the
+// degridding table (the conjugated copy for w < 0): quadrant (columns below
+// or above, rows below or above) = plane offset + CN or CP + RN or RP.
 template <typename T>
 __global__ void k_gather_plan(const Rec<T> *__restrict__ rec_tmp, const uint4 *__restrict__ geo_tmp, int n,
                               const int *__restrict__ n_binned, int *__restrict__ perm, Rec<T> *__restrict__ rec,
-                              uint4 *__restrict__ geo)
+                              uint4 *__restrict__ geo, uint4 *__restrict__ gbase, const int *__restrict__ dpoff,
+                              int conj_off)
 {
     int pos = blockIdx.x * blockDim.x + threadIdx.x;
     if (pos >= n) return;
@@ -368,7 +373,19 @@ __global__ void k_gather_plan(const Rec<T> *__restrict__ rec_tmp, const uint4 *_
     }
     const int i = perm[pos];
     rec[pos] = rec_tmp[i];
-    geo[pos] = geo_tmp[i];
+    const uint4 g = geo_tmp[i];
+    geo[pos] = g;
+    if (gbase) {
+        uint4 q = make_uint4(0u, 0u, 0u, 0u);
+        if (g.w & (1u << 5)) {
+            const int o = dpoff[g.x >> 16] + ((g.w & (1u << 4)) ? conj_off : 0);
+            const int cn = (int)(g.y & 0xffffu), cp = (int)(g.y >> 16);
+            const int rn = (int)(g.z & 0xffffu), rp = (int)(g.z >> 16);
+            q = make_uint4((uint32_t)(o + cn + rn), (uint32_t)(o + cp + rn), (uint32_t)(o + cn + rp),
+                           (uint32_t)(o + cp + rp));
+        }
+        gbase[pos] = q;
+    }
 }
 
 __global__ void k_item_counts(const int *__restrict__ offsets, int ntiles, int nk, int chunk,
@@ -1026,6 +1043,7 @@ __device__ __forceinline__ bool stage_wait(uint32_t bar, uint32_t parity)
 // mbarrier's phase.
 struct ItemStage {
     uint4 *geo;         // chunk records
+    uint4 *gb;          // chunk quadrant bases (plans with gbase)
     float2 *meas;       // chunk + 2 values (from the even index at or below the item's first)
     uint64_t *bar;
     uint32_t phase;     // parity of the next completion
@@ -1064,8 +1082,10 @@ __device__ __forceinline__ bool fast_item(const PlanDev &Pin, const int4 it, Ite
         asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
         const uint32_t gbytes = (uint32_t)(it.z - it.y) * 16u;
         const uint32_t mbytes = (OP == OP_CYCLE_CONV) ? (uint32_t)(((it.z + 1) & ~1) - m0) * 8u : 0u;
-        stage_arm(bar, gbytes + mbytes);
+        const uint32_t bbytes = (kConv && P.gbase) ? gbytes : 0u;
+        stage_arm(bar, gbytes + bbytes + mbytes);
         stage_copy((uint32_t)__cvta_generic_to_shared(stg.geo), P.geo + it.y, gbytes, bar);
+        if (bbytes) stage_copy((uint32_t)__cvta_generic_to_shared(stg.gb), P.gbase + it.y, bbytes, bar);
         if (OP == OP_CYCLE_CONV) stage_copy((uint32_t)__cvta_generic_to_shared(stg.meas), measured + m0, mbytes, bar);
     }
     if (kConv) {
@@ -1090,13 +1110,27 @@ __device__ __forceinline__ bool fast_item(const PlanDev &Pin, const int4 it, Ite
     if (*stg.fail) return false;
     const uint4 *sgeo = stg.geo - it.y;   // indexed by plan position
     const float2 *smeas = stg.meas - m0;
+    // four-visibility path (half support 4): lane (r, c) reads the quadrant
+    // bases of its two taps (columns c < 4 below the visibility, rows r below
+    // and r + 4 above) and its visibility r's geometry word w directly from
+    // shared memory; the lane's offsets within the quadrants fold into its
+    // table pointers
+    const int cq = (c < 4) ? 0 : 1;
+    const unsigned *sgb0 = reinterpret_cast<const unsigned *>(stg.gb - it.y) + cq;      // rows below
+    const unsigned *sgb1 = reinterpret_cast<const unsigned *>(stg.gb - it.y) + 2 + cq;  // rows above
+    const unsigned *sgw = reinterpret_cast<const unsigned *>(sgeo) + 3;
+    const int cofs4 = (c < 4) ? -c : c - 4;
+    const float2 *dk_l0 = reinterpret_cast<const float2 *>(reinterpret_cast<uintptr_t>(P.dk) +
+                                                           (intptr_t)(cofs4 - 5 * r) * (intptr_t)sizeof(float2));
+    const float2 *dk_l1 = reinterpret_cast<const float2 *>(reinterpret_cast<uintptr_t>(P.dk) +
+                                                           (intptr_t)(cofs4 + 5 * r) * (intptr_t)sizeof(float2));
 
     const int lanecell = r * pitch + c;
     const int pm = P.phase_major;
     // half support 4: column c < 4 of a box reads CN - c, the others CP + c - 4
     // (byte_perm picks the 16-bit field of the geometry word)
     const unsigned csel = (c < 4) ? 0x4410u : 0x4432u;
-    const int cofs = (c < 4) ? -c : c - 4;
+    const int cofs = cofs4;
     for (int b = it.y + warp * kFastVB; b < it.z; b += NW * kFastVB) {
         const int nv = min(kFastVB, it.z - b);  // visibilities in this batch (warp-uniform)
         uint4 g[kFastVB];
@@ -1109,7 +1143,7 @@ __device__ __forceinline__ bool fast_item(const PlanDev &Pin, const int4 it, Ite
         // tap of the 8 x 8 box active (rows r below the visibility at RN - 5 r,
         // rows r + 4 above it at RP + 5 r; columns c < 4 at CN - c, the others
         // at CP + c - 4), packed FP32x2 arithmetic.
-        bool all4 = (nv == kFastVB) && pm && P.dinv != nullptr;
+        bool all4 = (nv == kFastVB) && (kConv ? P.gbase != nullptr : pm != 0);
 #pragma unroll
         for (int j = 0; j < kFastVB; ++j) all4 = all4 && (g[j].w & 0x2fu) == 0x24u;  // fast, hs = 4
         if (all4) {
@@ -1117,30 +1151,24 @@ __device__ __forceinline__ bool fast_item(const PlanDev &Pin, const int4 it, Ite
             int ce4[kFastVB];
             float2 gv4 = make_float2(0.f, 0.f);
             float ie = 0.f;  // lanes 8 j ..: visibility j's normalisation entry, loaded ahead of its use
-            if (kConv) {
-                const unsigned wr = r == 0 ? g[0].w : r == 1 ? g[1].w : r == 2 ? g[2].w : g[3].w;
-                ie = __ldg(&P.dinv[wr >> 6]);
-            }
+            if (kConv) ie = __ldg(&P.dinv[sgw[4 * (b + r)] >> 7]);
             if (kConv) {
                 // per visibility the lane's share of the real and imaginary
-                // parts of sum m k (the kernel's imaginary part conjugated for
-                // w < 0, degridgrid.c:176-183); the normalisation comes from
-                // the plan's table
+                // parts of sum m k; the samples come from the plan's
+                // conjugated copy for w < 0 (degridgrid.c:176-183), the
+                // normalisation from its table
                 float acc[kFastVB][2];
                 float2 m0 = make_float2(0.f, 0.f), m1 = m0;
 #pragma unroll
                 for (int j = 0; j < kFastVB; ++j) {
-                    const uint4 gj = g[j];
-                    const int colp = (int)__byte_perm(gj.y, 0u, csel) + cofs;
-                    const float2 *kp = P.dk + planes[gj.x >> 16].y + colp;
-                    q0[j] = __ldg(kp + (int)(gj.z & 0xffffu) - 5 * r);
-                    q1[j] = __ldg(kp + (int)(gj.z >> 16) + 5 * r);
-                    const int ce = (int)(gj.x & 0xffffu) + lanecell;
+                    q0[j] = __ldg(dk_l0 + sgb0[4 * (b + j)]);
+                    q1[j] = __ldg(dk_l1 + sgb1[4 * (b + j)]);
+                    const int ce = (int)(g[j].x & 0xffffu) + lanecell;
                     ce4[j] = ce;
                     // the plan orders a tile's visibilities by tap-box origin:
                     // a visibility with its predecessor's origin reads the same
                     // model cells
-                    if (j == 0 || ((gj.x ^ g[j - 1].x) & 0xffffu) != 0u) {
+                    if (j == 0 || ce != ce4[j > 0 ? j - 1 : 0]) {
                         m0 = mtile[ce];
                         m1 = mtile[ce + 4 * pitch];
                     }
@@ -1149,9 +1177,8 @@ __device__ __forceinline__ bool fast_item(const PlanDev &Pin, const int4 it, Ite
                                                  __fmul2_rn(m0, make_float2(q0[j].x, q0[j].x)));
                     const float2 a2 = __ffma2_rn(m1, make_float2(q1[j].y, q1[j].y),
                                                  __fmul2_rn(m0, make_float2(q0[j].y, q0[j].y)));
-                    const float cj = (gj.w & (1u << 4)) ? -1.f : 1.f;
-                    acc[j][0] = fmaf(-cj, a2.y, a1.x);
-                    acc[j][1] = fmaf(cj, a2.x, a1.y);
+                    acc[j][0] = a1.x - a2.y;
+                    acc[j][1] = a1.y + a2.x;
                 }
                 float sx, sy;
                 reduce4x2(acc, sx, sy);
@@ -1192,23 +1219,25 @@ __device__ __forceinline__ bool fast_item(const PlanDev &Pin, const int4 it, Ite
                     }
                     float2 t0, t1;
                     int ce;
-                    float ks;
+                    float2 nc;
                     if (kConv && share) {
+                        // the degridding samples (conjugated for w < 0) with the
+                        // gridding set's sign of the imaginary part:
+                        // vis * (kr + i ks ki) = (vr kr - ks vi ki, vi kr + ks vr ki)
                         t0 = q0[j];
                         t1 = q1[j];
                         ce = ce4[j];
-                        ks = share_sign;
+                        nc = make_float2(-share_sign * gv.y, share_sign * gv.x);
                     } else {
                         const int colp = (int)__byte_perm(gj.y, 0u, csel) + cofs;
                         const float2 *kp = P.gk + planes[gj.x >> 16].w + colp;
                         t0 = __ldg(kp + (int)(gj.z & 0xffffu) - 5 * r);
                         t1 = __ldg(kp + (int)(gj.z >> 16) + 5 * r);
                         ce = (int)(gj.x & 0xffffu) + lanecell;
-                        ks = 1.f;
+                        // vis * (kr + i conj ki): re = vr kr - (conj vi) ki, im = vi kr + (conj vr) ki
+                        const float conj = (gj.w & (1u << 4)) ? -1.f : 1.f;
+                        nc = make_float2(-conj * gv.y, conj * gv.x);
                     }
-                    // vis * (kr + i conj ki): re = vr kr - (conj vi) ki, im = vi kr + (conj vr) ki
-                    const float conj = (gj.w & (1u << 4)) ? -1.f : 1.f;
-                    const float2 nc = make_float2(-conj * ks * gv.y, conj * ks * gv.x);
                     if (j == 0 || ((gj.x ^ g[j - 1].x) & 0xffffu) != 0u) {
                         if (j > 0) {
                             sub[run_ce] = s0;
@@ -1410,9 +1439,9 @@ __device__ __forceinline__ bool fast_item(const PlanDev &Pin, const int4 it, Ite
 }
 
 // Shared-memory layout of the warp-per-visibility kernels: the staged
-// records of one work item (chunk 16-byte records, chunk + 2 measured
-// values), per-plane constants (nk int4), then the model tile and the NW
-// subgrids.
+// records of one work item (chunk 16-byte geometry records, chunk 16-byte
+// quadrant bases, chunk + 2 measured values), per-plane constants (nk int4),
+// then the model tile and the NW subgrids.
 // Shared memory of a block on sm_100 (opt-in limit) and an upper bound on
 // the static arrays of the tile kernels (at most 896 B): the dynamic part
 // must fit in what is left, and needs the opt-in attribute once the two
@@ -1422,7 +1451,8 @@ constexpr size_t kStaticSmem = 1024;
 
 __host__ __device__ __forceinline__ size_t fast_stage_bytes(int chunk)
 {
-    return (16 * (size_t)chunk + 8 * ((size_t)chunk + 2) + 15) / 16 * 16;  // the plane table after it is int4
+    // geometry, quadrant bases, measured values; the plane table after it is int4
+    return (32 * (size_t)chunk + 8 * ((size_t)chunk + 2) + 15) / 16 * 16;
 }
 __host__ __device__ __forceinline__ size_t fast_smem_bytes(int op, int nw, int S, int pitch, int nk, int chunk)
 {
@@ -1446,8 +1476,8 @@ __global__ void __launch_bounds__(32 * NW, 20 / NW) k_vis_fast(PlanDev P, const 
     __shared__ float s_wscr[NW * kFastVB * 5];
     __shared__ int s_item, s_fail;
     __shared__ __align__(8) uint64_t s_bar;
-    ItemStage stg{reinterpret_cast<uint4 *>(smem_fast), reinterpret_cast<float2 *>(smem_fast + 16 * (size_t)P.chunk),
-                  &s_bar, 0u, &s_fail};
+    ItemStage stg{reinterpret_cast<uint4 *>(smem_fast), reinterpret_cast<uint4 *>(smem_fast + 16 * (size_t)P.chunk),
+                  reinterpret_cast<float2 *>(smem_fast + 32 * (size_t)P.chunk), &s_bar, 0u, &s_fail};
     if (threadIdx.x == 0) {
         s_fail = 0;
         asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"((uint32_t)__cvta_generic_to_shared(&s_bar)));
@@ -1494,8 +1524,8 @@ __global__ void __launch_bounds__(32 * NW, 20 / NW) k_vis_fast_batch(const PlanD
     __shared__ int s_item, s_share, s_fail;
     __shared__ float s_wscr[NW * kFastVB * 5];
     __shared__ __align__(8) uint64_t s_bar;
-    ItemStage stg{reinterpret_cast<uint4 *>(smem_fast), reinterpret_cast<float2 *>(smem_fast + 16 * (size_t)chunk_max),
-                  &s_bar, 0u, &s_fail};
+    ItemStage stg{reinterpret_cast<uint4 *>(smem_fast), reinterpret_cast<uint4 *>(smem_fast + 16 * (size_t)chunk_max),
+                  reinterpret_cast<float2 *>(smem_fast + 32 * (size_t)chunk_max), &s_bar, 0u, &s_fail};
     if (threadIdx.x == 0) {
         s_fail = 0;
         asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"((uint32_t)__cvta_generic_to_shared(&s_bar)));
@@ -1563,6 +1593,15 @@ __global__ void k_dinv(const float2 *__restrict__ dk2, const int *__restrict__ d
         v = cn < 1e-5f ? -1e5f : __frcp_rn(cn);
     }
     dinv[e] = v;
+}
+
+// dst = conj(src), n samples.
+__global__ void k_conj_copy(const float2 *__restrict__ src, long long n, float2 *__restrict__ dst)
+{
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
+        const float2 v = src[i];
+        dst[i] = make_float2(v.x, -v.y);
+    }
 }
 
 // Phase-major copy of a kernel set (see kcol / krow).  One thread per output
@@ -1699,6 +1738,7 @@ static PlanDev plan_dev(const sdp_visplan *p)
     d.geo = p->geo;
     d.perm = p->perm;
     d.dinv = p->dinv;
+    d.gbase = p->gbase;
     return d;
 }
 
@@ -1765,11 +1805,22 @@ static size_t plan_sort_temp_bytes(const sdp_visplan *p)
 
 // Entries of the degridding normalisation table (0: not built).  The fast
 // path's packed geometry has 26 bits for the entry index.
+// Samples of one plane's phase-major copy (the largest half support).
+static size_t plan_per_plane(const sdp_visplan *p)
+{
+    return (size_t)(p->hs_max + 1) * p->geom.oversampling * (p->hs_max + 1) * p->geom.oversampling;
+}
+
+// Entries of the degridding normalisation table, 0 when the four-visibility
+// path is not available (it needs the phase-major layout, a table index
+// that fits the geometry's 25 bits, and table bases, the conjugated copy
+// included, that fit an int).
 static size_t plan_dinv_entries(const sdp_visplan *p)
 {
     if (!p->phase_major || p->dinv_nc <= 0) return 0;
     const size_t e = (size_t)p->dk.num_kernels * p->dinv_nc * p->dinv_nc;
-    return e < ((size_t)1 << 26) ? e : 0;
+    if (2 * plan_per_plane(p) * (size_t)p->dk.num_kernels >= ((size_t)1 << 31)) return 0;
+    return e < ((size_t)1 << 25) ? e : 0;
 }
 
 // Arena layout of a plan (offsets in bytes).
@@ -1795,11 +1846,15 @@ static void plan_layout(const sdp_visplan *p, size_t *off, size_t *total)
     off[13] = o; o = align_up(o + sizeof(int) * (size_t)p->dk.num_kernels, 256);          // dpoff
     const size_t per = (size_t)(p->hs_max + 1) * p->geom.oversampling * (p->hs_max + 1) * p->geom.oversampling;
     off[14] = o; o = align_up(o + (p->phase_major ? sizeof(float2) * per * p->gk.num_kernels : 0), 256);  // gk2
-    off[15] = o; o = align_up(o + (p->phase_major ? sizeof(float2) * per * p->dk.num_kernels : 0), 256);  // dk2
+    // dk2: the phase-major degridding set, then (four-visibility path) its
+    // conjugate at dk_conj_off = per * num_kernels
+    off[15] = o; o = align_up(o + (p->phase_major ? sizeof(float2) * per * p->dk.num_kernels : 0) *
+                                      (plan_dinv_entries(p) ? 2 : 1), 256);
     off[16] = o; o = align_up(o + sizeof(uint4) * (size_t)std::max(n, 1), 256);          // geo
     off[17] = o; o = align_up(o + sizeof(uint4) * (size_t)std::max(n, 1), 256);          // geo_tmp
     off[18] = o; o = align_up(o + plan_sort_temp_bytes(p), 256);                           // sort temp
     off[19] = o; o = align_up(o + sizeof(float) * plan_dinv_entries(p), 256);              // dinv
+    off[20] = o; o = align_up(o + (plan_dinv_entries(p) ? sizeof(uint4) * (size_t)std::max(n, 1) : 0), 256);  // gbase
     *total = o;
 }
 
@@ -1847,7 +1902,7 @@ int visplan_setup(sdp_visplan *p, const sdp_geometry *geom, const sdp_wkernels *
 
 size_t visplan_arena_bytes(const sdp_visplan *p)
 {
-    size_t off[20], total;
+    size_t off[21], total;
     plan_layout(p, off, &total);
     return total;
 }
@@ -1890,6 +1945,12 @@ int visplan_kernels(sdp_visplan *p, cudaStream_t st)
             p->dpoff, p->gk2, p->dk2, related, nk, os, per, p->kshare);
         SDP_LAUNCH_CHECK();
         if (p->dinv) {
+            // conjugated copy of the degridding set: a w < 0 visibility's taps
+            // read it, so the four-visibility path needs no sign per sample
+            const long long nconj = (long long)p->dk_conj_off;
+            k_conj_copy<<<(int)std::min<long long>((nconj + 255) / 256, 148 * 16), 256, 0, st>>>(
+                p->dk2, nconj, p->dk2 + nconj);
+            SDP_LAUNCH_CHECK();
             const int ne = (int)plan_dinv_entries(p);
             k_dinv<<<(ne + 255) / 256, 256, 0, st>>>(p->dk2, p->dpoff, reinterpret_cast<const int2 *>(p->dk.supports),
                                                      p->dk.num_kernels, os, os_shift, p->dinv_nc, p->dinv);
@@ -1902,7 +1963,7 @@ int visplan_kernels(sdp_visplan *p, cudaStream_t st)
 
 int visplan_build(sdp_visplan *p, void *arena, const float3 *uvw, cudaStream_t st)
 {
-    size_t off[20], total;
+    size_t off[21], total;
     plan_layout(p, off, &total);
     char *a = static_cast<char *>(arena);
     p->arena = arena;
@@ -1930,6 +1991,8 @@ int visplan_build(sdp_visplan *p, void *arena, const float3 *uvw, cudaStream_t s
     uint4 *geo_tmp = reinterpret_cast<uint4 *>(a + off[17]);
     void *sort_temp = a + off[18];
     p->dinv = plan_dinv_entries(p) ? reinterpret_cast<float *>(a + off[19]) : nullptr;
+    p->gbase = p->dinv ? reinterpret_cast<uint4 *>(a + off[20]) : nullptr;
+    p->dk_conj_off = p->dinv ? (int)(plan_per_plane(p) * (size_t)p->dk.num_kernels) : 0;
     // sort keys: both buffers in the geo region (16 bytes per visibility),
     // written by the gather only after the sort
     unsigned long long *skeys0 = reinterpret_cast<unsigned long long *>(p->geo);
@@ -1978,11 +2041,13 @@ int visplan_build(sdp_visplan *p, void *arena, const float3 *uvw, cudaStream_t s
         if (p->coord_f64)
             k_gather_plan<double><<<(n + 255) / 256, 256, 0, st>>>(static_cast<const Rec<double> *>(rec_tmp), geo_tmp,
                                                                    n, n_binned, p->perm,
-                                                                   static_cast<Rec<double> *>(p->rec), p->geo);
+                                                                   static_cast<Rec<double> *>(p->rec), p->geo,
+                                                                   p->gbase, p->dpoff, p->dk_conj_off);
         else
             k_gather_plan<float><<<(n + 255) / 256, 256, 0, st>>>(static_cast<const Rec<float> *>(rec_tmp), geo_tmp,
                                                                   n, n_binned, p->perm,
-                                                                  static_cast<Rec<float> *>(p->rec), p->geo);
+                                                                  static_cast<Rec<float> *>(p->rec), p->geo,
+                                                                  p->gbase, p->dpoff, p->dk_conj_off);
         SDP_LAUNCH_CHECK();
     }
     k_item_counts<<<(p->ntiles + 255) / 256, 256, 0, st>>>(offsets, p->ntiles, p->nk, p->chunk, item_counts);
