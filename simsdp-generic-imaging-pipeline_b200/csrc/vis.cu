@@ -234,7 +234,8 @@ __device__ __forceinline__ int geo_krow(int ky, int A, int pm, int OS, int shift
 //   y: CN (0-15), CP (16-31): table offsets of the columns; tap column i < hs
 //      sits at CN - i * SC, column i >= hs at CP + (i - hs) * SC;
 //   z: RN (0-15), RP (16-31): the same for the rows with step RS;
-//   w: hs (0-3), kernel conjugated (4: w < 0), fast path (5), index of the
+//   w: hs (0-3), kernel conjugated (4: w < 0), fast path (5), first of a
+//      batch of four half-support-4 fast visibilities (6, k_batch_flags), index of the
 //      tap box's degridding normalisation in the plan's dinv table (7-31:
 //      (plane NC + row configuration) NC + column configuration, NC =
 //      2 (OS + 1); a configuration is 2 ko + h of fast_kidx).
@@ -405,6 +406,24 @@ __global__ void k_item_fill(const int *__restrict__ offsets, const int *__restri
     int b = offsets[t * nk], e = offsets[(t + 1) * nk];
     int o = item_offsets[t];
     for (int s = b; s < e; s += chunk) items[o++] = make_int4(t, s, min(e, s + chunk), 0);
+}
+
+// Marks (bit 6 of w) the first visibility of every batch of four, counted
+// from its work item's start, whose four visibilities all take the fast path
+// with half support 4: the warp-per-visibility kernels run such a batch
+// branch-free.  One thread per work item.
+__global__ void k_batch_flags(const int4 *__restrict__ items, const int *__restrict__ n_items, int cap,
+                              uint4 *__restrict__ geo)
+{
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= cap || k >= *n_items) return;
+    const int4 it = items[k];
+    for (int b = it.y; b + 3 < it.z; b += 4) {
+        bool all = true;
+#pragma unroll
+        for (int j = 0; j < 4; ++j) all = all && (geo[b + j].w & 0x2fu) == 0x24u;
+        if (all) geo[b].w |= 1u << 6;
+    }
 }
 
 // ----------------------------------------------------------------------------
@@ -1143,12 +1162,12 @@ __device__ __forceinline__ bool fast_item(const PlanDev &Pin, const int4 it, Ite
         // tap of the 8 x 8 box active (rows r below the visibility at RN - 5 r,
         // rows r + 4 above it at RP + 5 r; columns c < 4 at CN - c, the others
         // at CP + c - 4), packed FP32x2 arithmetic.
-        bool all4 = (nv == kFastVB) && (kConv ? P.gbase != nullptr : pm != 0);
-#pragma unroll
-        for (int j = 0; j < kFastVB; ++j) all4 = all4 && (g[j].w & 0x2fu) == 0x24u;  // fast, hs = 4
+        // (the plan marks the first visibility of such a batch, k_batch_flags)
+        const bool all4 = (nv == kFastVB) && (g[0].w & (1u << 6)) && (kConv ? P.gbase != nullptr : pm != 0);
         if (all4) {
             float2 q0[kFastVB], q1[kFastVB];
             int ce4[kFastVB];
+            bool fresh[kFastVB];  // visibility j starts a run of one tap-box origin
             float2 gv4 = make_float2(0.f, 0.f);
             float ie = 0.f;  // lanes 8 j ..: visibility j's normalisation entry, loaded ahead of its use
             if (kConv) ie = __ldg(&P.dinv[sgw[4 * (b + r)] >> 7]);
@@ -1168,7 +1187,8 @@ __device__ __forceinline__ bool fast_item(const PlanDev &Pin, const int4 it, Ite
                     // the plan orders a tile's visibilities by tap-box origin:
                     // a visibility with its predecessor's origin reads the same
                     // model cells
-                    if (j == 0 || ce != ce4[j > 0 ? j - 1 : 0]) {
+                    fresh[j] = (j == 0) || ce != ce4[j > 0 ? j - 1 : 0];
+                    if (fresh[j]) {
                         m0 = mtile[ce];
                         m1 = mtile[ce + 4 * pitch];
                     }
@@ -1238,7 +1258,7 @@ __device__ __forceinline__ bool fast_item(const PlanDev &Pin, const int4 it, Ite
                         const float conj = (gj.w & (1u << 4)) ? -1.f : 1.f;
                         nc = make_float2(-conj * gv.y, conj * gv.x);
                     }
-                    if (j == 0 || ((gj.x ^ g[j - 1].x) & 0xffffu) != 0u) {
+                    if (kConv ? fresh[j] : (j == 0 || ((gj.x ^ g[j > 0 ? j - 1 : 0].x) & 0xffffu) != 0u)) {
                         if (j > 0) {
                             sub[run_ce] = s0;
                             sub[run_ce + 4 * pitch] = s1;
@@ -2057,6 +2077,11 @@ int visplan_build(sdp_visplan *p, void *arena, const float3 *uvw, cudaStream_t s
                                                           p->items);
     SDP_LAUNCH_CHECK();
     SDP_CUDA_TRY(cudaMemcpyAsync(p->n_items, item_offsets + p->ntiles, sizeof(int), cudaMemcpyDeviceToDevice, st));
+    if (n > 0) {
+        const int cap = n / p->chunk + p->ntiles + 1;  // the items region's capacity
+        k_batch_flags<<<(cap + 255) / 256, 256, 0, st>>>(p->items, p->n_items, cap, p->geo);
+        SDP_LAUNCH_CHECK();
+    }
     return SDP_OK;
 }
 
