@@ -359,7 +359,9 @@ __global__ void k_bin(const float3 *__restrict__ uvw, int n, int mode, int snap,
 // occupy positions [0, offsets[nbins]), the rest are marked -1.
 // With gbase, also each fast visibility's four tap-quadrant bases in the
 // degridding table (the conjugated copy for w < 0): quadrant (columns below
-// or above, rows below or above) = plane offset + CN or CP + RN or RP.
+// or above, rows below or above) = plane offset + CN or CP + RN or RP, in
+// the order (CN RN, CN RP, CP RN, CP RP) so that a lane's two quadrants are
+// one 8-byte pair.
 template <typename T>
 __global__ void k_gather_plan(const Rec<T> *__restrict__ rec_tmp, const uint4 *__restrict__ geo_tmp, int n,
                               const int *__restrict__ n_binned, int *__restrict__ perm, Rec<T> *__restrict__ rec,
@@ -382,7 +384,7 @@ __global__ void k_gather_plan(const Rec<T> *__restrict__ rec_tmp, const uint4 *_
             const int o = dpoff[g.x >> 16] + ((g.w & (1u << 4)) ? conj_off : 0);
             const int cn = (int)(g.y & 0xffffu), cp = (int)(g.y >> 16);
             const int rn = (int)(g.z & 0xffffu), rp = (int)(g.z >> 16);
-            q = make_uint4((uint32_t)(o + cn + rn), (uint32_t)(o + cp + rn), (uint32_t)(o + cn + rp),
+            q = make_uint4((uint32_t)(o + cn + rn), (uint32_t)(o + cn + rp), (uint32_t)(o + cp + rn),
                            (uint32_t)(o + cp + rp));
         }
         gbase[pos] = q;
@@ -1135,8 +1137,7 @@ __device__ __forceinline__ bool fast_item(const PlanDev &Pin, const int4 it, Ite
     // shared memory; the lane's offsets within the quadrants fold into its
     // table pointers
     const int cq = (c < 4) ? 0 : 1;
-    const unsigned *sgb0 = reinterpret_cast<const unsigned *>(stg.gb - it.y) + cq;      // rows below
-    const unsigned *sgb1 = reinterpret_cast<const unsigned *>(stg.gb - it.y) + 2 + cq;  // rows above
+    const uint2 *sgb = reinterpret_cast<const uint2 *>(stg.gb - it.y) + cq;  // (rows below, rows above)
     const unsigned *sgw = reinterpret_cast<const unsigned *>(sgeo) + 3;
     const int cofs4 = (c < 4) ? -c : c - 4;
     const float2 *dk_l0 = reinterpret_cast<const float2 *>(reinterpret_cast<uintptr_t>(P.dk) +
@@ -1180,8 +1181,9 @@ __device__ __forceinline__ bool fast_item(const PlanDev &Pin, const int4 it, Ite
                 float2 m0 = make_float2(0.f, 0.f), m1 = m0;
 #pragma unroll
                 for (int j = 0; j < kFastVB; ++j) {
-                    q0[j] = __ldg(dk_l0 + sgb0[4 * (b + j)]);
-                    q1[j] = __ldg(dk_l1 + sgb1[4 * (b + j)]);
+                    const uint2 qb = sgb[2 * (b + j)];
+                    q0[j] = __ldg(dk_l0 + qb.x);
+                    q1[j] = __ldg(dk_l1 + qb.y);
                     const int ce = (int)(g[j].x & 0xffffu) + lanecell;
                     ce4[j] = ce;
                     // the plan orders a tile's visibilities by tap-box origin:
@@ -1222,6 +1224,15 @@ __device__ __forceinline__ bool fast_item(const PlanDev &Pin, const int4 it, Ite
                 }
             }
             if (kGrids) {
+                // the batch's four residuals to every lane: lane 8 j stores
+                // visibility j's, each lane reads all four (two 16-byte loads)
+                float4 gvp[2];
+                if (kConv) {
+                    if (c == 0) reinterpret_cast<float2 *>(wscr)[r] = gv4;
+                    __syncwarp();
+                    gvp[0] = reinterpret_cast<const float4 *>(wscr)[0];
+                    gvp[1] = reinterpret_cast<const float4 *>(wscr)[1];
+                }
                 // a run of visibilities with one tap-box origin accumulates in
                 // registers: one read and one write of the lane's two cells per
                 // run, in the same order of operations as cell by cell
@@ -1232,8 +1243,8 @@ __device__ __forceinline__ bool fast_item(const PlanDev &Pin, const int4 it, Ite
                     const uint4 gj = g[j];
                     float2 gv;
                     if (kConv) {
-                        gv.x = __shfl_sync(0xffffffffu, gv4.x, 8 * j);
-                        gv.y = __shfl_sync(0xffffffffu, gv4.y, 8 * j);
+                        const float4 p2 = gvp[j >> 1];
+                        gv = (j & 1) ? make_float2(p2.z, p2.w) : make_float2(p2.x, p2.y);
                     } else {
                         gv = __ldg(&vis_in[P.perm[b + j]]);
                     }
@@ -1493,7 +1504,7 @@ __global__ void __launch_bounds__(32 * NW, 20 / NW) k_vis_fast(PlanDev P, const 
     int4 *planes = reinterpret_cast<int4 *>(smem_fast + stage_b);
     float2 *mtile = reinterpret_cast<float2 *>(smem_fast + stage_b + 16 * (size_t)P.nk_g);
     float2 *subs = mtile + (OP != OP_GRID ? (size_t)P.S * P.pitch : 0);
-    __shared__ float s_wscr[NW * kFastVB * 5];
+    __shared__ __align__(16) float s_wscr[NW * kFastVB * 5];
     __shared__ int s_item, s_fail;
     __shared__ __align__(8) uint64_t s_bar;
     ItemStage stg{reinterpret_cast<uint4 *>(smem_fast), reinterpret_cast<uint4 *>(smem_fast + 16 * (size_t)P.chunk),
@@ -1542,7 +1553,7 @@ __global__ void __launch_bounds__(32 * NW, 20 / NW) k_vis_fast_batch(const PlanD
     __shared__ PlanDev sP;
     __shared__ BatchIO sIO;
     __shared__ int s_item, s_share, s_fail;
-    __shared__ float s_wscr[NW * kFastVB * 5];
+    __shared__ __align__(16) float s_wscr[NW * kFastVB * 5];
     __shared__ __align__(8) uint64_t s_bar;
     ItemStage stg{reinterpret_cast<uint4 *>(smem_fast), reinterpret_cast<uint4 *>(smem_fast + 16 * (size_t)chunk_max),
                   reinterpret_cast<float2 *>(smem_fast + 32 * (size_t)chunk_max), &s_bar, 0u, &s_fail};
