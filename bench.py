@@ -823,6 +823,8 @@ def c4_learned_block(S, D, dev, skies: int):
         "speedup_median": med(sp), "speedup_geomean": float(np.exp(np.mean(np.log(sp)))) if sp else None,
         "speedup_min": min(sp) if sp else None, "speedup_max": max(sp) if sp else None,
         "reached": sum(1 for r in rows if r["learned_s"]),
+        "slower_than_plain": sum(1 for x in sp if x < 1.0),
+        "speedup_per_sky": [round(r["plain_s"] / r["learned_s"], 3) if r["learned_s"] else None for r in rows],
         "plain_ms_median": med([r["plain_s"] * 1e3 for r in rows]),
         "learned_ms_median": med([r["learned_s"] * 1e3 for r in rows if r["learned_s"]]),
         "learned_cycles": [r["learned_cycles"] for r in rows], "learned_kinds": [r["learned_kinds"] for r in rows],
@@ -834,6 +836,7 @@ def c4_learned_block(S, D, dev, skies: int):
                     "speedup_median": med(sp2),
                     "speedup_geomean": float(np.exp(np.mean(np.log(sp2)))) if sp2 else None,
                     "speedup_min": min(sp2) if sp2 else None,
+                    "slower_than_plain": sum(1 for x in sp2 if x < 1.0),
                     "plain_ms_median": med([r["plain_s"] * 1e3 for r in rows2]),
                     "learned_ms_median": med([r["learned_s"] * 1e3 for r in rows2 if r["learned_s"]]),
                     "learned_kinds": [r["learned_kinds"] for r in rows2]},

@@ -1103,7 +1103,7 @@ __device__ __forceinline__ bool fast_item(const PlanDev &Pin, const int4 it, Ite
         asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
         const uint32_t gbytes = (uint32_t)(it.z - it.y) * 16u;
         const uint32_t mbytes = (OP == OP_CYCLE_CONV) ? (uint32_t)(((it.z + 1) & ~1) - m0) * 8u : 0u;
-        const uint32_t bbytes = (kConv && P.gbase) ? gbytes : 0u;
+        const uint32_t bbytes = ((kConv || share) && P.gbase) ? gbytes : 0u;
         stage_arm(bar, gbytes + bbytes + mbytes);
         stage_copy((uint32_t)__cvta_generic_to_shared(stg.geo), P.geo + it.y, gbytes, bar);
         if (bbytes) stage_copy((uint32_t)__cvta_generic_to_shared(stg.gb), P.gbase + it.y, bbytes, bar);
@@ -1116,6 +1116,10 @@ __device__ __forceinline__ bool fast_item(const PlanDev &Pin, const int4 it, Ite
             mtile[y * pitch + x] =
                 (gx < P.G && gy < P.G) ? __ldg(&in_grid[(size_t)gy * P.G + gx]) : make_float2(0.f, 0.f);
         }
+    } else {
+        // the item's input visibilities in plan order (gathered through the
+        // permutation once per item, all loads of the CTA in flight together)
+        for (int k = threadIdx.x; k < it.z - it.y; k += 32 * NW) stg.meas[k] = __ldg(&vis_in[P.perm[it.y + k]]);
     }
     if (threadIdx.x == 0) {
         if (!stage_wait(bar, stg.phase)) {
@@ -1131,6 +1135,7 @@ __device__ __forceinline__ bool fast_item(const PlanDev &Pin, const int4 it, Ite
     if (*stg.fail) return false;
     const uint4 *sgeo = stg.geo - it.y;   // indexed by plan position
     const float2 *smeas = stg.meas - m0;
+    const float2 *svis = stg.meas - it.y;  // OP_GRID: the item's input visibilities in plan order
     // four-visibility path (half support 4): lane (r, c) reads the quadrant
     // bases of its two taps (columns c < 4 below the visibility, rows r below
     // and r + 4 above) and its visibility r's geometry word w directly from
@@ -1246,18 +1251,25 @@ __device__ __forceinline__ bool fast_item(const PlanDev &Pin, const int4 it, Ite
                         const float4 p2 = gvp[j >> 1];
                         gv = (j & 1) ? make_float2(p2.z, p2.w) : make_float2(p2.x, p2.y);
                     } else {
-                        gv = __ldg(&vis_in[P.perm[b + j]]);
+                        gv = svis[b + j];
                     }
                     float2 t0, t1;
                     int ce;
                     float2 nc;
-                    if (kConv && share) {
+                    if (share && (kConv || P.gbase != nullptr)) {
                         // the degridding samples (conjugated for w < 0) with the
                         // gridding set's sign of the imaginary part:
                         // vis * (kr + i ks ki) = (vr kr - ks vi ki, vi kr + ks vr ki)
-                        t0 = q0[j];
-                        t1 = q1[j];
-                        ce = ce4[j];
+                        if (kConv) {
+                            t0 = q0[j];
+                            t1 = q1[j];
+                            ce = ce4[j];
+                        } else {
+                            const uint2 qb = sgb[2 * (b + j)];
+                            t0 = __ldg(dk_l0 + qb.x);
+                            t1 = __ldg(dk_l1 + qb.y);
+                            ce = (int)(gj.x & 0xffffu) + lanecell;
+                        }
                         nc = make_float2(-share_sign * gv.y, share_sign * gv.x);
                     } else {
                         const int colp = (int)__byte_perm(gj.y, 0u, csel) + cofs;
@@ -1389,7 +1401,7 @@ __device__ __forceinline__ bool fast_item(const PlanDev &Pin, const int4 it, Ite
                     gv.x = __shfl_sync(0xffffffffu, gval.x, 8 * j);
                     gv.y = __shfl_sync(0xffffffffu, gval.y, 8 * j);
                 } else {
-                    gv = __ldg(&vis_in[P.perm[b + j]]);
+                    gv = svis[b + j];
                 }
                 const float conj = (g[j].w & (1u << 4)) ? -1.f : 1.f;
                 float2 q0, q1;
@@ -1435,7 +1447,7 @@ __device__ __forceinline__ bool fast_item(const PlanDev &Pin, const int4 it, Ite
                         gv.x = __shfl_sync(0xffffffffu, gval.x, 8 * j);
                         gv.y = __shfl_sync(0xffffffffu, gval.y, 8 * j);
                     } else {
-                        gv = __ldg(&vis_in[P.perm[b + j]]);
+                        gv = svis[b + j];
                     }
                     const uint4 gj = pick4(g, j);
                     const int4 pl = planes[gj.x >> 16];
@@ -1520,7 +1532,7 @@ __global__ void __launch_bounds__(32 * NW, 20 / NW) k_vis_fast(PlanDev P, const 
                               OP != OP_DEGRID ? P.gpoff[k] : 0);
     if (OP != OP_DEGRID)
         for (size_t k = threadIdx.x; k < (size_t)NW * P.S * P.pitch; k += 32 * NW) subs[k] = make_float2(0.f, 0.f);
-    const int kdiff = (OP == OP_CYCLE_CONV) ? *P.kdiff : 3;
+    const int kdiff = (OP == OP_CYCLE_CONV || OP == OP_GRID) ? *P.kdiff : 3;
     const bool share = (kdiff & 1) == 0 || (kdiff & 2) == 0;
     const float share_sign = (kdiff & 1) == 0 ? 1.f : -1.f;
     __syncthreads();
