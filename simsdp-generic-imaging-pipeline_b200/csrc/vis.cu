@@ -357,11 +357,15 @@ __global__ void k_bin(const float3 *__restrict__ uvw, int n, int mode, int snap,
 
 // Plan order from the sorted visibility indices (perm): binned visibilities
 // occupy positions [0, offsets[nbins]), the rest are marked -1.
-// With gbase, also each fast visibility's four tap-quadrant bases in the
-// degridding table (the conjugated copy for w < 0): quadrant (columns below
-// or above, rows below or above) = plane offset + CN or CP + RN or RP, in
-// the order (CN RN, CN RP, CP RN, CP RP) so that a lane's two quadrants are
-// one 8-byte pair.
+// With gbase, also the quad record of each fast visibility of half support
+// 4, all that the four-visibility path reads of it:
+//   x: box origin as a cell of the shared tiles (bits 0-15), first of a
+//      flagged batch of four (16, k_batch_flags);
+//   y, z: table offsets of its tap quadrants (columns below, rows below) and
+//      (columns below, rows above) in the degridding table, the conjugated
+//      copy for w < 0 (plane offset + CN + RN, + CN + RP);
+//   w: CP - CN (bits 0-12, signed: the columns-above quadrants lie that far
+//      from the columns-below ones), its normalisation entry (13-31).
 template <typename T>
 __global__ void k_gather_plan(const Rec<T> *__restrict__ rec_tmp, const uint4 *__restrict__ geo_tmp, int n,
                               const int *__restrict__ n_binned, int *__restrict__ perm, Rec<T> *__restrict__ rec,
@@ -380,12 +384,12 @@ __global__ void k_gather_plan(const Rec<T> *__restrict__ rec_tmp, const uint4 *_
     geo[pos] = g;
     if (gbase) {
         uint4 q = make_uint4(0u, 0u, 0u, 0u);
-        if (g.w & (1u << 5)) {
+        if ((g.w & 0x2fu) == 0x24u) {
             const int o = dpoff[g.x >> 16] + ((g.w & (1u << 4)) ? conj_off : 0);
             const int cn = (int)(g.y & 0xffffu), cp = (int)(g.y >> 16);
             const int rn = (int)(g.z & 0xffffu), rp = (int)(g.z >> 16);
-            q = make_uint4((uint32_t)(o + cn + rn), (uint32_t)(o + cn + rp), (uint32_t)(o + cp + rn),
-                           (uint32_t)(o + cp + rp));
+            q = make_uint4(g.x & 0xffffu, (uint32_t)(o + cn + rn), (uint32_t)(o + cn + rp),
+                           ((uint32_t)(cp - cn) & 0x1fffu) | ((g.w >> 7) << 13));
         }
         gbase[pos] = q;
     }
@@ -415,7 +419,7 @@ __global__ void k_item_fill(const int *__restrict__ offsets, const int *__restri
 // with half support 4: the warp-per-visibility kernels run such a batch
 // branch-free.  One thread per work item.
 __global__ void k_batch_flags(const int4 *__restrict__ items, const int *__restrict__ n_items, int cap,
-                              uint4 *__restrict__ geo)
+                              uint4 *__restrict__ geo, uint4 *__restrict__ quad)
 {
     const int k = blockIdx.x * blockDim.x + threadIdx.x;
     if (k >= cap || k >= *n_items) return;
@@ -424,7 +428,10 @@ __global__ void k_batch_flags(const int4 *__restrict__ items, const int *__restr
         bool all = true;
 #pragma unroll
         for (int j = 0; j < 4; ++j) all = all && (geo[b + j].w & 0x2fu) == 0x24u;
-        if (all) geo[b].w |= 1u << 6;
+        if (all) {
+            geo[b].w |= 1u << 6;
+            if (quad) quad[b].x |= 1u << 16;
+        }
     }
 }
 
@@ -1136,14 +1143,14 @@ __device__ __forceinline__ bool fast_item(const PlanDev &Pin, const int4 it, Ite
     const uint4 *sgeo = stg.geo - it.y;   // indexed by plan position
     const float2 *smeas = stg.meas - m0;
     const float2 *svis = stg.meas - it.y;  // OP_GRID: the item's input visibilities in plan order
-    // four-visibility path (half support 4): lane (r, c) reads the quadrant
-    // bases of its two taps (columns c < 4 below the visibility, rows r below
-    // and r + 4 above) and its visibility r's geometry word w directly from
-    // shared memory; the lane's offsets within the quadrants fold into its
-    // table pointers
-    const int cq = (c < 4) ? 0 : 1;
-    const uint2 *sgb = reinterpret_cast<const uint2 *>(stg.gb - it.y) + cq;  // (rows below, rows above)
-    const unsigned *sgw = reinterpret_cast<const unsigned *>(sgeo) + 3;
+    // four-visibility path (half support 4): a batch reads only the quad
+    // records (k_gather_plan); lane (r, c) takes its two taps (rows r below
+    // the visibility, r + 4 above) from the columns-below quadrants, or for
+    // c >= 4 from the columns-above ones CP - CN further on; the lane's
+    // offsets within the quadrants fold into its table pointers
+    const bool quad = P.gbase != nullptr && (kConv || share);
+    const uint4 *squad = stg.gb - it.y;  // indexed by plan position
+    const int cqm = (c < 4) ? 0 : -1;
     const int cofs4 = (c < 4) ? -c : c - 4;
     const float2 *dk_l0 = reinterpret_cast<const float2 *>(reinterpret_cast<uintptr_t>(P.dk) +
                                                            (intptr_t)(cofs4 - 5 * r) * (intptr_t)sizeof(float2));
@@ -1158,9 +1165,11 @@ __device__ __forceinline__ bool fast_item(const PlanDev &Pin, const int4 it, Ite
     const int cofs = cofs4;
     for (int b = it.y + warp * kFastVB; b < it.z; b += NW * kFastVB) {
         const int nv = min(kFastVB, it.z - b);  // visibilities in this batch (warp-uniform)
+        const bool all4q = quad && nv == kFastVB && (squad[b].x & (1u << 16)) != 0u;
         uint4 g[kFastVB];
 #pragma unroll
-        for (int j = 0; j < kFastVB; ++j) g[j] = (j < nv) ? sgeo[b + j] : make_uint4(0u, 0u, 0u, 0u);
+        for (int j = 0; j < kFastVB; ++j)
+            g[j] = (j < nv && !all4q) ? sgeo[b + j] : make_uint4(0u, 0u, 0u, 0u);
         float2 meas_r = make_float2(0.f, 0.f);  // lanes 8 j ..: visibility j's measured value
         if (OP == OP_CYCLE_CONV && r < nv) meas_r = smeas[b + r];
         // A batch of four fast-path visibilities of half support 4 in the
@@ -1168,15 +1177,20 @@ __device__ __forceinline__ bool fast_item(const PlanDev &Pin, const int4 it, Ite
         // tap of the 8 x 8 box active (rows r below the visibility at RN - 5 r,
         // rows r + 4 above it at RP + 5 r; columns c < 4 at CN - c, the others
         // at CP + c - 4), packed FP32x2 arithmetic.
-        // (the plan marks the first visibility of such a batch, k_batch_flags)
-        const bool all4 = (nv == kFastVB) && (g[0].w & (1u << 6)) && (kConv ? P.gbase != nullptr : pm != 0);
+        // (the plan marks the first visibility of such a batch, k_batch_flags;
+        // plans without quad records take the grid-only form from the
+        // geometry records)
+        const bool all4 = all4q || (!kConv && !quad && nv == kFastVB && pm && (g[0].w & (1u << 6)));
         if (all4) {
+            uint4 qr[kFastVB];
+#pragma unroll
+            for (int j = 0; j < kFastVB; ++j) qr[j] = all4q ? squad[b + j] : make_uint4(0u, 0u, 0u, 0u);
             float2 q0[kFastVB], q1[kFastVB];
             int ce4[kFastVB];
             bool fresh[kFastVB];  // visibility j starts a run of one tap-box origin
             float2 gv4 = make_float2(0.f, 0.f);
             float ie = 0.f;  // lanes 8 j ..: visibility j's normalisation entry, loaded ahead of its use
-            if (kConv) ie = __ldg(&P.dinv[sgw[4 * (b + r)] >> 7]);
+            if (kConv) ie = __ldg(&P.dinv[squad[b + r].w >> 13]);
             if (kConv) {
                 // per visibility the lane's share of the real and imaginary
                 // parts of sum m k; the samples come from the plan's
@@ -1186,10 +1200,10 @@ __device__ __forceinline__ bool fast_item(const PlanDev &Pin, const int4 it, Ite
                 float2 m0 = make_float2(0.f, 0.f), m1 = m0;
 #pragma unroll
                 for (int j = 0; j < kFastVB; ++j) {
-                    const uint2 qb = sgb[2 * (b + j)];
-                    q0[j] = __ldg(dk_l0 + qb.x);
-                    q1[j] = __ldg(dk_l1 + qb.y);
-                    const int ce = (int)(g[j].x & 0xffffu) + lanecell;
+                    const int dc = ((int)(qr[j].w << 19) >> 19) & cqm;
+                    q0[j] = __ldg(dk_l0 + ((int)qr[j].y + dc));
+                    q1[j] = __ldg(dk_l1 + ((int)qr[j].z + dc));
+                    const int ce = (int)(qr[j].x & 0xffffu) + lanecell;
                     ce4[j] = ce;
                     // the plan orders a tile's visibilities by tap-box origin:
                     // a visibility with its predecessor's origin reads the same
@@ -1256,7 +1270,7 @@ __device__ __forceinline__ bool fast_item(const PlanDev &Pin, const int4 it, Ite
                     float2 t0, t1;
                     int ce;
                     float2 nc;
-                    if (share && (kConv || P.gbase != nullptr)) {
+                    if (all4q) {
                         // the degridding samples (conjugated for w < 0) with the
                         // gridding set's sign of the imaginary part:
                         // vis * (kr + i ks ki) = (vr kr - ks vi ki, vi kr + ks vr ki)
@@ -1265,10 +1279,10 @@ __device__ __forceinline__ bool fast_item(const PlanDev &Pin, const int4 it, Ite
                             t1 = q1[j];
                             ce = ce4[j];
                         } else {
-                            const uint2 qb = sgb[2 * (b + j)];
-                            t0 = __ldg(dk_l0 + qb.x);
-                            t1 = __ldg(dk_l1 + qb.y);
-                            ce = (int)(gj.x & 0xffffu) + lanecell;
+                            const int dc = ((int)(qr[j].w << 19) >> 19) & cqm;
+                            t0 = __ldg(dk_l0 + ((int)qr[j].y + dc));
+                            t1 = __ldg(dk_l1 + ((int)qr[j].z + dc));
+                            ce = (int)(qr[j].x & 0xffffu) + lanecell;
                         }
                         nc = make_float2(-share_sign * gv.y, share_sign * gv.x);
                     } else {
@@ -1281,7 +1295,9 @@ __device__ __forceinline__ bool fast_item(const PlanDev &Pin, const int4 it, Ite
                         const float conj = (gj.w & (1u << 4)) ? -1.f : 1.f;
                         nc = make_float2(-conj * gv.y, conj * gv.x);
                     }
-                    if (kConv ? fresh[j] : (j == 0 || ((gj.x ^ g[j > 0 ? j - 1 : 0].x) & 0xffffu) != 0u)) {
+                    const uint32_t xprev = all4q ? qr[j > 0 ? j - 1 : 0].x : g[j > 0 ? j - 1 : 0].x;
+                    const uint32_t xcur = all4q ? qr[j].x : gj.x;
+                    if (kConv ? fresh[j] : (j == 0 || ((xcur ^ xprev) & 0xffffu) != 0u)) {
                         if (j > 0) {
                             sub[run_ce] = s0;
                             sub[run_ce + 4 * pitch] = s1;
@@ -1857,13 +1873,14 @@ static size_t plan_per_plane(const sdp_visplan *p)
 // Entries of the degridding normalisation table, 0 when the four-visibility
 // path is not available (it needs the phase-major layout, a table index
 // that fits the geometry's 25 bits, and table bases, the conjugated copy
-// included, that fit an int).
+// included, that fit an int; the quad record holds the entry index in 19
+// bits).
 static size_t plan_dinv_entries(const sdp_visplan *p)
 {
     if (!p->phase_major || p->dinv_nc <= 0) return 0;
     const size_t e = (size_t)p->dk.num_kernels * p->dinv_nc * p->dinv_nc;
     if (2 * plan_per_plane(p) * (size_t)p->dk.num_kernels >= ((size_t)1 << 31)) return 0;
-    return e < ((size_t)1 << 25) ? e : 0;
+    return e < ((size_t)1 << 19) ? e : 0;
 }
 
 // Arena layout of a plan (offsets in bytes).
@@ -2102,7 +2119,7 @@ int visplan_build(sdp_visplan *p, void *arena, const float3 *uvw, cudaStream_t s
     SDP_CUDA_TRY(cudaMemcpyAsync(p->n_items, item_offsets + p->ntiles, sizeof(int), cudaMemcpyDeviceToDevice, st));
     if (n > 0) {
         const int cap = n / p->chunk + p->ntiles + 1;  // the items region's capacity
-        k_batch_flags<<<(cap + 255) / 256, 256, 0, st>>>(p->items, p->n_items, cap, p->geo);
+        k_batch_flags<<<(cap + 255) / 256, 256, 0, st>>>(p->items, p->n_items, cap, p->geo, p->gbase);
         SDP_LAUNCH_CHECK();
     }
     return SDP_OK;
