@@ -239,9 +239,10 @@ __device__ __forceinline__ int geo_krow(int ky, int A, int pm, int OS, int shift
 //      tap box's degridding normalisation in the plan's dinv table (7-31:
 //      (plane NC + row configuration) NC + column configuration, NC =
 //      2 (OS + 1); a configuration is 2 ko + h of fast_kidx).
-// SC = 1, RS = hs + 1 in the phase-major layout (SC = OS, RS = (hs + 1) OS
-// otherwise): below the visibility the kernel index falls by OS per tap
-// (the phase stays, the block index falls by one), above it rises by OS.
+// SC = 1, RS = hs + 1 in the phase-major layout (SC = OS, RS = (hs + 1) OS^2
+// in the reference layout, where row ky starts at ky (hs + 1) OS): below the
+// visibility the kernel index falls by OS per tap (the phase stays, the
+// block index falls by one), above it rises by OS.
 // Fast path: std_gridding plan, both kernel sets with the same half support
 // 1 <= hs <= 4, a 2 hs x 2 hs box inside the grid, and every tap's kernel
 // index equal to fast_kidx (the reference's float subtraction (g - p) is
@@ -963,7 +964,7 @@ __device__ __forceinline__ void fast_taps(const uint4 g, int c, int r, int lanec
     const int cn = (int)(g.y & 0xffffu), cp = (int)(g.y >> 16);
     const int rn = (int)(g.z & 0xffffu), rp = (int)(g.z >> 16);
     ce = (int)(g.x & 0xffffu) + lanecell;
-    const int sc = pm ? 1 : OS, rs = pm ? A : A * OS;
+    const int sc = pm ? 1 : OS, rs = pm ? A : A * OS * OS;
     const int colp = (c < hs) ? cn - c * sc : cp + (c - hs) * sc;
     const int r1 = r + 4;
     off0 = colp + ((r < hs) ? rn - r * rs : rp + (r - hs) * rs);
