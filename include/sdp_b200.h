@@ -351,7 +351,7 @@ int sdp_visplan_create(sdp_visplan **plan, const sdp_geometry *geom, const sdp_w
                        void *stream);
 int sdp_visplan_destroy(sdp_visplan *plan);
 /* Plan shape (no counterpart in the reference): uv tile side (a multiple of
- * 8 in 8..128, default 32), visibilities per work item (64..65536, default
+ * 8 in 8..128, default 16), visibilities per work item (64..65536, default
  * 1024), lanes per visibility (0: std_gridding plans with half supports up
  * to 4 take the warp-per-visibility kernel, one warp per visibility and a
  * private subgrid per warp, other plans the fewest lanes their support needs;
