@@ -1111,7 +1111,7 @@ __device__ __forceinline__ bool fast_item(const PlanDev &Pin, const int4 it, Ite
         asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
         const uint32_t gbytes = (uint32_t)(it.z - it.y) * 16u;
         const uint32_t mbytes = (OP == OP_CYCLE_CONV) ? (uint32_t)(((it.z + 1) & ~1) - m0) * 8u : 0u;
-        const uint32_t bbytes = ((kConv || share) && P.gbase) ? gbytes : 0u;
+        const uint32_t bbytes = (P.gbase && (kGrids ? share : true)) ? gbytes : 0u;
         stage_arm(bar, gbytes + bbytes + mbytes);
         stage_copy((uint32_t)__cvta_generic_to_shared(stg.geo), P.geo + it.y, gbytes, bar);
         if (bbytes) stage_copy((uint32_t)__cvta_generic_to_shared(stg.gb), P.gbase + it.y, bbytes, bar);
@@ -1144,12 +1144,13 @@ __device__ __forceinline__ bool fast_item(const PlanDev &Pin, const int4 it, Ite
     const uint4 *sgeo = stg.geo - it.y;   // indexed by plan position
     const float2 *smeas = stg.meas - m0;
     const float2 *svis = stg.meas - it.y;  // OP_GRID: the item's input visibilities in plan order
-    // four-visibility path (half support 4): a batch reads only the quad
-    // records (k_gather_plan); lane (r, c) takes its two taps (rows r below
+    // four-visibility path (half support 4, and for the passes that grid, a
+    // gridding set equal to the degridding set or its conjugate): a batch
+    // reads only the quad records (k_gather_plan); lane (r, c) takes its two taps (rows r below
     // the visibility, r + 4 above) from the columns-below quadrants, or for
     // c >= 4 from the columns-above ones CP - CN further on; the lane's
     // offsets within the quadrants fold into its table pointers
-    const bool quad = P.gbase != nullptr && (kConv || share);
+    const bool quad = P.gbase != nullptr && (kGrids ? share : true);  // the gridding half reuses the samples
     const uint4 *squad = stg.gb - it.y;  // indexed by plan position
     const int cqm = (c < 4) ? 0 : -1;
     const int cofs4 = (c < 4) ? -c : c - 4;
