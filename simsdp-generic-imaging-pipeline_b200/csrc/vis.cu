@@ -1082,7 +1082,10 @@ struct ItemStage {
 // One work item of the warp-per-visibility kernels (the whole CTA).
 // OP is OP_GRID, OP_DEGRID or OP_CYCLE_CONV.  smem: the model tile (OP !=
 // OP_GRID) and NW private subgrids (OP != OP_DEGRID), S rows of P.pitch cells.
-template <typename T, int OP, int NW>
+// kShared: the launch holds only plans whose two kernel sets are equal or
+// conjugate (the batched kernel checks this at creation), so the quad path
+// needs no test of share.
+template <typename T, int OP, int NW, bool kShared = false>
 __device__ __forceinline__ bool fast_item(const PlanDev &Pin, const int4 it, ItemStage &stg, float2 *mtile,
                                           float2 *subs,
                                           float *wscr_all, const int4 *planes, bool share, float share_sign,
@@ -1111,7 +1114,7 @@ __device__ __forceinline__ bool fast_item(const PlanDev &Pin, const int4 it, Ite
         asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
         const uint32_t gbytes = (uint32_t)(it.z - it.y) * 16u;
         const uint32_t mbytes = (OP == OP_CYCLE_CONV) ? (uint32_t)(((it.z + 1) & ~1) - m0) * 8u : 0u;
-        const uint32_t bbytes = (P.gbase && (kGrids ? share : true)) ? gbytes : 0u;
+        const uint32_t bbytes = (P.gbase && (kGrids ? (kShared || share) : true)) ? gbytes : 0u;
         stage_arm(bar, gbytes + bbytes + mbytes);
         stage_copy((uint32_t)__cvta_generic_to_shared(stg.geo), P.geo + it.y, gbytes, bar);
         if (bbytes) stage_copy((uint32_t)__cvta_generic_to_shared(stg.gb), P.gbase + it.y, bbytes, bar);
@@ -1150,7 +1153,7 @@ __device__ __forceinline__ bool fast_item(const PlanDev &Pin, const int4 it, Ite
     // the visibility, r + 4 above) from the columns-below quadrants, or for
     // c >= 4 from the columns-above ones CP - CN further on; the lane's
     // offsets within the quadrants fold into its table pointers
-    const bool quad = P.gbase != nullptr && (kGrids ? share : true);  // the gridding half reuses the samples
+    const bool quad = P.gbase != nullptr && (kGrids ? (kShared || share) : true);  // the gridding half reuses the samples
     const uint4 *squad = stg.gb - it.y;  // indexed by plan position
     const int cqm = (c < 4) ? 0 : -1;
     const int cofs4 = (c < 4) ? -c : c - 4;
@@ -1614,7 +1617,7 @@ __global__ void __launch_bounds__(32 * NW, 20 / NW) k_vis_fast_batch(const PlanD
             cur = it.w;
         }
         const int kdiff = s_share;
-        if (!fast_item<T, OP_CYCLE_CONV, NW>(sP, it, stg, mtile, subs, s_wscr, planes,
+        if (!fast_item<T, OP_CYCLE_CONV, NW, true>(sP, it, stg, mtile, subs, s_wscr, planes,
                                              (kdiff & 1) == 0 || (kdiff & 2) == 0, (kdiff & 1) == 0 ? 1.f : -1.f,
                                              nullptr, sIO.in_grid, sIO.out_grid, sIO.pred_out, sIO.delta_out,
                                              sIO.measured))
@@ -2636,6 +2639,18 @@ SDP_EXPORT int sdp_visbatch_create(sdp_visbatch **out, sdp_visplan *const *plans
         b->tile_f2 = std::max(b->tile_f2, (size_t)p->S * p->pitch);
         b->chunk_max = std::max(b->chunk_max, p->chunk);
         b->fast = b->fast && fast_eligible(p);
+        if (b->fast && p->gbase) {
+            // the batched warp-per-visibility kernel assumes each plan's two
+            // kernel sets are equal or conjugate (kShared in fast_item)
+            int kdiff = 3;
+            cudaError_t e = cudaMemcpyAsync(&kdiff, p->kshare, sizeof(int), cudaMemcpyDeviceToHost, st);
+            if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+            if (e != cudaSuccess) {
+                visbatch_free(b);
+                return cuda_error(e, "reading a plan's kernel-set relation");
+            }
+            if ((kdiff & 1) && (kdiff & 2)) b->fast = false;
+        }
         if (c == 0) b->warps = p->warps;
         b->nk_max = std::max(b->nk_max, p->gk.num_kernels);
         int ni = 0;
