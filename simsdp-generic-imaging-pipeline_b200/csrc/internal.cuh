@@ -52,7 +52,7 @@ struct sdp_visplan {
     float2 *dk2 = nullptr;        // phase-major degridding kernels
     float *dinv = nullptr;        // 1 / sqrt(sum |k|^2) of each fast-path tap box of the degridding set (nullptr: none)
     int dinv_nc = 0;              // tap-box configurations per axis of dinv, 2 (OS + 1)
-    uint4 *gbase = nullptr;       // plan order: table bases of a fast visibility's four tap quadrants (nullptr: none)
+    uint4 *gbase = nullptr;       // plan order: quad records of the half-support-4 fast visibilities (nullptr: none)
     int dk_conj_off = 0;          // offset of the conjugated copy of the phase-major degridding set in dk2
     void *arena = nullptr;
     bool owns_arena = true;

@@ -11,17 +11,20 @@
 //   g2g_degridgrid :204-326  nearest cell, regridded with the w = 0 kernel.
 //   gridding_CPU (gridding_run.c:55-137): snapped p, taps [ceil(p-hs), floor(p+hs)].
 //
-// B200 design.  Visibilities are binned once per uvw set by the 32 x 32 uv
-// tile holding the origin of their tap box, then by w-plane, with a
-// counting sort.  Each tile's list is cut into work items of at most
-// kChunk visibilities; persistent CTAs pull items from an atomic queue.  A
-// CTA keeps one (32 + 2 hs_max)^2 complex subgrid per warp in shared memory,
-// so a warp updates its subgrid with plain loads and stores (the lanes of a
-// warp always touch distinct cells of one visibility), and flushes the sum of
-// its warps' subgrids to HBM with one vector atomic per touched cell.  A
-// visibility's tap box is mapped onto lanes as (column = lane % W, row phase =
-// lane / W), W = 2 hs_max + 1, so a lane computes its column's kernel index
-// once per visibility and walks rows.
+// B200 design.  A plan bins the visibilities once per uvw set: a counting
+// sort by (uv tile of the tap-box origin, w-plane) gives the bins, a radix
+// sort orders each tile's visibilities by (origin, plane), and each tile's
+// list is cut into work items; persistent CTAs pull items from an atomic
+// queue.  The warp-per-visibility kernels (k_vis_fast*, half supports up to
+// 4) stage an item's records in shared memory with bulk copies, give every
+// warp a private subgrid (plain read-modify-writes; lane (r, c) owns tap
+// column c, rows r and r + 4) and flush the warps' sum with one vector
+// atomic per touched cell; batches of four half-support-4 visibilities read
+// one 16-byte quad record each (table bases, origin, normalisation index)
+// and reuse model reads and subgrid updates along runs of one origin.  The
+// group kernels (k_tiles*, several visibilities per warp on one shared
+// subgrid) serve the other plans: snapped coordinates, g2g, nearest-cell
+// cycles and half supports above 4.
 #include <cstdio>
 #include <cstring>
 
@@ -77,7 +80,7 @@ struct PlanDev {
     const uint4 *geo;   // packed tap-box geometry in plan order (see fast_geometry)
     const int *perm;    // plan position -> original visibility index
     const float *dinv;  // degridding normalisation of each fast-path tap box (nullptr: none), see k_dinv
-    const uint4 *gbase; // four-quadrant table bases of each fast visibility in plan order (nullptr: none)
+    const uint4 *gbase; // quad records of the fast visibilities in plan order (k_gather_plan; nullptr: none)
 };
 
 // ----------------------------------------------------------------------------
@@ -1072,7 +1075,7 @@ __device__ __forceinline__ bool stage_wait(uint32_t bar, uint32_t parity)
 // mbarrier's phase.
 struct ItemStage {
     uint4 *geo;         // chunk records
-    uint4 *gb;          // chunk quadrant bases (plans with gbase)
+    uint4 *gb;          // chunk quad records (plans with gbase)
     float2 *meas;       // chunk + 2 values (from the even index at or below the item's first)
     uint64_t *bar;
     uint32_t phase;     // parity of the next completion
@@ -1504,7 +1507,7 @@ __device__ __forceinline__ bool fast_item(const PlanDev &Pin, const int4 it, Ite
 
 // Shared-memory layout of the warp-per-visibility kernels: the staged
 // records of one work item (chunk 16-byte geometry records, chunk 16-byte
-// quadrant bases, chunk + 2 measured values), per-plane constants (nk int4),
+// quad records, chunk + 2 measured values), per-plane constants (nk int4),
 // then the model tile and the NW subgrids.
 // Shared memory of a block on sm_100 (opt-in limit) and an upper bound on
 // the static arrays of the tile kernels (at most 896 B): the dynamic part
@@ -1515,7 +1518,7 @@ constexpr size_t kStaticSmem = 1024;
 
 __host__ __device__ __forceinline__ size_t fast_stage_bytes(int chunk)
 {
-    // geometry, quadrant bases, measured values; the plane table after it is int4
+    // geometry, quad records, measured values; the plane table after it is int4
     return (32 * (size_t)chunk + 8 * ((size_t)chunk + 2) + 15) / 16 * 16;
 }
 __host__ __device__ __forceinline__ size_t fast_smem_bytes(int op, int nw, int S, int pitch, int nk, int chunk)
