@@ -352,14 +352,15 @@ int sdp_visplan_create(sdp_visplan **plan, const sdp_geometry *geom, const sdp_w
 int sdp_visplan_destroy(sdp_visplan *plan);
 /* Plan shape (no counterpart in the reference): uv tile side (a multiple of
  * 8 in 8..128, default 16), visibilities per work item (64..65536, default
- * 1024), lanes per visibility (0: std_gridding plans with half supports up
+ * 512), lanes per visibility (0: std_gridding plans with half supports up
  * to 4 take the warp-per-visibility kernel, one warp per visibility and a
  * private subgrid per warp, other plans the fewest lanes their support needs;
  * 8 / 16 / 32: the group kernels with that many lanes per visibility, several
  * visibilities per warp on one shared subgrid), warps per CTA of the
  * warp-per-visibility kernel (0: by occupancy, or 4 / 8).  Zero fields take
- * the defaults.  Results are the same for every shape up to the order of the
- * floating-point sums. */
+ * the defaults.  sdp_visplan_create and the actors use tile 16, 512
+ * visibilities per item, 4 warps.  Results are the same for every shape up
+ * to the order of the floating-point sums. */
 typedef struct sdp_plan_options {
     int tile;
     int chunk;

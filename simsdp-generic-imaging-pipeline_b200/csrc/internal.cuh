@@ -29,10 +29,10 @@ struct sdp_visplan {
     int mode;
     int n;
     int ntx, nty, nk, nbins, ntiles, hs_max, W, S;
-    int tile = 32;                // uv tile side (grid cells)
-    int chunk = 1024;             // visibilities per work item (at most)
+    int tile = 16;                // uv tile side (grid cells)
+    int chunk = 512;              // visibilities per work item (at most)
     int lanes = 0;                // lanes per visibility of the group kernels (0: warp-per-visibility kernel)
-    int warps = 0;                // warps per CTA of the warp-per-visibility kernel (0: by occupancy)
+    int warps = 4;                // warps per CTA of the warp-per-visibility kernel (0: by occupancy)
     int pitch = 0;                // row pitch (float2) of the shared tiles: >= S, = 8 mod 16
     uint4 *geo = nullptr;         // plan order: packed tap-box geometry (fast path), see fast_geometry
     void *rec = nullptr;          // Rec<float> or Rec<double>

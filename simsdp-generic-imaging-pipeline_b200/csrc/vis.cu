@@ -45,7 +45,7 @@ namespace sdp {
 #endif
 
 constexpr int kTile = 16;    // default uv tile side
-constexpr int kChunk = 1024;  // default visibilities per work item
+constexpr int kChunk = 512;   // default visibilities per work item
 constexpr int kMaxHalfSupport = 15;
 
 enum : int {

@@ -70,7 +70,7 @@ def test_plan_shapes_agree(sdp, device, setup, tile, chunk, lanes, warps):
     ref = _run(sdp, device, setup, None)
     got = _run(sdp, device, setup, sdp.PlanOptions(tile, chunk, lanes, warps))
     assert (got[4].tile, got[4].chunk, got[4].lanes, got[4].warps) == (tile, chunk, lanes, warps)
-    assert (ref[4].tile, ref[4].chunk) == (32, 1024)
+    assert (ref[4].tile, ref[4].chunk, ref[4].warps) == (16, 512, 4)  # sdp_visplan_create's shape
     for a, b in zip(got[:4], ref[:4]):
         assert rel_rms(a, b) <= 1e-6
 
